@@ -1,0 +1,49 @@
+// Plain-old-data descriptors shared by the host planner and the device
+// kernels.  One ItemDesc is one block contraction, i.e. one call of the
+// reference's inner kernel (contr_blk1blk2_wmaps_c / _blocked_mm) for a fixed
+// (Ms, IRREP, distribution) case of ex1, ex2 and the contraction string.
+#pragma once
+#include <cstdint>
+
+namespace gccu {
+
+constexpr int kDevMaxComp = 8;
+
+// composite string spaces of one item
+enum Space : int8_t { kEx1 = 0, kEx2 = 1, kCnt = 2, kNone = -1 };
+
+// How the components of one operand (op1, op2 or the result) are addressed.
+// Component j of the operand string is made from a component of space sp1
+// (index ci1) and/or of space sp2 (index ci2).  If both are present it is the
+// signed string map map[j][i2 * n1 + i1] (strings/set_strmap_kernel.f: str1
+// runs fastest); otherwise the component index is used as is (the trivial
+// map of strings/get_strmap_blk_c.f:190-198).  Element offset of the operand
+// = sum_j (|index_j| - 1) * ldim[j] (contract/set_op_ldim_c.f).
+struct OpndDesc {
+  int32_t ncomp;
+  int32_t nmap;  // number of components that need a map lookup
+  int8_t sp1[kDevMaxComp], ci1[kDevMaxComp], sp2[kDevMaxComp], ci2[kDevMaxComp];
+  int32_t n1[kDevMaxComp];
+  int64_t ldim[kDevMaxComp];
+  const int32_t* map[kDevMaxComp];
+};
+
+struct ItemDesc {
+  int64_t M, N, K;  // |ex1|, |ex2|, |cnt| composite string counts
+  double fac;       // xfac * casign * fac_scal
+  int64_t base1, base2, base12;
+  int32_t nsp[3];              // components per space
+  int32_t rad[3][kDevMaxComp];  // string counts per component (first fastest)
+  OpndDesc op[3];               // op1, op2, result
+  int32_t kfast1, kfast2;       // operand stride is smaller along cnt than along ex
+  int32_t pad;
+};
+
+struct TileDesc {
+  int32_t item;
+  int32_t m0, n0;
+  int32_t pad;
+  int64_t k0, k1;
+};
+
+}  // namespace gccu

@@ -1,0 +1,768 @@
+// Engine state behind the C ABI (include/gccu.h): the orbital model, ME
+// lists resident in device memory, the device string-map store, cached
+// contraction plans and their device work lists, CUDA-graph capture.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/gccu.h"
+#include "kernels.hpp"
+#include "model.hpp"
+#include "planner.hpp"
+
+namespace gccu {
+namespace {
+
+thread_local std::string g_error;
+
+#define CUDA_OK(x)                                                                   \
+  do {                                                                               \
+    cudaError_t e_ = (x);                                                            \
+    if (e_ != cudaSuccess)                                                           \
+      throw ::gccu::Error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x); \
+  } while (0)
+
+struct DevList {
+  ListLayout L;
+  double* d = nullptr;
+};
+
+struct DevGraph {
+  int64_t* W = nullptr;
+  int8_t* irrep = nullptr;
+  std::map<int, int32_t*> tables;  // (idxms-1)*nsym+gam-1 -> device string table
+};
+
+struct DevPlan {
+  Plan plan;
+  ItemDesc* d_items = nullptr;
+  TileDesc* d_tiles = nullptr;
+  int64_t ntiles = 0;
+  int64_t res_off = 0, res_len = 0;
+  int list1 = 0, list2 = 0, list12 = 0;
+  // sym_ab descriptors of the result class (use_tr)
+  FlipDesc* d_flip = nullptr;
+  int64_t nflip = 0, flip_maxlen = 0;
+};
+
+class Engine {
+ public:
+  Model model;
+  bool have_orbs = false;
+  int device = 0;
+  int64_t memmax = 0, mem_used = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<DevList> lists;
+  std::map<int, DevGraph> dgraphs;
+  std::map<MapKey, int32_t*> maps;
+  std::map<std::array<int, 3>, int32_t*> flips;
+  std::map<std::string, std::unique_ptr<DevPlan>> plans;
+  std::vector<void*> allocs;
+  double* d_red = nullptr;  // reduction scalars
+  double stats[8] = {};
+  int64_t launches = 0;
+  bool capturing = false;
+  std::vector<cudaGraphExec_t> graphs;
+
+  bool host_only = false;  // no device: model, layout and planning queries only
+
+  explicit Engine(int dev, int64_t mm) : device(dev), memmax(mm), host_only(dev < 0) {
+    if (host_only) return;
+    CUDA_OK(cudaSetDevice(dev));
+    CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    d_red = (double*)alloc(64 * sizeof(double));
+  }
+  ~Engine() {
+    for (auto g : graphs) cudaGraphExecDestroy(g);
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  void* alloc(size_t bytes) {
+    GCCU_REQUIRE(!host_only, "engine was initialised without a device (host-only mode)");
+    GCCU_REQUIRE(!capturing, "device allocation requested while capturing a CUDA graph");
+    if (memmax > 0 && mem_used + (int64_t)bytes > memmax)
+      throw Error("device memory cap (memmax) exceeded");
+    void* p = nullptr;
+    CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    allocs.push_back(p);
+    mem_used += (int64_t)bytes;
+    return p;
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = (T*)alloc(v.size() * sizeof(T));
+    if (!v.empty())
+      CUDA_OK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    CUDA_OK(cudaStreamSynchronize(stream));
+    return p;
+  }
+
+  DevList& list(int64_t id) {
+    GCCU_REQUIRE(id >= 1 && id <= (int64_t)lists.size(), "invalid ME-list handle");
+    return lists[id - 1];
+  }
+
+  DevGraph& dgraph(int gid) {
+    auto it = dgraphs.find(gid);
+    if (it != dgraphs.end()) return it->second;
+    Graph& g = model.G(gid);
+    DevGraph dg;
+    dg.W = upload(g.W);
+    std::vector<int8_t> ir(g.irrep.begin(), g.irrep.end());
+    if (ir.empty()) ir.push_back(0);
+    dg.irrep = upload(ir);
+    return dgraphs[gid] = dg;
+  }
+  int32_t* dtable(int gid, int idxms, int gam) {
+    DevGraph& dg = dgraph(gid);
+    int key = (idxms - 1) * model.os.nsym + gam - 1;
+    auto it = dg.tables.find(key);
+    if (it != dg.tables.end()) return it->second;
+    const auto& t = model.G(gid).table(idxms, gam);
+    std::vector<int32_t> v(t);
+    if (v.empty()) v.push_back(0);
+    return dg.tables[key] = upload(v);
+  }
+
+  // device string map of one block pair, built on first use
+  int32_t* strmap(const MapKey& k) {
+    auto it = maps.find(k);
+    if (it != maps.end()) return it->second;
+    Graph &g1 = model.G(k[0]), &g2 = model.G(k[1]);
+    GCCU_REQUIRE(g1.type == g2.type, "string map between different hpvx types");
+    int g12 = model.graph(g1.type, g1.nel + g2.nel);
+    int64_t n1 = g1.nstr(k[2], k[4]), n2 = g2.nstr(k[3], k[5]);
+    int32_t* t1 = dtable(k[0], k[2], k[4]);
+    int32_t* t2 = dtable(k[1], k[3], k[5]);
+    DevGraph& d12 = dgraph(g12);
+    int32_t* out = (int32_t*)alloc(std::max<int64_t>(n1 * n2, 1) * sizeof(int32_t));
+    launch_strmap(t1, g1.nel, n1, t2, g2.nel, n2, d12.W, d12.irrep, g1.nel + g2.nel,
+                  model.os.nsym, out, stream);
+    ++launches;
+    CUDA_OK(cudaGetLastError());
+    return maps[k] = out;
+  }
+
+  // spin-flip map of one graph block (set_flipmap_kernel,
+  // strings/set_flipmap_kernel.f:47-88): str -> sign * (address of the
+  // flipped string + 1), sign = std_spsign(str)*std_spsign(flipped)
+  int32_t* flipmap(int gid, int idxms, int gam) {
+    std::array<int, 3> key{gid, idxms, gam};
+    auto it = flips.find(key);
+    if (it != flips.end()) return it->second;
+    Graph& g = model.G(gid);
+    const auto& t = g.table(idxms, gam);
+    int nel = g.nel;
+    int64_t n = g.nstr(idxms, gam);
+    std::vector<int32_t> m(std::max<int64_t>(n, 1), 0);
+    std::vector<int> orb(nel), spn(nel), spf(nel);
+    auto spsign = [](const int* s, int ne) {
+      int trp = 0, nb = 0, i = 0;
+      while (i < ne) {
+        int sg = s[i];
+        if (sg == 1 || sg == 2) trp += nb, ++i;
+        if (sg == -1 || sg == 2) ++nb, ++i;
+      }
+      return (trp & 1) ? -1 : 1;
+    };
+    for (int64_t s = 0; s < n; ++s) {
+      for (int p = 0; p < nel; ++p) {
+        int v = t[s * nel + p], c = v & 3;
+        orb[p] = v >> 2;
+        spn[p] = c == 1 ? 1 : (c == 2 ? -1 : 2);
+        spf[p] = spn[p] == 2 ? 2 : -spn[p];
+      }
+      int sg = spsign(spn.data(), nel) * spsign(spf.data(), nel);
+      m[s] = sg * (int32_t)(g.address(orb.data(), spf.data()) + 1);
+    }
+    return flips[key] = upload(m);
+  }
+
+  DevPlan& plan_for(const gccu_bc_desc* bc, bool use_tr) {
+    std::ostringstream os;
+    os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr;
+    for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
+                                   << bc->occ_cnt[k];
+    std::string key = os.str();
+    auto it = plans.find(key);
+    if (it != plans.end()) return *it->second;
+    GCCU_REQUIRE(!capturing, "contraction must be run once before it is captured in a graph");
+    GCCU_REQUIRE(bc->tra_op1 == 0 && bc->tra_op2 == 0 && bc->tra_res == 0,
+                 "transposed operands are not supported by this engine version");
+    ContractionSpec s;
+    s.L1 = &list(bc->list_op1).L;
+    s.L2 = &list(bc->list_op2).L;
+    s.L12 = &list(bc->list_res).L;
+    s.ib1 = (int)bc->iblk_op1;
+    s.ib2 = (int)bc->iblk_op2;
+    s.ib12 = (int)bc->iblk_res;
+    for (int k = 0; k < 8; ++k) {
+      s.ex1[k] = (int)bc->occ_ex1[k];
+      s.ex2[k] = (int)bc->occ_ex2[k];
+      s.cnt[k] = (int)bc->occ_cnt[k];
+    }
+    s.use_tr = use_tr;
+    auto dp = std::make_unique<DevPlan>();
+    dp->plan = plan_contraction(model, s);
+    dp->list1 = (int)bc->list_op1;
+    dp->list2 = (int)bc->list_op2;
+    dp->list12 = (int)bc->list_res;
+    const LayoutBlock& B12 = s.L12->blk[s.ib12 - 1];
+    dp->res_off = B12.off;
+    dp->res_len = B12.len;
+    Plan& P = dp->plan;
+    if (host_only) return *(plans[key] = std::move(dp));
+    for (auto& r : P.maps) P.items[r.item].op[r.opnd].map[r.comp] = strmap(r.key);
+    // tiles: 64x64 output tiles, contraction index split when the item has
+    // few output tiles and a long contraction string
+    std::vector<TileDesc> tiles;
+    int64_t total_mn = 0;
+    for (auto& itm : P.items)
+      total_mn += ((itm.M + kTileM - 1) / kTileM) * ((itm.N + kTileN - 1) / kTileN);
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const ItemDesc& itm = P.items[i];
+      int64_t mt = (itm.M + kTileM - 1) / kTileM, nt = (itm.N + kTileN - 1) / kTileN;
+      int64_t ks = 1;
+      if (total_mn < 2 * 148 && itm.K > 1024) {
+        ks = std::min<int64_t>((itm.K + 511) / 512, (2 * 148 + total_mn - 1) / std::max<int64_t>(total_mn, 1));
+        ks = std::max<int64_t>(ks, 1);
+      }
+      int64_t kchunk = ((itm.K + ks - 1) / ks + kTileK - 1) / kTileK * kTileK;
+      for (int64_t m = 0; m < mt; ++m)
+        for (int64_t n = 0; n < nt; ++n)
+          for (int64_t k0 = 0; k0 < itm.K; k0 += kchunk) {
+            TileDesc t{};
+            t.item = (int32_t)i;
+            t.m0 = (int32_t)(m * kTileM);
+            t.n0 = (int32_t)(n * kTileN);
+            t.k0 = k0;
+            t.k1 = std::min(itm.K, k0 + kchunk);
+            tiles.push_back(t);
+          }
+    }
+    dp->ntiles = (int64_t)tiles.size();
+    if (!P.items.empty()) {
+      dp->d_items = upload(P.items);
+      dp->d_tiles = upload(tiles);
+    }
+    if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);
+    return *(plans[key] = std::move(dp));
+  }
+
+  // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
+  void build_flip(DevPlan& dp, DevList& dl, int iblk) {
+    ListLayout& L = dl.L;
+    GCCU_REQUIRE(L.mst == 0, "sym_ab: open-shell lists are not supported");
+    GCCU_REQUIRE(std::abs(L.absym) == 1, "sym_ab: absym must be +-1");
+    dp.nflip = 0;
+    std::vector<FlipDesc> v = flip_descs(L, iblk, (double)L.absym, dp.flip_maxlen);
+    if (!v.empty()) dp.d_flip = upload(v);
+    dp.nflip = (int64_t)v.size();
+  }
+
+  std::vector<FlipDesc> flip_descs(ListLayout& L, int iblk, double relfac, int64_t& maxlen) {
+    LayoutBlock& B = L.blk.at(iblk - 1);
+    int nsym = model.os.nsym;
+    std::vector<int> oc = comp_occs(B.c), oa = comp_occs(B.a);
+    int mscmax = 0, msamax = 0;
+    for (int v : oc) mscmax += v;
+    for (int v : oa) msamax += v;
+    double relfac2 =
+        ((((mscmax + msamax) / 2 + 1) * (mscmax - msamax) / 2) % 2 != 0) ? -relfac : relfac;
+    auto spsign_dist = [](const std::vector<int>& ms, const std::vector<int>& occ) {
+      if (ms.size() <= 1) return 1;
+      int trp = 0, nb = 0;
+      for (size_t b = 0; b < ms.size(); ++b) {
+        int na = (occ[b] + ms[b]) / 2, nbeta = (occ[b] - ms[b]) / 2;
+        trp += na * nb;
+        nb += nbeta;
+      }
+      return (trp & 1) ? -1 : 1;
+    };
+    std::vector<FlipDesc> out;
+    maxlen = 0;
+    for (int msa = msamax; msa >= 0; msa -= 2) {
+      int msc = msa + L.mst;
+      if (std::abs(msc) > mscmax) continue;
+      int ix1 = msa_to_idxms(msa, L.mst, msamax, mscmax);
+      int ix2 = msa_to_idxms(-msa, L.mst, msamax, mscmax);
+      for (int gama = 1; gama <= nsym; ++gama) {
+        int gamc = irrep_mult(gama, L.gamt);
+        if (B.gmlen(ix1, gama) <= 0) continue;
+        MsGam d;
+        for (bool first = true; next_msgam(first, d, oc, oa, msc, msa, gamc, gama, nsym);
+             first = false) {
+          std::vector<int> mc2(d.msc), ma2(d.msa);
+          for (auto& x : mc2) x = -x;
+          for (auto& x : ma2) x = -x;
+          int gsign = spsign_dist(d.msc, oc) * spsign_dist(d.msa, oa) * spsign_dist(mc2, oc) *
+                      spsign_dist(ma2, oa);
+          std::vector<int> ixc(B.c.size()), ixa(B.a.size()), ixc2(B.c.size()), ixa2(B.a.size());
+          std::vector<int64_t> lc, la;
+          int64_t lenc = 1, lena = 1;
+          for (size_t i = 0; i < B.c.size(); ++i) {
+            ixc[i] = ms_index(B.c[i].occ, d.msc[i]);
+            ixc2[i] = ms_index(B.c[i].occ, mc2[i]);
+            lc.push_back(model.G(B.c[i].graph).nstr(ixc[i], d.gc[i]));
+            lenc *= lc.back();
+          }
+          for (size_t i = 0; i < B.a.size(); ++i) {
+            ixa[i] = ms_index(B.a[i].occ, d.msa[i]);
+            ixa2[i] = ms_index(B.a[i].occ, ma2[i]);
+            la.push_back(model.G(B.a[i].graph).nstr(ixa[i], d.ga[i]));
+            lena *= la.back();
+          }
+          if (lenc == 0 || lena == 0) continue;
+          const auto& dl1 = B.dis.at({ix1, gama});
+          const auto& dl2 = B.dis.at({ix2, gama});
+          size_t id1 = 0, id2 = 0;
+          int64_t did1 = dist_id(B.c, ixc, d.gc, B.a, ixa, d.ga, nsym);
+          int64_t did2 = dist_id(B.c, ixc2, d.gc, B.a, ixa2, d.ga, nsym);
+          for (size_t q = 0; q < dl1.size(); ++q)
+            if (dl1[q].did == did1) id1 = q;
+          for (size_t q = 0; q < dl2.size(); ++q)
+            if (dl2[q].did == did2) id2 = q;
+          if (msa == 0 && id1 > id2) continue;
+          FlipDesc f{};
+          f.off1 = dl1[id1].off;
+          f.off2 = dl2[id2].off;
+          f.lenc = lenc;
+          f.lena = lena;
+          f.nc = (int32_t)B.c.size();
+          f.na = (int32_t)B.a.size();
+          std::vector<int64_t> ldc(B.c.size()), lda(B.a.size());
+          int64_t ld = 1;
+          for (int ih = 0; ih < 4; ++ih) {
+            int t = kHpvxSeq[ih];
+            for (size_t i = 0; i < B.c.size(); ++i)
+              if (B.c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
+            for (size_t i = 0; i < B.a.size(); ++i)
+              if (B.a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+          }
+          for (size_t i = 0; i < B.c.size(); ++i) {
+            f.lc[i] = (int32_t)lc[i];
+            f.ldc[i] = ldc[i];
+            f.fc[i] = flipmap(B.c[i].graph, ixc[i], d.gc[i]);
+          }
+          for (size_t i = 0; i < B.a.size(); ++i) {
+            f.la[i] = (int32_t)la[i];
+            f.lda[i] = lda[i];
+            f.fa[i] = flipmap(B.a[i].graph, ixa[i], d.ga[i]);
+          }
+          f.sgn = gsign * relfac2;
+          f.same = (f.off1 == f.off2);
+          out.push_back(f);
+          maxlen = std::max(maxlen, lenc * lena);
+        }
+      }
+    }
+    return out;
+  }
+
+  double read_red(int slot) {
+    double v = 0;
+    CUDA_OK(cudaMemcpyAsync(&v, d_red + slot, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CUDA_OK(cudaStreamSynchronize(stream));
+    return v;
+  }
+};
+
+std::unique_ptr<Engine> g_eng;
+
+Engine& eng() {
+  if (!g_eng) throw Error("gccu_init has not been called");
+  return *g_eng;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+Occ to_occ(const int64_t* o) {
+  Occ r{};
+  for (int k = 0; k < 8; ++k) {
+    GCCU_REQUIRE(o[k] >= 0 && o[k] <= kMaxNel, "occupation out of range");
+    r[k] = (int)o[k];
+  }
+  return r;
+}
+
+}  // namespace
+}  // namespace gccu
+
+using namespace gccu;
+
+extern "C" {
+
+int gccu_init(int64_t device, int64_t memmax_bytes) {
+  return guarded([&] {
+    GCCU_REQUIRE(!g_eng, "gccu_init called twice");
+    if (device >= 0) {
+      int n = 0;
+      CUDA_OK(cudaGetDeviceCount(&n));
+      GCCU_REQUIRE(device < n, "no such CUDA device");
+    }
+    g_eng = std::make_unique<Engine>((int)device, memmax_bytes);
+  });
+}
+
+int gccu_finalize(void) {
+  return guarded([&] { g_eng.reset(); });
+}
+
+int gccu_last_error(char* buf, int64_t len) {
+  if (!buf || len <= 0) return 1;
+  std::strncpy(buf, g_error.c_str(), (size_t)len - 1);
+  buf[len - 1] = '\0';
+  return 0;
+}
+
+int gccu_register_orbinfo(int64_t nsym, const int64_t* norb) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.have_orbs, "orbital space already registered");
+    GCCU_REQUIRE(nsym == 1 || nsym == 2 || nsym == 4 || nsym == 8, "nsym must be 1, 2, 4 or 8");
+    e.model.os.nsym = (int)nsym;
+    for (int t = 0; t < 4; ++t)
+      for (int g = 0; g < 8; ++g) {
+        int64_t v = g < nsym ? norb[t * 8 + g] : 0;
+        GCCU_REQUIRE(v >= 0 && v < (1 << 20), "orbital count out of range");
+        e.model.os.norb[t][g] = (int)v;
+      }
+    e.model.os.finalize();
+    e.have_orbs = true;
+  });
+}
+
+int gccu_graph_nstr(int64_t type, int64_t nel, int64_t idxms, int64_t gam, int64_t* nstr) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    GCCU_REQUIRE(type >= 0 && type < 4 && nel >= 0 && nel <= kMaxNel, "bad graph");
+    *nstr = e.model.G(e.model.graph((int)type, (int)nel)).nstr((int)idxms, (int)gam);
+  });
+}
+
+int gccu_graph_index(int64_t type, int64_t nel, const int64_t* orb, const int64_t* spn,
+                     int64_t* index) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    Graph& g = e.model.G(e.model.graph((int)type, (int)nel));
+    std::vector<int> o(nel), s(nel);
+    for (int i = 0; i < nel; ++i) {
+      GCCU_REQUIRE(orb[i] >= 1 && orb[i] <= g.norb, "orbital out of range");
+      o[i] = (int)orb[i] - 1;
+      s[i] = (int)spn[i];
+    }
+    *index = g.address(o.data(), s.data());
+  });
+}
+
+int gccu_strmap_block(int64_t type, int64_t nel1, int64_t nel2, int64_t idxms1, int64_t idxms2,
+                      int64_t gam1, int64_t gam2, int64_t* map, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    int g1 = e.model.graph((int)type, (int)nel1), g2 = e.model.graph((int)type, (int)nel2);
+    MapKey k{g1, g2, (int)idxms1, (int)idxms2, (int)gam1, (int)gam2};
+    int64_t n1 = e.model.G(g1).nstr((int)idxms1, (int)gam1),
+            n2 = e.model.G(g2).nstr((int)idxms2, (int)gam2);
+    GCCU_REQUIRE(n >= n1 * n2, "map buffer too small");
+    int32_t* d = e.strmap(k);
+    std::vector<int32_t> h(std::max<int64_t>(n1 * n2, 1));
+    CUDA_OK(cudaMemcpyAsync(h.data(), d, n1 * n2 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    for (int64_t i = 0; i < n1 * n2; ++i) map[i] = h[i];
+  });
+}
+
+int gccu_define_operator(const int64_t* occ, int64_t nblk, int64_t* op_id) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(nblk >= 1, "operator without occupation classes");
+    Operator op;
+    for (int64_t b = 0; b < nblk; ++b) op.occ.push_back(to_occ(occ + 8 * b));
+    e.model.ops.push_back(op);
+    *op_id = (int64_t)e.model.ops.size();
+  });
+}
+
+int gccu_register_list(int64_t op_id, int64_t gamt, int64_t mst, int64_t absym, int64_t* list_id,
+                       int64_t* len_op) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    GCCU_REQUIRE(op_id >= 1 && op_id <= (int64_t)e.model.ops.size(), "invalid operator id");
+    GCCU_REQUIRE(gamt >= 1 && gamt <= e.model.os.nsym, "invalid total irrep");
+    DevList dl;
+    dl.L.op = (int)op_id;
+    dl.L.gamt = (int)gamt;
+    dl.L.mst = (int)mst;
+    dl.L.absym = (int)absym;
+    e.model.layout(dl.L);
+    if (!e.host_only) {
+      dl.d = (double*)e.alloc(std::max<int64_t>(dl.L.len, 1) * sizeof(double));
+      CUDA_OK(cudaMemsetAsync(dl.d, 0, std::max<int64_t>(dl.L.len, 1) * sizeof(double),
+                              e.stream));
+    }
+    e.lists.push_back(std::move(dl));
+    *list_id = (int64_t)e.lists.size();
+    *len_op = e.lists.back().L.len;
+  });
+}
+
+int gccu_list_block(int64_t list_id, int64_t iblk, int64_t* off, int64_t* len) {
+  return guarded([&] {
+    DevList& dl = eng().list(list_id);
+    GCCU_REQUIRE(iblk >= 1 && iblk <= (int64_t)dl.L.blk.size(), "invalid occupation class");
+    *off = dl.L.blk[iblk - 1].off;
+    *len = dl.L.blk[iblk - 1].len;
+  });
+}
+
+int gccu_list_dists(int64_t list_id, int64_t* rows, int64_t maxrows, int64_t* nrows) {
+  return guarded([&] {
+    DevList& dl = eng().list(list_id);
+    int64_t n = 0;
+    for (size_t ib = 0; ib < dl.L.blk.size(); ++ib)
+      for (auto& kv : dl.L.blk[ib].dis)
+        for (size_t d = 0; d < kv.second.size(); ++d, ++n) {
+          if (n >= maxrows) continue;
+          int64_t* r = rows + 8 * n;
+          r[0] = (int64_t)ib + 1;
+          r[1] = kv.first.first;
+          r[2] = kv.first.second;
+          r[3] = (int64_t)d + 1;
+          r[4] = kv.second[d].off;
+          r[5] = kv.second[d].len;
+          r[6] = kv.second[d].ld;
+          r[7] = kv.second[d].did;
+        }
+    *nrows = n;
+  });
+}
+
+int gccu_upload_list(int64_t list_id, const double* host, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& dl = e.list(list_id);
+    GCCU_REQUIRE(n == dl.L.len, "upload length differs from the list length");
+    CUDA_OK(cudaMemcpyAsync(dl.d, host, n * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+  });
+}
+
+int gccu_download_list(int64_t list_id, double* host, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& dl = e.list(list_id);
+    GCCU_REQUIRE(n == dl.L.len, "download length differs from the list length");
+    CUDA_OK(cudaMemcpyAsync(host, dl.d, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+  });
+}
+
+int gccu_zero_list(int64_t list_id) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& dl = e.list(list_id);
+    CUDA_OK(cudaMemsetAsync(dl.d, 0, dl.L.len * sizeof(double), e.stream));
+  });
+}
+
+int gccu_list_device_ptr(int64_t list_id, void** dptr) {
+  return guarded([&] { *dptr = eng().list(list_id).d; });
+}
+
+int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(bc, "null contraction descriptor");
+    DevPlan& dp = e.plan_for(bc, use_tr != 0);
+    *nitems = (int64_t)dp.plan.items.size();
+    for (int k = 0; k < 8; ++k) stats8[k] = dp.plan.stats[k];
+  });
+}
+
+int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr,
+                  int64_t type_xret, double* xret) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_contract needs a device");
+    GCCU_REQUIRE(bc, "null contraction descriptor");
+    GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
+    DevPlan& dp = e.plan_for(bc, use_tr != 0);
+    DevList& r = e.list(dp.list12);
+    if (!update) {
+      CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
+    }
+    launch_contract(dp.d_items, dp.d_tiles, dp.ntiles, e.list(dp.list1).d, e.list(dp.list2).d,
+                    r.d, fact, e.stream);
+    if (dp.ntiles) ++e.launches;
+    if (dp.plan.use_tr && dp.nflip) {
+      launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);
+      ++e.launches;
+    }
+    CUDA_OK(cudaGetLastError());
+    for (int k = 0; k < 8; ++k) e.stats[k] += dp.plan.stats[k];
+    if (type_xret == 1) {
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+      launch_sumsq(r.d + dp.res_off, dp.res_len, e.d_red, e.stream);
+      ++e.launches;
+      *xret = e.read_red(0);
+    } else if (type_xret == 2) {
+      CUDA_OK(cudaMemcpyAsync(xret, r.d + dp.res_off, sizeof(double), cudaMemcpyDeviceToHost,
+                              e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
+  });
+}
+
+int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_out,
+                   int64_t iblk_out, int64_t reset, int64_t type, double* xnorm2) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList &a = e.list(list_in), &b = e.list(list_out);
+    GCCU_REQUIRE(iblk_in >= 1 && iblk_in <= (int64_t)a.L.blk.size(), "invalid input class");
+    GCCU_REQUIRE(iblk_out >= 1 && iblk_out <= (int64_t)b.L.blk.size(), "invalid output class");
+    const LayoutBlock &Bi = a.L.blk[iblk_in - 1], &Bo = b.L.blk[iblk_out - 1];
+    GCCU_REQUIRE(Bi.occ == Bo.occ && Bi.len == Bo.len, "add_opblk: blocks differ in occupation");
+    launch_axpy(b.d + Bo.off, a.d + Bi.off, fac, Bo.len, (int)reset, e.stream);
+    ++e.launches;
+    if (type == 1) {
+      GCCU_REQUIRE(!e.capturing, "type must be 0 inside a graph capture");
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+      launch_sumsq(b.d + Bo.off, Bo.len, e.d_red, e.stream);
+      ++e.launches;
+      *xnorm2 = e.read_red(0);
+    } else if (type == 2) {
+      GCCU_REQUIRE(!e.capturing, "type must be 0 inside a graph capture");
+      CUDA_OK(cudaMemcpyAsync(xnorm2, b.d + Bo.off, sizeof(double), cudaMemcpyDeviceToHost,
+                              e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_scale_list(int64_t list_id, double fac) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& l = e.list(list_id);
+    launch_scale(l.d, fac, l.L.len, e.stream);
+    ++e.launches;
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_dot_lists(int64_t list_a, int64_t list_b, double* dot) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList &a = e.list(list_a), &b = e.list(list_b);
+    GCCU_REQUIRE(a.L.len == b.L.len, "dot: lists differ in length");
+    CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+    launch_dot(a.d, b.d, a.L.len, e.d_red, e.stream);
+    ++e.launches;
+    *dot = e.read_red(0);
+  });
+}
+
+int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& l = e.list(list_id);
+    GCCU_REQUIRE(iblk >= 1 && iblk <= (int64_t)l.L.blk.size(), "invalid occupation class");
+    int64_t maxlen = 0;
+    std::vector<FlipDesc> v = e.flip_descs(l.L, (int)iblk, relfac, maxlen);
+    if (v.empty()) return;
+    FlipDesc* d = e.upload(v);
+    launch_sym_ab(d, (int64_t)v.size(), l.d, prefac, maxlen, e.stream);
+    ++e.launches;
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_precondition(int64_t list_out, int64_t list_in, int64_t list_diag, double fac,
+                      double shift) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList &o = e.list(list_out), &i = e.list(list_in), &d = e.list(list_diag);
+    GCCU_REQUIRE(o.L.len == i.L.len && i.L.len == d.L.len, "diavc: lists differ in length");
+    launch_diavc(o.d, i.d, d.d, fac, shift, o.L.len, e.stream);
+    ++e.launches;
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_graph_begin(void) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.capturing, "graph capture already active");
+    CUDA_OK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+    e.capturing = true;
+  });
+}
+
+int gccu_graph_end(int64_t* graph_id) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.capturing, "no graph capture active");
+    cudaGraph_t g = nullptr;
+    e.capturing = false;
+    CUDA_OK(cudaStreamEndCapture(e.stream, &g));
+    cudaGraphExec_t ex = nullptr;
+    CUDA_OK(cudaGraphInstantiate(&ex, g, 0));
+    cudaGraphDestroy(g);
+    e.graphs.push_back(ex);
+    *graph_id = (int64_t)e.graphs.size();
+  });
+}
+
+int gccu_graph_launch(int64_t graph_id) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(graph_id >= 1 && graph_id <= (int64_t)e.graphs.size(), "invalid graph id");
+    CUDA_OK(cudaGraphLaunch(e.graphs[graph_id - 1], e.stream));
+    ++e.launches;
+  });
+}
+
+int gccu_sync(void) {
+  return guarded([&] { CUDA_OK(cudaStreamSynchronize(eng().stream)); });
+}
+
+int gccu_stats(double* stats8, int64_t* launches) {
+  return guarded([&] {
+    Engine& e = eng();
+    for (int k = 0; k < 8; ++k) stats8[k] = e.stats[k];
+    *launches = e.launches;
+  });
+}
+
+int gccu_reset_stats(void) {
+  return guarded([&] {
+    Engine& e = eng();
+    for (double& s : e.stats) s = 0;
+    e.launches = 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+// Launchers of the device kernels (kernels.cu).  All launches go to the
+// given stream; none synchronises.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_types.hpp"
+
+namespace gccu {
+
+// contraction tile shape of the FP64 kernel
+constexpr int kTileM = 64, kTileN = 64, kTileK = 16;
+
+// signed string map of one (str1 block, str2 block) pair; tables hold the
+// strings of each block in address order (orb<<2 | code), W/irrep describe
+// the graph of the merged string
+void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab2, int nel2,
+                   int64_t n2, const int64_t* W12, const int8_t* irrep12, int nel12, int nsym,
+                   int32_t* out, cudaStream_t s);
+
+// grouped block contractions: one CTA per tile, tiles of all items of one
+// binary contraction in one launch; result accumulated with atomics
+void launch_contract(const ItemDesc* items, const TileDesc* tiles, int64_t ntiles,
+                     const double* x1, const double* x2, double* x12, double alpha,
+                     cudaStream_t s);
+
+// out = (reset ? 0 : out) + fac*in  (add_opblk)
+void launch_axpy(double* out, const double* in, double fac, int64_t n, int reset, cudaStream_t s);
+// *acc += sum x^2 over n elements (acc must be zeroed by the caller)
+void launch_sumsq(const double* x, int64_t n, double* acc, cudaStream_t s);
+// *acc += sum a*b
+void launch_dot(const double* a, const double* b, int64_t n, double* acc, cudaStream_t s);
+void launch_scale(double* x, double fac, int64_t n, cudaStream_t s);
+// out = fac*in/(diag+shift) with |diag+shift| <= 1e-10 -> 1e-10 (diavc)
+void launch_diavc(double* out, const double* in, const double* diag, double fac, double shift,
+                  int64_t n, cudaStream_t s);
+// spin-flip symmetrisation of one distribution pair (sym_ab_blk): for every
+// element index i < partner p: x[i] = pre*(x[i]+s*x[p]), x[p] = s*x[i]
+struct FlipDesc {
+  int64_t off1, off2;  // offsets of the distribution and of its flipped partner
+  int64_t lenc, lena;
+  int32_t nc, na;
+  int32_t lc[kDevMaxComp], la[kDevMaxComp];
+  int64_t ldc[kDevMaxComp], lda[kDevMaxComp];
+  const int32_t* fc[kDevMaxComp];  // flip maps (signed 1-based partner index)
+  const int32_t* fa[kDevMaxComp];
+  double sgn;  // gsign * relfac2
+  int32_t same;  // distribution is its own partner
+  int32_t pad;
+};
+void launch_sym_ab(const FlipDesc* d, int64_t n, double* x, double prefac, int64_t maxlen,
+                   cudaStream_t s);
+
+}  // namespace gccu

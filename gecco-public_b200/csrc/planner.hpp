@@ -1,0 +1,41 @@
+// Contraction planner: flattens the block enumeration of
+// contr_op1op2_wmaps_c (contract/contr_op1op2_wmaps_c.f:984-2070) for one
+// binary contraction into a static list of block contractions (ItemDesc).
+// The list depends only on the operator layouts, never on the numbers, so it
+// is built once per formula item and reused in every iteration.
+#pragma once
+
+#include <array>
+#include <vector>
+
+#include "device_types.hpp"
+#include "model.hpp"
+
+namespace gccu {
+
+// (graph1, graph2, idxms1, idxms2, gam1, gam2) of one string-map block
+using MapKey = std::array<int, 6>;
+
+struct MapRef {
+  int item, opnd, comp;
+  MapKey key;
+};
+
+struct Plan {
+  std::vector<ItemDesc> items;  // fac holds fac_scal only; the call's fact is a launch argument
+  std::vector<MapRef> maps;     // map pointers to patch before upload
+  bool use_tr = false;          // result class needs sym_ab after the contraction
+  double stats[8] = {};         // reference dgemm accounting (str_block = 200)
+  double flops = 0;
+};
+
+struct ContractionSpec {
+  const ListLayout *L1, *L2, *L12;
+  int ib1, ib2, ib12;
+  Occ ex1, ex2, cnt;
+  bool use_tr;
+};
+
+Plan plan_contraction(Model& m, const ContractionSpec& s);
+
+}  // namespace gccu

@@ -1,0 +1,286 @@
+"""Python binding of the engine's C ABI (include/gccu.h) over ctypes.
+
+The reference drives this path from Fortran (frm_sched2 -> fs_contr_drv ->
+contr_op1op2, contract/frm_sched2.f:288-306); here the same calls are made
+from Python for the tests, the solver driver and the benchmark.  The library
+is the in-tree build ``gecco-public_b200/libgccu.so``; nothing falls back to a
+CPU implementation: a missing library is an error.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgccu.so")
+
+I64 = ctypes.c_int64
+P64 = ctypes.POINTER(ctypes.c_int64)
+PD = ctypes.POINTER(ctypes.c_double)
+
+H, P, V, X = 0, 1, 2, 3  # hpvx types
+
+
+class BcDesc(ctypes.Structure):
+    _fields_ = [("list_op1", I64), ("iblk_op1", I64), ("list_op2", I64), ("iblk_op2", I64),
+                ("list_res", I64), ("iblk_res", I64), ("tra_op1", I64), ("tra_op2", I64),
+                ("tra_res", I64), ("occ_ex1", I64 * 8), ("occ_ex2", I64 * 8),
+                ("occ_cnt", I64 * 8)]
+
+
+class GccuError(RuntimeError):
+    pass
+
+
+_lib = None
+
+_SIGS = {
+    "gccu_init": [I64, I64],
+    "gccu_finalize": [],
+    "gccu_last_error": [ctypes.c_char_p, I64],
+    "gccu_register_orbinfo": [I64, P64],
+    "gccu_graph_nstr": [I64, I64, I64, I64, P64],
+    "gccu_graph_index": [I64, I64, P64, P64, P64],
+    "gccu_strmap_block": [I64, I64, I64, I64, I64, I64, I64, P64, I64],
+    "gccu_define_operator": [P64, I64, P64],
+    "gccu_register_list": [I64, I64, I64, I64, P64, P64],
+    "gccu_list_block": [I64, I64, P64, P64],
+    "gccu_list_dists": [I64, P64, I64, P64],
+    "gccu_upload_list": [I64, PD, I64],
+    "gccu_download_list": [I64, PD, I64],
+    "gccu_zero_list": [I64],
+    "gccu_list_device_ptr": [I64, ctypes.POINTER(ctypes.c_void_p)],
+    "gccu_contract": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64, I64, PD],
+    "gccu_plan_info": [ctypes.POINTER(BcDesc), I64, P64, PD],
+    "gccu_add_block": [ctypes.c_double, I64, I64, I64, I64, I64, I64, PD],
+    "gccu_scale_list": [I64, ctypes.c_double],
+    "gccu_dot_lists": [I64, I64, PD],
+    "gccu_sym_ab": [I64, I64, ctypes.c_double, ctypes.c_double],
+    "gccu_precondition": [I64, I64, I64, ctypes.c_double, ctypes.c_double],
+    "gccu_graph_begin": [],
+    "gccu_graph_end": [P64],
+    "gccu_graph_launch": [I64],
+    "gccu_sync": [],
+    "gccu_stats": [PD, P64],
+    "gccu_reset_stats": [],
+}
+
+
+def build(verbose=False):
+    """Compile libgccu.so in-tree for sm_100a (nvcc cross-compiles, no GPU needed)."""
+    cmd = ["make", "-C", HERE, "-j8"]
+    if verbose:
+        subprocess.check_call(cmd)
+    else:
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GccuError(f"engine library {LIB_PATH} is missing: build it with "
+                            "`make -C gecco-public_b200` (or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def _err():
+    buf = ctypes.create_string_buffer(1024)
+    lib().gccu_last_error(buf, 1024)
+    return buf.value.decode()
+
+
+def _call(name, *args):
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        raise GccuError(f"{name}: {_err()}")
+
+
+def _p64(a):
+    return a.ctypes.data_as(P64)
+
+
+def _pd(a):
+    return a.ctypes.data_as(PD)
+
+
+def occ8(c=None, a=None):
+    """occupation [C(H,P,V,X), A(H,P,V,X)] from dicts {type: count}"""
+    v = np.zeros(8, dtype=np.int64)
+    for t, n in (c or {}).items():
+        v[t] = n
+    for t, n in (a or {}).items():
+        v[4 + t] = n
+    return v
+
+
+class Engine:
+    """One engine instance (the library keeps one global engine per process)."""
+
+    def __init__(self, device=0, memmax=0):
+        _call("gccu_init", device, memmax)
+        self.device = device
+        self._alive = True
+
+    def close(self):
+        if self._alive:
+            _call("gccu_finalize")
+            self._alive = False
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- orbital space / graphs
+    def register_orbinfo(self, nsym, norb):
+        a = np.zeros((4, 8), dtype=np.int64)
+        norb = np.asarray(norb, dtype=np.int64)
+        a[:, : norb.shape[1]] = norb
+        self._norb = a.copy()
+        _call("gccu_register_orbinfo", nsym, _p64(a.reshape(-1)))
+
+    def nstr(self, typ, nel, idxms, gam):
+        r = np.zeros(1, np.int64)
+        _call("gccu_graph_nstr", typ, nel, idxms, gam, _p64(r))
+        return int(r[0])
+
+    def string_index(self, typ, orb, spn):
+        orb = np.ascontiguousarray(orb, dtype=np.int64)
+        spn = np.ascontiguousarray(spn, dtype=np.int64)
+        r = np.zeros(1, np.int64)
+        _call("gccu_graph_index", typ, orb.size, _p64(orb), _p64(spn), _p64(r))
+        return int(r[0])
+
+    def strmap(self, typ, nel1, nel2, idxms1, idxms2, gam1, gam2):
+        n1 = self.nstr(typ, nel1, idxms1, gam1)
+        n2 = self.nstr(typ, nel2, idxms2, gam2)
+        m = np.zeros(max(n1 * n2, 1), np.int64)
+        _call("gccu_strmap_block", typ, nel1, nel2, idxms1, idxms2, gam1, gam2, _p64(m), m.size)
+        return m[: n1 * n2].reshape(n2, n1)
+
+    # ---- operators / lists
+    def define_operator(self, occs):
+        o = np.ascontiguousarray(np.asarray(occs, dtype=np.int64).reshape(-1, 8))
+        r = np.zeros(1, np.int64)
+        _call("gccu_define_operator", _p64(o), o.shape[0], _p64(r))
+        return int(r[0])
+
+    def register_list(self, op, gamt=1, mst=0, absym=0):
+        lid = np.zeros(1, np.int64)
+        ln = np.zeros(1, np.int64)
+        _call("gccu_register_list", op, gamt, mst, absym, _p64(lid), _p64(ln))
+        return int(lid[0]), int(ln[0])
+
+    def block(self, lst, iblk):
+        off = np.zeros(1, np.int64)
+        ln = np.zeros(1, np.int64)
+        _call("gccu_list_block", lst, iblk, _p64(off), _p64(ln))
+        return int(off[0]), int(ln[0])
+
+    def dists(self, lst):
+        n = np.zeros(1, np.int64)
+        _call("gccu_list_dists", lst, _p64(np.zeros(8, np.int64)), 0, _p64(n))
+        rows = np.zeros((max(int(n[0]), 1), 8), np.int64)
+        _call("gccu_list_dists", lst, _p64(rows), int(n[0]), _p64(n))
+        return rows[: int(n[0])]
+
+    def upload(self, lst, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        _call("gccu_upload_list", lst, _pd(x), x.size)
+
+    def download(self, lst, n):
+        x = np.zeros(n)
+        _call("gccu_download_list", lst, _pd(x), n)
+        return x
+
+    def zero(self, lst):
+        _call("gccu_zero_list", lst)
+
+    def device_ptr(self, lst):
+        p = ctypes.c_void_p()
+        _call("gccu_list_device_ptr", lst, ctypes.byref(p))
+        return p.value
+
+    # ---- contraction / vector operations
+    @staticmethod
+    def desc(op1, op2, res, ex1, ex2, cnt):
+        d = BcDesc()
+        d.list_op1, d.iblk_op1 = op1
+        d.list_op2, d.iblk_op2 = op2
+        d.list_res, d.iblk_res = res
+        d.tra_op1 = d.tra_op2 = d.tra_res = 0
+        for k in range(8):
+            d.occ_ex1[k] = int(ex1[k])
+            d.occ_ex2[k] = int(ex2[k])
+            d.occ_cnt[k] = int(cnt[k])
+        return d
+
+    def contract(self, op1, op2, res, ex1, ex2, cnt, fact=1.0, update=True, use_tr=False,
+                 xret=0, desc=None):
+        d = desc if desc is not None else self.desc(op1, op2, res, ex1, ex2, cnt)
+        r = np.zeros(1)
+        _call("gccu_contract", ctypes.byref(d), fact, int(update), int(use_tr), xret, _pd(r))
+        return float(r[0])
+
+    def plan_info(self, op1, op2, res, ex1, ex2, cnt, use_tr=False):
+        d = self.desc(op1, op2, res, ex1, ex2, cnt)
+        n = np.zeros(1, np.int64)
+        st = np.zeros(8)
+        _call("gccu_plan_info", ctypes.byref(d), int(use_tr), _p64(n), _pd(st))
+        return int(n[0]), st
+
+    def add_block(self, fac, lin, iblk_in, lout, iblk_out, reset=False, typ=0):
+        r = np.zeros(1)
+        _call("gccu_add_block", fac, lin, iblk_in, lout, iblk_out, int(reset), typ, _pd(r))
+        return float(r[0])
+
+    def scale(self, lst, fac):
+        _call("gccu_scale_list", lst, fac)
+
+    def dot(self, a, b):
+        r = np.zeros(1)
+        _call("gccu_dot_lists", a, b, _pd(r))
+        return float(r[0])
+
+    def sym_ab(self, lst, iblk, prefac=0.5, relfac=1.0):
+        _call("gccu_sym_ab", lst, iblk, prefac, relfac)
+
+    def precondition(self, out, inp, diag, fac=1.0, shift=0.0):
+        _call("gccu_precondition", out, inp, diag, fac, shift)
+
+    # ---- graphs / sync / stats
+    def graph_begin(self):
+        _call("gccu_graph_begin")
+
+    def graph_end(self):
+        r = np.zeros(1, np.int64)
+        _call("gccu_graph_end", _p64(r))
+        return int(r[0])
+
+    def graph_launch(self, gid):
+        _call("gccu_graph_launch", gid)
+
+    def sync(self):
+        _call("gccu_sync")
+
+    def stats(self):
+        st = np.zeros(8)
+        n = np.zeros(1, np.int64)
+        _call("gccu_stats", _pd(st), _p64(n))
+        return st, int(n[0])
+
+    def reset_stats(self):
+        _call("gccu_reset_stats")

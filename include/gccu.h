@@ -1,0 +1,151 @@
+/*
+ * gccu.h -- C ABI of the B200 engine for GeCCo's blocked tensor contraction.
+ *
+ * Drop-in boundary: the Fortran host (formula interpreter frm_sched2, solvers)
+ * stays unchanged and calls these entry points through ISO_C_BINDING from a
+ * thin shim.  Conventions follow the reference:
+ *   - every integer is int64_t (the reference is built with 64-bit default
+ *     INTEGER, config/x86_64-linux.conf:39,51), reals are double;
+ *   - irreps, occupation-class indices and Ms indices are 1-based;
+ *   - an occupation is int64_t occ[2][4]: row 0 = creators, row 1 =
+ *     annihilators, columns = hole, particle, valence, external (the
+ *     reference's iocc(ngastp,2) transposed to C order);
+ *   - every call returns 0 on success and a non-zero status on failure; the
+ *     message is available from gccu_last_error (the shim turns a non-zero
+ *     status into quit(1,...), baserout/quit.F).
+ * Calls are not thread-safe (the reference host is single-threaded); all work
+ * is ordered on one CUDA stream; calls that return numbers to the host
+ * (norms, energies, downloads) synchronise that stream.
+ */
+#ifndef GCCU_H
+#define GCCU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- life cycle ----------------------------------------------------------
+ * replaces: memory set-up of gecco.x (gecco/gecco.f:125-130, mem_init);
+ * memmax_bytes caps the device memory the engine may hold (<=0: no cap).
+ * device < 0 starts a host-only engine: orbital model, graphs, ME-list
+ * layouts and contraction plans can be queried, nothing is executed. */
+int gccu_init(int64_t device, int64_t memmax_bytes);
+int gccu_finalize(void);
+/* copies the last error message (NUL-terminated, truncated to len) */
+int gccu_last_error(char* buf, int64_t len);
+
+/* ---- orbital space ---------------------------------------------------------
+ * replaces: orb_info set-up (include/def_orbinf.h; input/read_env_*.f).
+ * norb_hpvx[t*8+g] = number of active (non-frozen, non-deleted) orbitals of
+ * type t (0=H,1=P,2=V,3=X) in irrep g+1, g < nsym.  nsym in {1,2,4,8}. */
+int gccu_register_orbinfo(int64_t nsym, const int64_t* norb_hpvx);
+
+/* ---- graphs (string spaces) ------------------------------------------------
+ * replaces: set_graph2 / weight_* (strings/set_graph2.f:2-206).
+ * Number of strings of the graph (type,nel) with Ms index idxms (1..nel+1,
+ * Ms = nel-2*(idxms-1)) and irrep gam. */
+int gccu_graph_nstr(int64_t type, int64_t nel, int64_t idxms, int64_t gam, int64_t* nstr);
+/* lexical address of one string (idx4sg, strings/idx4sg.f:2-82): orb[] 1-based
+ * orbital numbers within the type, spn[] +1/-1/2 (2 = doubly occupied, listed
+ * twice), in canonical order; returns the 0-based index within its block. */
+int gccu_graph_index(int64_t type, int64_t nel, const int64_t* orb, const int64_t* spn,
+                     int64_t* index);
+/* one block of the signed string map, built on the device
+ * (set_strmap_kernel, strings/set_strmap_kernel.f:66-119): entry
+ * m[i2*n1+i1] = sign*(index12+1), 0 if Pauli-forbidden. */
+int gccu_strmap_block(int64_t type, int64_t nel1, int64_t nel2, int64_t idxms1,
+                      int64_t idxms2, int64_t gam1, int64_t gam2, int64_t* map, int64_t n);
+
+/* ---- operators and ME lists -------------------------------------------------
+ * replaces: operator definition (include/def_operator.h) + set_op_dim2
+ * (operators/set_op_dim2.f:1-531).  occ: nblk occupation classes. */
+int gccu_define_operator(const int64_t* occ, int64_t nblk, int64_t* op_id);
+/* ME list of an operator with total irrep gamt, total 2*Ms mst and spin-flip
+ * symmetry absym (0,+1,-1); its data live in device memory for the whole
+ * solve (include/def_me_list.h:37-115).  Returns handle and len_op. */
+int gccu_register_list(int64_t op_id, int64_t gamt, int64_t mst, int64_t absym,
+                       int64_t* list_id, int64_t* len_op);
+/* off_op_occ / len_op_occ of occupation class iblk (1-based) */
+int gccu_list_block(int64_t list_id, int64_t iblk, int64_t* off, int64_t* len);
+/* distribution table (same rows as the oracle): (iblk, idxmsa, gama, idxdis,
+ * offset, length, ld, did); returns the row count in *nrows */
+int gccu_list_dists(int64_t list_id, int64_t* rows, int64_t maxrows, int64_t* nrows);
+/* host <-> device transfer of a whole list (replaces get_vec/put_vec,
+ * fileutil/get_vec.f, for lists that are resident on the device) */
+int gccu_upload_list(int64_t list_id, const double* host, int64_t n);
+int gccu_download_list(int64_t list_id, double* host, int64_t n);
+int gccu_zero_list(int64_t list_id);
+/* raw device pointer of the list data (for callers that own device memory) */
+int gccu_list_device_ptr(int64_t list_id, void** dptr);
+
+/* ---- [CONTR] ------------------------------------------------------------------
+ * replaces: contr_op1op2 case(2,3) (contract/contr_op1op2.f:112-173) ->
+ * contr_op1op2_wmaps_c (contract/contr_op1op2_wmaps_c.f:2-2169) with the
+ * inner kernels contr_blk1blk2_wmaps_c / contr_blk1blk2_blocked_mm.
+ * Operands: occupation classes iblk_op1/iblk_op2 of lists list_op1/list_op2,
+ * result class iblk_res of list_res.  occ_ex1/occ_ex2/occ_cnt are the
+ * external / contracted parts (op1 = ex1+cnt, op2 = ex2+cnt^+,
+ * res = ex1+ex2).  fact = bc_sign*contr%fac from the formula file
+ * (formula/process_bc.f:528-535).  update=0 overwrites the result class.
+ * use_tr: spin-flip symmetry (calculate.routes.use_tr), applied when all three
+ * lists carry absym != 0.  type_xret: 0 none, 1 squared norm of the result
+ * class, 2 its first element (scalars); written to *xret. */
+typedef struct gccu_bc_desc {
+  int64_t list_op1, iblk_op1;
+  int64_t list_op2, iblk_op2;
+  int64_t list_res, iblk_res;
+  int64_t tra_op1, tra_op2, tra_res; /* must be 0 in this engine version */
+  int64_t occ_ex1[8], occ_ex2[8], occ_cnt[8];
+} gccu_bc_desc;
+int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr,
+                  int64_t type_xret, double* xret);
+/* the block contractions the engine plans for a [CONTR] (without running
+ * them): number of block contractions and the reference dgemm accounting of
+ * gccu_stats for this contraction alone */
+int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8);
+
+/* ---- [ADD] -------------------------------------------------------------------
+ * replaces: add_opblk (contract/add_opblk.f:2-313), in-core branch
+ * :299-307: out(iblkout) = (reset ? 0 : out) + fac*in(iblkin); type 1 returns
+ * the squared norm of the updated block, type 2 its first element. */
+int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_out,
+                   int64_t iblk_out, int64_t reset, int64_t type, double* xnorm2);
+/* scale a whole list in place (scale_copy_op with one operand) */
+int gccu_scale_list(int64_t list_id, double fac);
+/* dot product of two lists of identical layout (DIIS subspace products) */
+int gccu_dot_lists(int64_t list_a, int64_t list_b, double* dot);
+
+/* ---- spin-flip symmetrisation ---------------------------------------------
+ * replaces: sym_ab_blk (contract/sym_ab_blk.f:2-405) for one class:
+ * x <- prefac*(x + relfac*flip(x)) */
+int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac);
+
+/* ---- preconditioner ------------------------------------------------------
+ * replaces: diavc (baserout/diavc.f:31-35) on whole lists:
+ * out = fac*in/(diag+shift), |diag+shift| <= 1e-10 -> 1e-10 */
+int gccu_precondition(int64_t list_out, int64_t list_in, int64_t list_diag, double fac,
+                      double shift);
+
+/* ---- CUDA graphs -------------------------------------------------------------
+ * Capture the device work of a sequence of calls (one formula evaluation,
+ * contract/frm_sched.f:89-100) and replay it.  Calls inside a capture must not
+ * request host values (type_xret must be 0); plans are cached per descriptor,
+ * so a sequence is normally run once eagerly before it is captured. */
+int gccu_graph_begin(void);
+int gccu_graph_end(int64_t* graph_id);
+int gccu_graph_launch(int64_t graph_id);
+int gccu_sync(void);
+
+/* ---- statistics -----------------------------------------------------------
+ * dgemm shape statistics in the reference's accounting
+ * (contract/contr_blk1blk2_blocked_mm.f:454-460): [calls, sum dim1,
+ * sum dim1^2, sum dim2, sum dim2^2, sum cnt, sum cnt^2, flops] accumulated
+ * over the planned block contractions since the last reset, and the number of
+ * kernel launches issued. */
+int gccu_stats(double* stats8, int64_t* launches);
+int gccu_reset_stats(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
