@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -327,7 +328,7 @@ struct List {
 struct ora_ctx {
   OrbInfo oi;
   std::map<std::pair<int, int>, int> graph_id;  // (type,nel) -> id
-  std::vector<Graph> graphs;
+  std::deque<Graph> graphs;  // stable references while graphs are added
   std::vector<Op> ops;
   std::vector<List> lists;
   // string map blocks, keyed by (g1,g2,idxms1,idxms2,gam1,gam2)

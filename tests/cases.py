@@ -1,0 +1,61 @@
+"""Shared test cases: orbital spaces and binary contractions in the
+reference's occupation language (test helper, not product code)."""
+import numpy as np
+
+from gccu import H, P, V, occ8
+
+# (nsym, norb[type][irrep]) orbital spaces
+SPACES = {
+    "c1_small": (1, [[3], [5], [0], [0]]),
+    "c2v": (4, [[2, 1, 1, 0], [3, 2, 2, 1], [0] * 4, [0] * 4]),
+    "d2h": (8, [[1, 1, 0, 1, 0, 1, 0, 0], [2, 1, 1, 1, 1, 1, 1, 1], [0] * 8, [0] * 8]),
+    "c1_val": (1, [[2], [4], [2], [0]]),
+}
+
+
+def cnt_dag(c):
+    c = np.asarray(c)
+    return np.concatenate([c[4:], c[:4]])
+
+
+# binary contractions: (name, op1 occ, op2 occ, res occ, ex1, ex2, cnt)
+def _bc(name, ex1, ex2, cnt):
+    ex1, ex2, cnt = np.asarray(ex1), np.asarray(ex2), np.asarray(cnt)
+    op1 = ex1 + cnt
+    op2 = ex2 + cnt_dag(cnt)
+    res = ex1 + ex2
+    return (name, op1, op2, res, ex1, ex2, cnt)
+
+
+CONTRACTIONS = [
+    # Fock particle block on doubles: F(P;P) T2, one particle contracted
+    _bc("fpp_t2", occ8({P: 1}), occ8({P: 1}, {H: 2}), occ8(None, {P: 1})),
+    # Fock hole block on doubles: F(H;H) T2, one hole contracted
+    _bc("fhh_t2", occ8(None, {H: 1}), occ8({P: 2}, {H: 1}), occ8({H: 1})),
+    # particle ladder: H(PP;PP) T2
+    _bc("pp_ladder", occ8({P: 2}), occ8(None, {H: 2}), occ8(None, {P: 2})),
+    # hole ladder: W(HH;HH) T2 (contracts the holes of T2 with W's creators)
+    _bc("hh_ladder", occ8(None, {H: 2}), occ8({P: 2}), occ8({H: 2})),
+    # ring: W(PH;PH) T2, one hole and one particle contracted
+    _bc("ring", occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1}), occ8({H: 1}, {P: 1})),
+    # energy-like full contraction: H(HH;PP) T2 -> scalar
+    _bc("energy", occ8(), occ8(), occ8({H: 2}, {P: 2})),
+    # singles into doubles: T1 x H(PH;HH) -> (PP;HH)
+    _bc("t1_vphhh", occ8({P: 1}), occ8({P: 1}, {H: 2}), occ8(None, {H: 1})),
+    # outer product: T1 T1 -> T2-like, nothing contracted
+    _bc("t1t1", occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1}), occ8()),
+    # three-body: T3-like (PPP;HHH) x F(H;H)
+    _bc("t3_fhh", occ8({P: 3}, {H: 2}), occ8(None, {H: 1}), occ8(None, {H: 1})),
+]
+
+
+def contractions_for(space):
+    if space == "c1_val":
+        return CONTRACTIONS + [
+            _bc("val_mix", occ8({V: 1}, {H: 1}), occ8({P: 1}, {V: 1}), occ8({V: 1}, {P: 1}))]
+    return CONTRACTIONS
+
+
+def random_list(n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(n)
