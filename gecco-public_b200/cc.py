@@ -1,0 +1,304 @@
+"""Coupled-cluster drivers on top of the contraction engine.
+
+The reference generates its CC equations as formula files (lists of [ADD] /
+[CONTR] items over operator blocks, include/def_formula_item.h) and evaluates
+them with frm_sched2 (contract/frm_sched2.f:117-365) inside solve_nleq
+(solve/solve_nleq.f:377-787).  Formula generation is outside the engine's
+scope; the formulas below are closed-shell spin-orbital CCSD (the
+Stanton-Gauss intermediates, J. Chem. Phys. 94, 4334 (1991)) and MP2 written
+directly as binary contractions in the reference's occupation language.
+Each [CONTR] factor is the product of the topological sign and the
+combinatorial factor of that contraction (what the reference stores as
+binary_contr%fact); tests/test_cc_formula.py checks every item against its
+dense spin-orbital tensor expression.
+
+Evaluation goes through the engine's C ABI only (gccu_contract,
+gccu_add_block, gccu_precondition, ...); the first evaluation plans every
+contraction, later ones can be replayed from a CUDA graph.
+"""
+import numpy as np
+
+from gccu import H, P, occ8
+from melist import ListView, condensed
+
+# ---- operator blocks ---------------------------------------------------------
+HH, HP, PH, PP = occ8({H: 1}, {H: 1}), occ8({H: 1}, {P: 1}), occ8({P: 1}, {H: 1}), occ8(
+    {P: 1}, {P: 1})
+HHHH, HHPH, HHPP = occ8({H: 2}, {H: 2}), occ8({H: 2}, {H: 1, P: 1}), occ8({H: 2}, {P: 2})
+PHHH, PHPH, PHPP = (occ8({H: 1, P: 1}, {H: 2}), occ8({H: 1, P: 1}, {H: 1, P: 1}),
+                    occ8({H: 1, P: 1}, {P: 2}))
+PPHH, PPPH, PPPP = occ8({P: 2}, {H: 2}), occ8({P: 2}, {H: 1, P: 1}), occ8({P: 2}, {P: 2})
+SCAL = occ8()
+
+FOCK_BLOCKS = [HH, HP, PH, PP]
+V_BLOCKS = [HHHH, HHPH, HHPP, PHHH, PHPH, PHPP, PPHH, PPPH, PPPP]
+
+
+def cnt(c=None, a=None):
+    return occ8(c, a)
+
+
+# ---- formulas: ("ADD", res, src, fac, reset) / ("CONTR", res, op1, op2, cnt, fac, update)
+# res/src/op1/op2 = (operator name, block occupation)
+
+def _A(res, src, fac=1.0, reset=True, name=""):
+    return dict(kind="ADD", res=res, src=src, fac=fac, reset=reset, name=name)
+
+
+def _C(res, op1, op2, c, fac, update=True, name=""):
+    return dict(kind="CONTR", res=res, op1=op1, op2=op2, cnt=c, fac=fac, update=update, name=name)
+
+
+MP2_OPERATORS = {"F": FOCK_BLOCKS, "V": V_BLOCKS, "T2": [PPHH], "R2": [PPHH], "E": [SCAL]}
+
+MP2_FORMULA = [
+    _C(("E", SCAL), ("V", HHPP), ("T2", PPHH), cnt({H: 2}, {P: 2}), 1.0, False, "e_mp2"),
+    _A(("R2", PPHH), ("V", PPHH), 1.0, True, "r2_v"),
+    _C(("R2", PPHH), ("F", PP), ("T2", PPHH), cnt(None, {P: 1}), 1.0, True, "r2_fpp"),
+    _C(("R2", PPHH), ("F", HH), ("T2", PPHH), cnt({H: 1}), 1.0, True, "r2_fhh"),
+]
+
+CCSD_OPERATORS = {
+    "F": FOCK_BLOCKS, "V": V_BLOCKS, "T1": [PH], "T2": [PPHH], "R1": [PH], "R2": [PPHH],
+    "TAU": [PPHH], "TAUT": [PPHH], "E": [SCAL], "XFPP": [PP], "XFHH": [HH], "XFHP": [HP],
+    "F2PP": [PP], "F2HH": [HH], "XW": [HHHH], "XWT": [PHPH], "Y": [PHPP], "Z": [PHHH],
+    "HJB": [PH],
+}
+
+CCSD_FORMULA = [
+    # tau = t2 + P(ab) t1 t1 ; tau~ = t2 + 1/2 P(ab) t1 t1
+    _A(("TAU", PPHH), ("T2", PPHH), 1.0, True, "tau_t2"),
+    _C(("TAU", PPHH), ("T1", PH), ("T1", PH), cnt(), -0.5, True, "tau_t1t1"),
+    _A(("TAUT", PPHH), ("T2", PPHH), 1.0, True, "taut_t2"),
+    _C(("TAUT", PPHH), ("T1", PH), ("T1", PH), cnt(), -0.25, True, "taut_t1t1"),
+    # energy: f_ia t_i^a + 1/4 <ij||ab> tau_ij^ab
+    _C(("E", SCAL), ("F", HP), ("T1", PH), cnt({H: 1}, {P: 1}), 1.0, False, "e_ft1"),
+    _C(("E", SCAL), ("V", HHPP), ("TAU", PPHH), cnt({H: 2}, {P: 2}), 1.0, True, "e_vtau"),
+    # F_ae
+    _A(("XFPP", PP), ("F", PP), 1.0, True, "fae_f"),
+    _C(("XFPP", PP), ("F", HP), ("T1", PH), cnt({H: 1}), -0.5, True, "fae_ft1"),
+    _C(("XFPP", PP), ("V", PHPP), ("T1", PH), cnt({H: 1}, {P: 1}), -1.0, True, "fae_vt1"),
+    _C(("XFPP", PP), ("TAUT", PPHH), ("V", HHPP), cnt({P: 1}, {H: 2}), -1.0, True, "fae_tautv"),
+    # F_mi
+    _A(("XFHH", HH), ("F", HH), 1.0, True, "fmi_f"),
+    _C(("XFHH", HH), ("F", HP), ("T1", PH), cnt(None, {P: 1}), 0.5, True, "fmi_ft1"),
+    _C(("XFHH", HH), ("V", HHPH), ("T1", PH), cnt({H: 1}, {P: 1}), 1.0, True, "fmi_vt1"),
+    _C(("XFHH", HH), ("V", HHPP), ("TAUT", PPHH), cnt({H: 1}, {P: 2}), 1.0, True, "fmi_vtaut"),
+    # F_me
+    _A(("XFHP", HP), ("F", HP), 1.0, True, "fme_f"),
+    _C(("XFHP", HP), ("V", HHPP), ("T1", PH), cnt({H: 1}, {P: 1}), 1.0, True, "fme_vt1"),
+    # W_mnij (with 1/2 tau <mn||ef>, which absorbs the tau-tau part of W_abef)
+    _A(("XW", HHHH), ("V", HHHH), 1.0, True, "wmnij_v"),
+    _C(("XW", HHHH), ("V", HHPH), ("T1", PH), cnt(None, {P: 1}), 1.0, True, "wmnij_vt1"),
+    _C(("XW", HHHH), ("V", HHPP), ("TAU", PPHH), cnt(None, {P: 2}), 1.0, True, "wmnij_vtau"),
+    # W~_mbej (W_mbej without the bare integral), stored as [b m; e j]
+    _C(("XWT", PHPH), ("V", PHPP), ("T1", PH), cnt(None, {P: 1}), 1.0, False, "wmbej_vt1a"),
+    _C(("XWT", PHPH), ("V", HHPH), ("T1", PH), cnt({H: 1}), 1.0, True, "wmbej_vt1b"),
+    _C(("XWT", PHPH), ("V", HHPP), ("T2", PPHH), cnt({H: 1}, {P: 1}), 0.5, True, "wmbej_vt2"),
+    _C(("Y", PHPP), ("V", HHPP), ("T1", PH), cnt({H: 1}), -1.0, False, "y_vt1"),
+    _C(("XWT", PHPH), ("Y", PHPP), ("T1", PH), cnt(None, {P: 1}), 1.0, True, "wmbej_yt1"),
+    # T1 residual
+    _A(("R1", PH), ("F", PH), 1.0, True, "r1_f"),
+    _C(("R1", PH), ("XFPP", PP), ("T1", PH), cnt(None, {P: 1}), 1.0, True, "r1_fae"),
+    _C(("R1", PH), ("T1", PH), ("XFHH", HH), cnt(None, {H: 1}), -1.0, True, "r1_fmi"),
+    _C(("R1", PH), ("T2", PPHH), ("XFHP", HP), cnt({P: 1}, {H: 1}), 1.0, True, "r1_fme"),
+    _C(("R1", PH), ("V", PHPH), ("T1", PH), cnt({H: 1}, {P: 1}), -1.0, True, "r1_vt1"),
+    _C(("R1", PH), ("V", PHPP), ("T2", PPHH), cnt({H: 1}, {P: 2}), -1.0, True, "r1_vt2a"),
+    _C(("R1", PH), ("T2", PPHH), ("V", HHPH), cnt({P: 1}, {H: 2}), -1.0, True, "r1_vt2b"),
+    # T2 residual
+    _A(("F2PP", PP), ("XFPP", PP), 1.0, True, "f2pp"),
+    _C(("F2PP", PP), ("XFHP", HP), ("T1", PH), cnt({H: 1}), -0.5, True, "f2pp_t1"),
+    _A(("F2HH", HH), ("XFHH", HH), 1.0, True, "f2hh"),
+    _C(("F2HH", HH), ("XFHP", HP), ("T1", PH), cnt(None, {P: 1}), 0.5, True, "f2hh_t1"),
+    _A(("R2", PPHH), ("V", PPHH), 1.0, True, "r2_v"),
+    _C(("R2", PPHH), ("F2PP", PP), ("T2", PPHH), cnt(None, {P: 1}), 1.0, True, "r2_fae"),
+    _C(("R2", PPHH), ("F2HH", HH), ("T2", PPHH), cnt({H: 1}), 1.0, True, "r2_fmi"),
+    _C(("R2", PPHH), ("TAU", PPHH), ("XW", HHHH), cnt(None, {H: 2}), 1.0, True, "r2_wmnij"),
+    _C(("R2", PPHH), ("V", PPPP), ("TAU", PPHH), cnt(None, {P: 2}), 1.0, True, "r2_ladder"),
+    _C(("Z", PHHH), ("V", PHPP), ("TAU", PPHH), cnt(None, {P: 2}), 1.0, False, "z_vtau"),
+    _C(("R2", PPHH), ("Z", PHHH), ("T1", PH), cnt({H: 1}), -1.0, True, "r2_zt1"),
+    _C(("R2", PPHH), ("TAU", PPHH), ("V", PHPH), cnt({P: 1}, {H: 1}), 1.0, True, "r2_ring_v"),
+    _C(("R2", PPHH), ("T2", PPHH), ("XWT", PHPH), cnt({P: 1}, {H: 1}), -1.0, True, "r2_ring_w"),
+    _C(("HJB", PH), ("V", PHPH), ("T1", PH), cnt({H: 1}, {P: 1}), -1.0, False, "h_vt1"),
+    _C(("R2", PPHH), ("T1", PH), ("HJB", PH), cnt(), 1.0, True, "r2_t1h"),
+    _C(("R2", PPHH), ("V", PPPH), ("T1", PH), cnt(None, {P: 1}), 1.0, True, "r2_vt1a"),
+    _C(("R2", PPHH), ("T1", PH), ("V", PHHH), cnt(None, {H: 1}), 1.0, True, "r2_vt1b"),
+]
+
+
+# ---- filling the Hamiltonian lists -------------------------------------------
+
+def _axis_types(occ):
+    c, a = condensed(occ)
+    return [t for t, n in c for _ in range(n)] + [t for t, n in a for _ in range(n)]
+
+
+def fill_hamiltonian(view_f, view_v, nf, nv, ints):
+    """host vectors of the Fock list (blocks HH,HP,PH,PP) and the
+    antisymmetrised two-electron list <c1c2||a1a2> (9 blocks)"""
+    sp = ints.space
+
+    def glob(t, so):
+        return sp.type_orbitals(t)[so // 2], so % 2
+
+    xf = np.zeros(nf)
+    for ib, occ in enumerate(FOCK_BLOCKS, 1):
+        tc, ta = _axis_types(occ)
+
+        def val(ax, tc=tc, ta=ta):
+            (p, sp_), (q, sq) = glob(tc, ax[0]), glob(ta, ax[1])
+            return ints.fock(p, q) * (sp_ == sq)
+
+        view_f.fill(xf, ib, val)
+    xv = np.zeros(nv)
+    for ib, occ in enumerate(V_BLOCKS, 1):
+        t = _axis_types(occ)
+
+        def val(ax, t=t):
+            (c1, s1), (c2, s2) = glob(t[0], ax[0]), glob(t[1], ax[1])
+            (a1, r1), (a2, r2) = glob(t[2], ax[2]), glob(t[3], ax[3])
+            direct = ints.eri_elems(c1, a1, c2, a2) * ((s1 == r1) & (s2 == r2))
+            exch = ints.eri_elems(c1, a2, c2, a1) * ((s1 == r2) & (s2 == r1))
+            return direct - exch
+
+        view_v.fill(xv, ib, val)
+    return xf, xv
+
+
+def fill_denominators(view, n, occ, ints):
+    """orbital-energy differences sum eps(particles) - sum eps(holes) with the
+    shape of an excitation list (dia4op, contract/dia4op.f)"""
+    sp = ints.space
+    types = _axis_types(occ)
+    c, _ = condensed(occ)
+    ncre = sum(k for _, k in c)
+    x = np.zeros(n)
+
+    def val(ax):
+        d = 0.0
+        for k, (t, so) in enumerate(zip(types, ax)):
+            p = sp.type_orbitals(t)[so // 2]
+            e = ints.fock(p, p)
+            d = d + (e if k < ncre else -e)
+        return d
+
+    view.fill(x, 1, val)
+    return x
+
+
+# ---- solver -------------------------------------------------------------------
+
+class CCSolver:
+    """Jacobi/DIIS solution of the CC amplitude equations with device-resident
+    lists (solve_nleq with method=diis, solve/solve_nleq.f; diagonal step
+    diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
+
+    def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8):
+        self.e = engine
+        self.ints = ints
+        self.method = method
+        self.use_tr = use_tr
+        self.maxsub = maxsub
+        sp = ints.space
+        self.nsym = sp.nsym
+        engine.register_orbinfo(sp.nsym, sp.norb)
+        ops = MP2_OPERATORS if method == "mp2" else CCSD_OPERATORS
+        self.formula = MP2_FORMULA if method == "mp2" else CCSD_FORMULA
+        self.lists = {}
+        for name, blocks in ops.items():
+            opid = engine.define_operator(blocks)
+            absym = 1 if use_tr and name not in ("F", "V", "E") else 0
+            if use_tr and name in ("F", "V"):
+                absym = 1
+            lid, n = engine.register_list(opid, absym=absym)
+            self.lists[name] = (lid, n, blocks)
+        self.amps = ["T2"] if method == "mp2" else ["T1", "T2"]
+        self.res = {"T1": "R1", "T2": "R2"}
+        # denominators, steps and DIIS subspace
+        for a in self.amps:
+            blocks = self.lists[a][2]
+            for extra in ("D" + a, "S" + a):
+                opid = engine.define_operator(blocks)
+                lid, n = engine.register_list(opid)
+                self.lists[extra] = (lid, n, blocks)
+        self.graph = None
+        self.history = []
+
+    def lid(self, name):
+        return self.lists[name][0]
+
+    def blk(self, ref):
+        name, occ = ref
+        blocks = self.lists[name][2]
+        for i, b in enumerate(blocks, 1):
+            if np.array_equal(b, occ):
+                return (self.lists[name][0], i)
+        raise KeyError(ref)
+
+    def view(self, name):
+        lid, n, blocks = self.lists[name]
+        return ListView(self.e, lid, blocks, self.nsym)
+
+    def load_hamiltonian(self):
+        xf, xv = fill_hamiltonian(self.view("F"), self.view("V"), self.lists["F"][1],
+                                  self.lists["V"][1], self.ints)
+        self.e.upload(self.lid("F"), xf)
+        self.e.upload(self.lid("V"), xv)
+        for a in self.amps:
+            n = self.lists[a][1]
+            d = fill_denominators(self.view("D" + a), n, self.lists[a][2][0], self.ints)
+            self.e.upload(self.lid("D" + a), d)
+            self.e.zero(self.lid(a))
+
+    def evaluate(self):
+        """one formula evaluation (frm_sched2 over the item list)"""
+        for it in self.formula:
+            if it["kind"] == "ADD":
+                (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
+                self.e.add_block(it["fac"], li, bi, lo, bo, reset=it["reset"])
+            else:
+                o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
+                c = np.asarray(it["cnt"])
+                occ1 = np.asarray(it["op1"][1])
+                occ2 = np.asarray(it["op2"][1])
+                ex1 = occ1 - c
+                ex2 = occ2 - np.concatenate([c[4:], c[:4]])
+                use_tr = self.use_tr and it["res"][0] not in ("E",)
+                self.e.contract(o1, o2, r, ex1, ex2, c, fact=it["fac"], update=it["update"],
+                                use_tr=use_tr)
+
+    def energy(self):
+        return float(self.e.download(self.lid("E"), 1)[0])
+
+    def residual_norm(self):
+        return float(np.sqrt(sum(self.e.dot(self.lid(self.res[a]), self.lid(self.res[a]))
+                                 for a in self.amps)))
+
+    def step(self):
+        """t <- t - R/D (diagonal preconditioner)"""
+        for a in self.amps:
+            self.e.precondition(self.lid("S" + a), self.lid(self.res[a]), self.lid("D" + a),
+                                fac=-1.0)
+            self.e.add_block(1.0, self.lid("S" + a), 1, self.lid(a), 1)
+
+    def solve(self, maxiter=50, conv=1e-8, use_graph=False, callback=None):
+        e_old = 0.0
+        for it in range(1, maxiter + 1):
+            if use_graph and self.graph is None and it > 1:
+                self.e.graph_begin()
+                self.evaluate()
+                self.graph = self.e.graph_end()
+            if self.graph is not None:
+                self.e.graph_launch(self.graph)
+            else:
+                self.evaluate()
+            en = self.energy()
+            rn = self.residual_norm()
+            self.history.append((it, en, rn))
+            if callback:
+                callback(it, en, rn)
+            if rn < conv:
+                return en
+            self.step()
+            e_old = en
+        return e_old

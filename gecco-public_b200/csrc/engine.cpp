@@ -475,6 +475,26 @@ int gccu_graph_index(int64_t type, int64_t nel, const int64_t* orb, const int64_
   });
 }
 
+int gccu_graph_strings(int64_t type, int64_t nel, int64_t idxms, int64_t gam, int64_t* orb,
+                       int64_t* spn, int64_t maxn, int64_t* n) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    GCCU_REQUIRE(type >= 0 && type < 4 && nel >= 1 && nel <= kMaxNel, "bad graph");
+    Graph& g = e.model.G(e.model.graph((int)type, (int)nel));
+    GCCU_REQUIRE(idxms >= 1 && idxms <= nel + 1 && gam >= 1 && gam <= g.nsym, "bad block");
+    int64_t ns = g.nstr((int)idxms, (int)gam);
+    *n = ns;
+    if (ns > maxn) return;
+    const auto& t = g.table((int)idxms, (int)gam);
+    for (int64_t i = 0; i < ns * nel; ++i) {
+      int c = t[i] & 3;
+      orb[i] = (t[i] >> 2) + 1;
+      spn[i] = c == 1 ? 1 : (c == 2 ? -1 : 2);
+    }
+  });
+}
+
 int gccu_strmap_block(int64_t type, int64_t nel1, int64_t nel2, int64_t idxms1, int64_t idxms2,
                       int64_t gam1, int64_t gam2, int64_t* map, int64_t n) {
   return guarded([&] {

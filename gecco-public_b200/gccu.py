@@ -42,6 +42,7 @@ _SIGS = {
     "gccu_register_orbinfo": [I64, P64],
     "gccu_graph_nstr": [I64, I64, I64, I64, P64],
     "gccu_graph_index": [I64, I64, P64, P64, P64],
+    "gccu_graph_strings": [I64, I64, I64, I64, P64, P64, I64, P64],
     "gccu_strmap_block": [I64, I64, I64, I64, I64, I64, I64, P64, I64],
     "gccu_define_operator": [P64, I64, P64],
     "gccu_register_list": [I64, I64, I64, I64, P64, P64],
@@ -163,6 +164,17 @@ class Engine:
         r = np.zeros(1, np.int64)
         _call("gccu_graph_index", typ, orb.size, _p64(orb), _p64(spn), _p64(r))
         return int(r[0])
+
+    def strings(self, typ, nel, idxms, gam):
+        """strings of one graph block in address order: (orb[n,nel] 1-based, spn[n,nel])"""
+        n = np.zeros(1, np.int64)
+        e = np.zeros(1, np.int64)
+        _call("gccu_graph_strings", typ, nel, idxms, gam, _p64(e), _p64(e), 0, _p64(n))
+        ns = int(n[0])
+        orb = np.zeros(max(ns * nel, 1), np.int64)
+        spn = np.zeros(max(ns * nel, 1), np.int64)
+        _call("gccu_graph_strings", typ, nel, idxms, gam, _p64(orb), _p64(spn), ns, _p64(n))
+        return orb[: ns * nel].reshape(ns, nel), spn[: ns * nel].reshape(ns, nel)
 
     def strmap(self, typ, nel1, nel2, idxms1, idxms2, gam1, gam2):
         n1 = self.nstr(typ, nel1, idxms1, gam1)

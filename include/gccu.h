@@ -50,6 +50,11 @@ int gccu_graph_nstr(int64_t type, int64_t nel, int64_t idxms, int64_t gam, int64
  * twice), in canonical order; returns the 0-based index within its block. */
 int gccu_graph_index(int64_t type, int64_t nel, const int64_t* orb, const int64_t* spn,
                      int64_t* index);
+/* the strings of one graph block in address order: n*nel entries of orb[]
+ * (1-based) and spn[] (+1/-1/2); *n = number of strings (a host filling ME
+ * lists uses these to place integrals, cf. input/import_h2_molpro_dump.f) */
+int gccu_graph_strings(int64_t type, int64_t nel, int64_t idxms, int64_t gam, int64_t* orb,
+                       int64_t* spn, int64_t maxn, int64_t* n);
 /* one block of the signed string map, built on the device
  * (set_strmap_kernel, strings/set_strmap_kernel.f:66-119): entry
  * m[i2*n1+i1] = sign*(index12+1), 0 if Pauli-forbidden. */

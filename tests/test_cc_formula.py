@@ -1,0 +1,75 @@
+"""The CC drivers (formula items + solver) on the CPU oracle against the
+reference's golden MP2 run and a dense spin-orbital CCSD."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cc
+import dense_cc
+import hamiltonian as hm
+from engine import OracleEngine
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def hf_ints():
+    d = hm.read_fcidump(os.path.join(GOLD, "hf_ccpvdz_fcidump.npz"))
+    sp = hm.OrbitalSpace(d["orbsym"], [3, 1, 1, 0], [1, 0, 0, 0])
+    f = hm.fock(d["h"], d["eri"], sp.occ_all)
+    return hm.DenseIntegrals(sp, f, d["eri"])
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return json.load(open(os.path.join(GOLD, "hf_ccpvdz_ref.json")))
+
+
+def test_dense_mp2_matches_reference(hf_ints, gold):
+    sp, f, eri = hf_ints.space, hf_ints.f, hf_ints.eri
+    o, v = sp.hole, sp.part
+    eo, ev = np.diag(f)[o], np.diag(f)[v]
+    iajb = eri[np.ix_(o, v, o, v)]
+    D = eo[:, None, None, None] - ev[None, :, None, None] + eo[None, None, :, None] - \
+        ev[None, None, None, :]
+    e = np.sum(iajb * (2 * iajb - iajb.transpose(0, 3, 2, 1)) / D)
+    assert abs(e + gold["lmp2_norm"]) < 1e-13
+
+
+@pytest.mark.parametrize("route", [2, 3])
+def test_mp2_through_contractions_matches_reference(hf_ints, gold, route):
+    # the reference prints ">>> 1 0.000000000000 1.100" and then
+    # ">>> 2 -0.196151291382 0.6566E-14" (test/python-interface.s.ref:583,627)
+    s = cc.CCSolver(OracleEngine(route=route), hf_ints, method="mp2")
+    s.load_hamiltonian()
+    e = s.solve(maxiter=5, conv=1e-10)
+    (i1, e1, r1), (i2, e2, r2) = s.history[:2]
+    assert e1 == 0.0 and round(r1, 3) == 1.100
+    assert abs(e2 - gold["final_energy_12digits"]) < 1e-12
+    assert abs(e + gold["lmp2_norm"]) < 1e-13
+    assert r2 < 1e-13
+
+
+def test_ccsd_formula_matches_dense(hf_ints):
+    F, W, no = dense_cc.spin_orbital(hf_ints.space, hf_ints.f, hf_ints.eri_elems)
+    _, hd = dense_cc.ccsd(F, W, no, maxiter=5)
+    s = cc.CCSolver(OracleEngine(route=3), hf_ints, method="ccsd")
+    s.load_hamiltonian()
+    s.solve(maxiter=5, conv=1e-12)
+    for (i, ed, rd), (j, eo, ro) in zip(hd, s.history):
+        assert abs(ed - eo) < 1e-12 and abs(rd - ro) < 1e-11 * max(1, rd), (i, ed, eo, rd, ro)
+
+
+def test_ccsd_synthetic_c1(built):
+    # a seeded synthetic Hamiltonian of the benchmark family, o=3 v=6
+    sp, eps, B = hm.synthetic(3, 6, 20, seed=3)
+    ints = hm.FactorizedIntegrals(sp, eps, B)
+    dense = hm.DenseIntegrals(sp, np.diag(eps), ints.dense_eri())
+    F, W, no = dense_cc.spin_orbital(sp, dense.f, dense.eri_elems)
+    ed, hd = dense_cc.ccsd(F, W, no, maxiter=30, conv=1e-9)
+    s = cc.CCSolver(OracleEngine(route=3), ints, method="ccsd")
+    s.load_hamiltonian()
+    eo = s.solve(maxiter=30, conv=1e-9)
+    assert abs(ed - eo) < 1e-10
