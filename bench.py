@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per CCSD iteration on a seeded synthetic Hamiltonian.
+
+One step = one CC iteration: the full CCSD formula (43 [ADD]/[CONTR] items,
+every block contraction of every item on the device), energy and residual
+norm read back, DIIS update of the amplitudes.  Default workload: closed-shell
+CCSD, C1, n_occ=24, n_virt=200, n_aux=900 (the metric's headline size);
+--config 0 selects n_occ=8, n_virt=32, n_aux=160.
+
+--impl reference times the CPU restatement of the reference path (oracle/,
+route 3: gather, ILP64 OpenBLAS dgemm on all host cores, scatter) on the same
+workload, each step a bounded sample of the block contractions scaled to a
+full iteration.
+
+Multi-GPU: replicas only (each rank runs the whole iteration); the value is
+the job's iterations per ... expressed as seconds per iteration of the job.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gecco-public_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+CONFIGS = {
+    0: dict(nocc=8, nvir=32, naux=160, seed=1000, name="CCSD C1 o8 v32 naux160"),
+    2: dict(nocc=24, nvir=200, naux=900, seed=1002, name="CCSD C1 o24 v200 naux900"),
+}
+
+
+def clocks_sampler(stop, out, index):
+    cmd = ["nvidia-smi", f"--id={index}",
+           "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits"]
+    while not stop.is_set():
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=5).stdout.strip()
+            if r:
+                out.append([x.strip() for x in r.split(",")])
+        except Exception:
+            pass
+        stop.wait(0.2)
+
+
+def clock_summary(samples):
+    if not samples:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
+    sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+    mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
+    reasons = set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for s in samples:
+        for k, n in enumerate(names):
+            if len(s) > 4 + k and s[4 + k].lower() == "active":
+                reasons.add(n)
+    return {"sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons)}
+
+
+def fp64_peak():
+    """measured FP64 tensor peak: cuBLAS DGEMM 8192^3, best of 5"""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def setup_hamiltonian(cfg):
+    import hamiltonian as hm
+    sp, eps, B = hm.synthetic(cfg["nocc"], cfg["nvir"], cfg["naux"], seed=cfg["seed"])
+    return sp, eps, B
+
+
+def cpu_baseline_oracle(solver_lists, sp, eps, B, target_s, cores, host_lists):
+    """the oracle (route 3, OpenBLAS on all host cores) on the same workload:
+    every formula item, only every stride-th long-operand batch executed;
+    returns seconds per full iteration and the sample description"""
+    import binding
+    import cc
+    from engine import OracleEngine
+    import hamiltonian as hm
+    binding.set_blas(cores)
+    oe = OracleEngine(route=3)
+    s = cc.CCSolver(oe, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+    for name, x in host_lists.items():
+        oe.data[s.lid(name)][:] = x
+    # calibrate the stride on a short probe, then time one sampled iteration
+    stride = 4096
+    binding.sampling(stride)
+    t0 = time.time()
+    s.evaluate()
+    probe = time.time() - t0
+    rep = binding.sampling_report()
+    per_batch = rep["t_sampled"] / max(rep["done"], 1)
+    est_full = rep["t_always"] + per_batch * rep["batches"]
+    stride = int(max(1, min(stride, est_full / max(target_s, 1e-3))))
+    binding.sampling(stride)
+    t0 = time.time()
+    s.evaluate()
+    wall = time.time() - t0
+    rep = binding.sampling_report()
+    scaled = wall - rep["t_sampled"] + rep["t_sampled"] * rep["batches"] / max(rep["done"], 1)
+    sample = (f"one CCSD iteration of the same workload through the oracle (route 3 gathers, "
+              f"OpenBLAS dgemm, scatters) with every {stride}-th of {rep['batches']} "
+              f"long-operand batches executed ({rep['done']} run, {wall:.1f} s wall), "
+              f"scaled by batch count")
+    return scaled, sample
+
+
+def run_gpu(args, cfg):
+    import torch
+
+    import cc
+    import gccu
+    from devfill import TorchIntegrals, list_tensor
+    import hamiltonian as hm
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    peak = fp64_peak() if rank == 0 else None
+    sp, eps, B = setup_hamiltonian(cfg)
+    eng = gccu.Engine(local)
+    solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+    t0 = time.time()
+    solver.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+    setup_s = time.time() - t0
+    # warm-up iterations (the first one plans every contraction and builds the
+    # string maps on the device)
+    energies = []
+    for _ in range(args.warmup):
+        en, rn = solver.iterate()
+        energies.append(en)
+        solver.diis_step()
+    solver.capture()
+    eng.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stop, samples = threading.Event(), []
+    th = threading.Thread(target=clocks_sampler, args=(stop, samples, local), daemon=True)
+    th.start()
+    eng.reset_stats()
+    eng.event_record(0)
+    for _ in range(args.steps):
+        en, rn = solver.iterate()
+        energies.append(en)
+        solver.diis_step()
+    eng.event_record(1)
+    ms_total = eng.event_elapsed(0, 1)
+    stop.set()
+    th.join()
+    _, launches = eng.stats()
+    # per-kernel times: one more iteration, launched eagerly with every [CONTR]
+    # kernel bracketed by events on the engine's stream (outside the timed loop)
+    eng.profile(True)
+    solver.evaluate()
+    prof = eng.profile_report()
+    eng.profile(False)
+    ms = ms_total / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # e2e: the same iteration through the public API with host buffers: the
+    # amplitudes come from pinned host memory, the residual and energy go back
+    nT = {a: solver.lists[a][1] for a in solver.amps}
+    nR = {a: solver.lists[solver.res[a]][1] for a in solver.amps}
+    host_t = {a: torch.empty(n, dtype=torch.float64, pin_memory=True) for a, n in nT.items()}
+    host_r = {a: torch.empty(n, dtype=torch.float64, pin_memory=True) for a, n in nR.items()}
+    for a in solver.amps:
+        eng.get_vec(solver.lid(a), 0, host_t[a].data_ptr(), nT[a])
+    e2e_steps = max(1, min(args.steps, 5))
+    eng.sync()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for a in solver.amps:
+            eng.put_vec(solver.lid(a), 0, host_t[a].data_ptr(), nT[a])
+        en, rn = solver.iterate()
+        for a in solver.amps:
+            eng.get_vec(solver.lid(solver.res[a]), 0, host_r[a].data_ptr(), nR[a])
+    eng.sync()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    h2d = 8 * sum(nT.values())
+    d2h = 8 * sum(nR.values()) + 8
+    # dominant kernel: the contraction with the largest kernel time
+    dom = prof[np.argmax(prof[:, 2])]
+    dom_ms = dom[2] / dom[1]
+    achieved = dom[0] / (dom_ms * 1e-3) / 1e12
+    total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
+    line = {
+        "metric": "s/CC-iteration (CCSD, plain FP64)",
+        "value": (ms / 1e3) / world,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
+                "B~N(0,0.05^2)); inputs larger than L2 (two-electron list "
+                f"{8 * solver.lists['V'][1] / 1e9:.1f} GB)",
+        "config": {"workload": cfg["name"], "method": "CCSD spin-orbital, DIIS maxsub 8",
+                   "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
+                   "parallelism": f"replicas x{world}", "l2": "inputs > L2",
+                   "setup_s": round(setup_s, 2), "energy_last": energies[-1]},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if peak else None, "traffic": None,
+                     "kernel": "k_contract (pp ladder, FP64 DMMA)",
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
+                                    "MEASURED_PEAKS.json)",
+                     "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
+                     "iteration_flops": total_flops,
+                     "iteration_tflops": total_flops / (ms * 1e-3) / 1e12},
+        "clocks": clock_summary(samples),
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        host_lists = {}
+        for name in ("F", "V", "T1", "T2", "D" + "T1", "D" + "T2"):
+            lid, n, _ = solver.lists[name]
+            x = np.empty(n)
+            eng.get_vec(lid, 0, x.ctypes.data, n)
+            host_lists[name] = x
+        cores = os.cpu_count()
+        val, sample = cpu_baseline_oracle(solver.lists, sp, eps, B, args.cpu_seconds, cores,
+                                          host_lists)
+        line["cpu_baseline"] = {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                                "sample": sample}
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, cfg):
+    """the oracle port of the reference path on host cores (rank 0 only)"""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    import binding
+    import cc
+    from engine import OracleEngine
+    import hamiltonian as hm
+    sp, eps, B = setup_hamiltonian(cfg)
+    cores = os.cpu_count()
+    binding.set_blas(cores)
+    oe = OracleEngine(route=3)
+    s = cc.CCSolver(oe, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+    t0 = time.time()
+    from devfill import TorchIntegrals
+    s.load_hamiltonian_device(TorchIntegrals(sp, eps, B, device="cpu"))
+    setup_s = time.time() - t0
+    # amplitudes of one iteration so that no block is screened out
+    binding.sampling(1 << 30)
+    s.evaluate()
+    s.step()
+    stride = None
+    times = []
+    for i in range(args.warmup + args.steps):
+        if stride is None:
+            binding.sampling(4096)
+            t0 = time.time()
+            s.evaluate()
+            rep = binding.sampling_report()
+            per = rep["t_sampled"] / max(rep["done"], 1)
+            full = rep["t_always"] + per * rep["batches"]
+            stride = int(max(1, min(4096, full / max(args.ref_seconds, 1e-3))))
+            continue
+        binding.sampling(stride)
+        t0 = time.time()
+        s.evaluate()
+        wall = time.time() - t0
+        rep = binding.sampling_report()
+        scaled = wall - rep["t_sampled"] + rep["t_sampled"] * rep["batches"] / max(rep["done"], 1)
+        if i >= args.warmup:
+            times.append(scaled)
+    val = float(np.mean(times)) if times else None
+    line = {
+        "impl": "reference",
+        "metric": "s/CC-iteration (CCSD, plain FP64)",
+        "value": val, "unit": "s", "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3 if val else None,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (same seeded Hamiltonian as the GPU arm)",
+        "config": {"workload": cfg["name"], "method": "CCSD spin-orbital",
+                   "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
+                   "setup_s": round(setup_s, 1)},
+        "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": f"each step: one CCSD iteration through the oracle (route 3, "
+                                   f"OpenBLAS dgemm on {cores} cores) with every {stride}-th "
+                                   f"long-operand batch executed, scaled by batch count"},
+        "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gecco-b200")
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_gpu(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -250,6 +250,50 @@ class CCSolver:
             self.e.upload(self.lid("D" + a), d)
             self.e.zero(self.lid(a))
 
+    def load_hamiltonian_device(self, tints):
+        """generate the Hamiltonian and denominator lists on the device
+        (devfill.TorchIntegrals) directly in the engine's list memory"""
+        import torch
+
+        from devfill import DeviceListView, list_tensor
+        dev = tints.device
+        if dev == "cpu":
+            def tensor(lid, n):
+                return torch.from_numpy(self.e.data[lid])
+        else:
+            def tensor(lid, n):
+                return list_tensor(self.e, lid, n)
+        self.e.sync()
+        for name in ("F", "V"):
+            lid, n, blocks = self.lists[name]
+            x = tensor(lid, n)
+            view = DeviceListView(self.e, lid, blocks, self.nsym, device=dev)
+            for ib, occ in enumerate(blocks, 1):
+                t = _axis_types(occ)
+                if name == "F":
+                    view.fill(x, ib, lambda ax, t=t: tints.fock(t[0], ax[0], t[1], ax[1]))
+                else:
+                    view.fill(x, ib, lambda ax, t=t: tints.eri(t, ax))
+        tints.release()
+        for a in self.amps:
+            lid, n, blocks = self.lists["D" + a]
+            x = tensor(lid, n)
+            types = _axis_types(blocks[0])
+            ncre = sum(k for _, k in condensed(blocks[0])[0])
+
+            def den(ax, types=types, ncre=ncre):
+                d = 0.0
+                for k, (t, so) in enumerate(zip(types, ax)):
+                    e = tints.eps[tints.orbs[t][so // 2]]
+                    d = d + (e if k < ncre else -e)
+                return d
+
+            DeviceListView(self.e, lid, blocks, self.nsym, device=dev).fill(x, 1, den)
+        if dev != "cpu":
+            torch.cuda.synchronize()
+        for a in self.amps:
+            self.e.zero(self.lid(a))
+
     def evaluate(self):
         """one formula evaluation (frm_sched2 over the item list)"""
         for it in self.formula:
@@ -281,24 +325,90 @@ class CCSolver:
                                 fac=-1.0)
             self.e.add_block(1.0, self.lid("S" + a), 1, self.lid(a), 1)
 
-    def solve(self, maxiter=50, conv=1e-8, use_graph=False, callback=None):
-        e_old = 0.0
+    def _diis_lists(self):
+        if hasattr(self, "_diis"):
+            return self._diis
+        slots = []
+        for k in range(self.maxsub):
+            slot = {}
+            for a in self.amps:
+                blocks = self.lists[a][2]
+                for kind in ("t", "e"):
+                    lid, n = self.e.register_list(self.e.define_operator(blocks))
+                    slot[(kind, a)] = lid
+            slots.append(slot)
+        self._diis = dict(slots=slots, used=[], B=np.zeros((self.maxsub, self.maxsub)))
+        return self._diis
+
+    def diis_step(self):
+        """preconditioned step, then DIIS extrapolation over the last maxsub
+        (amplitude, step) pairs (optc_diis_sbsp_add / optc_diis_extr,
+        solve/optc_diis_sbsp_add.f:125-145, solve/optc_diis_extr.f:67,82)"""
+        d = self._diis_lists()
+        used = d["used"]
+        # slot to overwrite: the oldest one when the subspace is full
+        k = len(used) if len(used) < self.maxsub else used.pop(0)
+        used.append(k)
+        slot = d["slots"][k]
+        for a in self.amps:
+            self.e.precondition(slot[("e", a)], self.lid(self.res[a]), self.lid("D" + a), fac=-1.0)
+            self.e.add_block(1.0, self.lid(a), 1, slot[("t", a)], 1, reset=True)
+            self.e.add_block(1.0, slot[("e", a)], 1, slot[("t", a)], 1)
+        B = d["B"]
+        for j in used:
+            v = sum(self.e.dot(slot[("e", a)], d["slots"][j][("e", a)]) for a in self.amps)
+            B[k, j] = B[j, k] = v
+        m = len(used)
+        A = np.zeros((m + 1, m + 1))
+        A[:m, :m] = B[np.ix_(used, used)]
+        scale = np.max(np.abs(np.diag(A[:m, :m]))) or 1.0
+        A[:m, :m] /= scale
+        A[m, :m] = A[:m, m] = -1.0
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        try:
+            c = np.linalg.solve(A, rhs)[:m]
+        except np.linalg.LinAlgError:
+            c = np.zeros(m)
+            c[-1] = 1.0
+        for a in self.amps:
+            for i, j in enumerate(used):
+                self.e.add_block(float(c[i]), d["slots"][j][("t", a)], 1, self.lid(a), 1,
+                                 reset=(i == 0))
+        return c
+
+    def iterate(self, diis=True):
+        """one CC iteration: formula evaluation, energy and residual norm,
+        amplitude update"""
+        if self.graph is not None:
+            self.e.graph_launch(self.graph)
+        else:
+            self.evaluate()
+        en = self.energy()
+        rn = self.residual_norm()
+        return en, rn
+
+    def capture(self):
+        """record one formula evaluation as a CUDA graph (plans must exist)"""
+        self.e.graph_begin()
+        self.evaluate()
+        self.graph = self.e.graph_end()
+
+    def solve(self, maxiter=50, conv=1e-8, use_graph=False, diis=True, callback=None,
+              econv=None):
+        e_old = None
         for it in range(1, maxiter + 1):
             if use_graph and self.graph is None and it > 1:
-                self.e.graph_begin()
-                self.evaluate()
-                self.graph = self.e.graph_end()
-            if self.graph is not None:
-                self.e.graph_launch(self.graph)
-            else:
-                self.evaluate()
-            en = self.energy()
-            rn = self.residual_norm()
+                self.capture()
+            en, rn = self.iterate()
             self.history.append((it, en, rn))
             if callback:
                 callback(it, en, rn)
-            if rn < conv:
+            if rn < conv or (econv is not None and e_old is not None and abs(en - e_old) < econv):
                 return en
-            self.step()
+            if diis:
+                self.diis_step()
+            else:
+                self.step()
             e_old = en
-        return e_old
+        return en

@@ -49,6 +49,10 @@ struct DevPlan {
   // sym_ab descriptors of the result class (use_tr)
   FlipDesc* d_flip = nullptr;
   int64_t nflip = 0, flip_maxlen = 0;
+  // kernel timing (gccu_profile): events of launches not yet reported
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  int64_t calls = 0;
+  double ms = 0;
 };
 
 class Engine {
@@ -69,6 +73,23 @@ class Engine {
   int64_t launches = 0;
   bool capturing = false;
   std::vector<cudaGraphExec_t> graphs;
+  std::vector<int64_t> graph_kernels;  // kernel launches recorded in each graph
+  int64_t capture_start = 0;
+  cudaEvent_t slots[64] = {};
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<DevPlan*> plan_order;  // plans in first-use order (profile report)
+
+  cudaEvent_t get_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    CUDA_OK(cudaEventCreate(&e));
+    return e;
+  }
 
   bool host_only = false;  // no device: model, layout and planning queries only
 
@@ -80,6 +101,14 @@ class Engine {
   }
   ~Engine() {
     for (auto g : graphs) cudaGraphExecDestroy(g);
+    for (auto ev : slots)
+      if (ev) cudaEventDestroy(ev);
+    for (auto ev : event_pool) cudaEventDestroy(ev);
+    for (auto& kv : plans)
+      for (auto& pr : kv.second->pending) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+      }
     if (stream) cudaStreamSynchronize(stream);
     for (void* p : allocs) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
@@ -255,6 +284,7 @@ class Engine {
       dp->d_tiles = upload(tiles);
     }
     if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);
+    plan_order.push_back(dp.get());
     return *(plans[key] = std::move(dp));
   }
 
@@ -634,8 +664,20 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     if (!update) {
       CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
     }
+    const bool timed = e.profiling && !e.capturing && dp.ntiles;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (timed) {
+      ev0 = e.get_event();
+      ev1 = e.get_event();
+      CUDA_OK(cudaEventRecord(ev0, e.stream));
+    }
     launch_contract(dp.d_items, dp.d_tiles, dp.ntiles, e.list(dp.list1).d, e.list(dp.list2).d,
                     r.d, fact, e.stream);
+    if (timed) {
+      CUDA_OK(cudaEventRecord(ev1, e.stream));
+      dp.pending.emplace_back(ev0, ev1);
+    }
+    ++dp.calls;
     if (dp.ntiles) ++e.launches;
     if (dp.plan.use_tr && dp.nflip) {
       launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);
@@ -653,6 +695,26 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
                               e.stream));
       CUDA_OK(cudaStreamSynchronize(e.stream));
     }
+  });
+}
+
+int gccu_put_vec(int64_t list_id, int64_t offset, const void* src, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& dl = e.list(list_id);
+    GCCU_REQUIRE(offset >= 0 && n >= 0 && offset + n <= dl.L.len, "put_vec out of range");
+    CUDA_OK(cudaMemcpyAsync(dl.d + offset, src, n * sizeof(double), cudaMemcpyDefault, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+  });
+}
+
+int gccu_get_vec(int64_t list_id, int64_t offset, void* dst, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    DevList& dl = e.list(list_id);
+    GCCU_REQUIRE(offset >= 0 && n >= 0 && offset + n <= dl.L.len, "get_vec out of range");
+    CUDA_OK(cudaMemcpyAsync(dst, dl.d + offset, n * sizeof(double), cudaMemcpyDefault, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
   });
 }
 
@@ -738,6 +800,7 @@ int gccu_graph_begin(void) {
     GCCU_REQUIRE(!e.capturing, "graph capture already active");
     CUDA_OK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
     e.capturing = true;
+    e.capture_start = e.launches;
   });
 }
 
@@ -752,6 +815,8 @@ int gccu_graph_end(int64_t* graph_id) {
     CUDA_OK(cudaGraphInstantiate(&ex, g, 0));
     cudaGraphDestroy(g);
     e.graphs.push_back(ex);
+    e.graph_kernels.push_back(e.launches - e.capture_start);
+    e.launches = e.capture_start;
     *graph_id = (int64_t)e.graphs.size();
   });
 }
@@ -761,7 +826,7 @@ int gccu_graph_launch(int64_t graph_id) {
     Engine& e = eng();
     GCCU_REQUIRE(graph_id >= 1 && graph_id <= (int64_t)e.graphs.size(), "invalid graph id");
     CUDA_OK(cudaGraphLaunch(e.graphs[graph_id - 1], e.stream));
-    ++e.launches;
+    e.launches += e.graph_kernels[graph_id - 1];
   });
 }
 
@@ -774,6 +839,63 @@ int gccu_stats(double* stats8, int64_t* launches) {
     Engine& e = eng();
     for (int k = 0; k < 8; ++k) stats8[k] = e.stats[k];
     *launches = e.launches;
+  });
+}
+
+int gccu_event_record(int64_t slot) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(slot >= 0 && slot < 64, "event slot out of range");
+    if (!e.slots[slot]) CUDA_OK(cudaEventCreate(&e.slots[slot]));
+    CUDA_OK(cudaEventRecord(e.slots[slot], e.stream));
+  });
+}
+
+int gccu_event_elapsed(int64_t a, int64_t b, double* ms) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(a >= 0 && a < 64 && b >= 0 && b < 64 && e.slots[a] && e.slots[b],
+                 "event slot not recorded");
+    CUDA_OK(cudaEventSynchronize(e.slots[b]));
+    float f = 0;
+    CUDA_OK(cudaEventElapsedTime(&f, e.slots[a], e.slots[b]));
+    *ms = f;
+  });
+}
+
+int gccu_profile(int64_t enable) {
+  return guarded([&] { eng().profiling = enable != 0; });
+}
+
+int gccu_profile_report(double* rows, int64_t maxrows, int64_t* nrows) {
+  return guarded([&] {
+    Engine& e = eng();
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    int64_t n = 0;
+    for (DevPlan* dp : e.plan_order) {
+      for (auto& pr : dp->pending) {
+        float f = 0;
+        CUDA_OK(cudaEventElapsedTime(&f, pr.first, pr.second));
+        dp->ms += f;
+        e.event_pool.push_back(pr.first);
+        e.event_pool.push_back(pr.second);
+      }
+      dp->pending.clear();
+      if (dp->calls == 0) continue;
+      if (n < maxrows) {
+        double* r = rows + 6 * n;
+        r[0] = dp->plan.flops;
+        r[1] = (double)dp->calls;
+        r[2] = dp->ms;
+        r[3] = (double)dp->plan.items.size();
+        r[4] = (double)dp->ntiles;
+        r[5] = (double)dp->calls * (dp->ntiles ? 1 : 0);
+      }
+      ++n;
+      dp->calls = 0;
+      dp->ms = 0;
+    }
+    *nrows = n;
   });
 }
 

@@ -65,6 +65,12 @@ _SIGS = {
     "gccu_sync": [],
     "gccu_stats": [PD, P64],
     "gccu_reset_stats": [],
+    "gccu_put_vec": [I64, I64, ctypes.c_void_p, I64],
+    "gccu_get_vec": [I64, I64, ctypes.c_void_p, I64],
+    "gccu_event_record": [I64],
+    "gccu_event_elapsed": [I64, I64, PD],
+    "gccu_profile": [I64],
+    "gccu_profile_report": [PD, I64, P64],
 }
 
 
@@ -296,3 +302,29 @@ class Engine:
 
     def reset_stats(self):
         _call("gccu_reset_stats")
+
+    # ---- ranged transfers (host or device pointers)
+    def put_vec(self, lst, offset, ptr, n):
+        _call("gccu_put_vec", lst, offset, ctypes.c_void_p(ptr), n)
+
+    def get_vec(self, lst, offset, ptr, n):
+        _call("gccu_get_vec", lst, offset, ctypes.c_void_p(ptr), n)
+
+    # ---- timing
+    def event_record(self, slot):
+        _call("gccu_event_record", slot)
+
+    def event_elapsed(self, a, b):
+        r = np.zeros(1)
+        _call("gccu_event_elapsed", a, b, _pd(r))
+        return float(r[0])
+
+    def profile(self, enable=True):
+        _call("gccu_profile", int(enable))
+
+    def profile_report(self):
+        """rows (flops per call, calls, kernel ms, items, tiles, launches)"""
+        n = np.zeros(1, np.int64)
+        rows = np.zeros((4096, 6))
+        _call("gccu_profile_report", _pd(rows), 4096, _p64(n))
+        return rows[: min(int(n[0]), 4096)]

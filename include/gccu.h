@@ -80,6 +80,11 @@ int gccu_list_dists(int64_t list_id, int64_t* rows, int64_t maxrows, int64_t* nr
 int gccu_upload_list(int64_t list_id, const double* host, int64_t n);
 int gccu_download_list(int64_t list_id, double* host, int64_t n);
 int gccu_zero_list(int64_t list_id);
+/* ranged transfer of n elements starting at element offset (0-based):
+ * replaces get_vec/put_vec (fileutil/get_vec.f, put_vec.f); src/dst may be
+ * host (pageable or pinned) or device pointers */
+int gccu_put_vec(int64_t list_id, int64_t offset, const void* src, int64_t n);
+int gccu_get_vec(int64_t list_id, int64_t offset, void* dst, int64_t n);
 /* raw device pointer of the list data (for callers that own device memory) */
 int gccu_list_device_ptr(int64_t list_id, void** dptr);
 
@@ -149,6 +154,19 @@ int gccu_sync(void);
  * kernel launches issued. */
 int gccu_stats(double* stats8, int64_t* launches);
 int gccu_reset_stats(void);
+
+/* ---- timing (replaces the atim_cs timers of crout/atim.c and the
+ * contr_times counters, include/contr_times.h) --------------------------------
+ * CUDA events recorded on the engine's stream in slots 0..63 */
+int gccu_event_record(int64_t slot);
+int gccu_event_elapsed(int64_t slot_a, int64_t slot_b, double* ms);
+/* per-contraction kernel timing: while enabled every [CONTR] launch is
+ * bracketed by events on the engine's stream.  The report synchronises and
+ * returns one row per planned contraction that ran: (flops per call,
+ * calls, total kernel ms, block contractions, tiles, k_contract launches),
+ * then resets the accumulated times. */
+int gccu_profile(int64_t enable);
+int gccu_profile_report(double* rows, int64_t maxrows, int64_t* nrows);
 
 #ifdef __cplusplus
 }

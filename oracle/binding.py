@@ -160,6 +160,43 @@ class Oracle:
         _chk(lib().ora_sym_ab_blk(self.ctx, lst, iblk, _pd(x), prefac, relfac))
 
 
+def openblas_path():
+    import glob
+
+    import numpy
+    libs = glob.glob(os.path.join(os.path.dirname(numpy.__file__) + ".libs",
+                                  "libscipy_openblas64_*.so"))
+    return libs[0] if libs else None
+
+
+def set_blas(nthreads=0, path=None):
+    """route-3 dgemm through the ILP64 OpenBLAS bundled with numpy"""
+    L = lib()
+    L.ora_set_blas.restype = ctypes.c_int
+    L.ora_set_blas.argtypes = [ctypes.c_char_p, I64]
+    path = path or openblas_path()
+    if path is None:
+        raise OracleError("no ILP64 OpenBLAS found")
+    _chk(L.ora_set_blas(path.encode(), nthreads))
+    return path
+
+
+def sampling(stride):
+    L = lib()
+    L.ora_sampling.argtypes = [I64]
+    L.ora_sampling.restype = None
+    L.ora_sampling(stride)
+
+
+def sampling_report():
+    L = lib()
+    L.ora_sampling_report.argtypes = [PD]
+    L.ora_sampling_report.restype = None
+    out = np.zeros(4)
+    L.ora_sampling_report(_pd(out))
+    return dict(t_always=out[0], t_sampled=out[1], batches=int(out[2]), done=int(out[3]))
+
+
 def add_opblk(xout, xin, fac, reset=False, typ=1):
     xn = np.zeros(1)
     lib().ora_add_opblk(_pd(xn), typ, fac, _pd(xin), _pd(xout), xout.size, int(reset))

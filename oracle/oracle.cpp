@@ -14,8 +14,11 @@
 // of route 2 vs route 3 and invariance tests.
 #include "oracle.h"
 
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -880,6 +883,23 @@ void route2(const Blk& b) {
   }
 }
 
+// optional BLAS for the route-3 dgemm (the reference links an ILP64 BLAS,
+// configure.ac:107-108); without it a plain loop is used
+typedef void (*dgemm_t)(const char*, const char*, const int64_t*, const int64_t*, const int64_t*,
+                        const double*, const double*, const int64_t*, const double*,
+                        const int64_t*, const double*, double*, const int64_t*);
+dgemm_t g_dgemm = nullptr;
+
+// timing sample: only every g_stride-th long-operand batch of route 3 is
+// executed (the CPU baseline times a bounded sample of a large workload)
+int64_t g_stride = 1, g_batch = 0, g_batches_total = 0, g_batches_done = 0;
+double g_t_always = 0, g_t_sampled = 0;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
 // route 3: contr_blk1blk2_blocked_mm (contract/contr_blk1blk2_blocked_mm.f:
 // 184-595): batches of str_block ex strings and cnt_block cnt strings,
 // collect_block_impr gathers, dgemm('t','n'), scatter_block.
@@ -912,8 +932,14 @@ void route3(const Blk& b, int64_t str_block, int64_t cnt_block, Stats* st) {
   };
   for (int64_t c0 = 0; c0 < ncnt; c0 += mcnt) {
     int64_t nc = std::min(mcnt, ncnt - c0);
+    double t0 = now_s();
     gather(op1shorter, 0, nexs, c0, nc, ps);  // short operand, all ex strings
+    g_t_always += now_s() - t0;
     for (int64_t l0 = 0; l0 < nexl; l0 += mexl) {
+      ++g_batches_total;
+      if ((g_batch++) % g_stride != 0) continue;
+      ++g_batches_done;
+      double t1 = now_s();
       int64_t nl = std::min(mexl, nexl - l0);
       gather(!op1shorter, l0, nl, c0, nc, pl);
       for (int64_t s0 = 0; s0 < nexs; s0 += mexs) {
@@ -931,14 +957,20 @@ void route3(const Blk& b, int64_t str_block, int64_t cnt_block, Stats* st) {
         }
         // dgemm('t','n'): R(s,l) = xfac * sum_k S(k,s) L(k,l)
         pr.assign(ns * nl, 0.0);
-        for (int64_t l = 0; l < nl; ++l)
-          for (int64_t s = 0; s < ns; ++s) {
-            const double* a = &ps[(s0 + s) * nc];
-            const double* c = &pl[l * nc];
-            double acc = 0;
-            for (int64_t k = 0; k < nc; ++k) acc += a[k] * c[k];
-            pr[l * ns + s] = b.xfac * acc;
-          }
+        if (g_dgemm) {
+          const double zero = 0.0;
+          g_dgemm("T", "N", &ns, &nl, &nc, &b.xfac, &ps[s0 * nc], &nc, pl.data(), &nc, &zero,
+                  pr.data(), &ns);
+        } else {
+          for (int64_t l = 0; l < nl; ++l)
+            for (int64_t s = 0; s < ns; ++s) {
+              const double* a = &ps[(s0 + s) * nc];
+              const double* c = &pl[l * nc];
+              double acc = 0;
+              for (int64_t k = 0; k < nc; ++k) acc += a[k] * c[k];
+              pr[l * ns + s] = b.xfac * acc;
+            }
+        }
         // scatter_block: x12(idx) += sign * panel
         for (int64_t l = 0; l < nl; ++l)
           for (int64_t s = 0; s < ns; ++s) {
@@ -950,6 +982,7 @@ void route3(const Blk& b, int64_t str_block, int64_t cnt_block, Stats* st) {
             if (sg) b.x12[o] += sg * pr[l * ns + s];
           }
       }
+      g_t_sampled += now_s() - t1;
     }
   }
 }
@@ -1516,6 +1549,33 @@ int ora_add_opblk(double* xnorm2, int64_t type, double fac, const double* xin, d
     *xnorm2 = len > 0 ? xout[0] : 0.0;
   }
   return 0;
+}
+
+int ora_set_blas(const char* path, int64_t nthreads) {
+  GUARD_BEGIN
+  void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  CHECK(h, std::string("cannot load BLAS: ") + dlerror());
+  g_dgemm = (dgemm_t)dlsym(h, "scipy_dgemm_64_");
+  if (!g_dgemm) g_dgemm = (dgemm_t)dlsym(h, "dgemm_64_");
+  CHECK(g_dgemm, "no ILP64 dgemm in BLAS library");
+  typedef void (*nt_t)(int);
+  nt_t nt = (nt_t)dlsym(h, "scipy_openblas_set_num_threads64_");
+  if (nt && nthreads > 0) nt((int)nthreads);
+  return 0;
+  GUARD_END(-1)
+}
+
+void ora_sampling(int64_t stride) {
+  g_stride = stride > 0 ? stride : 1;
+  g_batch = g_batches_total = g_batches_done = 0;
+  g_t_always = g_t_sampled = 0;
+}
+
+void ora_sampling_report(double* out4) {
+  out4[0] = g_t_always;
+  out4[1] = g_t_sampled;
+  out4[2] = (double)g_batches_total;
+  out4[3] = (double)g_batches_done;
 }
 
 void ora_diavc(double* out, const double* in, double fac, const double* diag, double shift,
