@@ -192,9 +192,18 @@ def sampling_report():
     L = lib()
     L.ora_sampling_report.argtypes = [PD]
     L.ora_sampling_report.restype = None
-    out = np.zeros(4)
+    out = np.zeros(6)
     L.ora_sampling_report(_pd(out))
-    return dict(t_always=out[0], t_sampled=out[1], batches=int(out[2]), done=int(out[3]))
+    return dict(t_short=out[0], t_sampled=out[1], batches=int(out[2]), done=int(out[3]),
+                shorts=int(out[4]), shorts_done=int(out[5]))
+
+
+def scaled_time(wall, rep):
+    """wall time of a sampled evaluation scaled to the full work: executed
+    short-operand gathers and long-operand batches scaled by their counts"""
+    other = wall - rep["t_short"] - rep["t_sampled"]
+    return (other + rep["t_short"] * rep["shorts"] / max(rep["shorts_done"], 1) +
+            rep["t_sampled"] * rep["batches"] / max(rep["done"], 1))
 
 
 def add_opblk(xout, xin, fac, reset=False, typ=1):

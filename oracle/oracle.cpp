@@ -893,6 +893,7 @@ dgemm_t g_dgemm = nullptr;
 // timing sample: only every g_stride-th long-operand batch of route 3 is
 // executed (the CPU baseline times a bounded sample of a large workload)
 int64_t g_stride = 1, g_batch = 0, g_batches_total = 0, g_batches_done = 0;
+int64_t g_short_total = 0, g_short_done = 0;
 double g_t_always = 0, g_t_sampled = 0;
 
 double now_s() {
@@ -932,13 +933,21 @@ void route3(const Blk& b, int64_t str_block, int64_t cnt_block, Stats* st) {
   };
   for (int64_t c0 = 0; c0 < ncnt; c0 += mcnt) {
     int64_t nc = std::min(mcnt, ncnt - c0);
-    double t0 = now_s();
-    gather(op1shorter, 0, nexs, c0, nc, ps);  // short operand, all ex strings
-    g_t_always += now_s() - t0;
+    // the short operand (all its ex strings) is gathered once per cnt batch,
+    // here on first use by an executed long-operand batch
+    bool have_short = false;
+    ++g_short_total;
     for (int64_t l0 = 0; l0 < nexl; l0 += mexl) {
       ++g_batches_total;
       if ((g_batch++) % g_stride != 0) continue;
       ++g_batches_done;
+      if (!have_short) {
+        double t0 = now_s();
+        gather(op1shorter, 0, nexs, c0, nc, ps);
+        g_t_always += now_s() - t0;
+        ++g_short_done;
+        have_short = true;
+      }
       double t1 = now_s();
       int64_t nl = std::min(mexl, nexl - l0);
       gather(!op1shorter, l0, nl, c0, nc, pl);
@@ -1568,6 +1577,7 @@ int ora_set_blas(const char* path, int64_t nthreads) {
 void ora_sampling(int64_t stride) {
   g_stride = stride > 0 ? stride : 1;
   g_batch = g_batches_total = g_batches_done = 0;
+  g_short_total = g_short_done = 0;
   g_t_always = g_t_sampled = 0;
 }
 
@@ -1576,6 +1586,8 @@ void ora_sampling_report(double* out4) {
   out4[1] = g_t_sampled;
   out4[2] = (double)g_batches_total;
   out4[3] = (double)g_batches_done;
+  out4[4] = (double)g_short_total;
+  out4[5] = (double)g_short_done;
 }
 
 void ora_diavc(double* out, const double* in, double fac, const double* diag, double shift,

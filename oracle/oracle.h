@@ -74,10 +74,12 @@ int ora_sym_ab_blk(ora_ctx*, int64_t list, int64_t iblk, double* x,
  * instead of the plain loop; nthreads > 0 sets the BLAS thread count */
 int ora_set_blas(const char* path, int64_t nthreads);
 /* CPU-baseline sampling: execute only every stride-th long-operand batch of
- * route 3; the report gives [seconds always run, seconds in sampled batches,
- * batches total, batches executed] since the last ora_sampling call */
+ * route 3 (and the short-operand gathers those batches need); the report
+ * gives [seconds in short-operand gathers, seconds in executed batches,
+ * batches total, batches executed, short gathers total, short gathers
+ * executed] since the last ora_sampling call */
 void ora_sampling(int64_t stride);
-void ora_sampling_report(double* out4);
+void ora_sampling_report(double* out6);
 
 /* add_opblk (in-core branch) -- contract/add_opblk.f:299-307 */
 int ora_add_opblk(double* xnorm2, int64_t type, double fac, const double* xin,
