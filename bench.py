@@ -185,6 +185,13 @@ def run_gpu(args, cfg):
     solver.evaluate()
     prof = eng.profile_report()
     eng.profile(False)
+    if args.profile_out and rank == 0:
+        names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
+        with open(args.profile_out, "w") as f:
+            json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
+                        "tflops": r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12 if r[2] else None,
+                        "block_contractions": int(r[3]), "tiles": int(r[4])}
+                       for n, r in zip(names, prof)], f, indent=1)
     ms = ms_total / args.steps
     if dist:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -339,6 +346,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-out", default=None,
+                    help="write per-contraction kernel times (JSON)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

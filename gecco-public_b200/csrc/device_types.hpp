@@ -46,4 +46,41 @@ struct TileDesc {
   int64_t k0, k1;
 };
 
+// One block contraction as a GEMM over offset tables:
+//   C(r, c) += fac * sum_k A(r, k) B(k, c)
+//   A(r, k) = a[aro[r] + ako[k]],  B(k, c) = b[bco[c] + bko[k]]
+//   C(r, c) at c[cro[r] + cco[c] + mapped part]
+// An operand whose components need string-map lookups is first gathered
+// (with signs) into a dense panel by the pack kernel; the tables then address
+// the panel.  Rows are ex1 and columns ex2, or the other way round when the
+// item is swapped (thin ex1); rowspace tells the epilogue which.
+struct GemmDesc {
+  int64_t M, N, K;
+  double fac;
+  const double* a;
+  const int64_t *aro, *ako;
+  const double* b;
+  const int64_t *bco, *bko;
+  double* c;
+  const int64_t *cro, *cco;
+  int32_t afast, bfast;  // 1: contiguous along k (else along rows / columns)
+  int32_t rowspace;      // kEx1 or kEx2 (swapped)
+  int32_t cmapped;       // result components that need map lookups
+  int32_t nsp[3];
+  int32_t rad[3][kDevMaxComp];
+  OpndDesc cmap;  // result operand (map lookups in the epilogue)
+};
+
+// gather of one operand of one block contraction into a dense panel
+// panel[k * R + r] = sign * x[address(r, k)]
+struct PackJob {
+  int64_t R, K;  // rows (ex1 or ex2 composite) and contraction length
+  const double* src;
+  double* dst;
+  int32_t rowspace;  // kEx1 (op1) or kEx2 (op2)
+  int32_t nsp[3];
+  int32_t rad[3][kDevMaxComp];
+  OpndDesc op;
+};
+
 }  // namespace gccu

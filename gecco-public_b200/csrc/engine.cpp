@@ -41,9 +41,16 @@ struct DevGraph {
 
 struct DevPlan {
   Plan plan;
-  ItemDesc* d_items = nullptr;
-  TileDesc* d_tiles = nullptr;
+  // grouped GEMM launches (regular / thin tiles), pack jobs, tables, scratch
+  GemmDesc* d_desc[2] = {nullptr, nullptr};
+  TileDesc* d_tiles_g[2] = {nullptr, nullptr};
+  int64_t ntiles_g[2] = {0, 0};
   int64_t ntiles = 0;
+  PackJob* d_jobs = nullptr;
+  int64_t njobs = 0, pack_maxlen = 0;
+  int64_t* d_tabs = nullptr;
+  double* scratch = nullptr;
+  int64_t scratch_len = 0;
   int64_t res_off = 0, res_len = 0;
   int list1 = 0, list2 = 0, list12 = 0;
   // sym_ab descriptors of the result class (use_tr)
@@ -251,41 +258,177 @@ class Engine {
     Plan& P = dp->plan;
     if (host_only) return *(plans[key] = std::move(dp));
     for (auto& r : P.maps) P.items[r.item].op[r.opnd].map[r.comp] = strmap(r.key);
-    // tiles: 64x64 output tiles, contraction index split when the item has
-    // few output tiles and a long contraction string
-    std::vector<TileDesc> tiles;
-    int64_t total_mn = 0;
-    for (auto& itm : P.items)
-      total_mn += ((itm.M + kTileM - 1) / kTileM) * ((itm.N + kTileN - 1) / kTileN);
-    for (size_t i = 0; i < P.items.size(); ++i) {
-      const ItemDesc& itm = P.items[i];
-      int64_t mt = (itm.M + kTileM - 1) / kTileM, nt = (itm.N + kTileN - 1) / kTileN;
-      int64_t ks = 1;
-      if (total_mn < 2 * 148 && itm.K > 1024) {
-        ks = std::min<int64_t>((itm.K + 511) / 512, (2 * 148 + total_mn - 1) / std::max<int64_t>(total_mn, 1));
-        ks = std::max<int64_t>(ks, 1);
-      }
-      int64_t kchunk = ((itm.K + ks - 1) / ks + kTileK - 1) / kTileK * kTileK;
-      for (int64_t m = 0; m < mt; ++m)
-        for (int64_t n = 0; n < nt; ++n)
-          for (int64_t k0 = 0; k0 < itm.K; k0 += kchunk) {
-            TileDesc t{};
-            t.item = (int32_t)i;
-            t.m0 = (int32_t)(m * kTileM);
-            t.n0 = (int32_t)(n * kTileN);
-            t.k0 = k0;
-            t.k1 = std::min(itm.K, k0 + kchunk);
-            tiles.push_back(t);
-          }
-    }
-    dp->ntiles = (int64_t)tiles.size();
-    if (!P.items.empty()) {
-      dp->d_items = upload(P.items);
-      dp->d_tiles = upload(tiles);
-    }
+    build_gemm(*dp);
     if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);
     plan_order.push_back(dp.get());
     return *(plans[key] = std::move(dp));
+  }
+
+  // offsets of the single-source components of operand od that belong to
+  // space sp, for every composite index of that space
+  static void part_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
+                         std::vector<int64_t>& out) {
+    int32_t comp[kDevMaxComp];
+    for (int64_t x = 0; x < n; ++x) {
+      int64_t y = x;
+      for (int q = 0; q < it.nsp[sp]; ++q) {
+        comp[q] = (int32_t)(y % it.rad[sp][q]);
+        y /= it.rad[sp][q];
+      }
+      int64_t off = 0;
+      for (int j = 0; j < od.ncomp; ++j) {
+        if (od.map[j] || (od.sp1[j] != kNone && od.sp2[j] != kNone)) continue;
+        if (od.sp1[j] == sp) off += (int64_t)comp[od.ci1[j]] * od.ldim[j];
+        else if (od.sp2[j] == sp) off += (int64_t)comp[od.ci2[j]] * od.ldim[j];
+      }
+      out.push_back(off);
+    }
+  }
+
+  // GEMM descriptors, offset tables, pack jobs and tiles of one plan
+  void build_gemm(DevPlan& dp) {
+    Plan& P = dp.plan;
+    const double* x1 = list(dp.list1).d;
+    const double* x2 = list(dp.list2).d;
+    double* x12 = list(dp.list12).d;
+    std::vector<int64_t> tabs;
+    struct Tab { int64_t aro, ako, bco, bko, cro, cco; };
+    std::vector<Tab> toff(P.items.size());
+    std::vector<PackJob> jobs;
+    std::vector<int64_t> pack_off1(P.items.size(), -1), pack_off2(P.items.size(), -1);
+    int64_t scratch = 0;
+    dp.pack_maxlen = 0;
+    auto put = [&](auto&& fill) {
+      int64_t o = (int64_t)tabs.size();
+      fill(tabs);
+      return o;
+    };
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const ItemDesc& it = P.items[i];
+      Tab& t = toff[i];
+      if (it.op[0].nmap > 0) {  // panel[k*M + r]
+        pack_off1[i] = scratch;
+        scratch += it.M * it.K;
+        t.aro = put([&](std::vector<int64_t>& v) { for (int64_t r = 0; r < it.M; ++r) v.push_back(r); });
+        t.ako = put([&](std::vector<int64_t>& v) { for (int64_t k = 0; k < it.K; ++k) v.push_back(k * it.M); });
+      } else {
+        t.aro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kEx1, it.M, v); });
+        t.ako = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kCnt, it.K, v); });
+      }
+      if (it.op[1].nmap > 0) {  // panel[k*N + c]
+        pack_off2[i] = scratch;
+        scratch += it.N * it.K;
+        t.bco = put([&](std::vector<int64_t>& v) { for (int64_t c = 0; c < it.N; ++c) v.push_back(c); });
+        t.bko = put([&](std::vector<int64_t>& v) { for (int64_t k = 0; k < it.K; ++k) v.push_back(k * it.N); });
+      } else {
+        t.bco = put([&](std::vector<int64_t>& v) { part_table(it, it.op[1], kEx2, it.N, v); });
+        t.bko = put([&](std::vector<int64_t>& v) { part_table(it, it.op[1], kCnt, it.K, v); });
+      }
+      t.cro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[2], kEx1, it.M, v); });
+      t.cco = put([&](std::vector<int64_t>& v) { part_table(it, it.op[2], kEx2, it.N, v); });
+    }
+    if (tabs.empty()) tabs.push_back(0);
+    dp.d_tabs = upload(tabs);
+    dp.scratch = scratch ? (double*)alloc(scratch * sizeof(double)) : nullptr;
+    dp.scratch_len = scratch;
+    std::vector<GemmDesc> g[2];
+    std::vector<int32_t> group_of(P.items.size());
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const ItemDesc& it = P.items[i];
+      const Tab& t = toff[i];
+      GemmDesc d{};
+      d.M = it.M;
+      d.N = it.N;
+      d.K = it.K;
+      d.fac = it.fac;
+      d.a = pack_off1[i] >= 0 ? dp.scratch + pack_off1[i] : x1 + it.base1;
+      d.aro = dp.d_tabs + t.aro;
+      d.ako = dp.d_tabs + t.ako;
+      d.afast = pack_off1[i] >= 0 ? 0 : it.kfast1;
+      d.b = pack_off2[i] >= 0 ? dp.scratch + pack_off2[i] : x2 + it.base2;
+      d.bco = dp.d_tabs + t.bco;
+      d.bko = dp.d_tabs + t.bko;
+      d.bfast = pack_off2[i] >= 0 ? 0 : it.kfast2;
+      d.c = x12 + it.base12;
+      d.cro = dp.d_tabs + t.cro;
+      d.cco = dp.d_tabs + t.cco;
+      d.rowspace = kEx1;
+      d.cmapped = it.op[2].nmap > 0;
+      for (int q = 0; q < 3; ++q) {
+        d.nsp[q] = it.nsp[q];
+        for (int c = 0; c < kDevMaxComp; ++c) d.rad[q][c] = it.rad[q][c];
+      }
+      d.cmap = it.op[2];
+      int kind = kGemmRegular;
+      if (d.N <= kGemmSkinnyN) {
+        kind = kGemmSkinny;
+      } else if (d.M <= kGemmSkinnyN) {  // thin ex1: swap the operands
+        kind = kGemmSkinny;
+        std::swap(d.M, d.N);
+        std::swap(d.a, d.b);
+        std::swap(d.aro, d.bco);
+        std::swap(d.ako, d.bko);
+        std::swap(d.afast, d.bfast);
+        std::swap(d.cro, d.cco);
+        d.rowspace = kEx2;
+      }
+      group_of[i] = kind;
+      g[kind].push_back(d);
+      for (int op = 0; op < 2; ++op) {
+        int64_t po = op == 0 ? pack_off1[i] : pack_off2[i];
+        if (po < 0) continue;
+        PackJob j{};
+        j.R = op == 0 ? it.M : it.N;
+        j.K = it.K;
+        j.src = op == 0 ? x1 + it.base1 : x2 + it.base2;
+        j.dst = dp.scratch + po;
+        j.rowspace = op == 0 ? kEx1 : kEx2;
+        for (int q = 0; q < 3; ++q) {
+          j.nsp[q] = it.nsp[q];
+          for (int c = 0; c < kDevMaxComp; ++c) j.rad[q][c] = it.rad[q][c];
+        }
+        j.op = it.op[op];
+        jobs.push_back(j);
+        dp.pack_maxlen = std::max(dp.pack_maxlen, j.R * j.K);
+      }
+    }
+    dp.njobs = (int64_t)jobs.size();
+    if (!jobs.empty()) dp.d_jobs = upload(jobs);
+    for (int kind = 0; kind < 2; ++kind) {
+      const int TM = kind == kGemmRegular ? kGemmRegularM : kGemmSkinnyM;
+      const int TN = kind == kGemmRegular ? kGemmRegularN : kGemmSkinnyN;
+      std::vector<TileDesc> tiles;
+      int64_t total = 0;
+      for (auto& d : g[kind]) total += ((d.M + TM - 1) / TM) * ((d.N + TN - 1) / TN);
+      const int64_t want = 2 * 148;
+      for (size_t i = 0; i < g[kind].size(); ++i) {
+        const GemmDesc& d = g[kind][i];
+        int64_t mt = (d.M + TM - 1) / TM, nt = (d.N + TN - 1) / TN;
+        int64_t ks = 1;
+        if (total < want && d.K > 4 * kGemmK) {
+          ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
+          ks = std::max<int64_t>(ks, 1);
+        }
+        int64_t kchunk = ((d.K + ks - 1) / ks + kGemmK - 1) / kGemmK * kGemmK;
+        for (int64_t m = 0; m < mt; ++m)
+          for (int64_t n = 0; n < nt; ++n)
+            for (int64_t k0 = 0; k0 < d.K; k0 += kchunk) {
+              TileDesc tl{};
+              tl.item = (int32_t)i;
+              tl.m0 = (int32_t)(m * TM);
+              tl.n0 = (int32_t)(n * TN);
+              tl.k0 = k0;
+              tl.k1 = std::min(d.K, k0 + kchunk);
+              tiles.push_back(tl);
+            }
+      }
+      dp.ntiles_g[kind] = (int64_t)tiles.size();
+      if (!tiles.empty()) {
+        dp.d_desc[kind] = upload(g[kind]);
+        dp.d_tiles_g[kind] = upload(tiles);
+      }
+    }
+    dp.ntiles = dp.ntiles_g[0] + dp.ntiles_g[1];
   }
 
   // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
@@ -671,14 +814,20 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
       ev1 = e.get_event();
       CUDA_OK(cudaEventRecord(ev0, e.stream));
     }
-    launch_contract(dp.d_items, dp.d_tiles, dp.ntiles, e.list(dp.list1).d, e.list(dp.list2).d,
-                    r.d, fact, e.stream);
+    if (dp.njobs) {
+      launch_pack(dp.d_jobs, dp.njobs, dp.pack_maxlen, e.stream);
+      ++e.launches;
+    }
+    for (int kind = 0; kind < 2; ++kind) {
+      if (!dp.ntiles_g[kind]) continue;
+      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.stream);
+      ++e.launches;
+    }
     if (timed) {
       CUDA_OK(cudaEventRecord(ev1, e.stream));
       dp.pending.emplace_back(ev0, ev1);
     }
-    ++dp.calls;
-    if (dp.ntiles) ++e.launches;
+    if (timed) ++dp.calls;
     if (dp.plan.use_tr && dp.nflip) {
       launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);
       ++e.launches;

@@ -4,15 +4,9 @@
 //                (set_strmap_kernel, strings/set_strmap_kernel.f:66-119 with
 //                iordstr2, strings/iordstr2.f, and idx4sg,
 //                strings/idx4sg.f).  Integer work, bit-exact.
-//  k_contract    all block contractions of one binary contraction in one
-//                launch.  Per 64x64 output tile: the operand panels are
-//                gathered through the string maps into shared memory with
-//                their signs (collect_block_impr, contract/
-//                collect_block_impr.f), multiplied with FP64 tensor-core MMA
-//                (the dgemm of contract/contr_blk1blk2_blocked_mm.f:465,523)
-//                and scatter-added into the result with sign and factor
-//                (scatter_block, contract/scatter_block.f:163).
+//  (the block contractions themselves are in gemm.cu)
 //  bandwidth     add_opblk, diavc, norms, dot products, scaling, sym_ab.
+#include <algorithm>
 #include <cstdio>
 
 #include "kernels.hpp"
@@ -20,9 +14,6 @@
 namespace gccu {
 namespace {
 
-constexpr int BM = kTileM, BN = kTileN, BK = kTileK;
-constexpr int NT = 128;  // 4 warps, 2x2 warp grid of 32x32 sub-tiles
-constexpr int PAD = 8;
 
 // ---------------------------------------------------------------------------
 // string maps
@@ -89,193 +80,6 @@ __global__ void k_strmap(const int32_t* __restrict__ t1, int e1, int64_t n1,
   }
   int sign = (perm & 1) ? -1 : 1;
   out[idx] = sign * (int32_t)(a + 1);
-}
-
-// ---------------------------------------------------------------------------
-// grouped FP64 block contraction
-// ---------------------------------------------------------------------------
-struct __align__(16) Smem {
-  double As[BK][BM + PAD];
-  double Bs[BK][BN + PAD];
-  int64_t rp1[BM], rp12[BM], cp2[BN], cp12[BN], kp1[BK], kp2[BK];
-  int32_t rc[BM][kDevMaxComp];
-  int32_t cc[BN][kDevMaxComp];
-  int32_t kc[BK][kDevMaxComp];
-  ItemDesc it;
-};
-
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile(
-      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-      : "+d"(d0), "+d"(d1)
-      : "d"(a), "d"(b));
-}
-
-// decompose composite index x of a space into its component indices and the
-// part of the offsets of the operands that depends on this space only
-__device__ __forceinline__ void decomp(const ItemDesc& it, int space, int64_t x, int32_t* comp) {
-  for (int q = 0; q < it.nsp[space]; ++q) {
-    int32_t r = it.rad[space][q];
-    comp[q] = (int32_t)(x % r);
-    x /= r;
-  }
-}
-__device__ __forceinline__ int64_t part(const OpndDesc& od, int space, const int32_t* comp) {
-  int64_t off = 0;
-  for (int j = 0; j < od.ncomp; ++j) {
-    if (od.map[j]) continue;
-    if (od.sp1[j] == space) off += (int64_t)comp[od.ci1[j]] * od.ldim[j];
-    else if (od.sp2[j] == space) off += (int64_t)comp[od.ci2[j]] * od.ldim[j];
-  }
-  return off;
-}
-// contributions of the components that merge two spaces (map lookups)
-__device__ __forceinline__ bool mapped(const OpndDesc& od, int spA, const int32_t* cA,
-                                       const int32_t* cB, int64_t& off, double& sg) {
-  for (int j = 0; j < od.ncomp; ++j) {
-    const int32_t* mp = od.map[j];
-    if (!mp) continue;
-    int i1 = od.sp1[j] == spA ? cA[od.ci1[j]] : cB[od.ci1[j]];
-    int i2 = od.sp2[j] == spA ? cA[od.ci2[j]] : cB[od.ci2[j]];
-    int v = __ldg(mp + (int64_t)i2 * od.n1[j] + i1);
-    if (v == 0) return false;
-    if (v < 0) {
-      sg = -sg;
-      v = -v;
-    }
-    off += (int64_t)(v - 1) * od.ldim[j];
-  }
-  return true;
-}
-
-__global__ void __launch_bounds__(NT) k_contract(const ItemDesc* __restrict__ items,
-                                                 const TileDesc* __restrict__ tiles,
-                                                 const double* __restrict__ x1,
-                                                 const double* __restrict__ x2,
-                                                 double* __restrict__ x12, double alpha) {
-  __shared__ Smem S;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const TileDesc td = tiles[blockIdx.x];
-  {
-    const int* src = reinterpret_cast<const int*>(items + td.item);
-    int* dst = reinterpret_cast<int*>(&S.it);
-    for (int i = tid; i < (int)(sizeof(ItemDesc) / sizeof(int)); i += NT) dst[i] = src[i];
-  }
-  __syncthreads();
-  const ItemDesc& it = S.it;
-  const int64_t M = it.M, N = it.N;
-  // rows (ex1) and columns (ex2) of this tile
-  if (tid < BM) {
-    int64_t r = td.m0 + tid;
-    if (r < M) {
-      decomp(it, kEx1, r, S.rc[tid]);
-      S.rp1[tid] = part(it.op[0], kEx1, S.rc[tid]);
-      S.rp12[tid] = part(it.op[2], kEx1, S.rc[tid]);
-    }
-  } else {
-    int j = tid - BM;
-    int64_t c = td.n0 + j;
-    if (c < N) {
-      decomp(it, kEx2, c, S.cc[j]);
-      S.cp2[j] = part(it.op[1], kEx2, S.cc[j]);
-      S.cp12[j] = part(it.op[2], kEx2, S.cc[j]);
-    }
-  }
-  const int wm = warp >> 1, wn = warp & 1;
-  double acc[4][4][2];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  const bool map1 = it.op[0].nmap > 0, map2 = it.op[1].nmap > 0;
-  const double* X1 = x1 + it.base1;
-  const double* X2 = x2 + it.base2;
-  for (int64_t k0 = td.k0; k0 < td.k1; k0 += BK) {
-    __syncthreads();  // previous tile consumed, row/col info visible
-    if (tid < BK) {
-      int64_t k = k0 + tid;
-      if (k < td.k1) {
-        decomp(it, kCnt, k, S.kc[tid]);
-        S.kp1[tid] = part(it.op[0], kCnt, S.kc[tid]);
-        S.kp2[tid] = part(it.op[1], kCnt, S.kc[tid]);
-      }
-    }
-    __syncthreads();
-    // gather the op1 panel (rows ex1, columns cnt) with signs
-#pragma unroll
-    for (int e = 0; e < (BM * BK) / NT; ++e) {
-      int i, kk;
-      if (it.kfast1) {
-        kk = tid & (BK - 1);
-        i = (tid >> 4) + e * (NT / BK);
-      } else {
-        i = tid & (BM - 1);
-        kk = (tid >> 6) + e * (NT / BM);
-      }
-      double v = 0.0;
-      if (td.m0 + i < M && k0 + kk < td.k1) {
-        int64_t off = S.rp1[i] + S.kp1[kk];
-        double sg = 1.0;
-        bool ok = !map1 || mapped(it.op[0], kEx1, S.rc[i], S.kc[kk], off, sg);
-        if (ok) v = sg * __ldg(X1 + off);
-      }
-      S.As[kk][i] = v;
-    }
-    // gather the op2 panel (rows cnt, columns ex2)
-#pragma unroll
-    for (int e = 0; e < (BN * BK) / NT; ++e) {
-      int j, kk;
-      if (it.kfast2) {
-        kk = tid & (BK - 1);
-        j = (tid >> 4) + e * (NT / BK);
-      } else {
-        j = tid & (BN - 1);
-        kk = (tid >> 6) + e * (NT / BN);
-      }
-      double v = 0.0;
-      if (td.n0 + j < N && k0 + kk < td.k1) {
-        int64_t off = S.cp2[j] + S.kp2[kk];
-        double sg = 1.0;
-        bool ok = !map2 || mapped(it.op[1], kEx2, S.cc[j], S.kc[kk], off, sg);
-        if (ok) v = sg * __ldg(X2 + off);
-      }
-      S.Bs[kk][j] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k4 = 0; k4 < BK; k4 += 4) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = S.As[k4 + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = S.Bs[k4 + (lane & 3)][wn * 32 + j * 8 + (lane >> 2)];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
-  }
-  // signed scatter-add into the result (several items and K splits may hit
-  // the same elements, hence atomics)
-  const double f = alpha * it.fac;
-  const bool map12 = it.op[2].nmap > 0;
-  double* X12 = x12 + it.base12;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        int row = wm * 32 + i * 8 + (lane >> 2);
-        int col = wn * 32 + j * 8 + 2 * (lane & 3) + h;
-        double v = acc[i][j][h];
-        if (td.m0 + row >= M || td.n0 + col >= N || v == 0.0) continue;
-        int64_t off = S.rp12[row] + S.cp12[col];
-        double sg = 1.0;
-        if (map12 && !mapped(it.op[2], kEx1, S.rc[row], S.cc[col], off, sg)) continue;
-        atomicAdd(X12 + off, f * sg * v);
-      }
 }
 
 // ---------------------------------------------------------------------------
@@ -375,13 +179,6 @@ void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab
   if (n == 0) return;
   k_strmap<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(tab1, nel1, n1, tab2, nel2, n2, W12,
                                                        irrep12, nel12, nsym, out);
-}
-
-void launch_contract(const ItemDesc* items, const TileDesc* tiles, int64_t ntiles,
-                     const double* x1, const double* x2, double* x12, double alpha,
-                     cudaStream_t s) {
-  if (ntiles == 0) return;
-  k_contract<<<(unsigned)ntiles, NT, 0, s>>>(items, tiles, x1, x2, x12, alpha);
 }
 
 void launch_axpy(double* out, const double* in, double fac, int64_t n, int reset,

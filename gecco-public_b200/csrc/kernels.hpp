@@ -9,9 +9,6 @@
 
 namespace gccu {
 
-// contraction tile shape of the FP64 kernel
-constexpr int kTileM = 64, kTileN = 64, kTileK = 16;
-
 // signed string map of one (str1 block, str2 block) pair; tables hold the
 // strings of each block in address order (orb<<2 | code), W/irrep describe
 // the graph of the merged string
@@ -19,11 +16,17 @@ void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab
                    int64_t n2, const int64_t* W12, const int8_t* irrep12, int nel12, int nsym,
                    int32_t* out, cudaStream_t s);
 
-// grouped block contractions: one CTA per tile, tiles of all items of one
-// binary contraction in one launch; result accumulated with atomics
-void launch_contract(const ItemDesc* items, const TileDesc* tiles, int64_t ntiles,
-                     const double* x1, const double* x2, double* x12, double alpha,
-                     cudaStream_t s);
+// tile shapes of the grouped GEMM: regular items and thin items (<= 8 columns)
+constexpr int kGemmRegular = 0, kGemmSkinny = 1;
+constexpr int kGemmRegularM = 128, kGemmRegularN = 64;
+constexpr int kGemmSkinnyM = 128, kGemmSkinnyN = 8;
+constexpr int kGemmK = 16;
+
+// gather map-addressed operands into dense panels (one job per operand/item)
+void launch_pack(const PackJob* jobs, int64_t njobs, int64_t maxlen, cudaStream_t s);
+// grouped block-contraction GEMM over the tiles of one tile shape
+void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
+                 double alpha, cudaStream_t s);
 
 // out = (reset ? 0 : out) + fac*in  (add_opblk)
 void launch_axpy(double* out, const double* in, double fac, int64_t n, int reset, cudaStream_t s);
