@@ -34,6 +34,8 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
 CONFIGS = {
     0: dict(nocc=8, nvir=32, naux=160, seed=1000, name="CCSD C1 o8 v32 naux160"),
     2: dict(nocc=24, nvir=200, naux=900, seed=1002, name="CCSD C1 o24 v200 naux900"),
+    # reduced size of the same family, used for kernel captures (a few GB)
+    10: dict(nocc=12, nvir=100, naux=450, seed=1010, name="CCSD C1 o12 v100 naux450"),
 }
 
 
@@ -190,7 +192,8 @@ def run_gpu(args, cfg):
         with open(args.profile_out, "w") as f:
             json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
                         "tflops": r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12 if r[2] else None,
-                        "block_contractions": int(r[3]), "tiles": int(r[4])}
+                        "block_contractions": int(r[3]), "tiles": int(r[4]),
+                        "pack_ms": r[5] / max(r[1], 1)}
                        for n, r in zip(names, prof)], f, indent=1)
     ms = ms_total / args.steps
     if dist:

@@ -66,21 +66,34 @@ struct GemmDesc {
   int32_t afast, bfast;  // 1: contiguous along k (else along rows / columns)
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
+  int32_t exclusive;     // no other tile writes these result elements: plain update
   int32_t nsp[3];
   int32_t rad[3][kDevMaxComp];
   OpndDesc cmap;  // result operand (map lookups in the epilogue)
 };
 
 // gather of one operand of one block contraction into a dense panel
-// panel[k * R + r] = sign * x[address(r, k)]
+// panel[k * R + r] = sign * x[address(r, k)],
+// address(r, k) = roff[r] + koff[k] + sum_m (|map_m[i2 * n1_m + i1]| - 1) * ldim_m
+// where the string indices of map component m come from the tables rmi
+// (row side, rmi[m * R + r]) and kmi (contraction side, kmi[m * K + k]);
+// row_is_1[m] says which side is str1 (the fast index of the map).
+// A thread block covers F consecutive indices of the fast dimension (k when
+// the operand is stored contiguously along the contraction index, else r)
+// times 256/F indices of the other per pass, so the source reads coalesce.
 struct PackJob {
   int64_t R, K;  // rows (ex1 or ex2 composite) and contraction length
   const double* src;
   double* dst;
-  int32_t rowspace;  // kEx1 (op1) or kEx2 (op2)
-  int32_t nsp[3];
-  int32_t rad[3][kDevMaxComp];
-  OpndDesc op;
+  const int64_t *roff, *koff;
+  const int64_t *rmi, *kmi;
+  int32_t kfast;  // threads run fastest along k
+  int32_t F;      // power of two <= 256
+  int32_t nm;     // map components
+  int32_t row_is_1[kDevMaxComp];
+  int32_t n1[kDevMaxComp];
+  int64_t ldim[kDevMaxComp];
+  const int32_t* map[kDevMaxComp];
 };
 
 }  // namespace gccu

@@ -42,12 +42,12 @@ struct DevGraph {
 struct DevPlan {
   Plan plan;
   // grouped GEMM launches (regular / thin tiles), pack jobs, tables, scratch
-  GemmDesc* d_desc[2] = {nullptr, nullptr};
-  TileDesc* d_tiles_g[2] = {nullptr, nullptr};
-  int64_t ntiles_g[2] = {0, 0};
+  GemmDesc* d_desc[kGemmKinds] = {};
+  TileDesc* d_tiles_g[kGemmKinds] = {};
+  int64_t ntiles_g[kGemmKinds] = {};
   int64_t ntiles = 0;
   PackJob* d_jobs = nullptr;
-  int64_t njobs = 0, pack_maxlen = 0;
+  int64_t njobs = 0, pack_gx = 0, pack_gy = 0;
   int64_t* d_tabs = nullptr;
   double* scratch = nullptr;
   int64_t scratch_len = 0;
@@ -57,9 +57,9 @@ struct DevPlan {
   FlipDesc* d_flip = nullptr;
   int64_t nflip = 0, flip_maxlen = 0;
   // kernel timing (gccu_profile): events of launches not yet reported
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  std::vector<std::array<cudaEvent_t, 3>> pending;  // start, after pack, end
   int64_t calls = 0;
-  double ms = 0;
+  double ms = 0, pack_ms = 0;
 };
 
 class Engine {
@@ -112,10 +112,8 @@ class Engine {
       if (ev) cudaEventDestroy(ev);
     for (auto ev : event_pool) cudaEventDestroy(ev);
     for (auto& kv : plans)
-      for (auto& pr : kv.second->pending) {
-        cudaEventDestroy(pr.first);
-        cudaEventDestroy(pr.second);
-      }
+      for (auto& pr : kv.second->pending)
+        for (auto ev : pr) cudaEventDestroy(ev);
     if (stream) cudaStreamSynchronize(stream);
     for (void* p : allocs) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
@@ -285,6 +283,25 @@ class Engine {
     }
   }
 
+  // for each map component of operand od (in component order) and every
+  // composite index of space sp: the string index that space contributes to
+  // the map lookup (layout [map component][index])
+  static void map_index_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
+                              std::vector<int64_t>& out) {
+    int32_t comp[kDevMaxComp];
+    for (int j = 0; j < od.ncomp; ++j) {
+      if (!od.map[j]) continue;
+      for (int64_t x = 0; x < n; ++x) {
+        int64_t y = x;
+        for (int q = 0; q < it.nsp[sp]; ++q) {
+          comp[q] = (int32_t)(y % it.rad[sp][q]);
+          y /= it.rad[sp][q];
+        }
+        out.push_back(od.sp1[j] == sp ? comp[od.ci1[j]] : comp[od.ci2[j]]);
+      }
+    }
+  }
+
   // GEMM descriptors, offset tables, pack jobs and tiles of one plan
   void build_gemm(DevPlan& dp) {
     Plan& P = dp.plan;
@@ -297,16 +314,52 @@ class Engine {
     std::vector<PackJob> jobs;
     std::vector<int64_t> pack_off1(P.items.size(), -1), pack_off2(P.items.size(), -1);
     int64_t scratch = 0;
-    dp.pack_maxlen = 0;
+    dp.pack_gx = dp.pack_gy = 0;
     auto put = [&](auto&& fill) {
       int64_t o = (int64_t)tabs.size();
       fill(tabs);
       return o;
     };
+    // kernel kind per item: small result, skinny or medium (thin ex2, or thin
+    // ex1 with the operands swapped), else regular
+    std::vector<int> kind_of(P.items.size());
+    std::vector<char> swapped(P.items.size(), 0);
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const ItemDesc& it = P.items[i];
+      kind_of[i] = kGemmRegular;
+      if (it.M * it.N <= 16) {
+        kind_of[i] = kGemmSmall;
+      } else if (it.N <= kGemmSkinnyN) {
+        kind_of[i] = kGemmSkinny;
+      } else if (it.M <= kGemmSkinnyN) {
+        kind_of[i] = kGemmSkinny;
+        swapped[i] = 1;
+      } else if (it.N <= kGemmMediumN) {
+        kind_of[i] = kGemmMedium;
+      } else if (it.M <= kGemmMediumN) {
+        kind_of[i] = kGemmMedium;
+        swapped[i] = 1;
+      }
+    }
+    // an operand whose strings need map lookups is packed into a dense panel
+    auto packed = [&](size_t i, int op) { return P.items[i].op[op].nmap > 0; };
+    struct PackTab { int64_t roff, koff, rmi, kmi; };
+    std::vector<PackTab> ptab1(P.items.size()), ptab2(P.items.size());
+    auto pack_tabs = [&](const ItemDesc& it, int op, PackTab& pt) {
+      const OpndDesc& od = it.op[op];
+      const int rsp = op == 0 ? kEx1 : kEx2;
+      const int64_t R = op == 0 ? it.M : it.N;
+      pt.roff = put([&](std::vector<int64_t>& v) { part_table(it, od, rsp, R, v); });
+      pt.koff = put([&](std::vector<int64_t>& v) { part_table(it, od, kCnt, it.K, v); });
+      pt.rmi = put([&](std::vector<int64_t>& v) { map_index_table(it, od, rsp, R, v); });
+      pt.kmi = put([&](std::vector<int64_t>& v) { map_index_table(it, od, kCnt, it.K, v); });
+    };
     for (size_t i = 0; i < P.items.size(); ++i) {
       const ItemDesc& it = P.items[i];
       Tab& t = toff[i];
-      if (it.op[0].nmap > 0) {  // panel[k*M + r]
+      if (packed(i, 0)) pack_tabs(it, 0, ptab1[i]);
+      if (packed(i, 1)) pack_tabs(it, 1, ptab2[i]);
+      if (packed(i, 0)) {  // panel[k*M + r]
         pack_off1[i] = scratch;
         scratch += it.M * it.K;
         t.aro = put([&](std::vector<int64_t>& v) { for (int64_t r = 0; r < it.M; ++r) v.push_back(r); });
@@ -315,7 +368,7 @@ class Engine {
         t.aro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kEx1, it.M, v); });
         t.ako = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kCnt, it.K, v); });
       }
-      if (it.op[1].nmap > 0) {  // panel[k*N + c]
+      if (packed(i, 1)) {  // panel[k*N + c]
         pack_off2[i] = scratch;
         scratch += it.N * it.K;
         t.bco = put([&](std::vector<int64_t>& v) { for (int64_t c = 0; c < it.N; ++c) v.push_back(c); });
@@ -331,7 +384,7 @@ class Engine {
     dp.d_tabs = upload(tabs);
     dp.scratch = scratch ? (double*)alloc(scratch * sizeof(double)) : nullptr;
     dp.scratch_len = scratch;
-    std::vector<GemmDesc> g[2];
+    std::vector<GemmDesc> g[kGemmKinds];
     std::vector<int32_t> group_of(P.items.size());
     for (size_t i = 0; i < P.items.size(); ++i) {
       const ItemDesc& it = P.items[i];
@@ -359,11 +412,8 @@ class Engine {
         for (int c = 0; c < kDevMaxComp; ++c) d.rad[q][c] = it.rad[q][c];
       }
       d.cmap = it.op[2];
-      int kind = kGemmRegular;
-      if (d.N <= kGemmSkinnyN) {
-        kind = kGemmSkinny;
-      } else if (d.M <= kGemmSkinnyN) {  // thin ex1: swap the operands
-        kind = kGemmSkinny;
+      const int kind = kind_of[i];
+      if (swapped[i]) {  // thin ex1: ex2 becomes the row space
         std::swap(d.M, d.N);
         std::swap(d.a, d.b);
         std::swap(d.aro, d.bco);
@@ -382,34 +432,64 @@ class Engine {
         j.K = it.K;
         j.src = op == 0 ? x1 + it.base1 : x2 + it.base2;
         j.dst = dp.scratch + po;
-        j.rowspace = op == 0 ? kEx1 : kEx2;
-        for (int q = 0; q < 3; ++q) {
-          j.nsp[q] = it.nsp[q];
-          for (int c = 0; c < kDevMaxComp; ++c) j.rad[q][c] = it.rad[q][c];
+        const PackTab& pt = op == 0 ? ptab1[i] : ptab2[i];
+        j.roff = dp.d_tabs + pt.roff;
+        j.koff = dp.d_tabs + pt.koff;
+        j.rmi = dp.d_tabs + pt.rmi;
+        j.kmi = dp.d_tabs + pt.kmi;
+        const OpndDesc& od = it.op[op];
+        const int rsp = op == 0 ? kEx1 : kEx2;
+        j.nm = 0;
+        for (int c = 0; c < od.ncomp; ++c) {
+          if (!od.map[c]) continue;
+          GCCU_REQUIRE((od.sp1[c] == rsp && od.sp2[c] == kCnt) ||
+                           (od.sp1[c] == kCnt && od.sp2[c] == rsp),
+                       "string map of an operand must merge an external and a contracted string");
+          j.row_is_1[j.nm] = od.sp1[c] == rsp;
+          j.n1[j.nm] = od.n1[c];
+          j.ldim[j.nm] = od.ldim[c];
+          j.map[j.nm] = od.map[c];
+          ++j.nm;
         }
-        j.op = it.op[op];
+        GCCU_REQUIRE(j.R < INT32_MAX && j.K < INT32_MAX, "block too large for the pack kernel");
+        j.kfast = op == 0 ? it.kfast1 : it.kfast2;
+        const int64_t nf = j.kfast ? j.K : j.R;
+        j.F = 1;
+        while (j.F < 256 && j.F < nf) j.F *= 2;
+        int64_t gx, gy;
+        pack_geometry(j, gx, gy);
+        dp.pack_gx = std::max(dp.pack_gx, gx);
+        dp.pack_gy = std::max(dp.pack_gy, gy);
         jobs.push_back(j);
-        dp.pack_maxlen = std::max(dp.pack_maxlen, j.R * j.K);
       }
     }
     dp.njobs = (int64_t)jobs.size();
+    GCCU_REQUIRE(dp.njobs <= 65535 && dp.pack_gy <= 65535 && dp.pack_gx < INT32_MAX,
+                 "contraction has too many or too large map-addressed operand blocks");
     if (!jobs.empty()) dp.d_jobs = upload(jobs);
-    for (int kind = 0; kind < 2; ++kind) {
-      const int TM = kind == kGemmRegular ? kGemmRegularM : kGemmSkinnyM;
-      const int TN = kind == kGemmRegular ? kGemmRegularN : kGemmSkinnyN;
+    // result blocks written by more than one item need atomic updates
+    std::map<const double*, int> writers;
+    for (int kind = 0; kind < kGemmKinds; ++kind)
+      for (auto& d : g[kind]) writers[d.c]++;
+    for (int kind = 0; kind < kGemmKinds; ++kind) {
+      int TM, TN;
+      gemm_tile(kind, TM, TN);
       std::vector<TileDesc> tiles;
       int64_t total = 0;
       for (auto& d : g[kind]) total += ((d.M + TM - 1) / TM) * ((d.N + TN - 1) / TN);
       const int64_t want = 2 * 148;
       for (size_t i = 0; i < g[kind].size(); ++i) {
-        const GemmDesc& d = g[kind][i];
+        GemmDesc& d = g[kind][i];
         int64_t mt = (d.M + TM - 1) / TM, nt = (d.N + TN - 1) / TN;
         int64_t ks = 1;
-        if (total < want && d.K > 4 * kGemmK) {
+        if (kind == kGemmSmall) {
+          ks = std::max<int64_t>(1, (d.K + kSmallChunk - 1) / kSmallChunk);
+        } else if (total < want && d.K > 4 * kGemmK) {
           ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
           ks = std::max<int64_t>(ks, 1);
         }
         int64_t kchunk = ((d.K + ks - 1) / ks + kGemmK - 1) / kGemmK * kGemmK;
+        d.exclusive = kind != kGemmSmall && !d.cmapped && writers[d.c] == 1 && kchunk >= d.K;
         for (int64_t m = 0; m < mt; ++m)
           for (int64_t n = 0; n < nt; ++n)
             for (int64_t k0 = 0; k0 < d.K; k0 += kchunk) {
@@ -428,7 +508,8 @@ class Engine {
         dp.d_tiles_g[kind] = upload(tiles);
       }
     }
-    dp.ntiles = dp.ntiles_g[0] + dp.ntiles_g[1];
+    dp.ntiles = 0;
+    for (int kind = 0; kind < kGemmKinds; ++kind) dp.ntiles += dp.ntiles_g[kind];
   }
 
   // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
@@ -807,7 +888,7 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     if (!update) {
       CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
     }
-    const bool timed = e.profiling && !e.capturing && dp.ntiles;
+    const bool timed = e.profiling && !e.capturing;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (timed) {
       ev0 = e.get_event();
@@ -815,17 +896,22 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
       CUDA_OK(cudaEventRecord(ev0, e.stream));
     }
     if (dp.njobs) {
-      launch_pack(dp.d_jobs, dp.njobs, dp.pack_maxlen, e.stream);
+      launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
       ++e.launches;
     }
-    for (int kind = 0; kind < 2; ++kind) {
+    cudaEvent_t evp = nullptr;
+    if (timed) {
+      evp = e.get_event();
+      CUDA_OK(cudaEventRecord(evp, e.stream));
+    }
+    for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
       launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.stream);
       ++e.launches;
     }
     if (timed) {
       CUDA_OK(cudaEventRecord(ev1, e.stream));
-      dp.pending.emplace_back(ev0, ev1);
+      dp.pending.push_back({ev0, evp, ev1});
     }
     if (timed) ++dp.calls;
     if (dp.plan.use_tr && dp.nflip) {
@@ -1023,11 +1109,12 @@ int gccu_profile_report(double* rows, int64_t maxrows, int64_t* nrows) {
     int64_t n = 0;
     for (DevPlan* dp : e.plan_order) {
       for (auto& pr : dp->pending) {
-        float f = 0;
-        CUDA_OK(cudaEventElapsedTime(&f, pr.first, pr.second));
+        float f = 0, fp = 0;
+        CUDA_OK(cudaEventElapsedTime(&f, pr[0], pr[2]));
+        CUDA_OK(cudaEventElapsedTime(&fp, pr[0], pr[1]));
         dp->ms += f;
-        e.event_pool.push_back(pr.first);
-        e.event_pool.push_back(pr.second);
+        dp->pack_ms += fp;
+        for (auto ev : pr) e.event_pool.push_back(ev);
       }
       dp->pending.clear();
       if (dp->calls == 0) continue;
@@ -1038,11 +1125,12 @@ int gccu_profile_report(double* rows, int64_t maxrows, int64_t* nrows) {
         r[2] = dp->ms;
         r[3] = (double)dp->plan.items.size();
         r[4] = (double)dp->ntiles;
-        r[5] = (double)dp->calls * (dp->ntiles ? 1 : 0);
+        r[5] = dp->pack_ms;
       }
       ++n;
       dp->calls = 0;
       dp->ms = 0;
+      dp->pack_ms = 0;
     }
     *nrows = n;
   });

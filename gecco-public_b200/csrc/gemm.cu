@@ -58,27 +58,51 @@ __device__ __forceinline__ bool mapped(const OpndDesc& od, int spA, const int32_
 }
 
 // ---------------------------------------------------------------------------
-__global__ void k_pack(const PackJob* __restrict__ jobs) {
-  const PackJob& J = jobs[blockIdx.y];
-  const int64_t n = J.R * J.K;
-  const OpndDesc& od = J.op;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = e % J.R, k = e / J.R;
-    int32_t rc[kDevMaxComp], kc[kDevMaxComp];
-    decomp(J.rad[J.rowspace], J.nsp[J.rowspace], r, rc);
-    decomp(J.rad[kCnt], J.nsp[kCnt], k, kc);
-    int64_t off = 0;
-    double sg = 1.0;
-    bool ok = true;
-    for (int j = 0; j < od.ncomp && ok; ++j) {
-      if (od.map[j]) continue;
-      int sp = od.sp1[j] != kNone ? od.sp1[j] : od.sp2[j];
-      int ci = od.sp1[j] != kNone ? od.ci1[j] : od.ci2[j];
-      off += (int64_t)(sp == kCnt ? kc[ci] : rc[ci]) * od.ldim[j];
+// grid: x = blocks of (256/F) * kPackPasses slow-dimension indices, y =
+// blocks of F fast-dimension indices, z = job.  The fast index's table
+// entries are read once per thread, the slow one's (the same for the threads
+// of a row of the block) once per pass.
+constexpr int kPackThreads = 256, kPackPasses = 8;
+__global__ void __launch_bounds__(kPackThreads) k_pack(const PackJob* __restrict__ jobs) {
+  const PackJob& J = jobs[blockIdx.z];
+  const int F = J.F, S = kPackThreads / F;
+  const bool kf = J.kfast != 0;
+  const int64_t nf = kf ? J.K : J.R, ns = kf ? J.R : J.K;
+  const int64_t f = (int64_t)blockIdx.y * F + threadIdx.x % F;
+  const int64_t s0 = (int64_t)blockIdx.x * S * kPackPasses + threadIdx.x / F;
+  if (f >= nf || s0 >= ns) return;
+  const int64_t* __restrict__ soff = kf ? J.roff : J.koff;
+  const int64_t* __restrict__ smi = kf ? J.rmi : J.kmi;
+  const int64_t* __restrict__ fmi = kf ? J.kmi : J.rmi;
+  const int64_t foff = __ldg((kf ? J.koff : J.roff) + f);
+  const int nm = J.nm;
+  int32_t fi[kDevMaxComp];
+  for (int m = 0; m < nm; ++m) fi[m] = (int32_t)__ldg(fmi + m * nf + f);
+  const double* __restrict__ src = J.src;
+  double* __restrict__ dst = J.dst;
+  for (int p = 0; p < kPackPasses; ++p) {
+    const int64_t s = s0 + (int64_t)p * S;
+    if (s >= ns) break;
+    int64_t off = foff + __ldg(soff + s);
+    bool neg = false, ok = true;
+    for (int m = 0; m < nm; ++m) {
+      const int32_t si = (int32_t)__ldg(smi + m * ns + s);
+      const int32_t ir = kf ? si : fi[m], ik = kf ? fi[m] : si;
+      const int32_t i1 = J.row_is_1[m] ? ir : ik, i2 = J.row_is_1[m] ? ik : ir;
+      int32_t v = __ldg(J.map[m] + (int64_t)i2 * J.n1[m] + i1);
+      if (v == 0) {
+        ok = false;
+        break;
+      }
+      if (v < 0) {
+        neg = !neg;
+        v = -v;
+      }
+      off += (int64_t)(v - 1) * J.ldim[m];
     }
-    ok = mapped(od, J.rowspace, rc, kc, off, sg);
-    J.dst[e] = ok ? sg * J.src[off] : 0.0;
+    const int64_t r = kf ? s : f, k = kf ? f : s;
+    double x = ok ? __ldg(src + off) : 0.0;
+    dst[k * J.R + r] = neg ? -x : x;
   }
 }
 
@@ -101,12 +125,16 @@ struct __align__(16) GemmSmem {
   GemmDesc d;
 };
 
-// element (row r, k-slot kk) handled by thread t in slot e of a R x BK tile
+// element (row r, k-slot kk) handled by thread t in slot e of a R x BK tile.
+// Operand contiguous along k: a warp covers 8 rows x 4 consecutive k per slot
+// (32-byte sectors in global memory, distinct shared-memory banks for the
+// transposed store); contiguous along rows: a warp covers 32 consecutive rows.
 template <int R, int NT>
 __device__ __forceinline__ void slot(int fastk, int t, int e, int& r, int& kk) {
   if (fastk) {
-    kk = t % BK;
-    r = t / BK + (NT / BK) * e;
+    const int lane = t & 31, g = (t >> 5) + (NT / 32) * e;  // group of 4 k x 8 rows
+    kk = 4 * (g % (BK / 4)) + (lane & 3);
+    r = 8 * (g / (BK / 4)) + (lane >> 2);
   } else {
     r = t % R;
     kk = t / R + (NT / R) * e;
@@ -232,8 +260,61 @@ __global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT)
         int64_t off = S.cro[row] + S.cco[col];
         double sg = 1.0;
         if (d.cmapped && !mapped(d.cmap, d.rowspace, S.rc[row], S.cc[col], off, sg)) continue;
-        atomicAdd(X + off, f * sg * v);
+        if (d.exclusive)
+          X[off] += f * sg * v;
+        else
+          atomicAdd(X + off, f * sg * v);
       }
+}
+
+// Items with at most 16 result elements (energies, thin intermediates): a
+// block reduces a chunk of the contraction index for all M*N elements.
+constexpr int kSmallThreads = 256;
+__global__ void __launch_bounds__(kSmallThreads)
+    k_small(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles, double alpha) {
+  const TileDesc td = tiles[blockIdx.x];
+  const GemmDesc& d = descs[td.item];
+  const int M = (int)d.M, N = (int)d.N;
+  double acc[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+  int64_t ar[16], bc[16];
+  for (int r = 0; r < M; ++r) ar[r] = d.aro[r];
+  for (int c = 0; c < N; ++c) bc[c] = d.bco[c];
+  for (int64_t k = td.k0 + threadIdx.x; k < td.k1; k += kSmallThreads) {
+    const int64_t ak = __ldg(d.ako + k), bk = __ldg(d.bko + k);
+    double bv[16];
+    for (int c = 0; c < N; ++c) bv[c] = __ldg(d.b + bc[c] + bk);
+    for (int r = 0; r < M; ++r) {
+      const double av = __ldg(d.a + ar[r] + ak);
+      for (int c = 0; c < N; ++c) acc[r * N + c] += av * bv[c];
+    }
+  }
+  __shared__ double red[kSmallThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int e = 0; e < M * N; ++e) {
+    double v = acc[e];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < kSmallThreads / 32; ++w) s += red[w];
+      const int r = e / N, c = e % N;
+      int64_t off = d.cro[r] + d.cco[c];
+      double sg = 1.0;
+      bool ok = true;
+      if (d.cmapped) {
+        int32_t rc[kDevMaxComp], cc[kDevMaxComp];
+        const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
+        decomp(d.rad[d.rowspace], d.nsp[d.rowspace], r, rc);
+        decomp(d.rad[colspace], d.nsp[colspace], c, cc);
+        ok = mapped(d.cmap, d.rowspace, rc, cc, off, sg);
+      }
+      if (ok && s != 0.0) atomicAdd(d.c + off, alpha * d.fac * sg * s);
+    }
+    __syncthreads();
+  }
 }
 
 template <int BM, int BN, int WM, int WN>
@@ -252,12 +333,17 @@ void launch_gemm_cfg(const GemmDesc* descs, const TileDesc* tiles, int64_t ntile
 
 }  // namespace
 
-void launch_pack(const PackJob* jobs, int64_t njobs, int64_t maxlen, cudaStream_t s) {
-  if (njobs == 0 || maxlen == 0) return;
-  int64_t bx = (maxlen + 255) / 256;
-  if (bx > 4096) bx = 4096;
-  dim3 grid((unsigned)bx, (unsigned)njobs);
-  k_pack<<<grid, 256, 0, s>>>(jobs);
+void pack_geometry(const PackJob& j, int64_t& gx, int64_t& gy) {
+  const int64_t nf = j.kfast ? j.K : j.R, ns = j.kfast ? j.R : j.K;
+  const int64_t span = (int64_t)(kPackThreads / j.F) * kPackPasses;
+  gx = (ns + span - 1) / span;
+  gy = (nf + j.F - 1) / j.F;
+}
+
+void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cudaStream_t s) {
+  if (njobs == 0 || gx == 0 || gy == 0) return;
+  dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)njobs);
+  k_pack<<<grid, kPackThreads, 0, s>>>(jobs);
 }
 
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
@@ -265,8 +351,12 @@ void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t
   if (ntiles == 0) return;
   if (kind == kGemmRegular)
     launch_gemm_cfg<kGemmRegularM, kGemmRegularN, 4, 2>(descs, tiles, ntiles, alpha, s);
-  else
+  else if (kind == kGemmMedium)
+    launch_gemm_cfg<kGemmMediumM, kGemmMediumN, 4, 1>(descs, tiles, ntiles, alpha, s);
+  else if (kind == kGemmSkinny)
     launch_gemm_cfg<kGemmSkinnyM, kGemmSkinnyN, 4, 1>(descs, tiles, ntiles, alpha, s);
+  else
+    k_small<<<(unsigned)ntiles, kSmallThreads, 0, s>>>(descs, tiles, alpha);
 }
 
 }  // namespace gccu

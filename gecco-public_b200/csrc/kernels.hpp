@@ -16,14 +16,32 @@ void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab
                    int64_t n2, const int64_t* W12, const int8_t* irrep12, int nel12, int nsym,
                    int32_t* out, cudaStream_t s);
 
-// tile shapes of the grouped GEMM: regular items and thin items (<= 8 columns)
-constexpr int kGemmRegular = 0, kGemmSkinny = 1;
+// tile shapes of the grouped GEMM: regular items, medium (<= 32 columns) and
+// thin (<= 8 columns) items, items with at most 16 result elements
+constexpr int kGemmRegular = 0, kGemmSkinny = 1, kGemmSmall = 2, kGemmMedium = 3;
+constexpr int kGemmKinds = 4;
+constexpr int64_t kSmallChunk = 1 << 16;  // contraction elements per block of k_small
 constexpr int kGemmRegularM = 128, kGemmRegularN = 64;
+constexpr int kGemmMediumM = 128, kGemmMediumN = 32;
 constexpr int kGemmSkinnyM = 128, kGemmSkinnyN = 8;
 constexpr int kGemmK = 16;
+// output tile of a kernel kind (the small-item kernel takes a whole item)
+inline void gemm_tile(int kind, int& TM, int& TN) {
+  TM = kind == kGemmRegular ? kGemmRegularM
+       : kind == kGemmMedium ? kGemmMediumM
+       : kind == kGemmSkinny ? kGemmSkinnyM
+                             : 1 << 30;
+  TN = kind == kGemmRegular ? kGemmRegularN
+       : kind == kGemmMedium ? kGemmMediumN
+       : kind == kGemmSkinny ? kGemmSkinnyN
+                             : 1 << 30;
+}
 
-// gather map-addressed operands into dense panels (one job per operand/item)
-void launch_pack(const PackJob* jobs, int64_t njobs, int64_t maxlen, cudaStream_t s);
+// gather map-addressed operands into dense panels (one job per operand/item);
+// pack_geometry gives the grid extent one job needs, the launch uses the
+// maximum over its jobs
+void pack_geometry(const PackJob& j, int64_t& gx, int64_t& gy);
+void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cudaStream_t s);
 // grouped block-contraction GEMM over the tiles of one tile shape
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
                  double alpha, cudaStream_t s);

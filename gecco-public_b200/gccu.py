@@ -323,7 +323,7 @@ class Engine:
         _call("gccu_profile", int(enable))
 
     def profile_report(self):
-        """rows (flops per call, calls, kernel ms, items, tiles, launches)"""
+        """rows (flops per call, calls, kernel ms, items, tiles, gather ms)"""
         n = np.zeros(1, np.int64)
         rows = np.zeros((4096, 6))
         _call("gccu_profile_report", _pd(rows), 4096, _p64(n))

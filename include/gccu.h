@@ -163,8 +163,8 @@ int gccu_event_elapsed(int64_t slot_a, int64_t slot_b, double* ms);
 /* per-contraction kernel timing: while enabled every [CONTR] launch is
  * bracketed by events on the engine's stream.  The report synchronises and
  * returns one row per planned contraction that ran: (flops per call,
- * calls, total kernel ms, block contractions, tiles, k_contract launches),
- * then resets the accumulated times. */
+ * calls, total kernel ms, block contractions, tiles, of which ms in the
+ * operand gathers), then resets the accumulated times. */
 int gccu_profile(int64_t enable);
 int gccu_profile_report(double* rows, int64_t maxrows, int64_t* nrows);
 
