@@ -45,6 +45,7 @@ struct DevPlan {
   GemmDesc* d_desc[kGemmKinds] = {};
   TileDesc* d_tiles_g[kGemmKinds] = {};
   int64_t ntiles_g[kGemmKinds] = {};
+  int64_t ndesc_g[kGemmKinds] = {};
   int64_t ntiles = 0;
   PackJob* d_jobs = nullptr;
   int64_t njobs = 0, pack_gx = 0, pack_gy = 0;
@@ -84,6 +85,9 @@ class Engine {
   int64_t capture_start = 0;
   cudaEvent_t slots[64] = {};
   bool profiling = false;
+  // fixed scratch of gccu_contract_noalloc, looked up on its first call
+  bool have_static = false;
+  StaticScratch static_ss;
   std::vector<cudaEvent_t> event_pool;
   std::vector<DevPlan*> plan_order;  // plans in first-use order (profile report)
 
@@ -218,6 +222,17 @@ class Engine {
       m[s] = sg * (int32_t)(g.address(orb.data(), spf.data()) + 1);
     }
     return flips[key] = upload(m);
+  }
+
+  // cached plan of a descriptor, or null; never plans (gccu_contract_noalloc)
+  DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
+    std::ostringstream os;
+    os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr;
+    for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
+                                   << bc->occ_cnt[k];
+    auto it = plans.find(os.str());
+    return it == plans.end() ? nullptr : it->second.get();
   }
 
   DevPlan& plan_for(const gccu_bc_desc* bc, bool use_tr) {
@@ -503,6 +518,7 @@ class Engine {
             }
       }
       dp.ntiles_g[kind] = (int64_t)tiles.size();
+      dp.ndesc_g[kind] = (int64_t)g[kind].size();
       if (!tiles.empty()) {
         dp.d_desc[kind] = upload(g[kind]);
         dp.d_tiles_g[kind] = upload(tiles);
@@ -864,6 +880,62 @@ int gccu_zero_list(int64_t list_id) {
 
 int gccu_list_device_ptr(int64_t list_id, void** dptr) {
   return guarded([&] { *dptr = eng().list(list_id).d; });
+}
+
+int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_contract_noalloc needs a device");
+    GCCU_REQUIRE(bc, "null contraction descriptor");
+    DevPlan* pp = e.find_plan(bc, use_tr != 0);
+    GCCU_REQUIRE(pp, "gccu_contract_noalloc: this contraction has not been planned; planning "
+                     "allocates device memory, so run it once through gccu_contract first");
+    DevPlan& dp = *pp;
+    int64_t ndesc = 0;
+    for (int kind = 0; kind < kGemmKinds; ++kind) ndesc += dp.ndesc_g[kind];
+    if (dp.scratch_len > kStaticPanelDoubles) {
+      std::ostringstream os;
+      os << "gccu_contract_noalloc: the operand panels of this contraction need "
+         << (double)dp.scratch_len * sizeof(double) / (1 << 20) << " MiB, the fixed scratch holds "
+         << kStaticPanelDoubles * sizeof(double) / (1 << 20) << " MiB";
+      throw Error(os.str());
+    }
+    GCCU_REQUIRE(ndesc <= kStaticMaxDescs && dp.njobs <= kStaticMaxJobs,
+                 "gccu_contract_noalloc: the contraction has more block contractions than the "
+                 "fixed scratch holds descriptors for (16384)");
+    if (!e.have_static) {  // once per engine (and so per device), with its device current
+      CUDA_OK(cudaSetDevice(e.device));
+      CUDA_OK(static_scratch(&e.static_ss));
+      e.have_static = true;
+    }
+    const StaticScratch& ss = e.static_ss;
+    DevList& r = e.list(dp.list12);
+    if (!update) {
+      CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
+    }
+    if (dp.njobs) {
+      launch_rebase_jobs(dp.d_jobs, ss.jobs, dp.njobs, dp.scratch, dp.scratch_len, ss.panels,
+                         e.stream);
+      launch_pack(ss.jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
+      e.launches += 2;
+    }
+    int64_t first = 0;
+    for (int kind = 0; kind < kGemmKinds; ++kind) {
+      if (!dp.ntiles_g[kind]) continue;
+      GemmDesc* descs = ss.descs + first;
+      first += dp.ndesc_g[kind];
+      launch_rebase_descs(dp.d_desc[kind], descs, dp.ndesc_g[kind], dp.scratch, dp.scratch_len,
+                          ss.panels, e.stream);
+      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.stream);
+      e.launches += 2;
+    }
+    if (dp.plan.use_tr && dp.nflip) {
+      launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);
+      ++e.launches;
+    }
+    CUDA_OK(cudaGetLastError());
+    for (int k = 0; k < 8; ++k) e.stats[k] += dp.plan.stats[k];
+  });
 }
 
 int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8) {

@@ -73,4 +73,24 @@ struct FlipDesc {
 void launch_sym_ab(const FlipDesc* d, int64_t n, double* x, double prefac, int64_t maxlen,
                    cudaStream_t s);
 
+// Fixed scratch of the allocation-free contraction path (noalloc.cu): one
+// file-scope device array holding 64 MiB of operand panels and room for the
+// descriptors of one contraction.
+constexpr int64_t kStaticPanelDoubles = int64_t(8) << 20;
+constexpr int64_t kStaticMaxDescs = 16384;
+constexpr int64_t kStaticMaxJobs = 16384;
+struct StaticScratch {
+  double* panels = nullptr;  // kStaticPanelDoubles
+  GemmDesc* descs = nullptr;  // kStaticMaxDescs
+  PackJob* jobs = nullptr;    // kStaticMaxJobs
+};
+// device address of the array on the current device (cudaGetSymbolAddress)
+cudaError_t static_scratch(StaticScratch* out);
+// copy n descriptors, moving operand pointers that lie in the panel range
+// [old_base, old_base + old_len) to the same offset from new_base
+void launch_rebase_descs(const GemmDesc* src, GemmDesc* dst, int64_t n, const double* old_base,
+                         int64_t old_len, double* new_base, cudaStream_t s);
+void launch_rebase_jobs(const PackJob* src, PackJob* dst, int64_t n, const double* old_base,
+                        int64_t old_len, double* new_base, cudaStream_t s);
+
 }  // namespace gccu

@@ -54,6 +54,7 @@ _SIGS = {
     "gccu_list_device_ptr": [I64, ctypes.POINTER(ctypes.c_void_p)],
     "gccu_contract": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64, I64, PD],
     "gccu_plan_info": [ctypes.POINTER(BcDesc), I64, P64, PD],
+    "gccu_contract_noalloc": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64],
     "gccu_add_block": [ctypes.c_double, I64, I64, I64, I64, I64, I64, PD],
     "gccu_scale_list": [I64, ctypes.c_double],
     "gccu_dot_lists": [I64, I64, PD],
@@ -252,6 +253,14 @@ class Engine:
         r = np.zeros(1)
         _call("gccu_contract", ctypes.byref(d), fact, int(update), int(use_tr), xret, _pd(r))
         return float(r[0])
+
+    def contract_noalloc(self, op1, op2, res, ex1, ex2, cnt, fact=1.0, update=True,
+                         use_tr=False, desc=None):
+        """gccu_contract_noalloc: a contraction already run once through
+        contract(), with its operand panels in the library's fixed device
+        array; allocates nothing"""
+        d = desc if desc is not None else self.desc(op1, op2, res, ex1, ex2, cnt)
+        _call("gccu_contract_noalloc", ctypes.byref(d), fact, int(update), int(use_tr))
 
     def plan_info(self, op1, op2, res, ex1, ex2, cnt, use_tr=False):
         d = self.desc(op1, op2, res, ex1, ex2, cnt)

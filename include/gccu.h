@@ -113,6 +113,23 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
  * them): number of block contractions and the reference dgemm accounting of
  * gccu_stats for this contraction alone */
 int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8);
+/* [CONTR] without any device allocation.  No counterpart in the reference.
+ * For callers that must not allocate device memory while they run: a host
+ * that has given all device memory to its ME lists up front, or one that must
+ * not stall the device, since cudaMalloc and cudaFree may synchronise it and
+ * hold up work queued on other streams.  Same arguments and result as
+ * gccu_contract with type_xret = 0, but the operand panels and the launch
+ * descriptors go to one fixed device array compiled into the library
+ * (64 MiB of panels, descriptors for 16384 block contractions) instead of
+ * memory owned by the contraction; larger contractions are rejected with an
+ * error naming the size they need.  The contraction must have been run once
+ * through gccu_contract with the same descriptor and use_tr, because
+ * planning allocates; this call allocates nothing.  The first call of an
+ * engine looks up the array's device address (set-up, no allocation) and
+ * should come before any stream capture.  Every call uses the same array
+ * and leaves its contents behind; calls that overlap in time (from other
+ * host threads or on other streams) race on it. */
+int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr);
 
 /* ---- [ADD] -------------------------------------------------------------------
  * replaces: add_opblk (contract/add_opblk.f:2-313), in-core branch
