@@ -31,11 +31,32 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
+# the contraction whose k_gemm<128,64> launch stands for the dominant kernel
+ROOFLINE_CONTRACTION = "r2_ladder"
+PROFILES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles")
+
+
+def profiled_traffic(cfg):
+    """DRAM bytes (read + write) of one roofline launch at this workload, from
+    the ncu summary in profiles/ (a line 'traffic_bytes_per_launch: N'), or
+    None when no capture of this workload is committed"""
+    path = os.path.join(PROFILES, f"k_gemm_ladder_{cfg['tag']}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 CONFIGS = {
-    0: dict(nocc=8, nvir=32, naux=160, seed=1000, name="CCSD C1 o8 v32 naux160"),
-    2: dict(nocc=24, nvir=200, naux=900, seed=1002, name="CCSD C1 o24 v200 naux900"),
+    0: dict(nocc=8, nvir=32, naux=160, seed=1000, name="CCSD C1 o8 v32 naux160",
+            tag="ccsd_o8v32"),
+    2: dict(nocc=24, nvir=200, naux=900, seed=1002, name="CCSD C1 o24 v200 naux900",
+            tag="ccsd_o24v200"),
     # reduced size of the same family, used for kernel captures (a few GB)
-    10: dict(nocc=12, nvir=100, naux=450, seed=1010, name="CCSD C1 o12 v100 naux450"),
+    10: dict(nocc=12, nvir=100, naux=450, seed=1010, name="CCSD C1 o12 v100 naux450",
+             tag="ccsd_o12v100"),
 }
 
 
@@ -148,13 +169,26 @@ def run_gpu(args, cfg):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    peak = fp64_peak() if rank == 0 else None
+    peak = fp64_peak() if rank == 0 and not args.trace_contraction else None
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
     solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
     t0 = time.time()
     solver.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
     setup_s = time.time() - t0
+    if args.trace_contraction:
+        # one formula item, run once eagerly (the command profilers capture)
+        items = [it for it in solver.formula if it.get("name") == args.trace_contraction]
+        if not items:
+            raise SystemExit(f"no formula item named {args.trace_contraction!r}")
+        eng.event_record(0)
+        solver.run_item(items[0])
+        eng.event_record(1)
+        ms = eng.event_elapsed(0, 1)
+        eng.close()
+        print(json.dumps({"trace": args.trace_contraction, "workload": cfg["name"],
+                          "ms_including_planning": ms}), flush=True)
+        return
     # warm-up iterations (the first one plans every contraction and builds the
     # string maps on the device)
     energies = []
@@ -187,8 +221,10 @@ def run_gpu(args, cfg):
     solver.evaluate()
     prof = eng.profile_report()
     eng.profile(False)
+    names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
+    if len(names) != len(prof):
+        raise RuntimeError(f"profile rows ({len(prof)}) do not match contractions ({len(names)})")
     if args.profile_out and rank == 0:
-        names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
         with open(args.profile_out, "w") as f:
             json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
                         "tflops": r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12 if r[2] else None,
@@ -221,9 +257,12 @@ def run_gpu(args, cfg):
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     h2d = 8 * sum(nT.values())
     d2h = 8 * sum(nR.values()) + 8
-    # dominant kernel: the contraction with the largest kernel time
-    dom = prof[np.argmax(prof[:, 2])]
-    dom_ms = dom[2] / dom[1]
+    # dominant kernel: k_gemm<128,64>; its representative launch is the one of
+    # the pp-ladder contraction (the leading term; no operand gathers), timed
+    # with events around its GEMM launches in the profiled iteration
+    i_dom = names.index(ROOFLINE_CONTRACTION)
+    dom = prof[i_dom]
+    dom_ms = (dom[2] - dom[5]) / dom[1]
     achieved = dom[0] / (dom_ms * 1e-3) / 1e12
     total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
     line = {
@@ -246,8 +285,9 @@ def run_gpu(args, cfg):
                    "parallelism": f"replicas x{world}", "l2": "inputs > L2",
                    "setup_s": round(setup_s, 2), "energy_last": energies[-1]},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if peak else None, "traffic": None,
-                     "kernel": "k_contract (pp ladder, FP64 DMMA)",
+                     "frac": (achieved / peak) if peak else None,
+                     "traffic": profiled_traffic(cfg),
+                     "kernel": f"k_gemm<128,64> FP64 DMMA, launch of [CONTR] {ROOFLINE_CONTRACTION}",
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
                                     "MEASURED_PEAKS.json)",
                      "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
@@ -349,6 +389,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trace-contraction", default=None,
+                    help="set up, run one named [CONTR] of the formula once and exit "
+                         "(the command the ncu captures in profiles/ run)")
     ap.add_argument("--profile-out", default=None,
                     help="write per-contraction kernel times (JSON)")
     args = ap.parse_args()

@@ -297,19 +297,23 @@ class CCSolver:
     def evaluate(self):
         """one formula evaluation (frm_sched2 over the item list)"""
         for it in self.formula:
-            if it["kind"] == "ADD":
-                (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
-                self.e.add_block(it["fac"], li, bi, lo, bo, reset=it["reset"])
-            else:
-                o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
-                c = np.asarray(it["cnt"])
-                occ1 = np.asarray(it["op1"][1])
-                occ2 = np.asarray(it["op2"][1])
-                ex1 = occ1 - c
-                ex2 = occ2 - np.concatenate([c[4:], c[:4]])
-                use_tr = self.use_tr and it["res"][0] not in ("E",)
-                self.e.contract(o1, o2, r, ex1, ex2, c, fact=it["fac"], update=it["update"],
-                                use_tr=use_tr)
+            self.run_item(it)
+
+    def run_item(self, it):
+        """one [ADD] or [CONTR] item of the formula"""
+        if it["kind"] == "ADD":
+            (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
+            self.e.add_block(it["fac"], li, bi, lo, bo, reset=it["reset"])
+        else:
+            o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
+            c = np.asarray(it["cnt"])
+            occ1 = np.asarray(it["op1"][1])
+            occ2 = np.asarray(it["op2"][1])
+            ex1 = occ1 - c
+            ex2 = occ2 - np.concatenate([c[4:], c[:4]])
+            use_tr = self.use_tr and it["res"][0] not in ("E",)
+            self.e.contract(o1, o2, r, ex1, ex2, c, fact=it["fac"], update=it["update"],
+                            use_tr=use_tr)
 
     def energy(self):
         return float(self.e.download(self.lid("E"), 1)[0])
