@@ -72,6 +72,20 @@ struct GemmDesc {
   OpndDesc cmap;  // result operand (map lookups in the epilogue)
 };
 
+// One Ms/IRREP distribution case of a reorder (reo_blk_wmaps_c.f:209-840):
+// for every string tuple i of the unshifted part I0 (space kEx1: C
+// components, then A components) and k of the shifted strings K (space kEx2)
+//   reo[base_reo + addr_reo(i, k)] += alpha * signs * ori[base_ori + addr_ori(i, k)]
+// where both addresses merge I0 and K components through string maps
+// (creators: str1 = I0, str2 = K; annihilators: str1 = K, str2 = I0).
+struct ReoItem {
+  int64_t N0, NK;
+  int64_t base_ori, base_reo;
+  int32_t nsp[2];
+  int32_t rad[2][kDevMaxComp];
+  OpndDesc ori, reo;
+};
+
 // gather of one operand of one block contraction into a dense panel
 // panel[k * R + r] = sign * x[address(r, k)],
 // address(r, k) = roff[r] + koff[k] + sum_m (|map_m[i2 * n1_m + i1]| - 1) * ldim_m

@@ -21,6 +21,15 @@ namespace {
 
 thread_local std::string g_error;
 
+Occ to_occ(const int64_t* o) {
+  Occ r{};
+  for (int k = 0; k < 8; ++k) {
+    GCCU_REQUIRE(o[k] >= 0 && o[k] <= kMaxNel, "occupation out of range");
+    r[k] = (int)o[k];
+  }
+  return r;
+}
+
 #define CUDA_OK(x)                                                                   \
   do {                                                                               \
     cudaError_t e_ = (x);                                                            \
@@ -63,6 +72,14 @@ struct DevPlan {
   double ms = 0, pack_ms = 0;
 };
 
+struct DevReo {
+  ReoPlan plan;
+  ReoItem* d_items = nullptr;
+  int64_t maxlen = 0;
+  int list_ori = 0, list_reo = 0;
+  int64_t reo_off = 0, reo_len = 0;
+};
+
 class Engine {
  public:
   Model model;
@@ -90,6 +107,7 @@ class Engine {
   StaticScratch static_ss;
   std::vector<cudaEvent_t> event_pool;
   std::vector<DevPlan*> plan_order;  // plans in first-use order (profile report)
+  std::map<std::string, std::unique_ptr<DevReo>> reos;  // reorder plans per descriptor
 
   cudaEvent_t get_event() {
     if (!event_pool.empty()) {
@@ -224,6 +242,60 @@ class Engine {
     return flips[key] = upload(m);
   }
 
+  // reorder plan of a descriptor, built on first use
+  DevReo& reo_for(const gccu_reo_desc* r) {
+    GCCU_REQUIRE(r->nshift >= 0 && r->nshift <= kMaxShift, "reorder: nshift must be 0..4");
+    std::ostringstream os;
+    os << r->list_ori << ',' << r->iblk_ori << ',' << r->list_reo << ',' << r->iblk_reo << ','
+       << r->nshift;
+    for (int s = 0; s < r->nshift; ++s) {
+      os << ';' << r->from_vtx[s] << ',' << r->to_vtx[s];
+      for (int k = 0; k < 8; ++k) os << ',' << r->occ_shift[s][k];
+    }
+    auto it = reos.find(os.str());
+    if (it != reos.end()) return *it->second;
+    GCCU_REQUIRE(!capturing, "reorder must be run once before it is captured in a graph");
+    const ListLayout& Lo = list(r->list_ori).L;
+    const ListLayout& Lr = list(r->list_reo).L;
+    const int nj = model.ops.at(Lo.op - 1).nj;
+    GCCU_REQUIRE(model.ops.at(Lr.op - 1).nj == nj, "reorder: operators differ in njoined");
+    GCCU_REQUIRE(r->iblk_ori >= 1 && r->iblk_ori <= (int64_t)Lo.blk.size() && r->iblk_reo >= 1 &&
+                     r->iblk_reo <= (int64_t)Lr.blk.size(),
+                 "reorder: occupation class out of range");
+    ReorderSpec s;
+    s.Lori = &Lo;
+    s.Lreo = &Lr;
+    s.ib_ori = (int)r->iblk_ori;
+    s.ib_reo = (int)r->iblk_reo;
+    s.nj = nj;
+    s.nshift = (int)r->nshift;
+    for (int t = 0; t < s.nshift; ++t) {
+      s.shift[t] = to_occ(r->occ_shift[t]);
+      GCCU_REQUIRE(r->from_vtx[t] >= 1 && r->from_vtx[t] <= nj && r->to_vtx[t] >= 1 &&
+                       r->to_vtx[t] <= nj,
+                   "reorder: vertex out of range");
+      s.from[t] = (int)r->from_vtx[t] - 1;
+      s.to[t] = (int)r->to_vtx[t] - 1;
+    }
+    auto dr = std::make_unique<DevReo>();
+    dr->plan = plan_reorder(model, s);
+    dr->list_ori = (int)r->list_ori;
+    dr->list_reo = (int)r->list_reo;
+    dr->reo_off = Lr.blk[r->iblk_reo - 1].off;
+    dr->reo_len = Lr.blk[r->iblk_reo - 1].len;
+    ReoPlan& P = dr->plan;
+    GCCU_REQUIRE(P.items.size() <= 65535, "reorder: too many distribution cases");
+    for (auto& it2 : P.items) dr->maxlen = std::max(dr->maxlen, it2.N0 * it2.NK);
+    if (!host_only) {
+      for (auto& m : P.maps) {
+        ReoItem& ri = P.items[m.item];
+        (m.opnd == 0 ? ri.ori : ri.reo).map[m.comp] = strmap(m.key);
+      }
+      if (!P.items.empty()) dr->d_items = upload(P.items);
+    }
+    return *(reos[os.str()] = std::move(dr));
+  }
+
   // cached plan of a descriptor, or null; never plans (gccu_contract_noalloc)
   DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
     std::ostringstream os;
@@ -248,6 +320,10 @@ class Engine {
     GCCU_REQUIRE(bc->tra_op1 == 0 && bc->tra_op2 == 0 && bc->tra_res == 0,
                  "transposed operands are not supported by this engine version");
     ContractionSpec s;
+    for (int64_t l : {bc->list_op1, bc->list_op2, bc->list_res})
+      GCCU_REQUIRE(model.ops.at(list(l).L.op - 1).nj == 1,
+                   "contractions of joined (multi-vertex) operators are not supported by this "
+                   "engine version");
     s.L1 = &list(bc->list_op1).L;
     s.L2 = &list(bc->list_op2).L;
     s.L12 = &list(bc->list_res).L;
@@ -664,15 +740,6 @@ int guarded(F&& f) {
   }
 }
 
-Occ to_occ(const int64_t* o) {
-  Occ r{};
-  for (int k = 0; k < 8; ++k) {
-    GCCU_REQUIRE(o[k] >= 0 && o[k] <= kMaxNel, "occupation out of range");
-    r[k] = (int)o[k];
-  }
-  return r;
-}
-
 }  // namespace
 }  // namespace gccu
 
@@ -785,11 +852,18 @@ int gccu_strmap_block(int64_t type, int64_t nel1, int64_t nel2, int64_t idxms1, 
 }
 
 int gccu_define_operator(const int64_t* occ, int64_t nblk, int64_t* op_id) {
+  return gccu_define_operator_joined(occ, 1, nblk, op_id);
+}
+
+int gccu_define_operator_joined(const int64_t* occ, int64_t njoined, int64_t nblk,
+                                int64_t* op_id) {
   return guarded([&] {
     Engine& e = eng();
     GCCU_REQUIRE(nblk >= 1, "operator without occupation classes");
+    GCCU_REQUIRE(njoined >= 1 && njoined <= 8, "njoined must be 1..8");
     Operator op;
-    for (int64_t b = 0; b < nblk; ++b) op.occ.push_back(to_occ(occ + 8 * b));
+    op.nj = (int)njoined;
+    for (int64_t b = 0; b < nblk * njoined; ++b) op.occ.push_back(to_occ(occ + 8 * b));
     e.model.ops.push_back(op);
     *op_id = (int64_t)e.model.ops.size();
   });
@@ -880,6 +954,49 @@ int gccu_zero_list(int64_t list_id) {
 
 int gccu_list_device_ptr(int64_t list_id, void** dptr) {
   return guarded([&] { *dptr = eng().list(list_id).d; });
+}
+
+int gccu_reorder(const gccu_reo_desc* reo, double fac, int64_t sign_reo, int64_t update,
+                 int64_t type_xret, double* xret) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_reorder needs a device");
+    GCCU_REQUIRE(reo, "null reorder descriptor");
+    GCCU_REQUIRE(sign_reo == 1 || sign_reo == -1, "sign_reo must be +1 or -1");
+    GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
+    DevReo& dr = e.reo_for(reo);
+    DevList& lo = e.list(dr.list_ori);
+    DevList& lr = e.list(dr.list_reo);
+    GCCU_REQUIRE(lo.d != lr.d, "reorder: original and reordered list must differ");
+    if (!update)
+      CUDA_OK(cudaMemsetAsync(lr.d + dr.reo_off, 0, dr.reo_len * sizeof(double), e.stream));
+    if (!dr.plan.items.empty()) {
+      launch_reorder(dr.d_items, (int64_t)dr.plan.items.size(), dr.maxlen, lo.d, lr.d,
+                     fac * (double)sign_reo, e.stream);
+      ++e.launches;
+    }
+    CUDA_OK(cudaGetLastError());
+    if (type_xret == 1) {
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+      launch_sumsq(lr.d + dr.reo_off, dr.reo_len, e.d_red, e.stream);
+      ++e.launches;
+      *xret = e.read_red(0);
+    } else if (type_xret == 2) {
+      CUDA_OK(cudaMemcpyAsync(xret, lr.d + dr.reo_off, sizeof(double), cudaMemcpyDeviceToHost,
+                              e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
+  });
+}
+
+int gccu_reorder_info(const gccu_reo_desc* reo, int64_t* ncases, int64_t* nelements) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(reo, "null reorder descriptor");
+    DevReo& dr = e.reo_for(reo);
+    *ncases = (int64_t)dr.plan.items.size();
+    *nelements = dr.plan.elements;
+  });
 }
 
 int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr) {
@@ -1033,7 +1150,7 @@ int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_ou
     GCCU_REQUIRE(iblk_in >= 1 && iblk_in <= (int64_t)a.L.blk.size(), "invalid input class");
     GCCU_REQUIRE(iblk_out >= 1 && iblk_out <= (int64_t)b.L.blk.size(), "invalid output class");
     const LayoutBlock &Bi = a.L.blk[iblk_in - 1], &Bo = b.L.blk[iblk_out - 1];
-    GCCU_REQUIRE(Bi.occ == Bo.occ && Bi.len == Bo.len, "add_opblk: blocks differ in occupation");
+    GCCU_REQUIRE(Bi.vtx == Bo.vtx && Bi.len == Bo.len, "add_opblk: blocks differ in occupation");
     launch_axpy(b.d + Bo.off, a.d + Bi.off, fac, Bo.len, (int)reset, e.stream);
     ++e.launches;
     if (type == 1) {

@@ -14,6 +14,7 @@
 //             tables, so direct operands are read in place from the ME lists.
 #include <cstdio>
 
+#include "index.cuh"
 #include "kernels.hpp"
 
 namespace gccu {
@@ -27,34 +28,6 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
       "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
       : "+d"(d0), "+d"(d1)
       : "d"(a), "d"(b));
-}
-
-__device__ __forceinline__ void decomp(const int32_t* rad, int n, int64_t x, int32_t* comp) {
-  for (int q = 0; q < n; ++q) {
-    int32_t r = rad[q];
-    comp[q] = (int32_t)(x % r);
-    x /= r;
-  }
-}
-
-// address part of the components that merge two spaces (map lookups); cA
-// holds the component indices of space spA, cB those of the other space
-__device__ __forceinline__ bool mapped(const OpndDesc& od, int spA, const int32_t* cA,
-                                       const int32_t* cB, int64_t& off, double& sg) {
-  for (int j = 0; j < od.ncomp; ++j) {
-    const int32_t* mp = od.map[j];
-    if (!mp) continue;
-    int i1 = od.sp1[j] == spA ? cA[od.ci1[j]] : cB[od.ci1[j]];
-    int i2 = od.sp2[j] == spA ? cA[od.ci2[j]] : cB[od.ci2[j]];
-    int v = __ldg(mp + (int64_t)i2 * od.n1[j] + i1);
-    if (v == 0) return false;
-    if (v < 0) {
-      sg = -sg;
-      v = -v;
-    }
-    off += (int64_t)(v - 1) * od.ldim[j];
-  }
-  return true;
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,11 @@ void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cud
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
                  double alpha, cudaStream_t s);
 
+// reorder of a joined operator class (nitems <= 65535 distribution cases,
+// maxlen = largest N0*NK); reo += alpha * signs * ori
+void launch_reorder(const ReoItem* items, int64_t nitems, int64_t maxlen, const double* ori,
+                    double* reo, double alpha, cudaStream_t s);
+
 // out = (reset ? 0 : out) + fac*in  (add_opblk)
 void launch_axpy(double* out, const double* in, double fac, int64_t n, int reset, cudaStream_t s);
 // *acc += sum x^2 over n elements (acc must be zeroed by the caller)

@@ -159,15 +159,19 @@ int Model::graph(int type, int nel) {
   return id;
 }
 
-// condense_occ (operators/condense_occ.f) for one vertex: components in
-// X,P,V,H sequence, creators and annihilators separately
-void Model::condense(const Occ& o, std::vector<Comp>& c, std::vector<Comp>& a) {
+// condense_occ (operators/condense_occ.f:46-62): components in X,P,V,H
+// sequence and, within a type, by vertex; creators and annihilators
+// separately
+void Model::condense(const Occ* vtx, int nj, std::vector<Comp>& c, std::vector<Comp>& a) {
   c.clear();
   a.clear();
   for (int ih = 0; ih < 4; ++ih) {
     int t = kHpvxSeq[ih];
-    if (o[t] > 0) c.push_back({o[t], graph(t, o[t]), t});
-    if (o[4 + t] > 0) a.push_back({o[4 + t], graph(t, o[4 + t]), t});
+    for (int v = 0; v < nj; ++v) {
+      const Occ& o = vtx[v];
+      if (o[t] > 0) c.push_back({o[t], graph(t, o[t]), t, v});
+      if (o[4 + t] > 0) a.push_back({o[4 + t], graph(t, o[4 + t]), t, v});
+    }
   }
 }
 
@@ -290,11 +294,14 @@ void Model::layout(ListLayout& L) {
   const Operator& op = ops.at(L.op - 1);
   int nsym = os.nsym;
   int64_t pos = 0;
-  L.blk.assign(op.occ.size(), LayoutBlock());
-  for (size_t ib = 0; ib < op.occ.size(); ++ib) {
+  L.blk.assign(op.nblk(), LayoutBlock());
+  for (int64_t ib = 0; ib < op.nblk(); ++ib) {
     LayoutBlock& B = L.blk[ib];
-    B.occ = op.occ[ib];
-    condense(B.occ, B.c, B.a);
+    B.vtx.assign(op.occ.begin() + ib * op.nj, op.occ.begin() + (ib + 1) * op.nj);
+    B.occ = Occ{};
+    for (auto& o : B.vtx)
+      for (int k = 0; k < 8; ++k) B.occ[k] += o[k];
+    condense(B.vtx.data(), op.nj, B.c, B.a);
     std::vector<int> oc = comp_occs(B.c), oa = comp_occs(B.a);
     int mscmax = 0, msamax = 0;
     for (int v : oc) mscmax += v;

@@ -8,8 +8,10 @@
 //  * ListLayout: offsets of every (occupation class, Ms(A), IRREP(A),
 //    Ms/IRREP distribution) block of an ME list (operators/set_op_dim2.f).
 //
-// Scope: single-vertex operators (njoined = 1) and one GAS per H/P/V/X type;
-// frozen and deleted orbitals are not part of the string spaces.
+// Scope: operators with one or more vertices (njoined >= 1, condensed as
+// condense_occ does), one GAS per H/P/V/X type, no diagonal or vertex-Ms
+// restrictions; frozen and deleted orbitals are not part of the string
+// spaces.
 #pragma once
 
 #include <array>
@@ -75,6 +77,7 @@ struct Graph {
 // condensed component (cinfo row): occupation, graph id, hpvx type
 struct Comp {
   int occ = 0, graph = 0, hpvx = 0;
+  int vtx = 0;  // vertex of a joined operator the component belongs to
 };
 using Occ = std::array<int, 8>;  // C[H,P,V,X], A[H,P,V,X]
 
@@ -84,7 +87,8 @@ struct Dist {
 };
 
 struct LayoutBlock {
-  Occ occ{};
+  std::vector<Occ> vtx;  // occupation per vertex
+  Occ occ{};             // summed over the vertices
   std::vector<Comp> c, a;
   int64_t off = 0, len = 0;
   // per (idxmsa, gama): offset, length and distributions
@@ -97,7 +101,9 @@ struct LayoutBlock {
 };
 
 struct Operator {
-  std::vector<Occ> occ;
+  int nj = 1;             // vertices per occupation class (njoined)
+  std::vector<Occ> occ;   // nblk * nj entries, the vertices of a class consecutive
+  int64_t nblk() const { return (int64_t)occ.size() / nj; }
 };
 
 struct ListLayout {
@@ -115,7 +121,10 @@ class Model {
 
   int graph(int type, int nel);
   Graph& G(int id) { return *graphs.at(id - 1); }
-  void condense(const Occ& o, std::vector<Comp>& c, std::vector<Comp>& a);
+  void condense(const Occ& o, std::vector<Comp>& c, std::vector<Comp>& a) {
+    condense(&o, 1, c, a);
+  }
+  void condense(const Occ* vtx, int nj, std::vector<Comp>& c, std::vector<Comp>& a);
   void layout(ListLayout& L);
 };
 

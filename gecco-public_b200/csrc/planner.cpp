@@ -408,4 +408,161 @@ Plan plan_contraction(Model& m, const ContractionSpec& s) {
   return P;
 }
 
+namespace {
+
+// Sources of the components of the original (or reordered) class in the
+// unshifted part I0 and in the shifts K (get_reo_info2 / set_mapping_info):
+// component (type t, vertex v) of one side takes the I0 component of type t
+// on vertex v and the K component of type t of the shift that leaves
+// (arrives at) vertex v.
+std::vector<Src> reo_sources(const std::vector<Comp>& tgt, const std::vector<Comp>& i0,
+                             const std::vector<Comp>& k, const int* vtx_of_shift, bool k_first) {
+  std::vector<Src> r(tgt.size());
+  for (size_t j = 0; j < tgt.size(); ++j) {
+    int ii = -1, ik = -1;
+    for (size_t i = 0; i < i0.size(); ++i)
+      if (i0[i].hpvx == tgt[j].hpvx && i0[i].vtx == tgt[j].vtx) ii = (int)i;
+    for (size_t i = 0; i < k.size(); ++i)
+      if (k[i].hpvx == tgt[j].hpvx && vtx_of_shift[k[i].vtx] == tgt[j].vtx) {
+        GCCU_REQUIRE(ik < 0, "reorder: two shifted strings of one type meet on one vertex");
+        ik = (int)i;
+      }
+    GCCU_REQUIRE(ii >= 0 || ik >= 0, "reorder: component without source");
+    r[j].i1 = k_first ? ik : ii;
+    r[j].i2 = k_first ? ii : ik;
+  }
+  return r;
+}
+
+// Ms / IRREP of the unshifted part from the original distribution and the
+// shifts' distribution (split_msgmdis); false if impossible
+bool split_dist(const std::vector<Src>& src, bool k_first, const std::vector<int>& ms,
+                const std::vector<int>& g, const std::vector<int>& msk, const std::vector<int>& gk,
+                const std::vector<Comp>& i0, std::vector<int>& ms0, std::vector<int>& g0) {
+  ms0.assign(i0.size(), 0);
+  g0.assign(i0.size(), 1);
+  for (size_t j = 0; j < src.size(); ++j) {
+    const int ii = k_first ? src[j].i2 : src[j].i1, ik = k_first ? src[j].i1 : src[j].i2;
+    const int mk = ik >= 0 ? msk[ik] : 0, gkk = ik >= 0 ? gk[ik] : 1;
+    if (ii < 0) {
+      if (ms[j] != mk || g[j] != gkk) return false;
+      continue;
+    }
+    ms0[ii] = ms[j] - mk;
+    g0[ii] = irrep_mult(g[j], gkk);
+  }
+  for (size_t i = 0; i < i0.size(); ++i)  // check_ms
+    if (std::abs(ms0[i]) > i0[i].occ || ((i0[i].occ - ms0[i]) & 1)) return false;
+  return true;
+}
+
+}  // namespace
+
+ReoPlan plan_reorder(Model& m, const ReorderSpec& s) {
+  ReoPlan P;
+  const LayoutBlock& Bo = s.Lori->blk.at(s.ib_ori - 1);
+  const LayoutBlock& Br = s.Lreo->blk.at(s.ib_reo - 1);
+  const int nsym = m.os.nsym;
+  GCCU_REQUIRE((int)Bo.vtx.size() == s.nj && (int)Br.vtx.size() == s.nj,
+               "reorder: both classes must have njoined vertices");
+  GCCU_REQUIRE(s.Lori->mst == s.Lreo->mst && s.Lori->gamt == s.Lreo->gamt,
+               "reorder: lists differ in total Ms or IRREP");
+  // I0 per vertex: original minus what leaves, equal to reordered minus what arrives
+  std::vector<Occ> i0v(s.nj);
+  for (int v = 0; v < s.nj; ++v) {
+    for (int q = 0; q < 8; ++q) {
+      int a = Bo.vtx[v][q], b = Br.vtx[v][q];
+      for (int t = 0; t < s.nshift; ++t) {
+        if (s.from[t] == v) a -= s.shift[t][q];
+        if (s.to[t] == v) b -= s.shift[t][q];
+      }
+      GCCU_REQUIRE(a >= 0 && a == b, "reorder: shifts do not connect the two occupation classes");
+      i0v[v][q] = a;
+    }
+  }
+  std::vector<Comp> i0c, i0a, kc, ka;
+  m.condense(i0v.data(), s.nj, i0c, i0a);
+  std::vector<Occ> kv(s.shift, s.shift + s.nshift);
+  m.condense(kv.data(), s.nshift, kc, ka);
+  // creators merge (I0, K), annihilators (K, I0)
+  auto so_c = reo_sources(Bo.c, i0c, kc, s.from, false);
+  auto so_a = reo_sources(Bo.a, i0a, ka, s.from, true);
+  auto sr_c = reo_sources(Br.c, i0c, kc, s.to, false);
+  auto sr_a = reo_sources(Br.a, i0a, ka, s.to, true);
+  const int mskc_max = sum(kc), mska_max = sum(ka), ms0c_max = sum(i0c), ms0a_max = sum(i0a);
+  std::vector<int> okc = comp_occs(kc), oka = comp_occs(ka);
+  for (const auto& kvp : Bo.dis) {
+    const auto key = kvp.first;
+    for (const Dist& d : kvp.second) {
+      int msc = 0, msa = 0, gmc = 1, gma = 1;
+      for (size_t j = 0; j < Bo.c.size(); ++j) msc += d.msc[j], gmc = irrep_mult(gmc, d.gc[j]);
+      for (size_t j = 0; j < Bo.a.size(); ++j) msa += d.msa[j], gma = irrep_mult(gma, d.ga[j]);
+      for (int mska = mska_max; mska >= -mska_max; mska -= 2) {
+        if (std::abs(msa - mska) > ms0a_max) continue;
+        for (int mskc = mskc_max; mskc >= -mskc_max; mskc -= 2) {
+          if (std::abs(msc - mskc) > ms0c_max) continue;
+          for (int gka = 1; gka <= nsym; ++gka)
+            for (int gkc = 1; gkc <= nsym; ++gkc) {
+              MsGam dk;
+              bool first = true;
+              while (next_msgam(first, dk, okc, oka, mskc, mska, gkc, gka, nsym)) {
+                first = false;
+                std::vector<int> ms0c, g0c, ms0a, g0a;
+                if (!split_dist(so_c, false, d.msc, d.gc, dk.msc, dk.gc, i0c, ms0c, g0c)) continue;
+                if (!split_dist(so_a, true, d.msa, d.ga, dk.msa, dk.ga, i0a, ms0a, g0a)) continue;
+                // reordered distribution (merge_msgmdis)
+                std::vector<int> mrc, grc, mra, gra;
+                merge_dist(sr_c, ms0c, g0c, dk.msc, dk.gc, mrc, grc);
+                merge_dist(sr_a, dk.msa, dk.ga, ms0a, g0a, mra, gra);
+                auto ix0c = idxms_of(i0c, ms0c), ix0a = idxms_of(i0a, ms0a);
+                auto ixkc = idxms_of(kc, dk.msc), ixka = idxms_of(ka, dk.msa);
+                auto ixoc = idxms_of(Bo.c, d.msc), ixoa = idxms_of(Bo.a, d.msa);
+                auto ixrc = idxms_of(Br.c, mrc), ixra = idxms_of(Br.a, mra);
+                auto l0c = lengths(m, i0c, ix0c, g0c), l0a = lengths(m, i0a, ix0a, g0a);
+                auto lkc = lengths(m, kc, ixkc, dk.gc), lka = lengths(m, ka, ixka, dk.ga);
+                auto loc = lengths(m, Bo.c, ixoc, d.gc), loa = lengths(m, Bo.a, ixoa, d.ga);
+                auto lrc = lengths(m, Br.c, ixrc, grc), lra = lengths(m, Br.a, ixra, gra);
+                if (has_zero(l0c) || has_zero(l0a) || has_zero(lkc) || has_zero(lka) ||
+                    has_zero(lrc) || has_zero(lra) || has_zero(loc) || has_zero(loa))
+                  continue;
+                const Dist& dr =
+                    find_dist(Br, key.first, key.second, dist_id(Br.c, ixrc, grc, Br.a, ixra, gra, nsym));
+                ReoItem it{};
+                it.N0 = it.NK = 1;
+                it.nsp[0] = (int)(i0c.size() + i0a.size());
+                it.nsp[1] = (int)(kc.size() + ka.size());
+                GCCU_REQUIRE(it.nsp[0] <= kDevMaxComp && it.nsp[1] <= kDevMaxComp,
+                             "reorder: too many string components");
+                int q = 0;
+                for (auto x : l0c) it.rad[0][q++] = (int32_t)x, it.N0 *= x;
+                for (auto x : l0a) it.rad[0][q++] = (int32_t)x, it.N0 *= x;
+                q = 0;
+                for (auto x : lkc) it.rad[1][q++] = (int32_t)x, it.NK *= x;
+                for (auto x : lka) it.rad[1][q++] = (int32_t)x, it.NK *= x;
+                it.base_ori = d.off;
+                it.base_reo = dr.off;
+                const int item = (int)P.items.size();
+                const int nc0 = (int)i0c.size(), nck = (int)kc.size();
+                Side s0c{&i0c, kEx1, 0, &ix0c, &g0c, &l0c}, s0a{&i0a, kEx1, nc0, &ix0a, &g0a, &l0a};
+                Side skc{&kc, kEx2, 0, &ixkc, &dk.gc, &lkc}, ska{&ka, kEx2, nck, &ixka, &dk.ga, &lka};
+                std::vector<int64_t> ldc, lda;
+                int pos = 0;
+                leading_dims(Bo.c, Bo.a, loc, loa, ldc, lda);
+                fill_opnd(it.ori, pos, so_c, s0c, skc, ldc, item, 0, P.maps);
+                fill_opnd(it.ori, pos, so_a, ska, s0a, lda, item, 0, P.maps);
+                pos = 0;
+                leading_dims(Br.c, Br.a, lrc, lra, ldc, lda);
+                fill_opnd(it.reo, pos, sr_c, s0c, skc, ldc, item, 1, P.maps);
+                fill_opnd(it.reo, pos, sr_a, ska, s0a, lda, item, 1, P.maps);
+                P.elements += it.N0 * it.NK;
+                P.items.push_back(it);
+              }
+            }
+        }
+      }
+    }
+  }
+  return P;
+}
+
 }  // namespace gccu

@@ -38,4 +38,26 @@ struct ContractionSpec {
 
 Plan plan_contraction(Model& m, const ContractionSpec& s);
 
+// Reorder of one occupation class of a joined operator into another
+// (reo_op_wmaps_c / reo_blk_wmaps_c): the strings K (nshift shifts, each
+// moving from vertex from[s] of the original to vertex to[s] of the
+// reordered class) change vertex, the rest I0 stays.
+constexpr int kMaxShift = 4;
+struct ReorderSpec {
+  const ListLayout *Lori, *Lreo;
+  int ib_ori, ib_reo;
+  int nj;
+  int nshift;
+  Occ shift[kMaxShift];
+  int from[kMaxShift], to[kMaxShift];  // 0-based vertices
+};
+
+struct ReoPlan {
+  std::vector<ReoItem> items;
+  std::vector<MapRef> maps;  // opnd 0 = original, 1 = reordered
+  int64_t elements = 0;      // sum of N0*NK
+};
+
+ReoPlan plan_reorder(Model& m, const ReorderSpec& s);
+
 }  // namespace gccu

@@ -29,6 +29,12 @@ class BcDesc(ctypes.Structure):
                 ("occ_cnt", I64 * 8)]
 
 
+class ReoDesc(ctypes.Structure):
+    _fields_ = [("list_ori", I64), ("iblk_ori", I64), ("list_reo", I64), ("iblk_reo", I64),
+                ("nshift", I64), ("occ_shift", (I64 * 8) * 4), ("from_vtx", I64 * 4),
+                ("to_vtx", I64 * 4)]
+
+
 class GccuError(RuntimeError):
     pass
 
@@ -45,6 +51,9 @@ _SIGS = {
     "gccu_graph_strings": [I64, I64, I64, I64, P64, P64, I64, P64],
     "gccu_strmap_block": [I64, I64, I64, I64, I64, I64, I64, P64, I64],
     "gccu_define_operator": [P64, I64, P64],
+    "gccu_define_operator_joined": [P64, I64, I64, P64],
+    "gccu_reorder": [ctypes.POINTER(ReoDesc), ctypes.c_double, I64, I64, I64, PD],
+    "gccu_reorder_info": [ctypes.POINTER(ReoDesc), P64, P64],
     "gccu_register_list": [I64, I64, I64, I64, P64, P64],
     "gccu_list_block": [I64, I64, P64, P64],
     "gccu_list_dists": [I64, P64, I64, P64],
@@ -196,6 +205,42 @@ class Engine:
         r = np.zeros(1, np.int64)
         _call("gccu_define_operator", _p64(o), o.shape[0], _p64(r))
         return int(r[0])
+
+    def define_operator_joined(self, occs, njoined):
+        """joined operator: occs has nblk*njoined occupations, the vertices of
+        a class consecutive"""
+        o = np.ascontiguousarray(np.asarray(occs, dtype=np.int64).reshape(-1, 8))
+        assert o.shape[0] % njoined == 0
+        r = np.zeros(1, np.int64)
+        _call("gccu_define_operator_joined", _p64(o), njoined, o.shape[0] // njoined, _p64(r))
+        return int(r[0])
+
+    @staticmethod
+    def reo_desc(ori, reo, shifts):
+        """ori/reo = (list, iblk); shifts = [(occ8, from_vtx, to_vtx), ...] (1-based)"""
+        d = ReoDesc()
+        d.list_ori, d.iblk_ori = ori
+        d.list_reo, d.iblk_reo = reo
+        d.nshift = len(shifts)
+        for s, (occ, fr, to) in enumerate(shifts):
+            for k, v in enumerate(np.asarray(occ).reshape(8)):
+                d.occ_shift[s][k] = int(v)
+            d.from_vtx[s] = fr
+            d.to_vtx[s] = to
+        return d
+
+    def reorder(self, ori, reo, shifts, fac=1.0, sign_reo=1, update=True, xret=0):
+        d = self.reo_desc(ori, reo, shifts)
+        r = np.zeros(1)
+        _call("gccu_reorder", ctypes.byref(d), fac, sign_reo, int(update), xret, _pd(r))
+        return float(r[0])
+
+    def reorder_info(self, ori, reo, shifts):
+        d = self.reo_desc(ori, reo, shifts)
+        n = np.zeros(1, np.int64)
+        m = np.zeros(1, np.int64)
+        _call("gccu_reorder_info", ctypes.byref(d), _p64(n), _p64(m))
+        return int(n[0]), int(m[0])
 
     def register_list(self, op, gamt=1, mst=0, absym=0):
         lid = np.zeros(1, np.int64)

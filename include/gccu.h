@@ -65,6 +65,15 @@ int gccu_strmap_block(int64_t type, int64_t nel1, int64_t nel2, int64_t idxms1,
  * replaces: operator definition (include/def_operator.h) + set_op_dim2
  * (operators/set_op_dim2.f:1-531).  occ: nblk occupation classes. */
 int gccu_define_operator(const int64_t* occ, int64_t nblk, int64_t* op_id);
+/* joined (multi-vertex) operator, op%njoined > 1 (include/def_operator.h):
+ * occ holds nblk*njoined occupations, the njoined vertices of a class
+ * consecutive (the reference's ihpvca_occ(ngastp,2,njoined*nblk)); ME lists
+ * of it are laid out over the condensed components of all vertices
+ * (operators/condense_occ.f, operators/set_op_dim2.f). Such lists can be
+ * reordered, added and transferred; gccu_contract takes single-vertex
+ * operands only in this engine version. */
+int gccu_define_operator_joined(const int64_t* occ, int64_t njoined, int64_t nblk,
+                                int64_t* op_id);
 /* ME list of an operator with total irrep gamt, total 2*Ms mst and spin-flip
  * symmetry absym (0,+1,-1); its data live in device memory for the whole
  * solve (include/def_me_list.h:37-115).  Returns handle and len_op. */
@@ -130,6 +139,31 @@ int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, doub
  * and leaves its contents behind; calls that overlap in time (from other
  * host threads or on other streams) race on it. */
 int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr);
+
+/* ---- [REORDER] ------------------------------------------------------------------
+ * replaces: fs_reo_drv -> reo_op_wmaps_c -> reo_blk_wmaps_c
+ * (contract/fs_reo_drv.f:166-173, contract/reo_op_wmaps_c.f,
+ * contract/reo_blk_wmaps_c.f:2-854).  Occupation class iblk_ori of list_ori
+ * is reordered into class iblk_reo of list_reo; both operators have the same
+ * njoined.  Shift s (s < nshift <= 4), with occupation occ_shift[s] (layout as
+ * in gccu_bc_desc), leaves vertex from_vtx[s] (1-based) of the original class
+ * and arrives at vertex to_vtx[s] of the reordered one (the reference's
+ * reorder occ_shift / from_vtx / to_vtx); all other strings keep their
+ * vertex.  reo = (update ? reo : 0) + fac*sign_reo*(map signs)*ori, summed
+ * over every way of splitting the merged strings; sign_reo is the formula's
+ * reorder sign (contract/sign_reo.f, passed on by get_reo_info2.f:326).
+ * type_xret as for gccu_contract, for the reordered class. */
+typedef struct gccu_reo_desc {
+  int64_t list_ori, iblk_ori;
+  int64_t list_reo, iblk_reo;
+  int64_t nshift;
+  int64_t occ_shift[4][8];
+  int64_t from_vtx[4], to_vtx[4];
+} gccu_reo_desc;
+int gccu_reorder(const gccu_reo_desc* reo, double fac, int64_t sign_reo, int64_t update,
+                 int64_t type_xret, double* xret);
+/* number of distribution cases and elements the engine plans for a reorder */
+int gccu_reorder_info(const gccu_reo_desc* reo, int64_t* ncases, int64_t* nelements);
 
 /* ---- [ADD] -------------------------------------------------------------------
  * replaces: add_opblk (contract/add_opblk.f:2-313), in-core branch

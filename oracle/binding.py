@@ -41,6 +41,10 @@ def lib():
         L.ora_strmap_block.argtypes = [ctypes.c_void_p] + [I64] * 7 + [P64]
         L.ora_define_op.restype = I64
         L.ora_define_op.argtypes = [ctypes.c_void_p, P64, I64]
+        L.ora_define_op_joined.restype = I64
+        L.ora_define_op_joined.argtypes = [ctypes.c_void_p, P64, I64, I64]
+        L.ora_reorder.argtypes = [ctypes.c_void_p, I64, I64, PD, I64, I64, PD, I64, P64, P64,
+                                  P64, ctypes.c_double, I64, I64]
         L.ora_define_list.restype = I64
         L.ora_define_list.argtypes = [ctypes.c_void_p, I64, I64, I64, I64, P64]
         L.ora_list_block.restype = ctypes.c_int
@@ -120,6 +124,25 @@ class Oracle:
     def define_op(self, occ):
         occ = np.ascontiguousarray(np.asarray(occ, dtype=np.int64).reshape(-1, 8))
         return _chk(lib().ora_define_op(self.ctx, _p64(occ), occ.shape[0]))
+
+    def define_op_joined(self, occ, nj):
+        occ = np.ascontiguousarray(np.asarray(occ, dtype=np.int64).reshape(-1, 8))
+        assert occ.shape[0] % nj == 0
+        return _chk(lib().ora_define_op_joined(self.ctx, _p64(occ), nj, occ.shape[0] // nj))
+
+    def reorder(self, lori, bori, xori, lreo, breo, xreo, shifts, fac=1.0, sign_reo=1,
+                update=True):
+        """reo_op_wmaps_c: shifts = [(occ8, from_vtx, to_vtx), ...] (1-based);
+        xreo (the whole reordered list) is updated in place"""
+        n = len(shifts)
+        occ = np.zeros((max(n, 1), 8), dtype=np.int64)
+        fr = np.zeros(max(n, 1), dtype=np.int64)
+        to = np.zeros(max(n, 1), dtype=np.int64)
+        for s, (o, f, t) in enumerate(shifts):
+            occ[s] = np.asarray(o).reshape(8)
+            fr[s], to[s] = f, t
+        _chk(lib().ora_reorder(self.ctx, lori, bori, _pd(xori), lreo, breo, _pd(xreo), n,
+                               _p64(occ), _p64(fr), _p64(to), fac, sign_reo, int(update)))
 
     def define_list(self, op, gamt=1, mst=0, absym=0):
         ln = np.zeros(1, dtype=np.int64)

@@ -301,6 +301,7 @@ int std_spsign_msdis(const std::vector<int>& msdis, const std::vector<int>& occ)
 
 struct Comp {  // one row of a cinfo array (occupation, graph, hpvx)
   int occ, graph, hpvx;
+  int vtx = 0;  // vertex of a joined operator (or shift index of a reorder)
 };
 
 struct DistRow {
@@ -317,7 +318,8 @@ struct ListBlock {
 };
 
 struct Op {
-  std::vector<std::array<int, 8>> occ;  // C[H,P,V,X], A[H,P,V,X]
+  int nj = 1;                            // njoined
+  std::vector<std::array<int, 8>> occ;  // C[H,P,V,X], A[H,P,V,X]; nblk*nj, vertices consecutive
 };
 
 struct List {
@@ -417,16 +419,23 @@ struct ora_ctx {
 
 namespace {
 
-// condense_occ (operators/condense_occ.f), njoined = 1: components in
-// X,P,V,H order, C and A separately
-void condense(ora_ctx* cx, const int* occ8, std::vector<Comp>& c, std::vector<Comp>& a) {
+// condense_occ (operators/condense_occ.f:46-62): loop over the hpvx
+// sequence X,P,V,H, inside it over the vertices; C and A separately
+void condense_n(ora_ctx* cx, const int* occ, int nj, std::vector<Comp>& c,
+                std::vector<Comp>& a) {
   c.clear();
   a.clear();
   for (int ih = 0; ih < 4; ++ih) {
     int t = HPVXSEQ[ih];
-    if (occ8[t] > 0) c.push_back({occ8[t], cx->graph(t, occ8[t]), t});
-    if (occ8[4 + t] > 0) a.push_back({occ8[4 + t], cx->graph(t, occ8[4 + t]), t});
+    for (int v = 0; v < nj; ++v) {
+      const int* o = occ + 8 * v;
+      if (o[t] > 0) c.push_back({o[t], cx->graph(t, o[t]), t, v});
+      if (o[4 + t] > 0) a.push_back({o[4 + t], cx->graph(t, o[4 + t]), t, v});
+    }
   }
+}
+void condense(ora_ctx* cx, const int* occ8, std::vector<Comp>& c, std::vector<Comp>& a) {
+  condense_n(cx, occ8, 1, c, a);
 }
 
 // ---- Ms / IRREP distributions (operators/next_msgamdist2.f) ----
@@ -557,15 +566,17 @@ int msa2idxms4op(int msa, int mst, int occ_a, int occ_c) {
   return r;
 }
 
-// set_op_dim2 (operators/set_op_dim2.f:1-531), njoined = 1, no diag_type
+// set_op_dim2 (operators/set_op_dim2.f:1-531), no diag_type, no fixed
+// vertex Ms; joined operators through their condensed components
 void set_op_dim2(ora_ctx* cx, List& L) {
   const Op& op = cx->ops[L.op - 1];
   int nsym = cx->oi.nsym;
   int64_t idxstr = 0;
-  L.blk.assign(op.occ.size(), ListBlock());
-  for (size_t ib = 0; ib < op.occ.size(); ++ib) {
+  const size_t nblk = op.occ.size() / op.nj;
+  L.blk.assign(nblk, ListBlock());
+  for (size_t ib = 0; ib < nblk; ++ib) {
     ListBlock& B = L.blk[ib];
-    condense(cx, op.occ[ib].data(), B.c, B.a);
+    condense_n(cx, op.occ[ib * op.nj].data(), op.nj, B.c, B.a);
     int msc_max = 0, msa_max = 0;
     for (auto& x : B.c) msc_max += x.occ;
     for (auto& x : B.a) msa_max += x.occ;
@@ -1075,6 +1086,9 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
               int64_t str_block, int64_t cnt_block, double* xret, Stats* st) {
   const List &L1 = cx->lists[l1 - 1], &L2 = cx->lists[l2 - 1];
   List& L12 = cx->lists[l12 - 1];
+  CHECK(cx->ops[L1.op - 1].nj == 1 && cx->ops[L2.op - 1].nj == 1 &&
+            (ib12 == 0 || cx->ops[L12.op - 1].nj == 1),
+        "contract: joined operators are not restated");
   const ListBlock &B1 = L1.blk[ib1 - 1], &B2 = L2.blk[ib2 - 1];
   int nsym = cx->oi.nsym;
   // occupations of the operators
@@ -1309,6 +1323,269 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
 
 // sym_ab_blk (contract/sym_ab_blk.f:2-405): x(idx1) and its spin-flipped
 // partner x(idx2) both become prefac*(x1 + s*x2) (resp. times s)
+// ---- reorder (contract/reo_op_wmaps_c.f, contract/reo_blk_wmaps_c.f) ----
+
+// map_info_to_ori / map_info_to_reo (get_reo_info2): for each component of
+// one side of the operator, the I0 component on the same vertex and the
+// shifted component (type t) leaving/arriving at that vertex; -1 if none
+struct ReoSrc {
+  int i0 = -1, k = -1;
+};
+std::vector<ReoSrc> reo_map_info(const std::vector<Comp>& tgt, const std::vector<Comp>& i0,
+                                 const std::vector<Comp>& k, const int* vtx_of_shift) {
+  std::vector<ReoSrc> r(tgt.size());
+  for (size_t j = 0; j < tgt.size(); ++j) {
+    for (size_t i = 0; i < i0.size(); ++i)
+      if (i0[i].hpvx == tgt[j].hpvx && i0[i].vtx == tgt[j].vtx) r[j].i0 = (int)i;
+    for (size_t i = 0; i < k.size(); ++i)
+      if (k[i].hpvx == tgt[j].hpvx && vtx_of_shift[k[i].vtx] == tgt[j].vtx) {
+        CHECK(r[j].k < 0, "reorder: two shifted strings of one type on one vertex");
+        r[j].k = (int)i;
+      }
+    CHECK(r[j].i0 >= 0 || r[j].k >= 0, "reorder: component without source");
+  }
+  return r;
+}
+
+// string map of one component (get_strmap_blk_c): str1/str2 as given, the
+// trivial map when one of the two is absent
+struct CompMap {
+  const std::vector<int>* m = nullptr;  // null: identity
+  int64_t n1 = 1;
+};
+
+// reo_blk_wmaps_c (contract/reo_blk_wmaps_c.f:2-854) for one distribution of
+// the original class, xo = that distribution's elements
+void reo_blk(ora_ctx* cx, double fac, double* xreo, const double* xo, int sign_reo,
+             int ms_op_c, int ms_op_a, int gm_op_c, int gm_op_a,
+             const std::vector<int>& ms_i_c, const std::vector<int>& ms_i_a,
+             const std::vector<int>& gm_i_c, const std::vector<int>& gm_i_a,
+             const ListBlock& Bo, const ListBlock& Br, const std::vector<Comp>& kc,
+             const std::vector<Comp>& ka, const std::vector<Comp>& i0c,
+             const std::vector<Comp>& i0a, const std::vector<ReoSrc>& to_ori_c,
+             const std::vector<ReoSrc>& to_ori_a, const std::vector<ReoSrc>& to_reo_c,
+             const std::vector<ReoSrc>& to_reo_a, int idxms_op_a, int nsym) {
+  int ms_k_c_max = 0, ms_k_a_max = 0, ms_i0_c_max = 0, ms_i0_a_max = 0;
+  for (auto& x : kc) ms_k_c_max += x.occ;
+  for (auto& x : ka) ms_k_a_max += x.occ;
+  for (auto& x : i0c) ms_i0_c_max += x.occ;
+  for (auto& x : i0a) ms_i0_a_max += x.occ;
+  for (int ms_k_a = ms_k_a_max; ms_k_a >= -ms_k_a_max; ms_k_a -= 2) {
+    if (std::abs(ms_op_a - ms_k_a) > ms_i0_a_max) continue;
+    for (int ms_k_c = ms_k_c_max; ms_k_c >= -ms_k_c_max; ms_k_c -= 2) {
+      if (std::abs(ms_op_c - ms_k_c) > ms_i0_c_max) continue;
+      for (int gm_k_a = 1; gm_k_a <= nsym; ++gm_k_a) {
+        for (int gm_k_c = 1; gm_k_c <= nsym; ++gm_k_c) {
+          MsGamDist dk;
+          bool first = true;
+          while (next_msgamdist2(first, dk, occs(kc), occs(ka), ms_k_c, ms_k_a, gm_k_c, gm_k_a,
+                                 nsym)) {
+            first = false;
+            // split_msgmdis: I0 = I - K, component by component
+            std::vector<int> ms0c(i0c.size()), g0c(i0c.size()), ms0a(i0a.size()),
+                g0a(i0a.size());
+            bool possible = true;
+            auto split = [&](const std::vector<ReoSrc>& src, const std::vector<int>& ms,
+                             const std::vector<int>& gm, const std::vector<int>& msk,
+                             const std::vector<int>& gmk, std::vector<int>& ms0,
+                             std::vector<int>& g0) {
+              for (size_t j = 0; j < src.size(); ++j) {
+                int mk = src[j].k >= 0 ? msk[src[j].k] : 0;
+                int gk = src[j].k >= 0 ? gmk[src[j].k] : 1;
+                if (src[j].i0 < 0) {
+                  if (ms[j] != mk || gm[j] != gk) possible = false;
+                  continue;
+                }
+                ms0[src[j].i0] = ms[j] - mk;
+                g0[src[j].i0] = mult(gm[j], gk);
+              }
+            };
+            split(to_ori_c, ms_i_c, gm_i_c, dk.msc, dk.gc, ms0c, g0c);
+            split(to_ori_a, ms_i_a, gm_i_a, dk.msa, dk.ga, ms0a, g0a);
+            if (!possible) continue;
+            bool okms = true;  // check_ms
+            for (size_t i = 0; i < i0c.size(); ++i)
+              if (std::abs(ms0c[i]) > i0c[i].occ || ((i0c[i].occ - ms0c[i]) & 1)) okms = false;
+            for (size_t i = 0; i < i0a.size(); ++i)
+              if (std::abs(ms0a[i]) > i0a[i].occ || ((i0a[i].occ - ms0a[i]) & 1)) okms = false;
+            if (!okms) continue;
+            // merge_msgmdis: distribution of the reordered class
+            auto merge = [](const std::vector<ReoSrc>& src, const std::vector<int>& ms0,
+                            const std::vector<int>& g0, const std::vector<int>& msk,
+                            const std::vector<int>& gk, std::vector<int>& ms,
+                            std::vector<int>& gm) {
+              ms.assign(src.size(), 0);
+              gm.assign(src.size(), 1);
+              for (size_t j = 0; j < src.size(); ++j) {
+                if (src[j].i0 >= 0) ms[j] += ms0[src[j].i0], gm[j] = mult(gm[j], g0[src[j].i0]);
+                if (src[j].k >= 0) ms[j] += msk[src[j].k], gm[j] = mult(gm[j], gk[src[j].k]);
+              }
+            };
+            std::vector<int> msrc, gmrc, msra, gmra;
+            merge(to_reo_c, ms0c, g0c, dk.msc, dk.gc, msrc, gmrc);
+            merge(to_reo_a, ms0a, g0a, dk.msa, dk.ga, msra, gmra);
+            auto ixkc = ixms(kc, dk.msc), ixka = ixms(ka, dk.msa);
+            auto ix0c = ixms(i0c, ms0c), ix0a = ixms(i0a, ms0a);
+            auto ixrc = ixms(Br.c, msrc), ixra = ixms(Br.a, msra);
+            auto ixoc = ixms(Bo.c, ms_i_c), ixoa = ixms(Bo.a, ms_i_a);
+            auto lkc = lens(cx, kc, ixkc, dk.gc), lka = lens(cx, ka, ixka, dk.ga);
+            auto l0c = lens(cx, i0c, ix0c, g0c), l0a = lens(cx, i0a, ix0a, g0a);
+            auto lrc = lens(cx, Br.c, ixrc, gmrc), lra = lens(cx, Br.a, ixra, gmra);
+            auto loc = lens(cx, Bo.c, ixoc, gm_i_c), loa = lens(cx, Bo.a, ixoa, gm_i_a);
+            if (anyzero(lkc) || anyzero(lka) || anyzero(l0c) || anyzero(l0a) || anyzero(lrc) ||
+                anyzero(lra))
+              continue;
+            // set_op_ldim_c of both classes
+            std::vector<int64_t> lso(loc), lsr(lrc), ldoc, ldoa, ldrc, ldra;
+            lso.insert(lso.end(), loa.begin(), loa.end());
+            lsr.insert(lsr.end(), lra.begin(), lra.end());
+            ldims(Bo.c, Bo.a, lso, ldoc, ldoa);
+            ldims(Br.c, Br.a, lsr, ldrc, ldra);
+            // maps: creators (I0, K), annihilators (K, I0)
+            auto maps = [&](const std::vector<ReoSrc>& src, bool cside, std::vector<CompMap>& out) {
+              out.assign(src.size(), CompMap());
+              for (size_t j = 0; j < src.size(); ++j) {
+                const ReoSrc& s = src[j];
+                if (s.i0 < 0 || s.k < 0) {
+                  out[j].n1 = 1;
+                  continue;
+                }
+                if (cside) {
+                  out[j].m = &cx->strmap(i0c[s.i0].graph, kc[s.k].graph, ix0c[s.i0], ixkc[s.k],
+                                         g0c[s.i0], dk.gc[s.k]);
+                  out[j].n1 = l0c[s.i0];
+                } else {
+                  out[j].m = &cx->strmap(ka[s.k].graph, i0a[s.i0].graph, ixka[s.k], ix0a[s.i0],
+                                         dk.ga[s.k], g0a[s.i0]);
+                  out[j].n1 = lka[s.k];
+                }
+              }
+            };
+            std::vector<CompMap> m_ori_c, m_ori_a, m_reo_c, m_reo_a;
+            maps(to_ori_c, true, m_ori_c);
+            maps(to_ori_a, false, m_ori_a);
+            maps(to_reo_c, true, m_reo_c);
+            maps(to_reo_a, false, m_reo_a);
+            // offset of the reordered distribution (idx_msgmdst2 -> d_gam_ms)
+            int64_t did = msgmdid2(Br.c, ixrc, gmrc, Br.a, ixra, gmra, nsym);
+            const auto& dl = Br.dis.at({idxms_op_a, gm_op_a});
+            const int64_t idx00opreo = dl[find_dis(Br, idxms_op_a, gm_op_a, did)].off;
+            // element loops: K(A), I0(A), K(C), I0(C)
+            const int64_t nka = [&] { int64_t n = 1; for (auto x : lka) n *= x; return n; }();
+            const int64_t n0a = [&] { int64_t n = 1; for (auto x : l0a) n *= x; return n; }();
+            const int64_t nkc = [&] { int64_t n = 1; for (auto x : lkc) n *= x; return n; }();
+            const int64_t n0c = [&] { int64_t n = 1; for (auto x : l0c) n *= x; return n; }();
+            std::vector<int64_t> ska(ka.size()), s0a(i0a.size()), skc(kc.size()), s0c(i0c.size());
+            // string index of each target component from its sources (1-based map
+            // entry index: (str2-1)*n1 + str1)
+            auto elem = [](const std::vector<ReoSrc>& src, const std::vector<CompMap>& mp,
+                           const std::vector<int64_t>& ldim, bool cside,
+                           const std::vector<int64_t>& s0, const std::vector<int64_t>& sk,
+                           int64_t& idx, int& sgn) {
+              for (size_t j = 0; j < src.size(); ++j) {
+                int64_t i0s = src[j].i0 >= 0 ? s0[src[j].i0] : 0;
+                int64_t ks = src[j].k >= 0 ? sk[src[j].k] : 0;
+                int64_t el;
+                if (!mp[j].m) {
+                  el = (src[j].i0 >= 0 ? i0s : ks) + 1;
+                } else {
+                  int64_t i1 = cside ? i0s : ks, i2 = cside ? ks : i0s;
+                  el = (*mp[j].m)[i2 * mp[j].n1 + i1];
+                  if (el == 0) return false;
+                  if (el < 0) sgn = -sgn, el = -el;
+                }
+                idx += (el - 1) * ldim[j];
+              }
+              return true;
+            };
+            for (int64_t ika = 0; ika < nka; ++ika) {
+              decompose(ika, lka, ska.data());
+              for (int64_t i0a_ = 0; i0a_ < n0a; ++i0a_) {
+                decompose(i0a_, l0a, s0a.data());
+                int64_t io_a = 0, ir_a = 0;
+                int sgna = sign_reo;
+                if (!elem(to_ori_a, m_ori_a, ldoa, false, s0a, ska, io_a, sgna)) continue;
+                if (!elem(to_reo_a, m_reo_a, ldra, false, s0a, ska, ir_a, sgna)) continue;
+                for (int64_t ikc = 0; ikc < nkc; ++ikc) {
+                  decompose(ikc, lkc, skc.data());
+                  for (int64_t i0c_ = 0; i0c_ < n0c; ++i0c_) {
+                    decompose(i0c_, l0c, s0c.data());
+                    int64_t io = io_a, ir = ir_a;
+                    int sgnt = sgna;
+                    if (!elem(to_ori_c, m_ori_c, ldoc, true, s0c, skc, io, sgnt)) continue;
+                    if (!elem(to_reo_c, m_reo_c, ldrc, true, s0c, skc, ir, sgnt)) continue;
+                    xreo[idx00opreo + ir] += fac * (double)sgnt * xo[io];
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// reo_op_wmaps_c (contract/reo_op_wmaps_c.f): loop over Ms(A), IRREP(A) and
+// the distributions of the original class, reo_blk_wmaps_c for each
+void reorder(ora_ctx* cx, int lori, int ibori, const double* xori, int lreo, int ibreo,
+             double* xreo, int nshift, const int* occ_shift, const int* from, const int* to,
+             double fac, int sign_reo, bool update) {
+  const List& Lo = cx->lists.at(lori - 1);
+  const List& Lr = cx->lists.at(lreo - 1);
+  const Op& Oo = cx->ops[Lo.op - 1];
+  const Op& Or = cx->ops[Lr.op - 1];
+  CHECK(Oo.nj == Or.nj, "reorder: njoined differs");
+  CHECK(Lo.mst == Lr.mst && Lo.gamt == Lr.gamt, "reorder: inconsistent MS or symmetry");
+  const int nj = Oo.nj, nsym = cx->oi.nsym;
+  const ListBlock& Bo = Lo.blk.at(ibori - 1);
+  const ListBlock& Br = Lr.blk.at(ibreo - 1);
+  // I0 (occ_op0) per vertex
+  std::vector<int> i0(8 * nj);
+  for (int v = 0; v < nj; ++v)
+    for (int q = 0; q < 8; ++q) {
+      int a = Oo.occ[(ibori - 1) * nj + v][q], b = Or.occ[(ibreo - 1) * nj + v][q];
+      for (int s = 0; s < nshift; ++s) {
+        if (from[s] == v) a -= occ_shift[8 * s + q];
+        if (to[s] == v) b -= occ_shift[8 * s + q];
+      }
+      CHECK(a >= 0 && a == b, "reorder: shifts do not connect the classes");
+      i0[8 * v + q] = a;
+    }
+  std::vector<Comp> i0c, i0a, kc, ka;
+  condense_n(cx, i0.data(), nj, i0c, i0a);
+  condense_n(cx, occ_shift, nshift, kc, ka);
+  auto to_ori_c = reo_map_info(Bo.c, i0c, kc, from), to_ori_a = reo_map_info(Bo.a, i0a, ka, from);
+  auto to_reo_c = reo_map_info(Br.c, i0c, kc, to), to_reo_a = reo_map_info(Br.a, i0a, ka, to);
+  if (!update)
+    for (int64_t i = 0; i < Br.len_occ; ++i) xreo[Br.off_occ + i] = 0.0;
+  int msc_max = 0, msa_max = 0;
+  for (auto& x : Bo.c) msc_max += x.occ;
+  for (auto& x : Bo.a) msa_max += x.occ;
+  for (int msa = msa_max; msa >= -msa_max; msa -= 2) {
+    int msc = msa + Lo.mst;
+    if (std::abs(msc) > msc_max) continue;
+    int idxms = msa2idxms4op(msa, Lo.mst, msa_max, msc_max);
+    for (int gama = 1; gama <= nsym; ++gama) {
+      int gamc = mult(gama, Lo.gamt);
+      MsGamDist d;
+      bool first = true;
+      while (next_msgamdist2(first, d, occs(Bo.c), occs(Bo.a), msc, msa, gamc, gama, nsym)) {
+        first = false;
+        auto ixc = ixms(Bo.c, d.msc), ixa = ixms(Bo.a, d.msa);
+        auto lc = lens(cx, Bo.c, ixc, d.gc), la = lens(cx, Bo.a, ixa, d.ga);
+        if (anyzero(lc) || anyzero(la)) continue;
+        int64_t did = msgmdid2(Bo.c, ixc, d.gc, Bo.a, ixa, d.ga, nsym);
+        const auto& dl = Bo.dis.at({idxms, gama});
+        const int64_t off = dl[find_dis(Bo, idxms, gama, did)].off;
+        reo_blk(cx, fac, xreo, xori + off, sign_reo, msc, msa, gamc, gama, d.msc, d.msa, d.gc,
+                d.ga, Bo, Br, kc, ka, i0c, i0a, to_ori_c, to_ori_a, to_reo_c, to_reo_a, idxms,
+                nsym);
+      }
+    }
+  }
+}
+
 void sym_ab_blk(ora_ctx* cx, List& L, int iblk, double* buf, double prefac, double relfac) {
   CHECK(L.mst == 0, "sym_ab_blk: mst must be 0");
   ListBlock& B = L.blk[iblk - 1];
@@ -1454,9 +1731,15 @@ int64_t ora_strmap_block(ora_ctx* c, int64_t type, int64_t nel1, int64_t nel2, i
 }
 
 int64_t ora_define_op(ora_ctx* c, const int64_t* occ, int64_t nblk) {
+  return ora_define_op_joined(c, occ, 1, nblk);
+}
+
+int64_t ora_define_op_joined(ora_ctx* c, const int64_t* occ, int64_t nj, int64_t nblk) {
   GUARD_BEGIN
+  CHECK(nj >= 1 && nj <= 8, "njoined must be 1..8");
   Op op;
-  for (int64_t b = 0; b < nblk; ++b) {
+  op.nj = (int)nj;
+  for (int64_t b = 0; b < nblk * nj; ++b) {
     std::array<int, 8> o;
     for (int k = 0; k < 8; ++k) o[k] = (int)occ[b * 8 + k];
     op.occ.push_back(o);
@@ -1534,6 +1817,24 @@ int ora_contract(ora_ctx* c, int64_t route, int64_t list1, int64_t iblk1, const 
            str_block > 0 ? str_block : 200, cnt_block, xret, &st);
   if (stats)
     for (int k = 0; k < 8; ++k) stats[k] += st.v[k];
+  return 0;
+  GUARD_END(-1)
+}
+
+int ora_reorder(ora_ctx* c, int64_t list_ori, int64_t iblk_ori, const double* xori,
+                int64_t list_reo, int64_t iblk_reo, double* xreo, int64_t nshift,
+                const int64_t* occ_shift, const int64_t* from_vtx, const int64_t* to_vtx,
+                double fac, int64_t sign_reo, int64_t update) {
+  GUARD_BEGIN
+  CHECK(nshift >= 0 && nshift <= 4, "reorder: nshift must be 0..4");
+  std::vector<int> sh(8 * nshift), fr(nshift), to(nshift);
+  for (int64_t s = 0; s < nshift; ++s) {
+    for (int q = 0; q < 8; ++q) sh[8 * s + q] = (int)occ_shift[8 * s + q];
+    fr[s] = (int)from_vtx[s] - 1;
+    to[s] = (int)to_vtx[s] - 1;
+  }
+  reorder(c, (int)list_ori, (int)iblk_ori, xori, (int)list_reo, (int)iblk_reo, xreo,
+          (int)nshift, sh.data(), fr.data(), to.data(), fac, (int)sign_reo, update != 0);
   return 0;
   GUARD_END(-1)
 }

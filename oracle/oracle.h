@@ -41,6 +41,8 @@ int64_t ora_strmap_block(ora_ctx*, int64_t type, int64_t nel1, int64_t nel2,
 
 /* operator = list of occupation classes occ[nblk][2][4] */
 int64_t ora_define_op(ora_ctx*, const int64_t* occ, int64_t nblk);
+/* joined operator: occ holds nblk*nj occupations, vertices of a class consecutive */
+int64_t ora_define_op_joined(ora_ctx*, const int64_t* occ, int64_t nj, int64_t nblk);
 /* ME list layout -- operators/set_op_dim2.f; returns list id, *len = len_op */
 int64_t ora_define_list(ora_ctx*, int64_t op, int64_t gamt, int64_t mst,
                         int64_t absym, int64_t* len);
@@ -67,6 +69,13 @@ int ora_contract(ora_ctx*, int64_t route,
                  double* xret, double* stats);
 
 /* spin-flip symmetrisation of a result block -- contract/sym_ab_blk.f */
+/* reorder (reo_op_wmaps_c / reo_blk_wmaps_c) of class iblk_ori of list_ori
+ * into class iblk_reo of list_reo: shift s (occ_shift[8*s..]) moves from
+ * vertex from_vtx[s] to to_vtx[s] (1-based); xreo (whole list) updated */
+int ora_reorder(ora_ctx*, int64_t list_ori, int64_t iblk_ori, const double* xori,
+                int64_t list_reo, int64_t iblk_reo, double* xreo, int64_t nshift,
+                const int64_t* occ_shift, const int64_t* from_vtx, const int64_t* to_vtx,
+                double fac, int64_t sign_reo, int64_t update);
 int ora_sym_ab_blk(ora_ctx*, int64_t list, int64_t iblk, double* x,
                    double prefac, double relfac);
 

@@ -56,6 +56,45 @@ def contractions_for(space):
     return CONTRACTIONS
 
 
+# reorders of joined operators: (name, njoined, vertices of the original
+# class, vertices of the reordered class, shifts [(occ, from_vtx, to_vtx)]);
+# every operator has as many creators as annihilators (total Ms 0 lists)
+def _reo(name, ori, shifts):
+    nj = len(ori)
+    ori = [np.asarray(o) for o in ori]
+    reo = [o.copy() for o in ori]
+    for occ, fr, to in shifts:
+        reo[fr - 1] = reo[fr - 1] - np.asarray(occ)
+        reo[to - 1] = reo[to - 1] + np.asarray(occ)
+        assert (reo[fr - 1] >= 0).all()
+    return (name, nj, ori, reo, shifts)
+
+
+REORDERS = [
+    # a creator moves to a vertex that holds only an annihilator: same
+    # condensed components, a pure change of vertex
+    _reo("move_p", [occ8({P: 1}), occ8(None, {H: 1})], [(occ8({P: 1}), 1, 2)]),
+    # two T1-like vertices: a particle creator joins the other vertex (merge)
+    _reo("merge_p", [occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1})], [(occ8({P: 1}), 1, 2)]),
+    # a hole annihilator joins the other vertex
+    _reo("merge_h", [occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1})], [(occ8(None, {H: 1}), 2, 1)]),
+    # two shifts in opposite directions
+    _reo("swap_ph", [occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1})],
+         [(occ8({P: 1}), 1, 2), (occ8(None, {H: 1}), 2, 1)]),
+    # a one-body vertex hands its creator to a doubles-like vertex
+    _reo("merge_pp", [occ8({P: 2}, {H: 2}), occ8({P: 1}, {H: 1})], [(occ8({P: 1}), 2, 1)]),
+    # nothing moves
+    _reo("none", [occ8({P: 1}, {H: 1}), occ8({P: 1}, {H: 1})], []),
+]
+
+
+def reorders_for(space):
+    if space == "c1_val":
+        return REORDERS + [_reo("val_move", [occ8({V: 1}, {H: 1}), occ8({P: 1}, {V: 1})],
+                                [(occ8({V: 1}), 1, 2)])]
+    return REORDERS
+
+
 def random_list(n, seed):
     rng = np.random.default_rng(seed)
     return rng.standard_normal(n)
