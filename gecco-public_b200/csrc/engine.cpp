@@ -296,6 +296,44 @@ class Engine {
     return *(reos[os.str()] = std::move(dr));
   }
 
+  // trace plan (same device form as a reorder), built on first use
+  DevReo& trace_for(int64_t lop, int64_t ibop, int64_t lres, int64_t ibres, const int64_t* cnt) {
+    std::ostringstream os;
+    os << "T" << lop << ',' << ibop << ',' << lres << ',' << ibres;
+    for (int k = 0; k < 8; ++k) os << ',' << cnt[k];
+    auto it = reos.find(os.str());
+    if (it != reos.end()) return *it->second;
+    GCCU_REQUIRE(!capturing, "trace must be run once before it is captured in a graph");
+    const ListLayout& Lo = list(lop).L;
+    const ListLayout& Lr = list(lres).L;
+    GCCU_REQUIRE(ibop >= 1 && ibop <= (int64_t)Lo.blk.size() && ibres >= 1 &&
+                     ibres <= (int64_t)Lr.blk.size(),
+                 "trace: occupation class out of range");
+    TraceSpec s;
+    s.Lop = &Lo;
+    s.Lres = &Lr;
+    s.ib_op = (int)ibop;
+    s.ib_res = (int)ibres;
+    s.cnt = to_occ(cnt);
+    auto dr = std::make_unique<DevReo>();
+    dr->plan = plan_trace(model, s);
+    dr->list_ori = (int)lop;
+    dr->list_reo = (int)lres;
+    dr->reo_off = Lr.blk[ibres - 1].off;
+    dr->reo_len = Lr.blk[ibres - 1].len;
+    ReoPlan& P = dr->plan;
+    GCCU_REQUIRE(P.items.size() <= 65535, "trace: too many distribution cases");
+    for (auto& it2 : P.items) dr->maxlen = std::max(dr->maxlen, it2.N0 * it2.NK);
+    if (!host_only) {
+      for (auto& m : P.maps) {
+        ReoItem& ri = P.items[m.item];
+        (m.opnd == 0 ? ri.ori : ri.reo).map[m.comp] = strmap(m.key);
+      }
+      if (!P.items.empty()) dr->d_items = upload(P.items);
+    }
+    return *(reos[os.str()] = std::move(dr));
+  }
+
   // cached plan of a descriptor, or null; never plans (gccu_contract_noalloc)
   DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
     std::ostringstream os;
@@ -986,6 +1024,50 @@ int gccu_reorder(const gccu_reo_desc* reo, double fac, int64_t sign_reo, int64_t
                               e.stream));
       CUDA_OK(cudaStreamSynchronize(e.stream));
     }
+  });
+}
+
+int gccu_trace(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t iblk_res,
+               const int64_t* occ_cnt, double fact, int64_t update, int64_t type_xret,
+               double* xret) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_trace needs a device");
+    GCCU_REQUIRE(occ_cnt, "null contraction occupation");
+    GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
+    DevReo& dr = e.trace_for(list_op, iblk_op, list_res, iblk_res, occ_cnt);
+    DevList& lo = e.list(dr.list_ori);
+    DevList& lr = e.list(dr.list_reo);
+    GCCU_REQUIRE(lo.d != lr.d, "trace: operator and result list must differ");
+    if (!update)
+      CUDA_OK(cudaMemsetAsync(lr.d + dr.reo_off, 0, dr.reo_len * sizeof(double), e.stream));
+    if (!dr.plan.items.empty()) {
+      launch_reorder(dr.d_items, (int64_t)dr.plan.items.size(), dr.maxlen, lo.d, lr.d, fact,
+                     e.stream);
+      ++e.launches;
+    }
+    CUDA_OK(cudaGetLastError());
+    if (type_xret == 1) {
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+      launch_sumsq(lr.d + dr.reo_off, dr.reo_len, e.d_red, e.stream);
+      ++e.launches;
+      *xret = e.read_red(0);
+    } else if (type_xret == 2) {
+      CUDA_OK(cudaMemcpyAsync(xret, lr.d + dr.reo_off, sizeof(double), cudaMemcpyDeviceToHost,
+                              e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
+  });
+}
+
+int gccu_trace_info(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t iblk_res,
+                    const int64_t* occ_cnt, int64_t* ncases, int64_t* nelements) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(occ_cnt, "null contraction occupation");
+    DevReo& dr = e.trace_for(list_op, iblk_op, list_res, iblk_res, occ_cnt);
+    *ncases = (int64_t)dr.plan.items.size();
+    *nelements = dr.plan.elements;
   });
 }
 

@@ -565,4 +565,105 @@ ReoPlan plan_reorder(Model& m, const ReorderSpec& s) {
   return P;
 }
 
+ReoPlan plan_trace(Model& m, const TraceSpec& s) {
+  ReoPlan P;
+  const LayoutBlock& Bo = s.Lop->blk.at(s.ib_op - 1);
+  const LayoutBlock& Bt = s.Lres->blk.at(s.ib_res - 1);
+  const int nsym = m.os.nsym;
+  GCCU_REQUIRE(Bo.vtx.size() == 1 && Bt.vtx.size() == 1, "trace: single-vertex operators only");
+  GCCU_REQUIRE(s.Lop->mst == s.Lres->mst && s.Lop->gamt == s.Lres->gamt,
+               "trace: operator and result differ in total Ms or IRREP");
+  for (int t = 0; t < 4; ++t) {
+    GCCU_REQUIRE(s.cnt[t] == s.cnt[4 + t], "trace: contracted creators and annihilators differ");
+    GCCU_REQUIRE(Bo.occ[t] == Bt.occ[t] + s.cnt[t] && Bo.occ[4 + t] == Bt.occ[4 + t] + s.cnt[4 + t],
+                 "trace: operator != result + contracted strings");
+  }
+  std::vector<Comp> jc, ja;
+  m.condense(s.cnt, jc, ja);  // jc and ja list the same types in the same order
+  // sources of the operator's components: J (str1) and the result (str2)
+  auto src_of = [](const std::vector<Comp>& tgt, const std::vector<Comp>& j,
+                   const std::vector<Comp>& r) {
+    std::vector<Src> v(tgt.size());
+    for (size_t q = 0; q < tgt.size(); ++q) {
+      for (size_t i = 0; i < j.size(); ++i)
+        if (j[i].hpvx == tgt[q].hpvx) v[q].i1 = (int)i;
+      for (size_t i = 0; i < r.size(); ++i)
+        if (r[i].hpvx == tgt[q].hpvx) v[q].i2 = (int)i;
+      GCCU_REQUIRE(v[q].i1 >= 0 || v[q].i2 >= 0, "trace: component without source");
+    }
+    return v;
+  };
+  auto so_c = src_of(Bo.c, jc, Bt.c), so_a = src_of(Bo.a, ja, Bt.a);
+  const int msj_max = sum(ja);
+  std::vector<int> oja = comp_occs(ja);
+  for (const auto& kvp : Bt.dis) {
+    for (const Dist& d : kvp.second) {
+      int msta = 0, gta = 1;
+      for (size_t q = 0; q < Bt.a.size(); ++q) msta += d.msa[q], gta = irrep_mult(gta, d.ga[q]);
+      for (int msj = msj_max; msj >= -msj_max; msj -= 2)
+        for (int gj = 1; gj <= nsym; ++gj) {
+          MsGam dj;  // next_msgamdist_diag: one distribution for both sides of J
+          bool first = true;
+          while (next_msgam(first, dj, {}, oja, 0, msj, 1, gj, nsym)) {
+            first = false;
+            std::vector<int> moc, goc, moa, goa;
+            merge_dist(so_c, dj.msa, dj.ga, d.msc, d.gc, moc, goc);
+            merge_dist(so_a, dj.msa, dj.ga, d.msa, d.ga, moa, goa);
+            auto ixj = idxms_of(ja, dj.msa);
+            auto ixtc = idxms_of(Bt.c, d.msc), ixta = idxms_of(Bt.a, d.msa);
+            auto ixoc = idxms_of(Bo.c, moc), ixoa = idxms_of(Bo.a, moa);
+            auto lj = lengths(m, ja, ixj, dj.ga);
+            auto ltc = lengths(m, Bt.c, ixtc, d.gc), lta = lengths(m, Bt.a, ixta, d.ga);
+            auto loc = lengths(m, Bo.c, ixoc, goc), loa = lengths(m, Bo.a, ixoa, goa);
+            if (has_zero(lj) || has_zero(ltc) || has_zero(lta) || has_zero(loc) || has_zero(loa))
+              continue;
+            int msoa = msta + msj, goa_tot = irrep_mult(gta, gj);
+            const int ixms_op = msa_to_idxms(msoa, s.Lop->mst, sum(Bo.a), sum(Bo.c));
+            const Dist& dop = find_dist(Bo, ixms_op, goa_tot,
+                                        dist_id(Bo.c, ixoc, goc, Bo.a, ixoa, goa, nsym));
+            ReoItem it{};
+            it.N0 = it.NK = 1;
+            it.nsp[0] = (int)(Bt.c.size() + Bt.a.size());
+            it.nsp[1] = (int)ja.size();
+            int q = 0;
+            for (auto x : ltc) it.rad[0][q++] = (int32_t)x, it.N0 *= x;
+            for (auto x : lta) it.rad[0][q++] = (int32_t)x, it.N0 *= x;
+            q = 0;
+            for (auto x : lj) it.rad[1][q++] = (int32_t)x, it.NK *= x;
+            it.base_ori = dop.off;
+            it.base_reo = d.off;
+            const int item = (int)P.items.size();
+            const int ntc = (int)Bt.c.size();
+            // J's creator components take the indices of the annihilator ones
+            Side sj{&ja, kEx2, 0, &ixj, &dj.ga, &lj};
+            Side stc{&Bt.c, kEx1, 0, &ixtc, &d.gc, &ltc}, sta{&Bt.a, kEx1, ntc, &ixta, &d.ga, &lta};
+            std::vector<int64_t> ldc, lda;
+            int pos = 0;
+            leading_dims(Bo.c, Bo.a, loc, loa, ldc, lda);
+            std::vector<Src> so_cj(so_c);
+            for (auto& x : so_cj)  // creator J component -> index of the same type in ja
+              if (x.i1 >= 0) {
+                int idx = -1;
+                for (size_t i = 0; i < ja.size(); ++i)
+                  if (ja[i].hpvx == jc[x.i1].hpvx) idx = (int)i;
+                x.i1 = idx;
+              }
+            fill_opnd(it.ori, pos, so_cj, sj, stc, ldc, item, 0, P.maps);
+            fill_opnd(it.ori, pos, so_a, sj, sta, lda, item, 0, P.maps);
+            pos = 0;
+            leading_dims(Bt.c, Bt.a, ltc, lta, ldc, lda);
+            std::vector<Src> dc(Bt.c.size()), da(Bt.a.size());
+            for (size_t i = 0; i < dc.size(); ++i) dc[i].i2 = (int)i;
+            for (size_t i = 0; i < da.size(); ++i) da[i].i2 = (int)i;
+            fill_opnd(it.reo, pos, dc, sj, stc, ldc, item, 1, P.maps);
+            fill_opnd(it.reo, pos, da, sj, sta, lda, item, 1, P.maps);
+            P.elements += it.N0 * it.NK;
+            P.items.push_back(it);
+          }
+        }
+    }
+  }
+  return P;
+}
+
 }  // namespace gccu

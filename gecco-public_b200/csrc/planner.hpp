@@ -60,4 +60,17 @@ struct ReoPlan {
 
 ReoPlan plan_reorder(Model& m, const ReorderSpec& s);
 
+// Partial trace of one occupation class (trace_op / trace_op_blk):
+// res(IC, IA) += f * sum_J op(IC*J, IA*J), the contracted strings J equal on
+// the creator and annihilator side.  Planned as a ReoPlan: space kEx1 = the
+// result's strings (C, then A components), kEx2 = J (its annihilator
+// components; the creator components use the same indices), opnd 0 = op,
+// opnd 1 = result.
+struct TraceSpec {
+  const ListLayout *Lop, *Lres;
+  int ib_op, ib_res;
+  Occ cnt;
+};
+ReoPlan plan_trace(Model& m, const TraceSpec& s);
+
 }  // namespace gccu

@@ -54,6 +54,8 @@ _SIGS = {
     "gccu_define_operator_joined": [P64, I64, I64, P64],
     "gccu_reorder": [ctypes.POINTER(ReoDesc), ctypes.c_double, I64, I64, I64, PD],
     "gccu_reorder_info": [ctypes.POINTER(ReoDesc), P64, P64],
+    "gccu_trace": [I64, I64, I64, I64, P64, ctypes.c_double, I64, I64, PD],
+    "gccu_trace_info": [I64, I64, I64, I64, P64, P64, P64],
     "gccu_register_list": [I64, I64, I64, I64, P64, P64],
     "gccu_list_block": [I64, I64, P64, P64],
     "gccu_list_dists": [I64, P64, I64, P64],
@@ -240,6 +242,22 @@ class Engine:
         n = np.zeros(1, np.int64)
         m = np.zeros(1, np.int64)
         _call("gccu_reorder_info", ctypes.byref(d), _p64(n), _p64(m))
+        return int(n[0]), int(m[0])
+
+    def trace(self, op, res, cnt, fact=1.0, update=True, xret=0):
+        """partial trace res(IC,IA) += fact * sum_J op(IC*J, IA*J); op/res =
+        (list, iblk), cnt = occupation of J (creators = annihilators)"""
+        c = np.ascontiguousarray(np.asarray(cnt, dtype=np.int64).reshape(8))
+        r = np.zeros(1)
+        _call("gccu_trace", op[0], op[1], res[0], res[1], _p64(c), fact, int(update), xret,
+              _pd(r))
+        return float(r[0])
+
+    def trace_info(self, op, res, cnt):
+        c = np.ascontiguousarray(np.asarray(cnt, dtype=np.int64).reshape(8))
+        n = np.zeros(1, np.int64)
+        m = np.zeros(1, np.int64)
+        _call("gccu_trace_info", op[0], op[1], res[0], res[1], _p64(c), _p64(n), _p64(m))
         return int(n[0]), int(m[0])
 
     def register_list(self, op, gamt=1, mst=0, absym=0):

@@ -165,6 +165,23 @@ int gccu_reorder(const gccu_reo_desc* reo, double fac, int64_t sign_reo, int64_t
 /* number of distribution cases and elements the engine plans for a reorder */
 int gccu_reorder_info(const gccu_reo_desc* reo, int64_t* ncases, int64_t* nelements);
 
+/* ---- self-contraction (partial trace) ----------------------------------------
+ * replaces: contr_op1op2 -> trace_op -> trace_op_blk for a [CONTR] whose two
+ * operands are the same operator (contract/contr_op1op2.f:162-169,
+ * contract/trace_op.f:2-830, contract/trace_op_blk.f:2-178), without a
+ * reordered result:
+ *   res(IC,IA) = (update ? res : 0) + fact * sum_J op(IC*J, IA*J),
+ * the contracted strings J identical on the creator and annihilator side
+ * (occ_cnt: creator row equal to annihilator row).  fact = xfac*bc_sign as
+ * for gccu_contract; type_xret as for gccu_contract.  Single-vertex
+ * operators. */
+int gccu_trace(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t iblk_res,
+               const int64_t* occ_cnt, double fact, int64_t update, int64_t type_xret,
+               double* xret);
+/* number of distribution cases and elements the engine plans for a trace */
+int gccu_trace_info(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t iblk_res,
+                    const int64_t* occ_cnt, int64_t* ncases, int64_t* nelements);
+
 /* ---- [ADD] -------------------------------------------------------------------
  * replaces: add_opblk (contract/add_opblk.f:2-313), in-core branch
  * :299-307: out(iblkout) = (reset ? 0 : out) + fac*in(iblkin); type 1 returns

@@ -41,6 +41,8 @@ def lib():
         L.ora_strmap_block.argtypes = [ctypes.c_void_p] + [I64] * 7 + [P64]
         L.ora_define_op.restype = I64
         L.ora_define_op.argtypes = [ctypes.c_void_p, P64, I64]
+        L.ora_trace.argtypes = [ctypes.c_void_p, I64, I64, PD, I64, I64, PD, P64,
+                                ctypes.c_double, I64]
         L.ora_define_op_joined.restype = I64
         L.ora_define_op_joined.argtypes = [ctypes.c_void_p, P64, I64, I64]
         L.ora_reorder.argtypes = [ctypes.c_void_p, I64, I64, PD, I64, I64, PD, I64, P64, P64,
@@ -143,6 +145,12 @@ class Oracle:
             fr[s], to[s] = f, t
         _chk(lib().ora_reorder(self.ctx, lori, bori, _pd(xori), lreo, breo, _pd(xreo), n,
                                _p64(occ), _p64(fr), _p64(to), fac, sign_reo, int(update)))
+
+    def trace(self, lop, bop, xop, lres, bres, xres, cnt, fac=1.0, update=True):
+        """trace_op: xres (whole result list) += fac * sum_J xop(IC*J, IA*J)"""
+        c = np.ascontiguousarray(np.asarray(cnt, dtype=np.int64).reshape(8))
+        _chk(lib().ora_trace(self.ctx, lop, bop, _pd(xop), lres, bres, _pd(xres), _p64(c), fac,
+                             int(update)))
 
     def define_list(self, op, gamt=1, mst=0, absym=0):
         ln = np.zeros(1, dtype=np.int64)

@@ -1586,6 +1586,184 @@ void reorder(ora_ctx* cx, int lori, int ibori, const double* xori, int lreo, int
   }
 }
 
+// ---- partial trace (contract/trace_op.f, contract/trace_op_blk.f) ----
+
+// trace_op without a reordered result: for every Ms/IRREP case of
+// (Op(A), TrOp(A)), every distribution of TrOp and every diagonal
+// distribution of the contracted strings J, trace_op_blk adds
+// xfac*casign*signs*op(IC*J, IA*J) to trop(IC, IA)
+void trace(ora_ctx* cx, int lop, int ibop, const double* xop, int ltr, int ibtr, double* xtr,
+           const int* ocnt, double fac, bool update) {
+  const List& Lo = cx->lists.at(lop - 1);
+  const List& Lt = cx->lists.at(ltr - 1);
+  CHECK(cx->ops[Lo.op - 1].nj == 1 && cx->ops[Lt.op - 1].nj == 1,
+        "trace: single-vertex operators only");
+  CHECK(Lo.gamt == Lt.gamt, "trace_op: inconsistent symmetries");
+  const int nsym = cx->oi.nsym;
+  const ListBlock& Bo = Lo.blk.at(ibop - 1);
+  const ListBlock& Bt = Lt.blk.at(ibtr - 1);
+  std::vector<Comp> cntc, cnta;
+  condense(cx, ocnt, cntc, cnta);
+  // map_info_c / map_info_a: op component <- (J component, TrOp component)
+  auto info = [](const std::vector<Comp>& op, const std::vector<Comp>& j,
+                 const std::vector<Comp>& t) {
+    std::vector<std::pair<int, int>> r(op.size(), {-1, -1});
+    for (size_t q = 0; q < op.size(); ++q) {
+      for (size_t i = 0; i < j.size(); ++i)
+        if (j[i].hpvx == op[q].hpvx) r[q].first = (int)i;
+      for (size_t i = 0; i < t.size(); ++i)
+        if (t[i].hpvx == op[q].hpvx) r[q].second = (int)i;
+    }
+    return r;
+  };
+  auto mi_c = info(Bo.c, cntc, Bt.c), mi_a = info(Bo.a, cnta, Bt.a);
+  if (!update)
+    for (int64_t i = 0; i < Bt.len_occ; ++i) xtr[Bt.off_occ + i] = 0.0;
+  int na_op = 0, nc_op = 0, na_tr = 0, nc_tr = 0, na_cnt = 0;
+  for (auto& x : Bo.a) na_op += x.occ;
+  for (auto& x : Bo.c) nc_op += x.occ;
+  for (auto& x : Bt.a) na_tr += x.occ;
+  for (auto& x : Bt.c) nc_tr += x.occ;
+  for (auto& x : cnta) na_cnt += x.occ;
+  // ms_loop: (Ms(Op(A)), Ms(TrOp(A))) from the maxima down, first fastest
+  for (int ms_tr_a = na_tr; ms_tr_a >= -na_tr; ms_tr_a -= 2) {
+    for (int ms_op_a = na_op; ms_op_a >= -na_op; ms_op_a -= 2) {
+      int ms_op_c = ms_op_a + Lo.mst, ms_tr_c = ms_tr_a + Lt.mst;
+      if (std::abs(ms_op_c) > nc_op || std::abs(ms_tr_c) > nc_tr) continue;
+      int msc_a = ms_op_a - ms_tr_a;
+      CHECK(ms_op_c - ms_tr_c == msc_a, "trace_op: trap 1");
+      if (std::abs(msc_a) > na_cnt) continue;
+      for (int g_tr_a = 1; g_tr_a <= nsym; ++g_tr_a) {
+        for (int g_op_a = 1; g_op_a <= nsym; ++g_op_a) {
+          int g_tr_c = mult(g_tr_a, Lt.gamt);
+          int g_c_a = mult(g_op_a, g_tr_a);
+          int idxms_tr = msa2idxms4op(ms_tr_a, Lt.mst, na_tr, nc_tr);
+          int idxms_op = msa2idxms4op(ms_op_a, Lo.mst, na_op, nc_op);
+          MsGamDist dt;
+          bool first3 = true;
+          while (next_msgamdist2(first3, dt, occs(Bt.c), occs(Bt.a), ms_tr_c, ms_tr_a, g_tr_c,
+                                 g_tr_a, nsym)) {
+            first3 = false;
+            auto ixtc = ixms(Bt.c, dt.msc), ixta = ixms(Bt.a, dt.msa);
+            auto ltc = lens(cx, Bt.c, ixtc, dt.gc), lta = lens(cx, Bt.a, ixta, dt.ga);
+            if (anyzero(ltc) || anyzero(lta)) continue;
+            int64_t tdid = msgmdid2(Bt.c, ixtc, dt.gc, Bt.a, ixta, dt.ga, nsym);
+            const int64_t idxtrop =
+                Bt.dis.at({idxms_tr, g_tr_a})[find_dis(Bt, idxms_tr, g_tr_a, tdid)].off;
+            std::vector<int64_t> lst(ltc), ldtc, ldta;
+            lst.insert(lst.end(), lta.begin(), lta.end());
+            ldims(Bt.c, Bt.a, lst, ldtc, ldta);
+            // cac_loop: distributions of J, the same on both sides (next_msgamdist_diag)
+            MsGamDist dj;
+            bool first5 = true;
+            while (next_msgamdist2(first5, dj, {}, occs(cnta), 0, msc_a, 1, g_c_a, nsym)) {
+              first5 = false;
+              auto ixj = ixms(cnta, dj.msa);
+              auto lj = lens(cx, cnta, ixj, dj.ga);
+              if (anyzero(lj)) continue;
+              // merge_msgmdis: distribution of the operator
+              auto merge = [](const std::vector<std::pair<int, int>>& mi,
+                              const std::vector<int>& msj, const std::vector<int>& gj,
+                              const std::vector<int>& mst, const std::vector<int>& gt,
+                              std::vector<int>& ms, std::vector<int>& g) {
+                ms.assign(mi.size(), 0);
+                g.assign(mi.size(), 1);
+                for (size_t q = 0; q < mi.size(); ++q) {
+                  if (mi[q].first >= 0) ms[q] += msj[mi[q].first], g[q] = mult(g[q], gj[mi[q].first]);
+                  if (mi[q].second >= 0) ms[q] += mst[mi[q].second], g[q] = mult(g[q], gt[mi[q].second]);
+                }
+              };
+              std::vector<int> moc, goc, moa, goa;
+              merge(mi_c, dj.msa, dj.ga, dt.msc, dt.gc, moc, goc);
+              merge(mi_a, dj.msa, dj.ga, dt.msa, dt.ga, moa, goa);
+              auto ixoc = ixms(Bo.c, moc), ixoa = ixms(Bo.a, moa);
+              auto loc = lens(cx, Bo.c, ixoc, goc), loa = lens(cx, Bo.a, ixoa, goa);
+              if (anyzero(loc) || anyzero(loa)) continue;
+              int64_t odid = msgmdid2(Bo.c, ixoc, goc, Bo.a, ixoa, goa, nsym);
+              const auto& odl = Bo.dis.at({idxms_op, g_op_a});
+              const int64_t idxop = odl[find_dis(Bo, idxms_op, g_op_a, odid)].off;
+              int64_t nop = 1;
+              for (auto x : loc) nop *= x;
+              for (auto x : loa) nop *= x;
+              double xnrm = 0;
+              for (int64_t i = 0; i < nop; ++i) xnrm += xop[idxop + i] * xop[idxop + i];
+              if (xnrm < 1e-28) continue;
+              std::vector<int64_t> lso(loc), ldoc, ldoa;
+              lso.insert(lso.end(), loa.begin(), loa.end());
+              ldims(Bo.c, Bo.a, lso, ldoc, ldoa);
+              // maps (str1 = J, str2 = TrOp); trivial where one is absent
+              auto maps = [&](const std::vector<std::pair<int, int>>& mi,
+                              const std::vector<Comp>& tc, const std::vector<int>& ixt,
+                              const std::vector<int>& gt, std::vector<const std::vector<int>*>& m,
+                              std::vector<int64_t>& n1) {
+                m.assign(mi.size(), nullptr);
+                n1.assign(mi.size(), 1);
+                for (size_t q = 0; q < mi.size(); ++q) {
+                  int ij = mi[q].first, it = mi[q].second;
+                  if (ij < 0 || it < 0) continue;
+                  m[q] = &cx->strmap(cnta[ij].graph, tc[it].graph, ixj[ij], ixt[it], dj.ga[ij],
+                                     gt[it]);
+                  n1[q] = lj[ij];
+                }
+              };
+              std::vector<const std::vector<int>*> mc, ma;
+              std::vector<int64_t> n1c, n1a;
+              maps(mi_c, Bt.c, ixtc, dt.gc, mc, n1c);
+              maps(mi_a, Bt.a, ixta, dt.ga, ma, n1a);
+              // trace_op_blk
+              int64_t ntra = 1, ntrc = 1, nj = 1;
+              for (auto x : lta) ntra *= x;
+              for (auto x : ltc) ntrc *= x;
+              for (auto x : lj) nj *= x;
+              std::vector<int64_t> sta(lta.size()), stc(ltc.size()), sj(lj.size());
+              auto side = [](const std::vector<std::pair<int, int>>& mi,
+                             const std::vector<const std::vector<int>*>& m,
+                             const std::vector<int64_t>& n1, const std::vector<int64_t>& ld,
+                             const std::vector<int64_t>& str, const std::vector<int64_t>& sj,
+                             int64_t& idx, int& sgn) {
+                for (size_t q = 0; q < mi.size(); ++q) {
+                  int64_t i1 = mi[q].first >= 0 ? sj[mi[q].first] : 0;
+                  int64_t i2 = mi[q].second >= 0 ? str[mi[q].second] : 0;
+                  int64_t el;
+                  if (!m[q]) {
+                    el = (mi[q].first >= 0 ? i1 : i2) + 1;
+                  } else {
+                    el = (*m[q])[i2 * n1[q] + i1];
+                    if (el == 0) return false;
+                    if (el < 0) sgn = -sgn, el = -el;
+                  }
+                  idx += (el - 1) * ld[q];
+                }
+                return true;
+              };
+              for (int64_t ia = 0; ia < ntra; ++ia) {
+                decompose(ia, lta, sta.data());
+                int64_t ta_off = 0;
+                for (size_t q = 0; q < lta.size(); ++q) ta_off += sta[q] * ldta[q];
+                for (int64_t ij = 0; ij < nj; ++ij) {
+                  decompose(ij, lj, sj.data());
+                  int64_t ida = 0;
+                  int sgna = 1;
+                  if (!side(mi_a, ma, n1a, ldoa, sta, sj, ida, sgna)) continue;
+                  for (int64_t ic = 0; ic < ntrc; ++ic) {
+                    decompose(ic, ltc, stc.data());
+                    int64_t tc_off = 0;
+                    for (size_t q = 0; q < ltc.size(); ++q) tc_off += stc[q] * ldtc[q];
+                    int64_t idc = ida;
+                    int sgnc = sgna;
+                    if (!side(mi_c, mc, n1c, ldoc, stc, sj, idc, sgnc)) continue;
+                    xtr[idxtrop + tc_off + ta_off] += fac * (double)sgnc * xop[idxop + idc];
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 void sym_ab_blk(ora_ctx* cx, List& L, int iblk, double* buf, double prefac, double relfac) {
   CHECK(L.mst == 0, "sym_ab_blk: mst must be 0");
   ListBlock& B = L.blk[iblk - 1];
@@ -1835,6 +2013,18 @@ int ora_reorder(ora_ctx* c, int64_t list_ori, int64_t iblk_ori, const double* xo
   }
   reorder(c, (int)list_ori, (int)iblk_ori, xori, (int)list_reo, (int)iblk_reo, xreo,
           (int)nshift, sh.data(), fr.data(), to.data(), fac, (int)sign_reo, update != 0);
+  return 0;
+  GUARD_END(-1)
+}
+
+int ora_trace(ora_ctx* c, int64_t list_op, int64_t iblk_op, const double* xop, int64_t list_res,
+              int64_t iblk_res, double* xres, const int64_t* occ_cnt, double fac,
+              int64_t update) {
+  GUARD_BEGIN
+  int cn[8];
+  for (int k = 0; k < 8; ++k) cn[k] = (int)occ_cnt[k];
+  trace(c, (int)list_op, (int)iblk_op, xop, (int)list_res, (int)iblk_res, xres, cn, fac,
+        update != 0);
   return 0;
   GUARD_END(-1)
 }

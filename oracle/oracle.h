@@ -76,6 +76,11 @@ int ora_reorder(ora_ctx*, int64_t list_ori, int64_t iblk_ori, const double* xori
                 int64_t list_reo, int64_t iblk_reo, double* xreo, int64_t nshift,
                 const int64_t* occ_shift, const int64_t* from_vtx, const int64_t* to_vtx,
                 double fac, int64_t sign_reo, int64_t update);
+/* partial trace (trace_op / trace_op_blk): xres (whole list) +=
+ * fac * sum_J xop(IC*J, IA*J), J of occupation occ_cnt on both sides */
+int ora_trace(ora_ctx*, int64_t list_op, int64_t iblk_op, const double* xop,
+              int64_t list_res, int64_t iblk_res, double* xres, const int64_t* occ_cnt,
+              double fac, int64_t update);
 int ora_sym_ab_blk(ora_ctx*, int64_t list, int64_t iblk, double* x,
                    double prefac, double relfac);
 

@@ -95,6 +95,28 @@ def reorders_for(space):
     return REORDERS
 
 
+# partial traces (self-contractions): (name, operator, result, contracted J);
+# operator = result + J on both sides, J the same on creators and annihilators
+def _tr(name, res, cnt):
+    res, cnt = np.asarray(res), np.asarray(cnt)
+    return (name, res + cnt, res, cnt)
+
+
+TRACES = [
+    _tr("full_p", occ8(), occ8({P: 1}, {P: 1})),
+    _tr("w_over_h", occ8({P: 1}, {P: 1}), occ8({H: 1}, {H: 1})),
+    _tr("pp_over_p", occ8({P: 1}, {P: 1}), occ8({P: 1}, {P: 1})),
+    _tr("full_hh", occ8(), occ8({H: 2}, {H: 2})),
+    _tr("t2like_over_ph", occ8({P: 1}, {H: 1}), occ8({P: 1, H: 1}, {P: 1, H: 1})),
+]
+
+
+def traces_for(space):
+    if space == "c1_val":
+        return TRACES + [_tr("v_over_v", occ8({P: 1}, {P: 1}), occ8({V: 1}, {V: 1}))]
+    return TRACES
+
+
 def random_list(n, seed):
     rng = np.random.default_rng(seed)
     return rng.standard_normal(n)
