@@ -172,6 +172,7 @@ def run_gpu(args, cfg):
     peak = fp64_peak() if rank == 0 and not args.trace_contraction else None
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
+    eng.set_precision(args.precision)
     solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
     t0 = time.time()
     solver.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
@@ -266,7 +267,8 @@ def run_gpu(args, cfg):
     achieved = dom[0] / (dom_ms * 1e-3) / 1e12
     total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
     line = {
-        "metric": "s/CC-iteration (CCSD, plain FP64)",
+        "metric": ("s/CC-iteration (CCSD, plain FP64)" if args.precision == 0 else
+                   "s/CC-iteration (CCSD, split-TF32 tensor cores, FP64 accumulation)"),
         "value": (ms / 1e3) / world,
         "unit": "s",
         "n_gpus": world,
@@ -276,7 +278,7 @@ def run_gpu(args, cfg):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if args.precision == 0 else "tf32x3/f32->f64",
         "data": "synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
                 "B~N(0,0.05^2)); inputs larger than L2 (two-electron list "
                 f"{8 * solver.lists['V'][1] / 1e9:.1f} GB)",
@@ -389,6 +391,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", type=int, default=0,
+                    help="0: FP64 contractions; 1: split-TF32 tensor-core contractions")
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")

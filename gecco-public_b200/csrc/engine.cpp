@@ -102,6 +102,8 @@ class Engine {
   int64_t capture_start = 0;
   cudaEvent_t slots[64] = {};
   bool profiling = false;
+  int precision = 0;     // 0: FP64 DMMA, 1: split TF32 on tcgen05 for regular/medium items
+  int* d_err = nullptr;  // set by kernels whose bounded pipeline waits ran out
   // fixed scratch of gccu_contract_noalloc, looked up on its first call
   bool have_static = false;
   StaticScratch static_ss;
@@ -127,6 +129,8 @@ class Engine {
     CUDA_OK(cudaSetDevice(dev));
     CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     d_red = (double*)alloc(64 * sizeof(double));
+    d_err = (int*)alloc(sizeof(int));
+    CUDA_OK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
   }
   ~Engine() {
     for (auto g : graphs) cudaGraphExecDestroy(g);
@@ -338,7 +342,7 @@ class Engine {
   DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
     std::ostringstream os;
     os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
-       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr;
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision;
     for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
                                    << bc->occ_cnt[k];
     auto it = plans.find(os.str());
@@ -348,7 +352,7 @@ class Engine {
   DevPlan& plan_for(const gccu_bc_desc* bc, bool use_tr) {
     std::ostringstream os;
     os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
-       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr;
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision;
     for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
                                    << bc->occ_cnt[k];
     std::string key = os.str();
@@ -469,6 +473,10 @@ class Engine {
         kind_of[i] = kGemmMedium;
         swapped[i] = 1;
       }
+      // split-TF32 mode: the GEMM-sized items go to the tensor-core kernel
+      // (items with at most 32 columns keep the FP64 128 x 32 tile, which
+      // wastes less than a 256-wide tensor-core tile)
+      if (precision == 1 && kind_of[i] == kGemmRegular) kind_of[i] = kGemmTc;
     }
     // an operand whose strings need map lookups is packed into a dense panel
     auto packed = [&](size_t i, int op) { return P.items[i].op[op].nmap > 0; };
@@ -613,6 +621,8 @@ class Engine {
         int64_t ks = 1;
         if (kind == kGemmSmall) {
           ks = std::max<int64_t>(1, (d.K + kSmallChunk - 1) / kSmallChunk);
+        } else if (kind == kGemmTc) {  // FP32 accumulation over at most kTcChunk indices
+          ks = std::max<int64_t>(1, (d.K + kTcChunk - 1) / kTcChunk);
         } else if (total < want && d.K > 4 * kGemmK) {
           ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
           ks = std::max<int64_t>(ks, 1);
@@ -756,7 +766,17 @@ class Engine {
     double v = 0;
     CUDA_OK(cudaMemcpyAsync(&v, d_red + slot, sizeof(double), cudaMemcpyDeviceToHost, stream));
     CUDA_OK(cudaStreamSynchronize(stream));
+    check_err();
     return v;
+  }
+  // after a synchronisation: did a tensor-core pipeline wait time out?
+  void check_err() {
+    int h = 0;
+    CUDA_OK(cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+      CUDA_OK(cudaMemset(d_err, 0, sizeof(int)));
+      throw Error("a tensor-core pipeline wait timed out in a contraction kernel");
+    }
   }
 };
 
@@ -1125,7 +1145,7 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       first += dp.ndesc_g[kind];
       launch_rebase_descs(dp.d_desc[kind], descs, dp.ndesc_g[kind], dp.scratch, dp.scratch_len,
                           ss.panels, e.stream);
-      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.stream);
+      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err, e.stream);
       e.launches += 2;
     }
     if (dp.plan.use_tr && dp.nflip) {
@@ -1177,7 +1197,8 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     }
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
-      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.stream);
+      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err,
+                  e.stream);
       ++e.launches;
     }
     if (timed) {
@@ -1337,7 +1358,18 @@ int gccu_graph_launch(int64_t graph_id) {
 }
 
 int gccu_sync(void) {
-  return guarded([&] { CUDA_OK(cudaStreamSynchronize(eng().stream)); });
+  return guarded([&] {
+    Engine& e = eng();
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    if (!e.host_only) e.check_err();
+  });
+}
+
+int gccu_set_precision(int64_t mode) {
+  return guarded([&] {
+    GCCU_REQUIRE(mode == 0 || mode == 1, "precision mode must be 0 (FP64) or 1 (split TF32)");
+    eng().precision = (int)mode;
+  });
 }
 
 int gccu_stats(double* stats8, int64_t* launches) {

@@ -320,8 +320,12 @@ void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cud
 }
 
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
-                 double alpha, cudaStream_t s) {
+                 double alpha, int* err, cudaStream_t s) {
   if (ntiles == 0) return;
+  if (kind == kGemmTc) {
+    launch_gemm_tc(descs, tiles, ntiles, alpha, err, s);
+    return;
+  }
   if (kind == kGemmRegular)
     launch_gemm_cfg<kGemmRegularM, kGemmRegularN, 4, 2>(descs, tiles, ntiles, alpha, s);
   else if (kind == kGemmMedium)

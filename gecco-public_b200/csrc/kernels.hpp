@@ -19,7 +19,10 @@ void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab
 // tile shapes of the grouped GEMM: regular items, medium (<= 32 columns) and
 // thin (<= 8 columns) items, items with at most 16 result elements
 constexpr int kGemmRegular = 0, kGemmSkinny = 1, kGemmSmall = 2, kGemmMedium = 3;
-constexpr int kGemmKinds = 4;
+constexpr int kGemmTc = 4;  // split-TF32 tensor-core tiles (precision mode 1)
+constexpr int kGemmKinds = 5;
+constexpr int kGemmTcM = 128, kGemmTcN = 256;
+constexpr int64_t kTcChunk = 4096;  // contraction range of one FP32 accumulation
 constexpr int64_t kSmallChunk = 1 << 16;  // contraction elements per block of k_small
 constexpr int kGemmRegularM = 128, kGemmRegularN = 64;
 constexpr int kGemmMediumM = 128, kGemmMediumN = 32;
@@ -30,10 +33,12 @@ inline void gemm_tile(int kind, int& TM, int& TN) {
   TM = kind == kGemmRegular ? kGemmRegularM
        : kind == kGemmMedium ? kGemmMediumM
        : kind == kGemmSkinny ? kGemmSkinnyM
+       : kind == kGemmTc     ? kGemmTcM
                              : 1 << 30;
   TN = kind == kGemmRegular ? kGemmRegularN
        : kind == kGemmMedium ? kGemmMediumN
        : kind == kGemmSkinny ? kGemmSkinnyN
+       : kind == kGemmTc     ? kGemmTcN
                              : 1 << 30;
 }
 
@@ -42,9 +47,14 @@ inline void gemm_tile(int kind, int& TM, int& TN) {
 // maximum over its jobs
 void pack_geometry(const PackJob& j, int64_t& gx, int64_t& gy);
 void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cudaStream_t s);
-// grouped block-contraction GEMM over the tiles of one tile shape
+// split-TF32 tensor-core GEMM (tcgen05) over 128 x kGemmTcN tiles; *err is
+// set if a pipeline wait timed out
+void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
+                    int* err, cudaStream_t s);
+// grouped block-contraction GEMM over the tiles of one tile shape (err: see
+// launch_gemm_tc, used by kind kGemmTc)
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
-                 double alpha, cudaStream_t s);
+                 double alpha, int* err, cudaStream_t s);
 
 // reorder of a joined operator class (nitems <= 65535 distribution cases,
 // maxlen = largest N0*NK); reo += alpha * signs * ori

@@ -55,6 +55,7 @@ _SIGS = {
     "gccu_reorder": [ctypes.POINTER(ReoDesc), ctypes.c_double, I64, I64, I64, PD],
     "gccu_reorder_info": [ctypes.POINTER(ReoDesc), P64, P64],
     "gccu_trace": [I64, I64, I64, I64, P64, ctypes.c_double, I64, I64, PD],
+    "gccu_set_precision": [I64],
     "gccu_trace_info": [I64, I64, I64, I64, P64, P64, P64],
     "gccu_register_list": [I64, I64, I64, I64, P64, P64],
     "gccu_list_block": [I64, I64, P64, P64],
@@ -243,6 +244,10 @@ class Engine:
         m = np.zeros(1, np.int64)
         _call("gccu_reorder_info", ctypes.byref(d), _p64(n), _p64(m))
         return int(n[0]), int(m[0])
+
+    def set_precision(self, mode):
+        """0 = FP64 (default), 1 = split TF32 on the tcgen05 tensor cores"""
+        _call("gccu_set_precision", int(mode))
 
     def trace(self, op, res, cnt, fact=1.0, update=True, xret=0):
         """partial trace res(IC,IA) += fact * sum_J op(IC*J, IA*J); op/res =

@@ -213,6 +213,17 @@ int gccu_graph_begin(void);
 int gccu_graph_end(int64_t* graph_id);
 int gccu_graph_launch(int64_t graph_id);
 int gccu_sync(void);
+/* Precision of the contractions planned after this call (no counterpart in
+ * the reference, whose route-3 products are FP64 dgemm): 0 = FP64 on the FP64
+ * tensor pipe (default); 1 = split TF32 on the tcgen05 tensor cores for the
+ * GEMM-sized block contractions: each operand is split into two TF32 terms,
+ * three products accumulate in FP32 over at most 4096 contraction indices,
+ * and the partial results are added in FP64 (about FP32 accuracy per
+ * product; items with at most 32 rows or columns stay FP64).  Plans are kept per mode, so a
+ * solver can switch back to FP64 for its final iterations.  A pipeline wait
+ * that times out inside a kernel is reported as an error by the next call
+ * that synchronises (gccu_sync, norms, downloads). */
+int gccu_set_precision(int64_t mode);
 
 /* ---- statistics -----------------------------------------------------------
  * dgemm shape statistics in the reference's accounting

@@ -1,0 +1,54 @@
+"""Split-TF32 tensor-core contractions (gccu_set_precision(1)) against the
+oracle's FP64 route 2: every test contraction on the test spaces plus a
+larger C1 space whose ladders and rings have a few hundred rows, columns and
+contraction indices (so the tensor-core tiles see full K slices), to FP32-level
+accuracy; switching back to FP64 restores the 1e-12 agreement."""
+import numpy as np
+import pytest
+
+import gccu
+from binding import Oracle
+from cases import SPACES, contractions_for, random_list
+
+pytestmark = pytest.mark.gpu
+
+RTOL_TC = 5e-6    # split TF32: ~2^-21 per product, FP32 accumulation over <= 4096 terms
+RTOL_FP64 = 1e-12
+
+TC_SPACES = dict(SPACES, c1_tc=(1, [[4], [14], [0], [0]]))
+
+
+@pytest.fixture
+def engine(built):
+    e = gccu.Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("space", list(TC_SPACES))
+def test_split_tf32_contractions(engine, space):
+    nsym, norb = TC_SPACES[space]
+    engine.register_orbinfo(nsym, norb)
+    cases = contractions_for(space if space in SPACES else "c1_small")
+    for i, case in enumerate(cases):
+        o = Oracle(nsym, norb)
+        ls = []
+        for occ in case[1:4]:
+            le, n = engine.register_list(engine.define_operator([occ]))
+            lo, _ = o.define_list(o.define_op([occ]))
+            ls.append((le, lo, n))
+        (l1, o1, n1), (l2, o2, n2), (l12, o12, n12) = ls
+        x1, x2 = random_list(n1, 10 * i), random_list(n2, 10 * i + 1)
+        engine.upload(l1, x1)
+        engine.upload(l2, x2)
+        ref = np.zeros(n12)
+        o.contract(2, o1, 1, x1, o2, 1, x2, o12, 1, ref, case[4], case[5], case[6], 0.5,
+                   update=False)
+        scale = max(1.0, np.abs(ref).max())
+        for mode, tol in ((1, RTOL_TC), (0, RTOL_FP64)):
+            engine.set_precision(mode)
+            engine.contract((l1, 1), (l2, 1), (l12, 1), case[4], case[5], case[6], fact=0.5,
+                            update=False)
+            got = engine.download(l12, n12)
+            assert np.max(np.abs(got - ref)) <= tol * scale, (case[0], mode)
+        engine.set_precision(0)
