@@ -36,11 +36,11 @@ ROOFLINE_CONTRACTION = "r2_ladder"
 PROFILES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles")
 
 
-def profiled_traffic(cfg):
+def profiled_traffic(cfg, kernel="k_gemm"):
     """DRAM bytes (read + write) of one roofline launch at this workload, from
     the ncu summary in profiles/ (a line 'traffic_bytes_per_launch: N'), or
     None when no capture of this workload is committed"""
-    path = os.path.join(PROFILES, f"k_gemm_ladder_{cfg['tag']}.md")
+    path = os.path.join(PROFILES, f"{kernel}_ladder_{cfg['tag']}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -190,8 +190,83 @@ def run_gpu(args, cfg):
         print(json.dumps({"trace": args.trace_contraction, "workload": cfg["name"],
                           "ms_including_planning": ms}), flush=True)
         return
-    # warm-up iterations (the first one plans every contraction and builds the
-    # string maps on the device)
+    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else [])
+    results = {}
+    for mode in modes:
+        if mode != modes[0]:  # fresh amplitudes and DIIS subspace for the next mode
+            for a in solver.amps:
+                eng.zero(solver.lid(a))
+            if hasattr(solver, "_diis"):
+                del solver._diis
+            solver.graph = None
+        eng.set_precision(mode)
+        results[mode] = measure(args, cfg, eng, solver, local, dist, mode)
+    r = results[modes[0]]
+    line = {
+        "metric": METRIC[modes[0]],
+        "value": (r["ms"] / 1e3) / world,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms"],
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": DTYPE[modes[0]],
+        "data": "synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
+                "B~N(0,0.05^2)); inputs larger than L2 (two-electron list "
+                f"{8 * solver.lists['V'][1] / 1e9:.1f} GB)",
+        "config": {"workload": cfg["name"], "method": "CCSD spin-orbital, DIIS maxsub 8",
+                   "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
+                   "parallelism": f"replicas x{world}", "l2": "inputs > L2",
+                   "setup_s": round(setup_s, 2), "energy_last": r["energies"][-1]},
+        "roofline": roofline(cfg, r, peak, modes[0]),
+        "clocks": clock_summary(r["samples"]),
+        "e2e": r["e2e"],
+        "gpu_launches": r["launches"],
+    }
+    if 0 in results and modes[0] != 0:
+        f = results[0]
+        line["fp64"] = {"metric": METRIC[0], "value": (f["ms"] / 1e3) / world,
+                        "ms_per_step": f["ms"], "e2e": f["e2e"], "gpu_launches": f["launches"],
+                        "roofline": roofline(cfg, f, peak, 0),
+                        "energy_last": f["energies"][-1]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        host_lists = {}
+        for name in ("F", "V", "T1", "T2", "D" + "T1", "D" + "T2"):
+            lid, n, _ = solver.lists[name]
+            x = np.empty(n)
+            eng.get_vec(lid, 0, x.ctypes.data, n)
+            host_lists[name] = x
+        cores = os.cpu_count()
+        val, sample = cpu_baseline_oracle(solver.lists, sp, eps, B, args.cpu_seconds, cores,
+                                          host_lists)
+        line["cpu_baseline"] = {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                                "sample": sample}
+    eng.close()
+    del solver
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_convergence:
+        line["convergence"] = convergence(local)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+METRIC = {0: "s/CC-iteration (CCSD, plain FP64)",
+          1: "s/CC-iteration (CCSD, split-TF32 tensor cores, FP64 accumulation)"}
+DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums"}
+
+
+def measure(args, cfg, eng, solver, local, dist, mode):
+    """warm-up (plans every contraction in this precision mode), the timed
+    graph-replayed iterations, one eagerly profiled iteration and the
+    end-to-end iterations through host buffers"""
+    import torch
+
     energies = []
     for _ in range(args.warmup):
         en, rn = solver.iterate()
@@ -225,7 +300,7 @@ def run_gpu(args, cfg):
     names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
     if len(names) != len(prof):
         raise RuntimeError(f"profile rows ({len(prof)}) do not match contractions ({len(names)})")
-    if args.profile_out and rank == 0:
+    if args.profile_out and mode == args.precision and int(os.environ.get("RANK", 0)) == 0:
         with open(args.profile_out, "w") as f:
             json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
                         "tflops": r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12 if r[2] else None,
@@ -256,68 +331,96 @@ def run_gpu(args, cfg):
             eng.get_vec(solver.lid(solver.res[a]), 0, host_r[a].data_ptr(), nR[a])
     eng.sync()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    h2d = 8 * sum(nT.values())
-    d2h = 8 * sum(nR.values()) + 8
-    # dominant kernel: k_gemm<128,64>; its representative launch is the one of
-    # the pp-ladder contraction (the leading term; no operand gathers), timed
-    # with events around its GEMM launches in the profiled iteration
-    i_dom = names.index(ROOFLINE_CONTRACTION)
-    dom = prof[i_dom]
+    return {"ms": ms, "launches": int(launches), "samples": samples, "prof": prof,
+            "names": names, "energies": energies,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * sum(nT.values()),
+                    "d2h_bytes_per_step": 8 * sum(nR.values()) + 8}}
+
+
+def roofline(cfg, r, fp64_peak_tflops, mode):
+    """dominant kernel: the GEMM launch(es) of the pp-ladder contraction (the
+    leading term; no operand gathers), timed with events in the profiled
+    iteration: k_gemm<128,64> (FP64 DMMA) in mode 0, k_gemm_tc (split TF32 on
+    tcgen05) in mode 1"""
+    names, prof = r["names"], r["prof"]
+    dom = prof[names.index(ROOFLINE_CONTRACTION)]
     dom_ms = (dom[2] - dom[5]) / dom[1]
     achieved = dom[0] / (dom_ms * 1e-3) / 1e12
     total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
-    line = {
-        "metric": ("s/CC-iteration (CCSD, plain FP64)" if args.precision == 0 else
-                   "s/CC-iteration (CCSD, split-TF32 tensor cores, FP64 accumulation)"),
-        "value": (ms / 1e3) / world,
-        "unit": "s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": ms,
-        "higher_is_better": False,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f64" if args.precision == 0 else "tf32x3/f32->f64",
-        "data": "synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
-                "B~N(0,0.05^2)); inputs larger than L2 (two-electron list "
-                f"{8 * solver.lists['V'][1] / 1e9:.1f} GB)",
-        "config": {"workload": cfg["name"], "method": "CCSD spin-orbital, DIIS maxsub 8",
-                   "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
-                   "parallelism": f"replicas x{world}", "l2": "inputs > L2",
-                   "setup_s": round(setup_s, 2), "energy_last": energies[-1]},
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if peak else None,
-                     "traffic": profiled_traffic(cfg),
-                     "kernel": f"k_gemm<128,64> FP64 DMMA, launch of [CONTR] {ROOFLINE_CONTRACTION}",
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
-                                    "MEASURED_PEAKS.json)",
-                     "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
-                     "iteration_flops": total_flops,
-                     "iteration_tflops": total_flops / (ms * 1e-3) / 1e12},
-        "clocks": clock_summary(samples),
-        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches),
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        host_lists = {}
-        for name in ("F", "V", "T1", "T2", "D" + "T1", "D" + "T2"):
-            lid, n, _ = solver.lists[name]
-            x = np.empty(n)
-            eng.get_vec(lid, 0, x.ctypes.data, n)
-            host_lists[name] = x
-        cores = os.cpu_count()
-        val, sample = cpu_baseline_oracle(solver.lists, sp, eps, B, args.cpu_seconds, cores,
-                                          host_lists)
-        line["cpu_baseline"] = {"value": val, "unit": "s", "cores": cores, "kind": "port",
-                                "sample": sample}
-    eng.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    out = {"bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
+           "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
+           "iteration_flops": total_flops,
+           "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12}
+    if mode == 0:
+        out.update(peak=fp64_peak_tflops,
+                   traffic=profiled_traffic(cfg, "k_gemm"),
+                   kernel=f"k_gemm<128,64> FP64 DMMA, launch of [CONTR] {ROOFLINE_CONTRACTION}",
+                   peak_source="cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
+                               "MEASURED_PEAKS.json)")
+    else:
+        bf16 = measured_bf16_tflops()
+        peak = bf16 / 2.0 / 3.0 if bf16 else None
+        out.update(peak=peak,
+                   traffic=profiled_traffic(cfg, "k_gemm_tc"),
+                   kernel=f"k_gemm_tc<256> split TF32 (tcgen05), launch of [CONTR] "
+                          f"{ROOFLINE_CONTRACTION}",
+                   peak_source="of measured: MEASURED_PEAKS.json bf16_tflops (burst) / 2 "
+                               "(dense TF32 = half of dense BF16) / 3 (three TF32 products "
+                               "per useful product)")
+    out["frac"] = (achieved / out["peak"]) if out["peak"] else None
+    return out
+
+
+def measured_bf16_tflops():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def convergence(local):
+    """time to |dE| < 1 uEh against the converged FP64 energy, plain FP64 and
+    mixed (split TF32 until the residual norm is below 1e-5, then FP64), on
+    the largest size of the synthetic family that converges under
+    diagonal+DIIS (o8 v32; o12 v100 and larger diverge with these integral
+    distributions).  Wall time of the solve loop (device work, energy and
+    residual reads, DIIS solves), graphs replayed after the first iteration
+    of each mode."""
+    import cc
+    import gccu
+    import hamiltonian as hm
+    from devfill import TorchIntegrals
+
+    cfg = CONFIGS[0]
+    sp, eps, B = setup_hamiltonian(cfg)
+    out = {"workload": cfg["name"]}
+    ref = None
+    for label in ("fp64", "mixed"):
+        eng = gccu.Engine(local)
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+        eng.sync()
+        hist = []
+        t0 = time.perf_counter()
+
+        def cb(it, en, rn):
+            hist.append((it, en, rn, time.perf_counter() - t0))
+
+        if label == "fp64":
+            s.solve(maxiter=60, conv=1e-9, use_graph=True, callback=cb)
+        else:
+            s.solve_mixed(maxiter=60, conv=1e-9, switch=1e-5, callback=cb)
+        eng.close()
+        if ref is None:
+            ref = hist[-1][1]
+        hit = next((h for h in hist if abs(h[1] - ref) < 1e-6), None)
+        out[label] = {"iterations": hist[-1][0], "energy": hist[-1][1],
+                      "residual": hist[-1][2], "s_total": hist[-1][3],
+                      "iterations_to_1uEh": hit[0] if hit else None,
+                      "s_to_1uEh": hit[3] if hit else None}
+    out["dE_mixed_vs_fp64"] = out["mixed"]["energy"] - out["fp64"]["energy"]
+    return out
 
 
 def run_reference(args, cfg):
@@ -391,8 +494,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", type=int, default=0,
-                    help="0: FP64 contractions; 1: split-TF32 tensor-core contractions")
+    ap.add_argument("--precision", type=int, default=1,
+                    help="1 (default): split-TF32 tensor-core contractions, with the FP64 "
+                         "path measured beside them; 0: FP64 only")
+    ap.add_argument("--no-fp64", action="store_true",
+                    help="with --precision 1, skip the FP64 measurement")
+    ap.add_argument("--no-convergence", action="store_true",
+                    help="skip the time-to-convergence comparison on o8 v32")
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")

@@ -193,12 +193,13 @@ class CCSolver:
     lists (solve_nleq with method=diis, solve/solve_nleq.f; diagonal step
     diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
 
-    def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8):
+    def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0):
         self.e = engine
         self.ints = ints
         self.method = method
         self.use_tr = use_tr
         self.maxsub = maxsub
+        self.shift = shift  # level shift of the diagonal preconditioner (diavc)
         sp = ints.space
         self.nsym = sp.nsym
         engine.register_orbinfo(sp.nsym, sp.norb)
@@ -326,7 +327,7 @@ class CCSolver:
         """t <- t - R/D (diagonal preconditioner)"""
         for a in self.amps:
             self.e.precondition(self.lid("S" + a), self.lid(self.res[a]), self.lid("D" + a),
-                                fac=-1.0)
+                                fac=-1.0, shift=self.shift)
             self.e.add_block(1.0, self.lid("S" + a), 1, self.lid(a), 1)
 
     def _diis_lists(self):
@@ -355,7 +356,8 @@ class CCSolver:
         used.append(k)
         slot = d["slots"][k]
         for a in self.amps:
-            self.e.precondition(slot[("e", a)], self.lid(self.res[a]), self.lid("D" + a), fac=-1.0)
+            self.e.precondition(slot[("e", a)], self.lid(self.res[a]), self.lid("D" + a), fac=-1.0,
+                                shift=self.shift)
             self.e.add_block(1.0, self.lid(a), 1, slot[("t", a)], 1, reset=True)
             self.e.add_block(1.0, slot[("e", a)], 1, slot[("t", a)], 1)
         B = d["B"]
@@ -397,6 +399,39 @@ class CCSolver:
         self.e.graph_begin()
         self.evaluate()
         self.graph = self.e.graph_end()
+
+    def solve_mixed(self, maxiter=60, conv=1e-8, switch=1e-5, callback=None, stop=None):
+        """Mixed-precision solve: the contractions run in split TF32 on the
+        tensor cores (engine precision 1) while the residual norm is above
+        `switch`, in FP64 after that; the CC fixed-point iteration corrects
+        the errors of the cheaper iterations, the DIIS subspace, residuals,
+        energies and amplitude updates stay FP64 throughout.  Each mode's
+        evaluation runs once eagerly (planning) and is then replayed from its
+        own CUDA graph.  stop(it, energy, residual) may end the solve early.
+        Returns the last energy."""
+        graphs, planned = {}, set()
+        mode = 1
+        self.e.set_precision(mode)
+        en = None
+        for it in range(1, maxiter + 1):
+            if mode not in graphs and mode in planned:
+                self.capture()
+                graphs[mode] = self.graph
+            self.graph = graphs.get(mode)
+            en, rn = self.iterate()
+            planned.add(mode)
+            self.history.append((it, en, rn))
+            if callback:
+                callback(it, en, rn)
+            if rn < conv or (stop is not None and stop(it, en, rn)):
+                break
+            if mode == 1 and rn < switch:
+                mode = 0
+                self.e.set_precision(mode)
+            self.diis_step()
+        self.e.set_precision(0)
+        self.graph = None
+        return en
 
     def solve(self, maxiter=50, conv=1e-8, use_graph=False, diis=True, callback=None,
               econv=None):

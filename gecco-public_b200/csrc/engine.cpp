@@ -475,8 +475,10 @@ class Engine {
       }
       // split-TF32 mode: the GEMM-sized items go to the tensor-core kernel
       // (items with at most 32 columns keep the FP64 128 x 32 tile, which
-      // wastes less than a 256-wide tensor-core tile)
-      if (precision == 1 && kind_of[i] == kGemmRegular) kind_of[i] = kGemmTc;
+      // wastes less than a 256-wide tensor-core tile; items with fewer than
+      // kTcMinK contraction indices keep FP64, their tiles would be set-up
+      // and epilogue only)
+      if (precision == 1 && kind_of[i] == kGemmRegular && it.K >= kTcMinK) kind_of[i] = kGemmTc;
     }
     // an operand whose strings need map lookups is packed into a dense panel
     auto packed = [&](size_t i, int op) { return P.items[i].op[op].nmap > 0; };

@@ -23,6 +23,7 @@ constexpr int kGemmTc = 4;  // split-TF32 tensor-core tiles (precision mode 1)
 constexpr int kGemmKinds = 5;
 constexpr int kGemmTcM = 128, kGemmTcN = 256;
 constexpr int64_t kTcChunk = 4096;  // contraction range of one FP32 accumulation
+constexpr int64_t kTcMinK = 256;    // shortest contraction sent to the tensor cores
 constexpr int64_t kSmallChunk = 1 << 16;  // contraction elements per block of k_small
 constexpr int kGemmRegularM = 128, kGemmRegularN = 64;
 constexpr int kGemmMediumM = 128, kGemmMediumN = 32;

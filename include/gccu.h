@@ -219,7 +219,8 @@ int gccu_sync(void);
  * GEMM-sized block contractions: each operand is split into two TF32 terms,
  * three products accumulate in FP32 over at most 4096 contraction indices,
  * and the partial results are added in FP64 (about FP32 accuracy per
- * product; items with at most 32 rows or columns stay FP64).  Plans are kept per mode, so a
+ * product; items with at most 32 rows or columns or fewer than 256
+ * contraction indices stay FP64).  Plans are kept per mode, so a
  * solver can switch back to FP64 for its final iterations.  A pipeline wait
  * that times out inside a kernel is reported as an error by the next call
  * that synchronises (gccu_sync, norms, downloads). */
