@@ -631,17 +631,27 @@ class Engine {
         }
         int64_t kchunk = ((d.K + ks - 1) / ks + kGemmK - 1) / kGemmK * kGemmK;
         d.exclusive = kind != kGemmSmall && !d.cmapped && writers[d.c] == 1 && kchunk >= d.K;
-        for (int64_t m = 0; m < mt; ++m)
-          for (int64_t n = 0; n < nt; ++n)
-            for (int64_t k0 = 0; k0 < d.K; k0 += kchunk) {
-              TileDesc tl{};
-              tl.item = (int32_t)i;
-              tl.m0 = (int32_t)(m * TM);
-              tl.n0 = (int32_t)(n * TN);
-              tl.k0 = k0;
-              tl.k1 = std::min(d.K, k0 + kchunk);
-              tiles.push_back(tl);
-            }
+        auto add = [&](int64_t m, int64_t n, int64_t k0) {
+          TileDesc tl{};
+          tl.item = (int32_t)i;
+          tl.m0 = (int32_t)(m * TM);
+          tl.n0 = (int32_t)(n * TN);
+          tl.k0 = k0;
+          tl.k1 = std::min(d.K, k0 + kchunk);
+          tiles.push_back(tl);
+        };
+        if (kind == kGemmTc) {
+          // contraction chunk outermost: the tiles in flight share one chunk,
+          // whose column operand stays in L2 while each row band's chunk is
+          // reused by its column tiles one after the other
+          for (int64_t k0 = 0; k0 < d.K; k0 += kchunk)
+            for (int64_t m = 0; m < mt; ++m)
+              for (int64_t n = 0; n < nt; ++n) add(m, n, k0);
+        } else {
+          for (int64_t m = 0; m < mt; ++m)
+            for (int64_t n = 0; n < nt; ++n)
+              for (int64_t k0 = 0; k0 < d.K; k0 += kchunk) add(m, n, k0);
+        }
       }
       dp.ntiles_g[kind] = (int64_t)tiles.size();
       dp.ndesc_g[kind] = (int64_t)g[kind].size();

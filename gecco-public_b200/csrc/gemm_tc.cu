@@ -140,38 +140,54 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   lo = __uint_as_float(l);
 }
 
-// Loads of one operand slice: group g of 32 elements = core matrix (kg, rg)
-// = rows 8rg..8rg+7 x k 4kg..4kg+3; lane -> row 8rg + lane/4, k 4kg + lane%4,
-// which is also its float offset within the group's 32 floats.  The slice's
-// 32 k offsets arrive in one register per lane (kreg, lane = k - k0) and are
-// handed out by shuffles; elements outside the item are not loaded (zero).
-template <int R, int NG>
+// Operand slice of R rows x 32 contraction indices.  A thread owns the four
+// consecutive indices of one core-matrix row: row = 8 rg + lane%8 (fixed for
+// the whole tile, so its offset stays in a register), kgroup kg = 4 kq +
+// lane/8 for its NU units kq (kq = unit index: (R/8) row groups x 2 halves of
+// the slice are spread over the warps).  The slice's 32 k offsets arrive in
+// one register per lane (kreg, lane = k - k0) and are handed out by
+// shuffles; elements outside the item are not loaded (zero).  hi/lo go to
+// shared memory as one 16-byte store each per unit; a warp writes four whole
+// 128-byte core matrices.
+template <int R>
+struct Unit {
+  static constexpr int NU = R * 8 / (32 * NW);  // units (4 elements) per thread
+  static __device__ __forceinline__ int rg(int warp, int i) { return (warp + NW * i) % (R / 8); }
+  static __device__ __forceinline__ int kq(int warp, int i) { return (warp + NW * i) / (R / 8); }
+};
+
+template <int R>
 __device__ __forceinline__ void gather(const double* __restrict__ x, int64_t kreg,
-                                       const int64_t* rofs_s, int warp, int lane, int64_t kvalid,
-                                       int64_t rows, double (&v)[NG]) {
+                                       int64_t roff, bool rok, int warp, int lane, int64_t kvalid,
+                                       double (&v)[Unit<R>::NU][4]) {
 #pragma unroll
-  for (int i = 0; i < NG; ++i) {
-    const int g = warp + NW * i;
-    const int kg = g / (R / 8), rg = g % (R / 8);
-    const int r = 8 * rg + (lane >> 2);
-    const int kk = 4 * kg + (lane & 3);
-    const int64_t ko = __shfl_sync(0xffffffffu, kreg, kk);
-    double val = 0.0;
-    if (r < rows && kk < kvalid) val = __ldg(x + rofs_s[r] + ko);
-    v[i] = val;
+  for (int i = 0; i < Unit<R>::NU; ++i) {
+    const int kg = 4 * Unit<R>::kq(warp, i) + (lane >> 3);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int kk = 4 * kg + j;
+      const int64_t ko = __shfl_sync(0xffffffffu, kreg, kk);
+      double val = 0.0;
+      if (rok && kk < kvalid) val = __ldg(x + roff + ko);
+      v[i][j] = val;
+    }
   }
 }
 
-template <int R, int NG>
+template <int R>
 __device__ __forceinline__ void store_split(float* hi, float* lo, int warp, int lane,
-                                            const double (&v)[NG]) {
+                                            const double (&v)[Unit<R>::NU][4]) {
 #pragma unroll
-  for (int i = 0; i < NG; ++i) {
-    const int g = warp + NW * i;
-    float h, l;
-    split_tf32(v[i], h, l);
-    hi[32 * g + lane] = h;
-    lo[32 * g + lane] = l;
+  for (int i = 0; i < Unit<R>::NU; ++i) {
+    const int kg = 4 * Unit<R>::kq(warp, i) + (lane >> 3);
+    const int off = (kg * (R / 8) + Unit<R>::rg(warp, i)) * 32 + (lane & 7) * 4;
+    float4 h, l;
+    split_tf32(v[i][0], h.x, l.x);
+    split_tf32(v[i][1], h.y, l.y);
+    split_tf32(v[i][2], h.z, l.z);
+    split_tf32(v[i][3], h.w, l.w);
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
   }
 }
 
@@ -220,8 +236,12 @@ __global__ void __launch_bounds__(TNT, 1)
     }
   __syncthreads();
 
-  constexpr int NGA = TBM * TBK / 32 / NW;  // groups per warp and slice
-  constexpr int NGB = BN * TBK / 32 / NW;
+  static_assert(Unit<TBM>::NU >= 1 && Unit<BN>::NU >= 1, "tile too small for the threads");
+  // the row of this thread in each operand tile (the same in all its units)
+  const int ra = 8 * Unit<TBM>::rg(warp, 0) + (lane & 7);
+  const int rb = 8 * Unit<BN>::rg(warp, 0) + (lane & 7);
+  const bool rok_a = ra < rows, rok_b = rb < cols;
+  const int64_t roff_a = rok_a ? S.aro[ra] : 0, roff_b = rok_b ? S.bco[rb] : 0;
   const uint32_t kIdesc = idesc_tf32<TBM, BN>();
   const int64_t nk = (td.k1 - td.k0 + TBK - 1) / TBK;
   bool ok = true;
@@ -246,13 +266,13 @@ __global__ void __launch_bounds__(TNT, 1)
     }
     const int64_t kvalid = td.k1 - (td.k0 + t * TBK);
     {
-      double va[NGA], vb[NGB];
-      gather<TBM, NGA>(d.a, ka, S.aro, warp, lane, kvalid, rows, va);
-      gather<BN, NGB>(d.b, kb, S.bco, warp, lane, kvalid, cols, vb);
+      double va[Unit<TBM>::NU][4], vb[Unit<BN>::NU][4];
+      gather<TBM>(d.a, ka, roff_a, rok_a, warp, lane, kvalid, va);
+      gather<BN>(d.b, kb, roff_b, rok_b, warp, lane, kvalid, vb);
       ka = kfetch(d.ako, t + 1);  // next slice's offsets, in flight during the stores
       kb = kfetch(d.bko, t + 1);
-      store_split<TBM, NGA>(S.a[s][0], S.a[s][1], warp, lane, va);
-      store_split<BN, NGB>(S.b[s][0], S.b[s][1], warp, lane, vb);
+      store_split<TBM>(S.a[s][0], S.a[s][1], warp, lane, va);
+      store_split<BN>(S.b[s][0], S.b[s][1], warp, lane, vb);
     }
     // generic-proxy stores -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
