@@ -64,6 +64,8 @@ struct GemmDesc {
   double* c;
   const int64_t *cro, *cco;
   int32_t afast, bfast;  // 1: contiguous along k (else along rows / columns)
+  // k offset tables that are affine, ako[k] = ako[0] + k * akstep (0: not affine)
+  int64_t akstep, bkstep;
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update

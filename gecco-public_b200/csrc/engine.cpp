@@ -435,6 +435,17 @@ class Engine {
     }
   }
 
+  // step of an offset table that is affine in its index (tab[k] = tab[0] +
+  // k * step, step != 0), else 0
+  static int64_t affine_step(const std::vector<int64_t>& tabs, int64_t at, int64_t n) {
+    if (n < 2) return 0;
+    const int64_t step = tabs[at + 1] - tabs[at];
+    if (step == 0) return 0;
+    for (int64_t k = 2; k < n; ++k)
+      if (tabs[at + k] - tabs[at] != k * step) return 0;
+    return step;
+  }
+
   // GEMM descriptors, offset tables, pack jobs and tiles of one plan
   void build_gemm(DevPlan& dp) {
     Plan& P = dp.plan;
@@ -536,10 +547,12 @@ class Engine {
       d.a = pack_off1[i] >= 0 ? dp.scratch + pack_off1[i] : x1 + it.base1;
       d.aro = dp.d_tabs + t.aro;
       d.ako = dp.d_tabs + t.ako;
+      d.akstep = affine_step(tabs, t.ako, it.K);
       d.afast = pack_off1[i] >= 0 ? 0 : it.kfast1;
       d.b = pack_off2[i] >= 0 ? dp.scratch + pack_off2[i] : x2 + it.base2;
       d.bco = dp.d_tabs + t.bco;
       d.bko = dp.d_tabs + t.bko;
+      d.bkstep = affine_step(tabs, t.bko, it.K);
       d.bfast = pack_off2[i] >= 0 ? 0 : it.kfast2;
       d.c = x12 + it.base12;
       d.cro = dp.d_tabs + t.cro;
@@ -557,6 +570,7 @@ class Engine {
         std::swap(d.a, d.b);
         std::swap(d.aro, d.bco);
         std::swap(d.ako, d.bko);
+        std::swap(d.akstep, d.bkstep);
         std::swap(d.afast, d.bfast);
         std::swap(d.cro, d.cco);
         d.rowspace = kEx2;

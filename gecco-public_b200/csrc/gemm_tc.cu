@@ -140,54 +140,46 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   lo = __uint_as_float(l);
 }
 
-// Operand slice of R rows x 32 contraction indices.  A thread owns the four
-// consecutive indices of one core-matrix row: row = 8 rg + lane%8 (fixed for
-// the whole tile, so its offset stays in a register), kgroup kg = 4 kq +
-// lane/8 for its NU units kq (kq = unit index: (R/8) row groups x 2 halves of
-// the slice are spread over the warps).  The slice's 32 k offsets arrive in
-// one register per lane (kreg, lane = k - k0) and are handed out by
-// shuffles; elements outside the item are not loaded (zero).  hi/lo go to
-// shared memory as one 16-byte store each per unit; a warp writes four whole
-// 128-byte core matrices.
+// Operand slice of R rows x 32 contraction indices.  Group g (one per warp
+// and unit i, g = warp + NW i) is the core matrix (kg, rg) = rows 8rg..8rg+7
+// x indices 4kg..4kg+3; lane -> row 8rg + lane/4, index 4kg + lane%4, which is
+// also its float offset within the group's 32 floats.  A warp's load covers
+// 8 rows x 4 consecutive indices (coalesced whichever way the operand is
+// stored); a thread's row is the same in all its units (its offset stays in
+// a register).  The k offset comes from k0 + step*k when the operand's table
+// is affine, else from the slice's 32 table values (one per lane, kreg) by
+// shuffle.  Elements outside the item are not loaded (zero).
 template <int R>
 struct Unit {
-  static constexpr int NU = R * 8 / (32 * NW);  // units (4 elements) per thread
+  static constexpr int NU = R * TBK / (32 * NW);  // elements per thread and slice
   static __device__ __forceinline__ int rg(int warp, int i) { return (warp + NW * i) % (R / 8); }
-  static __device__ __forceinline__ int kq(int warp, int i) { return (warp + NW * i) / (R / 8); }
+  static __device__ __forceinline__ int kg(int warp, int i) { return (warp + NW * i) / (R / 8); }
 };
 
 template <int R>
-__device__ __forceinline__ void gather(const double* __restrict__ x, int64_t kreg,
-                                       int64_t roff, bool rok, int warp, int lane, int64_t kvalid,
-                                       double (&v)[Unit<R>::NU][4]) {
+__device__ __forceinline__ void gather(const double* __restrict__ x, int64_t kreg, int64_t kbase,
+                                       int64_t kstep, int64_t roff, bool rok, int warp, int lane,
+                                       int64_t kvalid, double (&v)[Unit<R>::NU]) {
 #pragma unroll
   for (int i = 0; i < Unit<R>::NU; ++i) {
-    const int kg = 4 * Unit<R>::kq(warp, i) + (lane >> 3);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int kk = 4 * kg + j;
-      const int64_t ko = __shfl_sync(0xffffffffu, kreg, kk);
-      double val = 0.0;
-      if (rok && kk < kvalid) val = __ldg(x + roff + ko);
-      v[i][j] = val;
-    }
+    const int kk = 4 * Unit<R>::kg(warp, i) + (lane & 3);
+    const int64_t ko = kstep ? kbase + kk * kstep : __shfl_sync(0xffffffffu, kreg, kk);
+    double val = 0.0;
+    if (rok && kk < kvalid) val = __ldg(x + roff + ko);
+    v[i] = val;
   }
 }
 
 template <int R>
 __device__ __forceinline__ void store_split(float* hi, float* lo, int warp, int lane,
-                                            const double (&v)[Unit<R>::NU][4]) {
+                                            const double (&v)[Unit<R>::NU]) {
 #pragma unroll
   for (int i = 0; i < Unit<R>::NU; ++i) {
-    const int kg = 4 * Unit<R>::kq(warp, i) + (lane >> 3);
-    const int off = (kg * (R / 8) + Unit<R>::rg(warp, i)) * 32 + (lane & 7) * 4;
-    float4 h, l;
-    split_tf32(v[i][0], h.x, l.x);
-    split_tf32(v[i][1], h.y, l.y);
-    split_tf32(v[i][2], h.z, l.z);
-    split_tf32(v[i][3], h.w, l.w);
-    *reinterpret_cast<float4*>(hi + off) = h;
-    *reinterpret_cast<float4*>(lo + off) = l;
+    const int g = warp + NW * i;
+    float h, l;
+    split_tf32(v[i], h, l);
+    hi[32 * g + lane] = h;
+    lo[32 * g + lane] = l;
   }
 }
 
@@ -238,8 +230,10 @@ __global__ void __launch_bounds__(TNT, 1)
 
   static_assert(Unit<TBM>::NU >= 1 && Unit<BN>::NU >= 1, "tile too small for the threads");
   // the row of this thread in each operand tile (the same in all its units)
-  const int ra = 8 * Unit<TBM>::rg(warp, 0) + (lane & 7);
-  const int rb = 8 * Unit<BN>::rg(warp, 0) + (lane & 7);
+  static_assert(NW % (TBM / 8) == 0 && NW % (BN / 8) == 0,
+                "a thread's row must be the same in all its units");
+  const int ra = 8 * Unit<TBM>::rg(warp, 0) + (lane >> 2);
+  const int rb = 8 * Unit<BN>::rg(warp, 0) + (lane >> 2);
   const bool rok_a = ra < rows, rok_b = rb < cols;
   const int64_t roff_a = rok_a ? S.aro[ra] : 0, roff_b = rok_b ? S.bco[rb] : 0;
   const uint32_t kIdesc = idesc_tf32<TBM, BN>();
@@ -247,11 +241,13 @@ __global__ void __launch_bounds__(TNT, 1)
   bool ok = true;
   int64_t last = -1;  // last slice whose MMAs were committed
   // k offsets of a slice, one per lane (prefetched a slice ahead)
-  auto kfetch = [&](const int64_t* tab, int64_t t) -> int64_t {
+  auto kfetch = [&](const int64_t* tab, int64_t step, int64_t t) -> int64_t {
     const int64_t k = td.k0 + t * TBK + lane;
-    return (t < nk && k < td.k1) ? __ldg(tab + k) : 0;
+    return (!step && t < nk && k < td.k1) ? __ldg(tab + k) : 0;
   };
-  int64_t ka = kfetch(d.ako, 0), kb = kfetch(d.bko, 0);
+  const int64_t akstep = d.akstep, bkstep = d.bkstep;
+  const int64_t ak0 = akstep ? __ldg(d.ako + td.k0) : 0, bk0 = bkstep ? __ldg(d.bko + td.k0) : 0;
+  int64_t ka = kfetch(d.ako, akstep, 0), kb = kfetch(d.bko, bkstep, 0);
   for (int64_t t = 0; t < nk && ok; ++t) {
     const int s = (int)(t & 1);
     if (t >= kTcStages) {  // the MMAs that read this stage two slices ago are done
@@ -266,11 +262,11 @@ __global__ void __launch_bounds__(TNT, 1)
     }
     const int64_t kvalid = td.k1 - (td.k0 + t * TBK);
     {
-      double va[Unit<TBM>::NU][4], vb[Unit<BN>::NU][4];
-      gather<TBM>(d.a, ka, roff_a, rok_a, warp, lane, kvalid, va);
-      gather<BN>(d.b, kb, roff_b, rok_b, warp, lane, kvalid, vb);
-      ka = kfetch(d.ako, t + 1);  // next slice's offsets, in flight during the stores
-      kb = kfetch(d.bko, t + 1);
+      double va[Unit<TBM>::NU], vb[Unit<BN>::NU];
+      gather<TBM>(d.a, ka, ak0 + t * TBK * akstep, akstep, roff_a, rok_a, warp, lane, kvalid, va);
+      gather<BN>(d.b, kb, bk0 + t * TBK * bkstep, bkstep, roff_b, rok_b, warp, lane, kvalid, vb);
+      ka = kfetch(d.ako, akstep, t + 1);  // next slice's offsets, in flight during the stores
+      kb = kfetch(d.bko, bkstep, t + 1);
       store_split<TBM>(S.a[s][0], S.a[s][1], warp, lane, va);
       store_split<BN>(S.b[s][0], S.b[s][1], warp, lane, vb);
     }
