@@ -128,13 +128,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// x -> (tf32(x), tf32(x - tf32(x))) as f32 bit patterns
+// x -> (tf32(xf), tf32(xf - tf32(xf))) with xf = f32(x), as f32 bit patterns:
+// one FP64 conversion per element, the rest on the FP32 pipe; hi + lo keeps
+// the 24 bits of xf to within 2^-22 relative
 __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   const float xf = (float)x;
   uint32_t h;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(xf));
   hi = __uint_as_float(h);
-  const float r = (float)(x - (double)hi);
+  const float r = xf - hi;  // exact in f32
   uint32_t l;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
   lo = __uint_as_float(l);
