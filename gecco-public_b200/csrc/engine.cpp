@@ -338,29 +338,27 @@ class Engine {
     return *(reos[os.str()] = std::move(dr));
   }
 
-  // cached plan of a descriptor, or null; never plans (gccu_contract_noalloc)
-  DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
+  std::string plan_key(const gccu_bc_desc* bc, bool use_tr) const {
     std::ostringstream os;
     os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
-       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision;
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision << ",t"
+       << (bc->tra_op1 != 0) << (bc->tra_op2 != 0) << (bc->tra_res != 0);
     for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
                                    << bc->occ_cnt[k];
-    auto it = plans.find(os.str());
+    return os.str();
+  }
+
+  // cached plan of a descriptor, or null; never plans (gccu_contract_noalloc)
+  DevPlan* find_plan(const gccu_bc_desc* bc, bool use_tr) {
+    auto it = plans.find(plan_key(bc, use_tr));
     return it == plans.end() ? nullptr : it->second.get();
   }
 
   DevPlan& plan_for(const gccu_bc_desc* bc, bool use_tr) {
-    std::ostringstream os;
-    os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
-       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision;
-    for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
-                                   << bc->occ_cnt[k];
-    std::string key = os.str();
+    std::string key = plan_key(bc, use_tr);
     auto it = plans.find(key);
     if (it != plans.end()) return *it->second;
     GCCU_REQUIRE(!capturing, "contraction must be run once before it is captured in a graph");
-    GCCU_REQUIRE(bc->tra_op1 == 0 && bc->tra_op2 == 0 && bc->tra_res == 0,
-                 "transposed operands are not supported by this engine version");
     ContractionSpec s;
     for (int64_t l : {bc->list_op1, bc->list_op2, bc->list_res})
       GCCU_REQUIRE(model.ops.at(list(l).L.op - 1).nj == 1,
@@ -378,6 +376,9 @@ class Engine {
       s.cnt[k] = (int)bc->occ_cnt[k];
     }
     s.use_tr = use_tr;
+    s.tra1 = bc->tra_op1 != 0;
+    s.tra2 = bc->tra_op2 != 0;
+    s.tra12 = bc->tra_res != 0;
     auto dp = std::make_unique<DevPlan>();
     dp->plan = plan_contraction(model, s);
     dp->list1 = (int)bc->list_op1;

@@ -70,20 +70,75 @@ int sum(const std::vector<Comp>& c) {
 }
 
 // leading dimensions, creator/annihilator sequence, X,P,V,H major
-// (contract/set_op_ldim_c.f:38-58)
+// (contract/set_op_ldim_c.f:38-58); for a class used transposed the
+// annihilators of each type come first, in reverse order, then the
+// creators (set_op_ldim_c.f:60-76), which is the stored order of the class
 void leading_dims(const std::vector<Comp>& c, const std::vector<Comp>& a,
                   const std::vector<int64_t>& lc, const std::vector<int64_t>& la,
-                  std::vector<int64_t>& ldc, std::vector<int64_t>& lda) {
+                  std::vector<int64_t>& ldc, std::vector<int64_t>& lda, bool transpose = false) {
   ldc.assign(c.size(), 0);
   lda.assign(a.size(), 0);
   int64_t ld = 1;
   for (int ih = 0; ih < 4; ++ih) {
     int t = kHpvxSeq[ih];
-    for (size_t i = 0; i < c.size(); ++i)
-      if (c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
-    for (size_t i = 0; i < a.size(); ++i)
-      if (a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+    if (!transpose) {
+      for (size_t i = 0; i < c.size(); ++i)
+        if (c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
+      for (size_t i = 0; i < a.size(); ++i)
+        if (a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+    } else {
+      for (size_t i = a.size(); i-- > 0;)
+        if (a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+      for (size_t i = c.size(); i-- > 0;)
+        if (c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
+    }
   }
+}
+
+// One occupation class seen as its adjoint (tra_op flags,
+// contract/contr_op1op2_wmaps_c.f:427-429,1127-1145): creators and
+// annihilators exchange roles, the total Ms of the list changes sign; every
+// stored distribution reappears with its C and A Ms / IRREP exchanged, under
+// the (Ms(A), IRREP(A)) key and distribution id of the adjoint, at its stored
+// offset.  Returned as a one-class layout (the class at index ib-1).
+ListLayout transposed_view(const ListLayout& L, int ib, int nsym) {
+  ListLayout T;
+  T.op = L.op;
+  T.gamt = L.gamt;
+  T.mst = -L.mst;
+  T.absym = L.absym;
+  T.len = L.len;
+  T.blk.resize(ib);
+  const LayoutBlock& B = L.blk.at(ib - 1);
+  LayoutBlock& V = T.blk[ib - 1];
+  V.vtx = B.vtx;
+  for (auto& o : V.vtx)
+    for (int t = 0; t < 4; ++t) std::swap(o[t], o[4 + t]);
+  for (int t = 0; t < 4; ++t) V.occ[t] = B.occ[4 + t], V.occ[4 + t] = B.occ[t];
+  V.c = B.a;
+  V.a = B.c;
+  V.off = B.off;
+  V.len = B.len;
+  const int na = sum(V.a), nc = sum(V.c);
+  for (const auto& kv : B.dis) {
+    for (const Dist& d : kv.second) {
+      Dist e = d;
+      e.msc = d.msa;
+      e.msa = d.msc;
+      e.gc = d.ga;
+      e.ga = d.gc;
+      int msa = 0, ga = 1;
+      for (size_t i = 0; i < e.msa.size(); ++i) msa += e.msa[i], ga = irrep_mult(ga, e.ga[i]);
+      std::vector<int> ixc(V.c.size()), ixa(V.a.size());
+      for (size_t i = 0; i < V.c.size(); ++i) ixc[i] = ms_index(V.c[i].occ, e.msc[i]);
+      for (size_t i = 0; i < V.a.size(); ++i) ixa[i] = ms_index(V.a[i].occ, e.msa[i]);
+      e.did = dist_id(V.c, ixc, e.gc, V.a, ixa, e.ga, nsym);
+      const auto key = std::make_pair(msa_to_idxms(msa, T.mst, na, nc), ga);
+      V.dis[key].push_back(e);
+      V.gm_len[key] += e.len;
+    }
+  }
+  return T;
 }
 
 const Dist& find_dist(const LayoutBlock& B, int ixms, int gam, int64_t did) {
@@ -177,7 +232,12 @@ void account(double* st, int64_t M, int64_t N, int64_t K) {
 Plan plan_contraction(Model& m, const ContractionSpec& s) {
   Plan P;
   const int nsym = m.os.nsym;
-  const ListLayout &L1 = *s.L1, &L2 = *s.L2, &L12 = *s.L12;
+  ListLayout T1, T2, T12;  // adjoint views of operands used transposed
+  if (s.tra1) T1 = transposed_view(*s.L1, s.ib1, nsym);
+  if (s.tra2) T2 = transposed_view(*s.L2, s.ib2, nsym);
+  if (s.tra12) T12 = transposed_view(*s.L12, s.ib12, nsym);
+  const ListLayout &L1 = s.tra1 ? T1 : *s.L1, &L2 = s.tra2 ? T2 : *s.L2,
+                   &L12 = s.tra12 ? T12 : *s.L12;
   GCCU_REQUIRE(s.ib1 >= 1 && s.ib1 <= (int)L1.blk.size(), "planner: bad op1 block");
   GCCU_REQUIRE(s.ib2 >= 1 && s.ib2 <= (int)L2.blk.size(), "planner: bad op2 block");
   GCCU_REQUIRE(s.ib12 >= 1 && s.ib12 <= (int)L12.blk.size(), "planner: bad result block");
@@ -373,9 +433,9 @@ Plan plan_contraction(Model& m, const ContractionSpec& s) {
                 it.N = dims[kEx2];
                 it.K = dims[kCnt];
                 std::vector<int64_t> ld1c, ld1a, ld2c, ld2a, ld12c, ld12a;
-                leading_dims(op1c, op1a, lo1c, lo1a, ld1c, ld1a);
-                leading_dims(op2c, op2a, lo2c, lo2a, ld2c, ld2a);
-                leading_dims(o12c, o12a, l12c, l12a, ld12c, ld12a);
+                leading_dims(op1c, op1a, lo1c, lo1a, ld1c, ld1a, s.tra1);
+                leading_dims(op2c, op2a, lo2c, lo2a, ld2c, ld2a, s.tra2);
+                leading_dims(o12c, o12a, l12c, l12a, ld12c, ld12a, s.tra12);
                 const int ncx1 = (int)ex1c.size(), ncx2 = (int)ex2c.size(),
                           ncn = (int)cntc.size();
                 Side s_cntc{&cntc, kCnt, 0, &ixcc, &dc.gc, &lcc};

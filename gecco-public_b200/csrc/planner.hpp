@@ -34,6 +34,9 @@ struct ContractionSpec {
   int ib1, ib2, ib12;
   Occ ex1, ex2, cnt;
   bool use_tr;
+  // operands used transposed (the reference's tra_op1 / tra_op2 / tra_op1op2):
+  // the class enters as its adjoint, creators and annihilators swapped
+  bool tra1 = false, tra2 = false, tra12 = false;
 };
 
 Plan plan_contraction(Model& m, const ContractionSpec& s);

@@ -303,12 +303,13 @@ class Engine:
 
     # ---- contraction / vector operations
     @staticmethod
-    def desc(op1, op2, res, ex1, ex2, cnt):
+    def desc(op1, op2, res, ex1, ex2, cnt, tra=(0, 0, 0)):
+        """tra = (tra_op1, tra_op2, tra_res): classes used as their adjoints"""
         d = BcDesc()
         d.list_op1, d.iblk_op1 = op1
         d.list_op2, d.iblk_op2 = op2
         d.list_res, d.iblk_res = res
-        d.tra_op1 = d.tra_op2 = d.tra_res = 0
+        d.tra_op1, d.tra_op2, d.tra_res = (int(t) for t in tra)
         for k in range(8):
             d.occ_ex1[k] = int(ex1[k])
             d.occ_ex2[k] = int(ex2[k])
@@ -316,8 +317,8 @@ class Engine:
         return d
 
     def contract(self, op1, op2, res, ex1, ex2, cnt, fact=1.0, update=True, use_tr=False,
-                 xret=0, desc=None):
-        d = desc if desc is not None else self.desc(op1, op2, res, ex1, ex2, cnt)
+                 xret=0, desc=None, tra=(0, 0, 0)):
+        d = desc if desc is not None else self.desc(op1, op2, res, ex1, ex2, cnt, tra)
         r = np.zeros(1)
         _call("gccu_contract", ctypes.byref(d), fact, int(update), int(use_tr), xret, _pd(r))
         return float(r[0])
@@ -330,8 +331,8 @@ class Engine:
         d = desc if desc is not None else self.desc(op1, op2, res, ex1, ex2, cnt)
         _call("gccu_contract_noalloc", ctypes.byref(d), fact, int(update), int(use_tr))
 
-    def plan_info(self, op1, op2, res, ex1, ex2, cnt, use_tr=False):
-        d = self.desc(op1, op2, res, ex1, ex2, cnt)
+    def plan_info(self, op1, op2, res, ex1, ex2, cnt, use_tr=False, tra=(0, 0, 0)):
+        d = self.desc(op1, op2, res, ex1, ex2, cnt, tra)
         n = np.zeros(1, np.int64)
         st = np.zeros(8)
         _call("gccu_plan_info", ctypes.byref(d), int(use_tr), _p64(n), _pd(st))

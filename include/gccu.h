@@ -108,12 +108,18 @@ int gccu_list_device_ptr(int64_t list_id, void** dptr);
  * (formula/process_bc.f:528-535).  update=0 overwrites the result class.
  * use_tr: spin-flip symmetry (calculate.routes.use_tr), applied when all three
  * lists carry absym != 0.  type_xret: 0 none, 1 squared norm of the result
- * class, 2 its first element (scalars); written to *xret. */
+ * class, 2 its first element (scalars); written to *xret.
+ * tra_op1/tra_op2/tra_res != 0: that class is used as its adjoint (the
+ * vertex's dagger flag, contract/get_bc_info3.f:173,191,391); the occ_*
+ * fields then describe the contraction of the adjoint, whose element
+ * (C strings I, A strings J) is the stored element (C = J, A = I), total Ms
+ * negated (contract/contr_op1op2_wmaps_c.f:427-429).  Operators of one
+ * vertex only. */
 typedef struct gccu_bc_desc {
   int64_t list_op1, iblk_op1;
   int64_t list_op2, iblk_op2;
   int64_t list_res, iblk_res;
-  int64_t tra_op1, tra_op2, tra_res; /* must be 0 in this engine version */
+  int64_t tra_op1, tra_op2, tra_res;
   int64_t occ_ex1[8], occ_ex2[8], occ_cnt[8];
 } gccu_bc_desc;
 int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr,

@@ -57,6 +57,10 @@ def lib():
         L.ora_contract.argtypes = ([ctypes.c_void_p, I64, I64, I64, PD, I64, I64, PD, I64, I64,
                                     PD, P64, P64, P64, ctypes.c_double, I64, I64, I64, I64, PD,
                                     PD])
+        L.ora_contract_t.restype = ctypes.c_int
+        L.ora_contract_t.argtypes = ([ctypes.c_void_p, I64, I64, I64, PD, I64, I64, PD, I64, I64,
+                                      PD, P64, P64, P64, ctypes.c_double, I64, I64, I64, I64, I64,
+                                      PD])
         L.ora_sym_ab_blk.restype = ctypes.c_int
         L.ora_sym_ab_blk.argtypes = [ctypes.c_void_p, I64, I64, PD, ctypes.c_double,
                                      ctypes.c_double]
@@ -170,8 +174,10 @@ class Oracle:
         return rows[:n]
 
     def contract(self, route, l1, b1, x1, l2, b2, x2, l12, b12, x12, ex1, ex2, cnt, fact,
-                 update=True, use_tr=False, str_block=200, cnt_block=-1, stats=None):
-        """x12 is updated in place (whole list buffer).  Returns xret."""
+                 update=True, use_tr=False, str_block=200, cnt_block=-1, stats=None,
+                 tra=(0, 0, 0)):
+        """x12 is updated in place (whole list buffer).  Returns xret.
+        tra = (tra_op1, tra_op2, tra_res): classes used as their adjoints."""
         xret = np.zeros(1)
         if b12 == 0:
             xret[0] = 0.0 if not update else (x12[0] if x12 is not None and x12.size else 0.0)
@@ -180,10 +186,16 @@ class Oracle:
         cn = np.ascontiguousarray(np.asarray(cnt, dtype=np.int64).reshape(8))
         st = stats if stats is not None else np.zeros(8)
         dummy = np.zeros(1)
-        rc = lib().ora_contract(self.ctx, route, l1, b1, _pd(x1), l2, b2, _pd(x2), l12, b12,
-                                _pd(x12 if x12 is not None else dummy), _p64(e1), _p64(e2),
-                                _p64(cn), fact, int(update), int(use_tr), str_block, cnt_block,
-                                _pd(xret), _pd(st))
+        if any(tra):
+            rc = lib().ora_contract_t(self.ctx, route, l1, b1, _pd(x1), l2, b2, _pd(x2), l12,
+                                      b12, _pd(x12 if x12 is not None else dummy), _p64(e1),
+                                      _p64(e2), _p64(cn), fact, int(update), int(use_tr),
+                                      int(tra[0]), int(tra[1]), int(tra[2]), _pd(xret))
+        else:
+            rc = lib().ora_contract(self.ctx, route, l1, b1, _pd(x1), l2, b2, _pd(x2), l12, b12,
+                                    _pd(x12 if x12 is not None else dummy), _p64(e1), _p64(e2),
+                                    _p64(cn), fact, int(update), int(use_tr), str_block,
+                                    cnt_block, _pd(xret), _pd(st))
         _chk(rc)
         return float(xret[0])
 

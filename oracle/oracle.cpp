@@ -3,8 +3,8 @@
 // TEST INFRASTRUCTURE ONLY (see oracle.h).  Restates, in plain C++, the
 // reference routines named at each function.  Scope: single-vertex operators
 // (njoined = 1), one GAS per hole/particle/valence/external type (frozen or
-// deleted orbitals are simply absent from the orbital counts), untransposed
-// operands, no reordering step.
+// deleted orbitals are simply absent from the orbital counts), no reordering
+// step inside a contraction.
 //
 // Parity pins (tests/golden): string counts and ME-list lengths printed by the
 // reference for the HF/cc-pVDZ MOLPRO fixture (test/python-interface.s.ref:
@@ -753,25 +753,39 @@ inline int mapval(const SideMap& s, int j, const int64_t* i1, const int64_t* i2)
   return s.ptr[j][i2[b] * s.n1[j] + i1[a]];
 }
 
-// set_op_ldim_c (contract/set_op_ldim_c.f), non-transposed
+// set_op_ldim_c (contract/set_op_ldim_c.f:27-76): per hpvx type C then A;
+// transposed, A (last component first) then C (last first)
 void ldims(const std::vector<Comp>& c, const std::vector<Comp>& a,
            const std::vector<int64_t>& ls, std::vector<int64_t>& ldc,
-           std::vector<int64_t>& lda) {
+           std::vector<int64_t>& lda, bool transpose = false) {
   ldc.assign(c.size(), 0);
   lda.assign(a.size(), 0);
   int64_t ld = 1;
   for (int ih = 0; ih < 4; ++ih) {
     int t = HPVXSEQ[ih];
-    for (size_t i = 0; i < c.size(); ++i)
-      if (c[i].hpvx == t) {
-        ldc[i] = ld;
-        ld *= ls[i];
-      }
-    for (size_t i = 0; i < a.size(); ++i)
-      if (a[i].hpvx == t) {
-        lda[i] = ld;
-        ld *= ls[c.size() + i];
-      }
+    if (!transpose) {
+      for (size_t i = 0; i < c.size(); ++i)
+        if (c[i].hpvx == t) {
+          ldc[i] = ld;
+          ld *= ls[i];
+        }
+      for (size_t i = 0; i < a.size(); ++i)
+        if (a[i].hpvx == t) {
+          lda[i] = ld;
+          ld *= ls[c.size() + i];
+        }
+    } else {
+      for (size_t i = a.size(); i-- > 0;)
+        if (a[i].hpvx == t) {
+          lda[i] = ld;
+          ld *= ls[c.size() + i];
+        }
+      for (size_t i = c.size(); i-- > 0;)
+        if (c[i].hpvx == t) {
+          ldc[i] = ld;
+          ld *= ls[i];
+        }
+    }
   }
 }
 
@@ -1079,11 +1093,21 @@ double ddot_blk(const double* x, int64_t n) {
 
 void sym_ab_blk(ora_ctx* cx, List& L, int iblk, double* buf, double prefac, double relfac);
 
-// contr_op1op2_wmaps_c (contract/contr_op1op2_wmaps_c.f:2-2169), buftyp 0
+// contr_op1op2_wmaps_c (contract/contr_op1op2_wmaps_c.f:2-2169), buftyp 0.
+// tra[0..2]: op1, op2, result used transposed (the vertex's dagger flag,
+// contract/get_bc_info3.f:173,191,391): the occupation enters daggered
+// (contract/occvtx4contr), the total Ms negated (:427-429), the IRREP loop
+// runs over the stored A IRREP which is the C IRREP of the adjoint
+// (:1127-1145), distribution ids are taken with C and A exchanged
+// (operators/idx_msgmdst2.f:64-66) and leading dimensions in A-C sequence
+// (contract/set_op_ldim_c.f:47-76).
 void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2, int ib2,
               const double* x2, int l12, int ib12, double* x12, const int* oex1,
               const int* oex2, const int* ocnt, double fact, bool update, bool use_tr,
-              int64_t str_block, int64_t cnt_block, double* xret, Stats* st) {
+              int64_t str_block, int64_t cnt_block, double* xret, Stats* st,
+              const bool* tra = nullptr) {
+  static const bool no_tra[3] = {false, false, false};
+  if (!tra) tra = no_tra;
   const List &L1 = cx->lists[l1 - 1], &L2 = cx->lists[l2 - 1];
   List& L12 = cx->lists[l12 - 1];
   CHECK(cx->ops[L1.op - 1].nj == 1 && cx->ops[L2.op - 1].nj == 1 &&
@@ -1091,19 +1115,20 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
         "contract: joined operators are not restated");
   const ListBlock &B1 = L1.blk[ib1 - 1], &B2 = L2.blk[ib2 - 1];
   int nsym = cx->oi.nsym;
-  // occupations of the operators
-  const int* o1 = cx->ops[L1.op - 1].occ[ib1 - 1].data();
-  const int* o2 = cx->ops[L2.op - 1].occ[ib2 - 1].data();
+  // occupations of the operators (daggered when used transposed)
+  int o1[8], o2[8];
+  auto dag = [](const int* o, bool t, int* out) {
+    for (int k = 0; k < 8; ++k) out[k] = t ? o[(k + 4) % 8] : o[k];
+  };
+  dag(cx->ops[L1.op - 1].occ[ib1 - 1].data(), tra[0], o1);
+  dag(cx->ops[L2.op - 1].occ[ib2 - 1].data(), tra[1], o2);
   int o12[8] = {0};
   static const ListBlock scalar_blk = [] {
     ListBlock s;
     return s;
   }();
   bool scalar = ib12 == 0;
-  if (!scalar) {
-    const int* oo = cx->ops[L12.op - 1].occ[ib12 - 1].data();
-    std::copy(oo, oo + 8, o12);
-  }
+  if (!scalar) dag(cx->ops[L12.op - 1].occ[ib12 - 1].data(), tra[2], o12);
   // consistency: op1 = ex1 + cnt, op2 = ex2 + cnt^+, op12 = ex1 + ex2
   for (int t = 0; t < 4; ++t) {
     CHECK(o1[t] == oex1[t] + ocnt[t] && o1[4 + t] == oex1[4 + t] + ocnt[4 + t],
@@ -1129,7 +1154,8 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
   ci.m12c = parse(mapping_info(oex1, false, oex2, false, o12, 0), (int)ci.op12c.size());
   ci.m12a = parse(mapping_info(oex2, false, oex1, false, o12, 1), (int)ci.op12a.size());
 
-  int mst1 = L1.mst, mst2 = L2.mst, mst12 = scalar ? 0 : L12.mst;
+  int mst1 = tra[0] ? -L1.mst : L1.mst, mst2 = tra[1] ? -L2.mst : L2.mst,
+      mst12 = scalar ? 0 : (tra[2] ? -L12.mst : L12.mst);
   int g1t = L1.gamt, g2t = L2.gamt, g12t = scalar ? 1 : L12.gamt;
   int na1 = sum_occ(ci.op1a), nc1 = sum_occ(ci.op1c), na2 = sum_occ(ci.op2a),
       nc2 = sum_occ(ci.op2c), na12 = sum_occ(ci.op12a), nc12 = sum_occ(ci.op12c);
@@ -1191,8 +1217,12 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
         } else if (!next_dist(graw, 3, gbnd, +1)) {
           break;
         }
-        int ga[3] = {graw[0], graw[1], graw[2]};
-        int gc[3] = {mult(ga[0], g1t), mult(ga[1], g2t), mult(ga[2], g12t)};
+        const int gt[3] = {g1t, g2t, g12t};
+        int ga[3], gc[3];
+        for (int q = 0; q < 3; ++q) {
+          ga[q] = tra[q] ? mult(graw[q], gt[q]) : graw[q];
+          gc[q] = tra[q] ? graw[q] : mult(graw[q], gt[q]);
+        }
         int ixm1 = msa2idxms4op(ms_a[0], mst1, na1, nc1);
         int ixm2 = msa2idxms4op(ms_a[1], mst2, na2, nc2);
         int ixm12 = msa2idxms4op(ms_a[2], mst12, na12, nc12);
@@ -1243,7 +1273,8 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
               SideMap m12a = side_map(cx, ci.m12a, ci.ex2a, ix2a, d2.ga, le2a, ci.ex1a, ix1a,
                                       d1.ga, le1a);
               if (!scalar && B12.dis.at({ixm12, graw[2]}).size() > 1) {
-                int64_t did = msgmdid2(ci.op12c, ixic, gic, ci.op12a, ixia, gia, nsym);
+                int64_t did = tra[2] ? msgmdid2(ci.op12a, ixia, gia, ci.op12c, ixic, gic, nsym)
+                                     : msgmdid2(ci.op12c, ixic, gic, ci.op12a, ixia, gia, nsym);
                 int64_t id = find_dis(B12, ixm12, graw[2], did);
                 idxop12 = B12.dis.at({ixm12, graw[2]})[id].off - ioff12;
               }
@@ -1262,7 +1293,8 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
                 auto lo1c = lens(cx, ci.op1c, ix1oc, g1c), lo1a = lens(cx, ci.op1a, ix1oa, g1a);
                 if (anyzero(lo1c) || anyzero(lo1a)) continue;
                 if (B1.dis.at({ixm1, graw[0]}).size() > 1) {
-                  int64_t did = msgmdid2(ci.op1c, ix1oc, g1c, ci.op1a, ix1oa, g1a, nsym);
+                  int64_t did = tra[0] ? msgmdid2(ci.op1a, ix1oa, g1a, ci.op1c, ix1oc, g1c, nsym)
+                                       : msgmdid2(ci.op1c, ix1oc, g1c, ci.op1a, ix1oa, g1a, nsym);
                   int64_t id = find_dis(B1, ixm1, graw[0], did);
                   idxop1 = B1.dis.at({ixm1, graw[0]})[id].off - ioff1;
                 }
@@ -1275,7 +1307,8 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
                 auto lo2c = lens(cx, ci.op2c, ix2oc, g2c), lo2a = lens(cx, ci.op2a, ix2oa, g2a);
                 if (anyzero(lo2c) || anyzero(lo2a)) continue;
                 if (B2.dis.at({ixm2, graw[1]}).size() > 1) {
-                  int64_t did = msgmdid2(ci.op2c, ix2oc, g2c, ci.op2a, ix2oa, g2a, nsym);
+                  int64_t did = tra[1] ? msgmdid2(ci.op2a, ix2oa, g2a, ci.op2c, ix2oc, g2c, nsym)
+                                       : msgmdid2(ci.op2c, ix2oc, g2c, ci.op2a, ix2oa, g2a, nsym);
                   int64_t id = find_dis(B2, ixm2, graw[1], did);
                   idxop2 = B2.dis.at({ixm2, graw[1]})[id].off - ioff2;
                 }
@@ -1295,9 +1328,9 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
                 b.lex1 = cat(le1c, le1a);
                 b.lex2 = cat(le2c, le2a);
                 b.lcnt = cat(lcc, lca);
-                ldims(ci.op1c, ci.op1a, cat(lo1c, lo1a), b.ld1c, b.ld1a);
-                ldims(ci.op2c, ci.op2a, cat(lo2c, lo2a), b.ld2c, b.ld2a);
-                ldims(ci.op12c, ci.op12a, cat(l12c, l12a), b.ld12c, b.ld12a);
+                ldims(ci.op1c, ci.op1a, cat(lo1c, lo1a), b.ld1c, b.ld1a, tra[0]);
+                ldims(ci.op2c, ci.op2a, cat(lo2c, lo2a), b.ld2c, b.ld2a, tra[1]);
+                ldims(ci.op12c, ci.op12a, cat(l12c, l12a), b.ld12c, b.ld12a, tra[2]);
                 b.m12c = m12c;
                 b.m12a = m12a;
                 b.m1c = side_map(cx, ci.m1c, ci.cntc, ixcc, dc.gc, lcc, ci.ex1c, ix1c, d1.gc, le1c);
@@ -1995,6 +2028,28 @@ int ora_contract(ora_ctx* c, int64_t route, int64_t list1, int64_t iblk1, const 
            str_block > 0 ? str_block : 200, cnt_block, xret, &st);
   if (stats)
     for (int k = 0; k < 8; ++k) stats[k] += st.v[k];
+  return 0;
+  GUARD_END(-1)
+}
+
+int ora_contract_t(ora_ctx* c, int64_t route, int64_t list1, int64_t iblk1, const double* x1,
+                   int64_t list2, int64_t iblk2, const double* x2, int64_t list12,
+                   int64_t iblk12, double* x12, const int64_t* occ_ex1, const int64_t* occ_ex2,
+                   const int64_t* occ_cnt, double fact, int64_t update, int64_t use_tr,
+                   int64_t tra_op1, int64_t tra_op2, int64_t tra_res, double* xret) {
+  GUARD_BEGIN
+  CHECK(route == 2 || route == 3, "route must be 2 or 3");
+  int e1[8], e2[8], cn[8];
+  for (int k = 0; k < 8; ++k) {
+    e1[k] = (int)occ_ex1[k];
+    e2[k] = (int)occ_ex2[k];
+    cn[k] = (int)occ_cnt[k];
+  }
+  const bool tra[3] = {tra_op1 != 0, tra_op2 != 0, tra_res != 0};
+  Stats st;
+  contract(c, (int)route, (int)list1, (int)iblk1, x1, (int)list2, (int)iblk2, x2, (int)list12,
+           (int)iblk12, x12, e1, e2, cn, fact, update != 0, use_tr != 0, 200, -1, xret, &st,
+           tra);
   return 0;
   GUARD_END(-1)
 }

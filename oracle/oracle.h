@@ -67,6 +67,18 @@ int ora_contract(ora_ctx*, int64_t route,
                  double fact, int64_t update, int64_t use_tr,
                  int64_t str_block, int64_t cnt_block,
                  double* xret, double* stats);
+/* the same with operands used transposed (tra_op1, tra_op2, tra_op1op2 of
+ * contract/contr_op1op2_wmaps_c.f): occ_ex1/occ_ex2/occ_cnt describe the
+ * contraction of the adjoint classes */
+int ora_contract_t(ora_ctx*, int64_t route,
+                   int64_t list1, int64_t iblk1, const double* x1,
+                   int64_t list2, int64_t iblk2, const double* x2,
+                   int64_t list12, int64_t iblk12, double* x12,
+                   const int64_t* occ_ex1, const int64_t* occ_ex2,
+                   const int64_t* occ_cnt,
+                   double fact, int64_t update, int64_t use_tr,
+                   int64_t tra_op1, int64_t tra_op2, int64_t tra_res,
+                   double* xret);
 
 /* spin-flip symmetrisation of a result block -- contract/sym_ab_blk.f */
 /* reorder (reo_op_wmaps_c / reo_blk_wmaps_c) of class iblk_ori of list_ori

@@ -120,3 +120,76 @@ def traces_for(space):
 def random_list(n, seed):
     rng = np.random.default_rng(seed)
     return rng.standard_normal(n)
+
+
+# operands used transposed: (tra_op1, tra_op2, tra_res) patterns
+TRANSPOSES = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 1, 1)]
+
+
+def _encode_did(comps, dist, nsym):
+    did, base = 0, 1
+    for (_, n), (ix, g) in zip(comps, dist):
+        did += ((ix - 1) * nsym + g - 1) * base
+        base *= (n + 1) * nsym
+    return did
+
+
+def transpose_list(src, lid_s, occ_s, x, lid_t, n_t, nsym):
+    """List vector of the adjoint class (occupation cnt_dag(occ_s), total
+    Ms negated) of the one-class list lid_s: its element with creator
+    strings J and annihilator strings I is the element of x with creator
+    strings I and annihilator strings J.  src: engine or oracle binding."""
+    from melist import condensed, decode_did, ldims
+
+    cs, as_ = condensed(occ_s)
+    ct, at = condensed(cnt_dag(occ_s))
+    where = {int(r[7]): int(r[4]) for r in src.dists(lid_t) if r[0] == 1}
+    y = np.full(n_t, np.nan)
+    for r in src.dists(lid_s):
+        if r[0] != 1:
+            continue
+        off, did = int(r[4]), int(r[7])
+        dist = decode_did(did, cs + as_, nsym)
+        lens = [src.strings(t, n, ix, g)[0].shape[0] for (t, n), (ix, g) in zip(cs + as_, dist)]
+        nc = len(cs)
+        dist_t, lens_t = dist[nc:] + dist[:nc], lens[nc:] + lens[:nc]
+        off_t = where[_encode_did(ct + at, dist_t, nsym)]
+        grids = np.meshgrid(*[np.arange(n) for n in lens], indexing="ij")
+        pos_s = np.asarray(sum(g * d for g, d in zip(grids, ldims(cs, as_, lens))))
+        pos_t = np.asarray(sum(g * d for g, d in zip(grids[nc:] + grids[:nc],
+                                                     ldims(ct, at, lens_t))))
+        y[off_t + pos_t.ravel()] = x[off + pos_s.ravel()]
+    assert not np.isnan(y).any()
+    return y
+
+
+def transpose_variants(space):
+    """(case, (gamt, mst) of op1, op2, result): symmetric lists, then a
+    non-totally-symmetric op1 and a spin-changing op2 where the space allows"""
+    nsym = SPACES[space][0]
+    for case in contractions_for(space):
+        yield case, ((1, 0), (1, 0), (1, 0))
+        if nsym > 1:
+            yield case, ((2, 0), (1, 0), (2, 0))
+        if case[2][:4].sum() > 0 and case[2][4:].sum() > 0:
+            yield case, ((1, 0), (1, 2), (1, 2))
+
+
+def _define_list(src, occ, gamt, mst, oracle):
+    op = src.define_op([occ]) if oracle else src.define_operator([occ])
+    return src.define_list(op, gamt, mst) if oracle else src.register_list(op, gamt, mst)
+
+
+def transpose_operands(src, case, sym, tra, oracle):
+    """per operand: (stored list, its length, explicit list, its length,
+    stored occupation); the stored list holds the adjoint class when the
+    operand is used transposed"""
+    out = []
+    for occ, (g, m), t in zip(case[1:4], sym, tra):
+        le, ne = _define_list(src, occ, g, m, oracle)
+        if t:
+            ls, ns = _define_list(src, cnt_dag(occ), g, -m, oracle)
+            out.append((ls, ns, le, ne, cnt_dag(occ)))
+        else:
+            out.append((le, ne, le, ne, occ))
+    return out
