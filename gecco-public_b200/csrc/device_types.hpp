@@ -66,6 +66,9 @@ struct GemmDesc {
   int32_t afast, bfast;  // 1: contiguous along k (else along rows / columns)
   // k offset tables that are affine, ako[k] = ako[0] + k * akstep (0: not affine)
   int64_t akstep, bkstep;
+  // tensor-core items: float offsets of the split operand panels in the
+  // split-TF32 workspace (see SplitJob)
+  int64_t pa, pb;
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update
@@ -86,6 +89,19 @@ struct ReoItem {
   int32_t nsp[2];
   int32_t rad[2][kDevMaxComp];
   OpndDesc ori, reo;
+};
+
+// Split of one operand of a tensor-core item into its TF32 panel: for the
+// row operand (op 0, tile rows TR = 128) and the column operand (op 1, TR =
+// 256) of descriptor `desc`, every (TR-row band, 32-index slice) of the
+// operand is stored as two planes (hi, lo) of TR x 32 floats in the
+// tensor core's K-major core-matrix order, [k/4][row][k%4]:
+//   panel[((band * nslice + slice) * 2 + plane) * TR * 32 + (k/4) * TR * 4 + row * 4 + k%4]
+// with rows and contraction indices outside the item set to zero.  The job's
+// blocks are 128-row x 32-index chunks numbered from cstart.
+struct SplitJob {
+  int32_t desc, op;
+  int64_t cstart;
 };
 
 // gather of one operand of one block contraction into a dense panel

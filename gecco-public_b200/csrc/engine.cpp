@@ -58,6 +58,9 @@ struct DevPlan {
   int64_t ntiles = 0;
   PackJob* d_jobs = nullptr;
   int64_t njobs = 0, pack_gx = 0, pack_gy = 0;
+  // split-TF32 panels of the tensor-core items (workspace floats, jobs)
+  SplitJob* d_split = nullptr;
+  int64_t nsplit = 0, split_chunks = 0, ws_floats = 0;
   int64_t* d_tabs = nullptr;
   double* scratch = nullptr;
   int64_t scratch_len = 0;
@@ -103,6 +106,10 @@ class Engine {
   cudaEvent_t slots[64] = {};
   bool profiling = false;
   int precision = 0;     // 0: FP64 DMMA, 1: split TF32 on tcgen05 for regular/medium items
+  // split-TF32 operand panels, shared by all plans (one stream orders them);
+  // grown to the largest plan's need, never while a graph is being captured
+  float* tc_ws = nullptr;
+  int64_t tc_ws_floats = 0;
   int* d_err = nullptr;  // set by kernels whose bounded pipeline waits ran out
   // fixed scratch of gccu_contract_noalloc, looked up on its first call
   bool have_static = false;
@@ -156,6 +163,28 @@ class Engine {
     mem_used += (int64_t)bytes;
     return p;
   }
+  void release(void* p, size_t bytes) {
+    for (size_t i = 0; i < allocs.size(); ++i)
+      if (allocs[i] == p) {
+        allocs.erase(allocs.begin() + (long)i);
+        CUDA_OK(cudaFree(p));
+        mem_used -= (int64_t)bytes;
+        return;
+      }
+  }
+
+  void ensure_tc_ws(int64_t floats) {
+    if (floats <= tc_ws_floats) return;
+    GCCU_REQUIRE(!capturing, "split-TF32 workspace must grow outside a graph capture");
+    CUDA_OK(cudaStreamSynchronize(stream));  // earlier launches may still read it
+    if (tc_ws) release(tc_ws, (size_t)tc_ws_floats * sizeof(float));
+    tc_ws = nullptr;
+    tc_ws_floats = 0;
+    tc_ws = (float*)alloc((size_t)floats * sizeof(float));
+    tc_ws_floats = floats;
+    CUDA_OK(set_tc_workspace(tc_ws));
+  }
+
   template <class T>
   T* upload(const std::vector<T>& v) {
     T* p = (T*)alloc(v.size() * sizeof(T));
@@ -668,6 +697,28 @@ class Engine {
               for (int64_t k0 = 0; k0 < d.K; k0 += kchunk) add(m, n, k0);
         }
       }
+      if (kind == kGemmTc && !g[kind].empty()) {
+        // operand panels of every item, row operand then column operand
+        std::vector<SplitJob> sj;
+        int64_t off = 0, cs = 0;
+        for (size_t i = 0; i < g[kind].size(); ++i) {
+          GemmDesc& d = g[kind][i];
+          d.pa = off;
+          off += tc_panel_floats(d.M, kGemmTcM, d.K);
+          d.pb = off;
+          off += tc_panel_floats(d.N, kGemmTcN, d.K);
+          sj.push_back(SplitJob{(int32_t)i, 0, cs});
+          cs += tc_split_chunks(d.M, kGemmTcM, d.K);
+          sj.push_back(SplitJob{(int32_t)i, 1, cs});
+          cs += tc_split_chunks(d.N, kGemmTcN, d.K);
+        }
+        GCCU_REQUIRE(cs < INT32_MAX, "tensor-core operands too large for one split launch");
+        dp.ws_floats = off;
+        dp.nsplit = (int64_t)sj.size();
+        dp.split_chunks = cs;
+        dp.d_split = upload(sj);
+        ensure_tc_ws(off);
+      }
       dp.ntiles_g[kind] = (int64_t)tiles.size();
       dp.ndesc_g[kind] = (int64_t)g[kind].size();
       if (!tiles.empty()) {
@@ -1172,6 +1223,10 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       first += dp.ndesc_g[kind];
       launch_rebase_descs(dp.d_desc[kind], descs, dp.ndesc_g[kind], dp.scratch, dp.scratch_len,
                           ss.panels, e.stream);
+      if (kind == kGemmTc && dp.nsplit) {  // panels in the engine's existing workspace
+        launch_split_tc(descs, dp.d_split, dp.nsplit, dp.split_chunks, e.stream);
+        ++e.launches;
+      }
       launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err, e.stream);
       e.launches += 2;
     }
@@ -1215,6 +1270,10 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     }
     if (dp.njobs) {
       launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
+      ++e.launches;
+    }
+    if (dp.nsplit) {  // operand split of the tensor-core items (after the pack it may read)
+      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, e.stream);
       ++e.launches;
     }
     cudaEvent_t evp = nullptr;

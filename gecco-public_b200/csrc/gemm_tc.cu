@@ -8,45 +8,53 @@
 // scatter_block, contract/scatter_block.f:163), so the FP32 accumulation
 // error does not grow with the full contraction length.
 //
-// One CTA per 128 x BN output tile, 1024 threads (32 warps: the gathers are
-// latency-bound, so many warps in flight matter more than per-thread
-// batching).  Per 32-wide slice of the
-// contraction index all threads gather the FP64 operand elements through the
-// offset tables (the same tables as the FP64 kernel), split them and store
-// them to shared memory in the K-major core-matrix layout the tensor core
-// reads (8 rows x 16 bytes per core matrix, no swizzle); one thread then
-// issues the 12 MMAs of the slice (4 K-steps x 3 products) and commits them to
-// the slice's mbarrier.  Two slices are in flight: the loads of slice t+1
-// overlap the MMAs of slice t.  The accumulator is read back with tcgen05.ld
-// (one TMEM lane per output row) and scattered with the map signs.
+// Two kernels.  k_split_tc reads each operand of each item once through the
+// item's offset tables (the gather of collect_block_impr,
+// contract/collect_block_impr.f:397, already done for map-addressed operands
+// by the pack kernel), splits it and writes both halves as panels in the
+// K-major core-matrix order the tensor core reads (8 rows x 16 bytes per core
+// matrix, no swizzle).  k_gemm_tc then runs one CTA per 128 x 256 output tile
+// with warp roles: one thread streams the tile's panel slices into a 4-stage
+// shared-memory ring with bulk asynchronous copies (cp.async.bulk, completion
+// counted in bytes on an mbarrier), one thread issues the MMAs of each stage
+// (2 K-steps x 3 products) and commits them to the stage's release barrier;
+// after the last stage all 8 warps read the accumulator back with tcgen05.ld
+// (one TMEM lane per output row) and scatter it with the map signs.
 //
 // Every wait on an mbarrier is bounded; on time-out the kernel records the
-// failure in *err, stops issuing work, waits (bounded) for the MMAs it has
-// issued, frees its TMEM and returns.
+// failure in *err, stops issuing work, waits (bounded) for the copies and
+// MMAs it has issued, frees its TMEM and returns.
 #include <cstdio>
 
 #include "index.cuh"
 #include "kernels.hpp"
 
 namespace gccu {
+
+// split-TF32 operand panels of the running contraction (set_tc_workspace)
+__device__ float* g_tc_ws;
+
 namespace {
 
-constexpr int TBM = 128;    // tile rows = TMEM lanes
-constexpr int TBK = 32;     // contraction indices per slice
-constexpr int TNT = 1024;   // threads: latency of the gathers is hidden by warps
+constexpr int TBM = kGemmTcM;  // tile rows = TMEM lanes
+constexpr int TBN = kGemmTcN;  // tile columns = TMEM columns
+constexpr int SK = (int)kTcSlice;  // contraction indices per panel slice
+constexpr int BK = 16;         // contraction indices per pipeline stage
+constexpr int NST = 4;         // pipeline stages
+constexpr int TNT = 256;       // threads: 8 warps (the epilogue reads TMEM lanes 32(w%4)..)
 constexpr int NW = TNT / 32;
-constexpr int kTcStages = 2;
 constexpr long kWaitLimit = 1L << 22;
+constexpr uint32_t kStageBytes = 2u * (TBM + TBN) * BK * sizeof(float);
 
-template <int BN>
 struct __align__(1024) TcSmem {
-  float a[kTcStages][2][TBM * TBK];  // [stage][hi/lo][core-matrix layout]
-  float b[kTcStages][2][BN * TBK];
-  int64_t aro[TBM], bco[BN], cro[TBM], cco[BN];
+  float a[NST][2][TBM * BK];  // [stage][hi/lo][k/4][row][k%4]
+  float b[NST][2][TBN * BK];
+  int64_t cro[TBM], cco[TBN];
   int32_t rc[TBM][kDevMaxComp];
-  int32_t cc[BN][kDevMaxComp];
+  int32_t cc[TBN][kDevMaxComp];
   GemmDesc d;
-  alignas(8) uint64_t bar[kTcStages];
+  alignas(8) uint64_t full[NST], empty[NST], done;
+  int64_t issued, consumed;  // stages whose copies were issued / whose MMAs were issued
   uint32_t tmem_base;
   int failed;
 };
@@ -91,8 +99,28 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(bar), "r"(count) : "memory");
 }
 
-// bounded wait for the completion of phase `parity`; false on time-out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// one arrival that also expects `bytes` of asynchronous copies in this phase
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :
+               : "r"(bar), "r"(bytes)
+               : "memory");
+}
+
+// bulk asynchronous copy global -> shared (no multicast), counted on bar
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :
+      : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// bounded wait for the completion of phase `parity`; false on time-out or
+// when another role of the CTA has failed
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          const volatile int* failed) {
   for (long it = 0; it < kWaitLimit; ++it) {
     uint32_t done;
     asm volatile(
@@ -103,6 +131,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if (failed && (it & 255) == 255 && *failed) return false;
   }
   return false;
 }
@@ -142,55 +171,95 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   lo = __uint_as_float(l);
 }
 
-// Operand slice of R rows x 32 contraction indices.  Group g (one per warp
-// and unit i, g = warp + NW i) is the core matrix (kg, rg) = rows 8rg..8rg+7
-// x indices 4kg..4kg+3; lane -> row 8rg + lane/4, index 4kg + lane%4, which is
-// also its float offset within the group's 32 floats.  A warp's load covers
-// 8 rows x 4 consecutive indices (coalesced whichever way the operand is
-// stored); a thread's row is the same in all its units (its offset stays in
-// a register).  The k offset comes from k0 + step*k when the operand's table
-// is affine, else from the slice's 32 table values (one per lane, kreg) by
-// shuffle.  Elements outside the item are not loaded (zero).
-template <int R>
-struct Unit {
-  static constexpr int NU = R * TBK / (32 * NW);  // elements per thread and slice
-  static __device__ __forceinline__ int rg(int warp, int i) { return (warp + NW * i) % (R / 8); }
-  static __device__ __forceinline__ int kg(int warp, int i) { return (warp + NW * i) / (R / 8); }
-};
+// ---- split pre-pass -------------------------------------------------------
+// One block per 128-row x 32-index chunk of one operand.  The chunk is read
+// coalesced along the operand's contiguous direction (contraction index when
+// kfast, else row), split, staged in shared memory in the panel order (each
+// k/4 plane padded by 4 floats so that neither read direction conflicts on
+// banks) and written out as 16-byte stores, consecutive threads on
+// consecutive rows.
+constexpr int kSplitThreads = 256;
+constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
 
-template <int R>
-__device__ __forceinline__ void gather(const double* __restrict__ x, int64_t kreg, int64_t kbase,
-                                       int64_t kstep, int64_t roff, bool rok, int warp, int lane,
-                                       int64_t kvalid, double (&v)[Unit<R>::NU]) {
+__global__ void __launch_bounds__(kSplitThreads)
+    k_split_tc(const GemmDesc* __restrict__ descs, const SplitJob* __restrict__ jobs,
+               int64_t njobs) {
+  __shared__ __align__(16) float sh[2][8 * kSplitPitch];
+  __shared__ int64_t ro[128];
+  __shared__ int64_t ko[SK];
+  const int tid = threadIdx.x;
+  const int64_t blk = blockIdx.x;
+  int64_t lo = 0, hi = njobs - 1;  // last job with cstart <= blk
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].cstart <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  const SplitJob J = jobs[lo];
+  const GemmDesc& d = descs[J.desc];
+  const bool row_op = J.op == 0;
+  const int64_t R = row_op ? d.M : d.N, K = d.K;
+  const int TR = row_op ? TBM : TBN;
+  const double* __restrict__ x = row_op ? d.a : d.b;
+  const int64_t* rtab = row_op ? d.aro : d.bco;
+  const int64_t* ktab = row_op ? d.ako : d.bko;
+  const int kfast = row_op ? d.afast : d.bfast;
+  const int64_t nsl = (K + SK - 1) / SK;
+  const int64_t c = blk - J.cstart;  // chunk = row chunk * nsl + slice
+  const int64_t r0 = (c / nsl) * 128, k0 = (c % nsl) * SK;
+  if (tid < 128) ro[tid] = r0 + tid < R ? __ldg(rtab + r0 + tid) : -1;
+  else if (tid < 128 + SK) ko[tid - 128] = k0 + (tid - 128) < K ? __ldg(ktab + k0 + tid - 128) : -1;
+  __syncthreads();
+  if (kfast) {  // warp: 16 rows, lane: contraction index
+    const int warp = tid >> 5, lane = tid & 31;
+    const int64_t kof = ko[lane];
+#pragma unroll 8
+    for (int i = 0; i < 16; ++i) {
+      const int r = warp * 16 + i;
+      const int64_t rof = ro[r];
+      const double v = (kof >= 0 && rof >= 0) ? __ldg(x + rof + kof) : 0.0;
+      float h, l;
+      split_tf32(v, h, l);
+      sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
+      sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
+    }
+  } else {  // thread: one row, 16 contraction indices
+    const int r = tid & 127, kh = tid >> 7;
+    const int64_t rof = ro[r];
 #pragma unroll
-  for (int i = 0; i < Unit<R>::NU; ++i) {
-    const int kk = 4 * Unit<R>::kg(warp, i) + (lane & 3);
-    const int64_t ko = kstep ? kbase + kk * kstep : __shfl_sync(0xffffffffu, kreg, kk);
-    double val = 0.0;
-    if (rok && kk < kvalid) val = __ldg(x + roff + ko);
-    v[i] = val;
+    for (int q = 0; q < 4; ++q) {
+      float4 h4, l4;
+      float* hp = &h4.x;
+      float* lp = &l4.x;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t kof = ko[16 * kh + 4 * q + e];
+        const double v = (kof >= 0 && rof >= 0) ? __ldg(x + rof + kof) : 0.0;
+        split_tf32(v, hp[e], lp[e]);
+      }
+      *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
+      *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+    }
+  }
+  __syncthreads();
+  const int64_t band = r0 / TR, rr0 = r0 % TR;
+  float* __restrict__ dst =
+      g_tc_ws + (row_op ? d.pa : d.pb) + (band * nsl + c % nsl) * 2 * TR * SK;
+#pragma unroll
+  for (int i = 0; i < 2 * 8 * 128 / kSplitThreads; ++i) {
+    const int u = tid + kSplitThreads * i;
+    const int plane = u >> 10, kq = (u >> 7) & 7, r = u & 127;
+    const float4 v = *reinterpret_cast<const float4*>(&sh[plane][kq * kSplitPitch + 4 * r]);
+    *reinterpret_cast<float4*>(dst + plane * TR * SK + kq * TR * 4 + (rr0 + r) * 4) = v;
   }
 }
 
-template <int R>
-__device__ __forceinline__ void store_split(float* hi, float* lo, int warp, int lane,
-                                            const double (&v)[Unit<R>::NU]) {
-#pragma unroll
-  for (int i = 0; i < Unit<R>::NU; ++i) {
-    const int g = warp + NW * i;
-    float h, l;
-    split_tf32(v[i], h, l);
-    hi[32 * g + lane] = h;
-    lo[32 * g + lane] = l;
-  }
-}
-
-template <int BN>
+// ---- GEMM ------------------------------------------------------------------
 __global__ void __launch_bounds__(TNT, 1)
     k_gemm_tc(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
               double alpha, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  TcSmem<BN>& S = *reinterpret_cast<TcSmem<BN>*>(smem_raw);
+  TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const TileDesc td = tiles[blockIdx.x];
   {
@@ -199,13 +268,20 @@ __global__ void __launch_bounds__(TNT, 1)
     for (int i = tid; i < (int)(sizeof(GemmDesc) / sizeof(int)); i += TNT) dst[i] = src[i];
   }
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&S.bar[s]), 1);
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(smem_u32(&S.full[s]), 1);
+      mbar_init(smem_u32(&S.empty[s]), 1);
+    }
+    mbar_init(smem_u32(&S.done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     S.failed = 0;
+    S.issued = 0;
+    S.consumed = 0;
   }
-  if (warp == 0) {  // TMEM: BN f32 columns x 128 lanes
+  if (warp == 0) {  // TMEM: TBN f32 columns x 128 lanes
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(&S.tmem_base)), "r"((uint32_t)BN)
+                 : "r"(smem_u32(&S.tmem_base)), "r"((uint32_t)TBN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -216,95 +292,90 @@ __global__ void __launch_bounds__(TNT, 1)
   const GemmDesc& d = S.d;
   const int64_t rows = d.M - td.m0, cols = d.N - td.n0;
   const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
-  for (int i = tid; i < TBM; i += TNT)
-    if (i < rows) {
-      S.aro[i] = d.aro[td.m0 + i];
-      S.cro[i] = d.cro[td.m0 + i];
-      if (d.cmapped) decomp(d.rad[d.rowspace], d.nsp[d.rowspace], td.m0 + i, S.rc[i]);
-    }
-  for (int i = tid; i < BN; i += TNT)
-    if (i < cols) {
-      S.bco[i] = d.bco[td.n0 + i];
-      S.cco[i] = d.cco[td.n0 + i];
-      if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
-    }
-  __syncthreads();
-
-  static_assert(Unit<TBM>::NU >= 1 && Unit<BN>::NU >= 1, "tile too small for the threads");
-  // the row of this thread in each operand tile (the same in all its units)
-  static_assert(NW % (TBM / 8) == 0 && NW % (BN / 8) == 0,
-                "a thread's row must be the same in all its units");
-  const int ra = 8 * Unit<TBM>::rg(warp, 0) + (lane >> 2);
-  const int rb = 8 * Unit<BN>::rg(warp, 0) + (lane >> 2);
-  const bool rok_a = ra < rows, rok_b = rb < cols;
-  const int64_t roff_a = rok_a ? S.aro[ra] : 0, roff_b = rok_b ? S.bco[rb] : 0;
-  const uint32_t kIdesc = idesc_tf32<TBM, BN>();
-  const int64_t nk = (td.k1 - td.k0 + TBK - 1) / TBK;
-  bool ok = true;
-  int64_t last = -1;  // last slice whose MMAs were committed
-  // k offsets of a slice, one per lane (prefetched a slice ahead)
-  auto kfetch = [&](const int64_t* tab, int64_t step, int64_t t) -> int64_t {
-    const int64_t k = td.k0 + t * TBK + lane;
-    return (!step && t < nk && k < td.k1) ? __ldg(tab + k) : 0;
-  };
-  const int64_t akstep = d.akstep, bkstep = d.bkstep;
-  const int64_t ak0 = akstep ? __ldg(d.ako + td.k0) : 0, bk0 = bkstep ? __ldg(d.bko + td.k0) : 0;
-  int64_t ka = kfetch(d.ako, akstep, 0), kb = kfetch(d.bko, bkstep, 0);
-  for (int64_t t = 0; t < nk && ok; ++t) {
-    const int s = (int)(t & 1);
-    if (t >= kTcStages) {  // the MMAs that read this stage two slices ago are done
-      if (!mbar_wait(smem_u32(&S.bar[s]), (uint32_t)(((t - kTcStages) >> 1) & 1))) {
-        atomicExch(&S.failed, 1);
+  volatile int* failed = &S.failed;
+  const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;  // stages of this tile
+  if (warp == 0) {
+    if (lane == 0) {  // producer: panel slices -> stage ring
+      const int64_t nsl = (d.K + SK - 1) / SK, g0 = td.k0 / BK;
+      const float* pa = g_tc_ws + d.pa + (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
+      const float* pb = g_tc_ws + d.pb + (int64_t)(td.n0 / TBN) * nsl * 2 * TBN * SK;
+      for (int64_t t = 0; t < nk; ++t) {
+        const int s = (int)(t % NST);
+        if (t >= NST &&
+            !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((t / NST - 1) & 1), failed)) {
+          *failed = 1;
+          break;
+        }
+        const int64_t g = g0 + t, sl = g / 2, half = g % 2;
+        const float* sa = pa + sl * 2 * TBM * SK + half * TBM * BK;
+        const float* sb = pb + sl * 2 * TBN * SK + half * TBN * BK;
+        const uint32_t bar = smem_u32(&S.full[s]);
+        mbar_expect_tx(bar, kStageBytes);
+        bulk_g2s(S.a[s][0], sa, TBM * BK * sizeof(float), bar);
+        bulk_g2s(S.a[s][1], sa + TBM * SK, TBM * BK * sizeof(float), bar);
+        bulk_g2s(S.b[s][0], sb, TBN * BK * sizeof(float), bar);
+        bulk_g2s(S.b[s][1], sb + TBN * SK, TBN * BK * sizeof(float), bar);
+        S.issued = t + 1;
       }
     }
-    __syncthreads();
-    if (S.failed) {
-      ok = false;
-      break;
-    }
-    const int64_t kvalid = td.k1 - (td.k0 + t * TBK);
-    {
-      double va[Unit<TBM>::NU], vb[Unit<BN>::NU];
-      gather<TBM>(d.a, ka, ak0 + t * TBK * akstep, akstep, roff_a, rok_a, warp, lane, kvalid, va);
-      gather<BN>(d.b, kb, bk0 + t * TBK * bkstep, bkstep, roff_b, rok_b, warp, lane, kvalid, vb);
-      ka = kfetch(d.ako, akstep, t + 1);  // next slice's offsets, in flight during the stores
-      kb = kfetch(d.bko, bkstep, t + 1);
-      store_split<TBM>(S.a[s][0], S.a[s][1], warp, lane, va);
-      store_split<BN>(S.b[s][0], S.b[s][1], warp, lane, vb);
-    }
-    // generic-proxy stores -> visible to the tensor core (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t ah = smem_u32(S.a[s][0]), al = smem_u32(S.a[s][1]);
-      const uint32_t bh = smem_u32(S.b[s][0]), bl = smem_u32(S.b[s][1]);
-      constexpr uint32_t kA = (TBM / 8) * 128, kB = (BN / 8) * 128;  // next core matrix along K
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      const uint32_t kIdesc = idesc_tf32<TBM, TBN>();
+      constexpr uint32_t kA = TBM * 16, kB = TBN * 16;  // next core matrix along K
+      for (int64_t t = 0; t < nk; ++t) {
+        const int s = (int)(t % NST);
+        if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((t / NST) & 1), failed)) {
+          *failed = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t ah = smem_u32(S.a[s][0]), al = smem_u32(S.a[s][1]);
+        const uint32_t bh = smem_u32(S.b[s][0]), bl = smem_u32(S.b[s][1]);
 #pragma unroll
-      for (int j = 0; j < TBK / 8; ++j) {  // K = 8 per MMA = two core matrices
-        const uint32_t oa = 2 * j * kA, ob = 2 * j * kB;
-        const uint64_t dah = smem_desc(ah + oa, kA, 128), dal = smem_desc(al + oa, kA, 128);
-        const uint64_t dbh = smem_desc(bh + ob, kB, 128), dbl = smem_desc(bl + ob, kB, 128);
-        mma_tf32(tmem, dah, dbh, kIdesc, (t > 0 || j > 0) ? 1u : 0u);
-        mma_tf32(tmem, dah, dbl, kIdesc, 1u);
-        mma_tf32(tmem, dal, dbh, kIdesc, 1u);
+        for (int j = 0; j < BK / 8; ++j) {  // K = 8 per MMA = two core matrices
+          const uint32_t oa = 2 * j * kA, ob = 2 * j * kB;
+          const uint64_t dah = smem_desc(ah + oa, kA, 128), dal = smem_desc(al + oa, kA, 128);
+          const uint64_t dbh = smem_desc(bh + ob, kB, 128), dbl = smem_desc(bl + ob, kB, 128);
+          mma_tf32(tmem, dah, dbh, kIdesc, (t > 0 || j > 0) ? 1u : 0u);
+          mma_tf32(tmem, dah, dbl, kIdesc, 1u);
+          mma_tf32(tmem, dal, dbh, kIdesc, 1u);
+        }
+        mma_commit(smem_u32(&S.empty[s]));
+        S.consumed = t + 1;
       }
-      mma_commit(smem_u32(&S.bar[s]));
+      mma_commit(smem_u32(&S.done));  // tracks every MMA this thread issued
     }
-    last = t;
+    __syncwarp();
+  } else {  // epilogue tables, loaded while the main loop runs
+    for (int i = tid - 64; i < TBM; i += TNT - 64)
+      if (i < rows) {
+        S.cro[i] = d.cro[td.m0 + i];
+        if (d.cmapped) decomp(d.rad[d.rowspace], d.nsp[d.rowspace], td.m0 + i, S.rc[i]);
+      }
+    for (int i = tid - 64; i < TBN; i += TNT - 64)
+      if (i < cols) {
+        S.cco[i] = d.cco[td.n0 + i];
+        if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
+      }
   }
-  // wait for the last committed slice (a commit covers all earlier MMAs)
-  if (last >= 0 && !mbar_wait(smem_u32(&S.bar[last & 1]), (uint32_t)((last >> 1) & 1)))
-    ok = false;
+  __syncthreads();
+  bool ok = !*failed;
+  if (!mbar_wait(smem_u32(&S.done), 0u, nullptr)) ok = false;  // all MMAs complete
+  if (tid == 0) {  // copies issued but never consumed (only after a failure)
+    for (int64_t t = S.consumed; t < S.issued; ++t)
+      if (!mbar_wait(smem_u32(&S.full[t % NST]), (uint32_t)((t / NST) & 1), nullptr)) ok = false;
+  }
   tc_fence_after();
-  if (!ok && tid == 0) atomicExch(err, 1);
-  if (ok && last >= 0) {
-    // epilogue: warp w reads TMEM lanes 32(w%4).. (its rows) and column block w/4
+  if (!ok && (tid & 31) == 0) atomicExch(err, 1);
+  if (ok) {
+    // warp w reads TMEM lanes 32(w%4).. (its rows) and column half w/4
     const int row = 32 * (warp & 3) + lane;
-    const int c0 = (warp >> 2) * (BN / (NW / 4));
+    const int c0 = (warp >> 2) * (TBN / (NW / 4));
     const double f = alpha * d.fac;
     double* __restrict__ X = d.c;
-    for (int cb = 0; cb < BN / (NW / 4); cb += 16) {
+    for (int cb = 0; cb < TBN / (NW / 4); cb += 16) {
+      if (c0 + cb >= cols) break;  // warp-uniform
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + cb), v);
       if (row >= rows) continue;
@@ -328,32 +399,40 @@ __global__ void __launch_bounds__(TNT, 1)
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                  :
-                 : "r"(tmem), "r"((uint32_t)BN)
+                 : "r"(tmem), "r"((uint32_t)TBN)
                  : "memory");
 }
 
-// one CTA per SM (the TMEM allocation of BN <= 256 columns never waits)
-static_assert(sizeof(TcSmem<kGemmTcN>) <= 227 * 1024, "tensor-core tile exceeds shared memory");
-static_assert(kGemmTcN <= 256 && kGemmTcN % 16 == 0, "UMMA N must be a multiple of 16 up to 256");
-
-template <int BN>
-void launch_tc_cfg(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
-                   int* err, cudaStream_t s) {
-  const size_t smem = sizeof(TcSmem<BN>);
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
-  k_gemm_tc<BN><<<(unsigned)ntiles, TNT, smem, s>>>(descs, tiles, alpha, err);
-}
+// one CTA per SM (the TMEM allocation of TBN <= 256 columns never waits)
+static_assert(sizeof(TcSmem) <= 227 * 1024, "tensor-core tile exceeds shared memory");
+static_assert(TBN <= 256 && TBN % 16 == 0, "UMMA N must be a multiple of 16 up to 256");
+static_assert(SK % BK == 0 && SK / BK == 2, "a stage is half a panel slice");
+static_assert((TBM * BK * sizeof(float)) % 16 == 0 && (TBN * BK * sizeof(float)) % 16 == 0,
+              "bulk copies move multiples of 16 bytes");
+static_assert(TBN / (NW / 4) % 16 == 0, "epilogue column blocks of 16");
 
 }  // namespace
+
+cudaError_t set_tc_workspace(float* ws) {
+  return cudaMemcpyToSymbol(g_tc_ws, &ws, sizeof(ws));
+}
+
+void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
+                     cudaStream_t s) {
+  if (njobs == 0 || nchunks == 0) return;
+  k_split_tc<<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs);
+}
 
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
                     int* err, cudaStream_t s) {
   if (ntiles == 0) return;
-  launch_tc_cfg<kGemmTcN>(descs, tiles, ntiles, alpha, err, s);
+  const size_t smem = sizeof(TcSmem);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = true;
+  }
+  k_gemm_tc<<<(unsigned)ntiles, TNT, smem, s>>>(descs, tiles, alpha, err);
 }
 
 }  // namespace gccu

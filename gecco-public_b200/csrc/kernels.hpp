@@ -48,10 +48,28 @@ inline void gemm_tile(int kind, int& TM, int& TN) {
 // maximum over its jobs
 void pack_geometry(const PackJob& j, int64_t& gx, int64_t& gy);
 void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cudaStream_t s);
-// split-TF32 tensor-core GEMM (tcgen05) over 128 x kGemmTcN tiles; *err is
-// set if a pipeline wait timed out
+// split-TF32 tensor-core GEMM (tcgen05) over 128 x kGemmTcN tiles, reading
+// the split panels of its items from the workspace; *err is set if a
+// pipeline wait timed out
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
                     int* err, cudaStream_t s);
+// floats of the split panels of one tensor-core item (both operands)
+constexpr int64_t kTcSlice = 32;  // contraction indices per panel slice
+inline int64_t tc_panel_floats(int64_t rows, int tile_rows, int64_t K) {
+  return (rows + tile_rows - 1) / tile_rows * tile_rows * ((K + kTcSlice - 1) / kTcSlice) *
+         kTcSlice * 2;
+}
+// number of 128-row x 32-index chunks of one operand's panel
+inline int64_t tc_split_chunks(int64_t rows, int tile_rows, int64_t K) {
+  return (rows + tile_rows - 1) / tile_rows * (tile_rows / 128) * ((K + kTcSlice - 1) / kTcSlice);
+}
+// split the operands of tensor-core items into their panels (jobs sorted by
+// cstart, nchunks = total chunks)
+void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
+                     cudaStream_t s);
+// device address of the split-TF32 workspace used by the two kernels above
+// (a device-side variable, so captured graphs follow a reallocation)
+cudaError_t set_tc_workspace(float* ws);
 // grouped block-contraction GEMM over the tiles of one tile shape (err: see
 // launch_gemm_tc, used by kind kGemmTc)
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
