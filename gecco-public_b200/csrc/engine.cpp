@@ -1239,6 +1239,29 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
   });
 }
 
+int gccu_plan_items(const gccu_bc_desc* bc, int64_t use_tr, int64_t* rows8, int64_t maxrows,
+                    int64_t* nrows) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(bc && nrows, "null argument");
+    DevPlan& dp = e.plan_for(bc, use_tr != 0);
+    const auto& items = dp.plan.items;
+    *nrows = (int64_t)items.size();
+    for (int64_t i = 0; i < std::min<int64_t>(maxrows, *nrows); ++i) {
+      const ItemDesc& it = items[i];
+      int64_t* r = rows8 + 8 * i;
+      r[0] = it.M;
+      r[1] = it.N;
+      r[2] = it.K;
+      r[3] = it.op[0].nmap;
+      r[4] = it.op[1].nmap;
+      r[5] = it.op[2].nmap;
+      r[6] = it.kfast1;
+      r[7] = it.kfast2;
+    }
+  });
+}
+
 int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8) {
   return guarded([&] {
     Engine& e = eng();

@@ -114,17 +114,29 @@ __device__ __forceinline__ void slot(int fastk, int t, int e, int& r, int& kk) {
   }
 }
 
+// k offset of contraction index k: kbase + k * kstep when the operand's
+// table is affine (no dependent table load), else the table entry
 template <int R, int NT, int EL>
 __device__ __forceinline__ void load_tile(const double* __restrict__ x,
-                                          const int64_t* __restrict__ kofs,
-                                          const int64_t* rofs_s, int fastk, int t, int64_t k0,
-                                          int64_t k1, int64_t rows, double (&v)[EL]) {
+                                          const int64_t* __restrict__ kofs, int64_t kbase,
+                                          int64_t kstep, const int64_t* rofs_s, int fastk, int t,
+                                          int64_t k0, int64_t k1, int64_t rows, double (&v)[EL]) {
+  if (kstep) {
+    const double* __restrict__ xk = x + kbase + k0 * kstep;
 #pragma unroll
-  for (int e = 0; e < EL; ++e) {
-    int r, kk;
-    slot<R, NT>(fastk, t, e, r, kk);
-    int64_t k = k0 + kk;
-    v[e] = (r < rows && k < k1) ? __ldg(x + rofs_s[r] + __ldg(kofs + k)) : 0.0;
+    for (int e = 0; e < EL; ++e) {
+      int r, kk;
+      slot<R, NT>(fastk, t, e, r, kk);
+      v[e] = (r < rows && k0 + kk < k1) ? __ldg(xk + rofs_s[r] + kk * kstep) : 0.0;
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < EL; ++e) {
+      int r, kk;
+      slot<R, NT>(fastk, t, e, r, kk);
+      const int64_t k = k0 + kk;
+      v[e] = (r < rows && k < k1) ? __ldg(x + rofs_s[r] + __ldg(kofs + k)) : 0.0;
+    }
   }
 }
 
@@ -139,8 +151,14 @@ __device__ __forceinline__ void store_tile(double (*S)[R + PAD], int fastk, int 
   }
 }
 
+// resident CTAs per SM the register budget is held to (two 256-thread
+// tiles, three 128-thread tiles, four thin ones)
+template <int NT, int BN>
+constexpr int kGemmMinBlocks = NT >= 256 ? 2 : BN <= 8 ? 4 : 3;
+
 template <int BM, int BN, int WARPS_M, int WARPS_N>
-__global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT)
+__global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT,
+                                  kGemmMinBlocks<Cfg<BM, BN, WARPS_M, WARPS_N>::NT, BN>)
     k_gemm(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
            double alpha) {
   using C = Cfg<BM, BN, WARPS_M, WARPS_N>;
@@ -183,9 +201,11 @@ __global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT)
     for (int j = 0; j < C::NTL; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
+  const int64_t akstep = d.akstep, bkstep = d.bkstep;
+  const int64_t ak0 = akstep ? __ldg(d.ako) : 0, bk0 = bkstep ? __ldg(d.bko) : 0;
   double va[C::ELA], vb[C::ELB];
-  load_tile<BM, C::NT, C::ELA>(A, d.ako, S.aro, afast, tid, td.k0, td.k1, rows, va);
-  load_tile<BN, C::NT, C::ELB>(B, d.bko, S.bco, bfast, tid, td.k0, td.k1, cols, vb);
+  load_tile<BM, C::NT, C::ELA>(A, d.ako, ak0, akstep, S.aro, afast, tid, td.k0, td.k1, rows, va);
+  load_tile<BN, C::NT, C::ELB>(B, d.bko, bk0, bkstep, S.bco, bfast, tid, td.k0, td.k1, cols, vb);
   store_tile<BM, C::NT, C::ELA>(S.As[0], afast, tid, va);
   store_tile<BN, C::NT, C::ELB>(S.Bs[0], bfast, tid, vb);
   __syncthreads();
@@ -194,8 +214,8 @@ __global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT)
     const bool more = kt + 1 < nk;
     if (more) {
       int64_t k0 = td.k0 + (kt + 1) * BK;
-      load_tile<BM, C::NT, C::ELA>(A, d.ako, S.aro, afast, tid, k0, td.k1, rows, va);
-      load_tile<BN, C::NT, C::ELB>(B, d.bko, S.bco, bfast, tid, k0, td.k1, cols, vb);
+      load_tile<BM, C::NT, C::ELA>(A, d.ako, ak0, akstep, S.aro, afast, tid, k0, td.k1, rows, va);
+      load_tile<BN, C::NT, C::ELB>(B, d.bko, bk0, bkstep, S.bco, bfast, tid, k0, td.k1, cols, vb);
     }
 #pragma unroll
     for (int k4 = 0; k4 < BK; k4 += 4) {
@@ -220,6 +240,31 @@ __global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT)
   // signed scatter-add (items and contraction splits may overlap: atomics)
   const double f = alpha * d.fac;
   double* __restrict__ X = d.c;
+  if (d.exclusive && !d.cmapped) {
+    // sole writer, no map lookups: the read-modify-writes of one row group
+    // of the thread's elements with their loads in flight together
+#pragma unroll
+    for (int i = 0; i < C::MT; ++i) {
+      const int row = wm * C::WTM + i * 8 + (lane >> 2);
+      const int64_t ro = row < rows ? S.cro[row] : -1;
+      int64_t off[C::NTL][2];
+      double old[C::NTL][2];
+#pragma unroll
+      for (int j = 0; j < C::NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int col = wn * C::WTN + j * 8 + 2 * (lane & 3) + h;
+          off[j][h] = (ro >= 0 && col < cols) ? ro + S.cco[col] : -1;
+          old[j][h] = off[j][h] >= 0 ? X[off[j][h]] : 0.0;
+        }
+#pragma unroll
+      for (int j = 0; j < C::NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (off[j][h] >= 0) X[off[j][h]] = old[j][h] + f * acc[i][j][h];
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < C::MT; ++i)
 #pragma unroll

@@ -66,6 +66,7 @@ _SIGS = {
     "gccu_list_device_ptr": [I64, ctypes.POINTER(ctypes.c_void_p)],
     "gccu_contract": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64, I64, PD],
     "gccu_plan_info": [ctypes.POINTER(BcDesc), I64, P64, PD],
+    "gccu_plan_items": [ctypes.POINTER(BcDesc), I64, P64, I64, P64],
     "gccu_contract_noalloc": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64],
     "gccu_add_block": [ctypes.c_double, I64, I64, I64, I64, I64, I64, PD],
     "gccu_scale_list": [I64, ctypes.c_double],
@@ -337,6 +338,17 @@ class Engine:
         st = np.zeros(8)
         _call("gccu_plan_info", ctypes.byref(d), int(use_tr), _p64(n), _pd(st))
         return int(n[0]), st
+
+    def plan_items(self, op1, op2, res, ex1, ex2, cnt, use_tr=False, tra=(0, 0, 0)):
+        """rows (M, N, K, maps op1, maps op2, maps result, kfast1, kfast2) of
+        the planned block contractions"""
+        d = self.desc(op1, op2, res, ex1, ex2, cnt, tra)
+        n = np.zeros(1, np.int64)
+        _call("gccu_plan_items", ctypes.byref(d), int(use_tr), _p64(np.zeros(8, np.int64)), 0,
+              _p64(n))
+        rows = np.zeros((max(int(n[0]), 1), 8), np.int64)
+        _call("gccu_plan_items", ctypes.byref(d), int(use_tr), _p64(rows), int(n[0]), _p64(n))
+        return rows[: int(n[0])]
 
     def add_block(self, fac, lin, iblk_in, lout, iblk_out, reset=False, typ=0):
         r = np.zeros(1)

@@ -128,6 +128,13 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
  * them): number of block contractions and the reference dgemm accounting of
  * gccu_stats for this contraction alone */
 int gccu_plan_info(const gccu_bc_desc* bc, int64_t use_tr, int64_t* nitems, double* stats8);
+/* the planned block contractions of a [CONTR] (planning only, also without a
+ * device): up to maxrows rows of (M, N, K, map components of op1, of op2, of
+ * the result, op1 contiguous along the contraction, op2 likewise); *nrows =
+ * number of block contractions.  No counterpart in the reference (its
+ * contr_op1op2_wmaps_c prints the same dimensions at ntest >= 100). */
+int gccu_plan_items(const gccu_bc_desc* bc, int64_t use_tr, int64_t* rows8, int64_t maxrows,
+                    int64_t* nrows);
 /* [CONTR] without any device allocation.  No counterpart in the reference.
  * For callers that must not allocate device memory while they run: a host
  * that has given all device memory to its ME lists up front, or one that must
