@@ -685,12 +685,17 @@ class Engine {
           tiles.push_back(tl);
         };
         if (kind == kGemmTc) {
-          // contraction chunk outermost: the tiles in flight share one chunk,
-          // whose column operand stays in L2 while each row band's chunk is
-          // reused by its column tiles one after the other
+          // contraction chunk outermost, then groups of column tiles whose
+          // split panels of the chunk (8 bytes per element) fit in about 32 MB
+          // of L2, then row bands, then the columns of the group: the tiles in
+          // flight share one group of column panels while each row band's
+          // chunk is reused by the group's tiles one after the other
+          const int64_t band = (int64_t)TN * kchunk * 8;
+          const int64_t grp = std::max<int64_t>(1, std::min<int64_t>(nt, (32ll << 20) / band));
           for (int64_t k0 = 0; k0 < d.K; k0 += kchunk)
-            for (int64_t m = 0; m < mt; ++m)
-              for (int64_t n = 0; n < nt; ++n) add(m, n, k0);
+            for (int64_t n0 = 0; n0 < nt; n0 += grp)
+              for (int64_t m = 0; m < mt; ++m)
+                for (int64_t n = n0; n < std::min(nt, n0 + grp); ++n) add(m, n, k0);
         } else {
           for (int64_t m = 0; m < mt; ++m)
             for (int64_t n = 0; n < nt; ++n)

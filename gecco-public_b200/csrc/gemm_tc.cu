@@ -254,6 +254,64 @@ __global__ void __launch_bounds__(kSplitThreads)
   }
 }
 
+// Scatter-add of NB accumulator values of tile row `row` (columns col[i])
+// into the result: offsets from the row and column tables plus the string-map
+// lookups of mapped result components, issued for all NB elements together
+// (one batch of independent loads per component), then the updates.
+template <int NB>
+__device__ __forceinline__ void scatter(const TcSmem& S, int row, const int (&col)[NB],
+                                        const float (&v)[NB], int64_t cols, double f) {
+  const GemmDesc& d = S.d;
+  int64_t off[NB];
+  float sg[NB];
+  bool ok[NB];
+  const int64_t ro = S.cro[row];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    ok[i] = col[i] < cols && v[i] != 0.0f;
+    off[i] = ok[i] ? ro + S.cco[col[i]] : 0;
+    sg[i] = 1.0f;
+  }
+  if (d.cmapped) {
+    const OpndDesc& od = d.cmap;
+    const int32_t* rc = S.rc[row];
+    for (int j = 0; j < od.ncomp; ++j) {
+      const int32_t* mp = od.map[j];
+      if (!mp) continue;
+      const bool r1 = od.sp1[j] == d.rowspace, r2 = od.sp2[j] == d.rowspace;
+      const int ci1 = od.ci1[j], ci2 = od.ci2[j];
+      const int64_t n1 = od.n1[j], ld = od.ldim[j];
+      int mv[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        const int32_t* cc = S.cc[col[i]];
+        const int i1 = r1 ? rc[ci1] : cc[ci1], i2 = r2 ? rc[ci2] : cc[ci2];
+        mv[i] = ok[i] ? __ldg(mp + (int64_t)i2 * n1 + i1) : 1;
+      }
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        int m = mv[i];
+        if (m == 0) ok[i] = false;
+        if (m < 0) {
+          sg[i] = -sg[i];
+          m = -m;
+        }
+        off[i] += (int64_t)(m - 1) * ld;
+      }
+    }
+  }
+  double* __restrict__ X = d.c;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    if (!ok[i]) continue;
+    const double val = f * (double)sg[i] * (double)v[i];
+    if (d.exclusive)
+      X[off[i]] += val;
+    else
+      atomicAdd(X + off[i], val);
+  }
+}
+
 // ---- GEMM ------------------------------------------------------------------
 __global__ void __launch_bounds__(TNT, 1)
     k_gemm_tc(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
@@ -360,38 +418,62 @@ __global__ void __launch_bounds__(TNT, 1)
       }
   }
   __syncthreads();
-  bool ok = !*failed;
-  if (!mbar_wait(smem_u32(&S.done), 0u, nullptr)) ok = false;  // all MMAs complete
+  if (!mbar_wait(smem_u32(&S.done), 0u, nullptr)) *failed = 1;  // all MMAs complete
   if (tid == 0) {  // copies issued but never consumed (only after a failure)
     for (int64_t t = S.consumed; t < S.issued; ++t)
-      if (!mbar_wait(smem_u32(&S.full[t % NST]), (uint32_t)((t / NST) & 1), nullptr)) ok = false;
+      if (!mbar_wait(smem_u32(&S.full[t % NST]), (uint32_t)((t / NST) & 1), nullptr))
+        *failed = 1;
   }
+  __syncthreads();
+  const bool ok = !*failed;  // the same in every thread
   tc_fence_after();
   if (!ok && (tid & 31) == 0) atomicExch(err, 1);
-  if (ok) {
+  // result elements adjacent in memory along the columns: the warps' lanes
+  // should run along columns, the transpose of TMEM's lane = row order
+  const bool colfast = ok && rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
+                       S.cro[1] - S.cro[0] != 1;
+  const double f = alpha * d.fac;
+  if (colfast) {
+    // stage the tile (FP32, row pitch kTp floats) in the idle stage buffers,
+    // then scatter row by row with lanes on consecutive columns
+    constexpr int kTp = TBN + 1;
+    static_assert(TBM * kTp * sizeof(float) <= sizeof(S.a) + sizeof(S.b), "staging tile");
+    float* T = &S.a[0][0][0];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const int row = 32 * (warp & 3) + lane;
+    const int c0 = (warp >> 2) * (TBN / (NW / 4));
+    for (int cb = 0; cb < TBN / (NW / 4); cb += 16) {
+      if (c0 + cb >= cols) break;  // warp-uniform
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + cb), v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) T[row * kTp + c0 + cb + i] = v[i];
+    }
+    __syncthreads();
+    const int nr = (int)(rows < TBM ? rows : TBM);
+    for (int r = warp; r < nr; r += NW) {
+      int col[TBN / 32];
+      float v[TBN / 32];
+#pragma unroll
+      for (int i = 0; i < TBN / 32; ++i) {
+        col[i] = lane + 32 * i;
+        v[i] = T[r * kTp + col[i]];
+      }
+      scatter<TBN / 32>(S, r, col, v, cols, f);
+    }
+  } else if (ok) {
     // warp w reads TMEM lanes 32(w%4).. (its rows) and column half w/4
     const int row = 32 * (warp & 3) + lane;
     const int c0 = (warp >> 2) * (TBN / (NW / 4));
-    const double f = alpha * d.fac;
-    double* __restrict__ X = d.c;
     for (int cb = 0; cb < TBN / (NW / 4); cb += 16) {
       if (c0 + cb >= cols) break;  // warp-uniform
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + cb), v);
       if (row >= rows) continue;
+      int col[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int col = c0 + cb + i;
-        if (col >= cols || v[i] == 0.0f) continue;
-        int64_t off = S.cro[row] + S.cco[col];
-        double sg = 1.0;
-        if (d.cmapped && !mapped(d.cmap, d.rowspace, S.rc[row], S.cc[col], off, sg)) continue;
-        const double val = f * sg * (double)v[i];
-        if (d.exclusive)
-          X[off] += val;
-        else
-          atomicAdd(X + off, val);
-      }
+      for (int i = 0; i < 16; ++i) col[i] = c0 + cb + i;
+      scatter<16>(S, row, col, v, cols, f);
     }
   }
   tc_fence_before();

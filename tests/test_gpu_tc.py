@@ -4,15 +4,17 @@ larger C1 space (6 holes, 24 particles) whose ladders and rings have
 hundreds of rows, columns and contraction indices, so that they take the
 tensor-core path (more than 32 rows and columns, at least 256 contraction
 indices), to FP32-level accuracy; switching back to FP64 restores the 1e-12
-agreement.  The test also checks that the tensor-core path ran: mode 1 must
-differ from mode 0 at the FP32 level for some contraction of the large
-space."""
+agreement.  The large space adds a contraction whose result is contiguous
+along the column space (its creator string comes from the second operand),
+which the tensor-core epilogue scatters column-major.  The test also checks
+that the tensor-core path ran: mode 1 must differ from mode 0 at the FP32
+level for some contraction of the large space."""
 import numpy as np
 import pytest
 
 import gccu
 from binding import Oracle
-from cases import SPACES, contractions_for, random_list
+from cases import H, P, SPACES, _bc, contractions_for, occ8, random_list
 
 pytestmark = pytest.mark.gpu
 
@@ -20,6 +22,10 @@ RTOL_TC = 2e-5    # split TF32 (~2^-22 per product) with FP32 accumulation over 
 RTOL_FP64 = 1e-12
 
 TC_SPACES = dict(SPACES, c1_tc=(1, [[6], [24], [0], [0]]))
+
+# result (PP;HH) with the particle pair from op2 (columns, stride 1) and the
+# hole pair from op1 (rows); one particle creator and annihilator contracted
+TC_EXTRA = [_bc("colmajor_result", occ8(None, {H: 2}), occ8({P: 2}), occ8({P: 1}, {P: 1}))]
 
 
 @pytest.fixture
@@ -33,7 +39,8 @@ def engine(built):
 def test_split_tf32_contractions(engine, space):
     nsym, norb = TC_SPACES[space]
     engine.register_orbinfo(nsym, norb)
-    cases = contractions_for(space if space in SPACES else "c1_small")
+    cases = (contractions_for(space) if space in SPACES
+             else contractions_for("c1_small") + TC_EXTRA)
     diffs = []
     for i, case in enumerate(cases):
         o = Oracle(nsym, norb)
