@@ -13,13 +13,17 @@
 // contract/collect_block_impr.f:397, already done for map-addressed operands
 // by the pack kernel), splits it and writes both halves as panels in the
 // K-major core-matrix order the tensor core reads (8 rows x 16 bytes per core
-// matrix, no swizzle).  k_gemm_tc then runs one CTA per 128 x 256 output tile
-// with warp roles: one thread streams the tile's panel slices into a 4-stage
-// shared-memory ring with bulk asynchronous copies (cp.async.bulk, completion
-// counted in bytes on an mbarrier), one thread issues the MMAs of each stage
-// (2 K-steps x 3 products) and commits them to the stage's release barrier;
-// after the last stage all 8 warps read the accumulator back with tcgen05.ld
-// (one TMEM lane per output row) and scatter it with the map signs.
+// matrix, no swizzle).  k_gemm_tc is persistent: one CTA per SM walks the
+// tiles (128 x 256 outputs, one contraction chunk) blockIdx.x, +gridDim.x, ...
+// with warp roles.  One thread streams the panel slices of its tiles into a
+// 4-stage shared-memory ring with bulk asynchronous copies (cp.async.bulk,
+// completion counted in bytes on an mbarrier); one thread issues the MMAs of
+// each stage (2 K-steps x 3 products) into one of two TMEM accumulators and
+// commits them to the stage's release barrier and, after a tile's last stage,
+// to the accumulator's full barrier; eight epilogue warps read a finished
+// accumulator back with tcgen05.ld (one TMEM lane per output row), release it
+// and scatter it with the map signs while the MMAs of the next tile run in
+// the other accumulator.
 //
 // Every wait on an mbarrier is bounded; on time-out the kernel records the
 // failure in *err, stops issuing work, waits (bounded) for the copies and
@@ -41,19 +45,23 @@ constexpr int TBN = kGemmTcN;  // tile columns = TMEM columns
 constexpr int SK = (int)kTcSlice;  // contraction indices per panel slice
 constexpr int BK = 16;         // contraction indices per pipeline stage
 constexpr int NST = 4;         // pipeline stages
-constexpr int TNT = 256;       // threads: 8 warps (the epilogue reads TMEM lanes 32(w%4)..)
-constexpr int NW = TNT / 32;
+// threads: warp 0 producer, warp 1 MMA issuer, warps 2-3 idle, warps 4-11
+// epilogue (warp w reads TMEM lanes 32(w%4).., two warps per lane quarter)
+constexpr int TNT = 384;
+constexpr int kEpiWarp0 = 4, kEpiWarps = 8, kEpiThreads = 32 * kEpiWarps;
 constexpr long kWaitLimit = 1L << 22;
 constexpr uint32_t kStageBytes = 2u * (TBM + TBN) * BK * sizeof(float);
+constexpr int kTcols = 32;  // columns per pass of the column-major epilogue
 
 struct __align__(1024) TcSmem {
   float a[NST][2][TBM * BK];  // [stage][hi/lo][k/4][row][k%4]
   float b[NST][2][TBN * BK];
+  float t[TBM][kTcols + 1];   // column-major epilogue staging
   int64_t cro[TBM], cco[TBN];
   int32_t rc[TBM][kDevMaxComp];
   int32_t cc[TBN][kDevMaxComp];
-  GemmDesc d;
-  alignas(8) uint64_t full[NST], empty[NST], done;
+  GemmDesc d;  // descriptor of the tile in the epilogue
+  alignas(8) uint64_t full[NST], empty[NST], accf[2], acce[2], done;
   int64_t issued, consumed;  // stages whose copies were issued / whose MMAs were issued
   uint32_t tmem_base;
   int failed;
@@ -97,6 +105,15 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(bar) : "memory");
+}
+
+// barrier among the epilogue warps only
+__device__ __forceinline__ void epi_sync() {
+  asm volatile("bar.sync 1, %0;" : : "n"(kEpiThreads) : "memory");
 }
 
 // one arrival that also expects `bytes` of asynchronous copies in this phase
@@ -254,27 +271,27 @@ __global__ void __launch_bounds__(kSplitThreads)
   }
 }
 
-// Scatter-add of NB accumulator values of tile row `row` (columns col[i])
-// into the result: offsets from the row and column tables plus the string-map
-// lookups of mapped result components, issued for all NB elements together
-// (one batch of independent loads per component), then the updates.
+// Scatter-add of NB accumulator values (tile rows row[i], columns col[i],
+// all inside the tile) into the result: offsets from the row and column
+// tables plus the string-map lookups of mapped result components, issued for
+// all NB elements together (one batch of independent loads per component),
+// then the updates.
 template <int NB>
-__device__ __forceinline__ void scatter(const TcSmem& S, int row, const int (&col)[NB],
-                                        const float (&v)[NB], int64_t cols, double f) {
+__device__ __forceinline__ void scatter(const TcSmem& S, const int (&row)[NB],
+                                        const int (&col)[NB], const float (&v)[NB],
+                                        int64_t rows, int64_t cols, double f) {
   const GemmDesc& d = S.d;
   int64_t off[NB];
   float sg[NB];
   bool ok[NB];
-  const int64_t ro = S.cro[row];
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
-    ok[i] = col[i] < cols && v[i] != 0.0f;
-    off[i] = ok[i] ? ro + S.cco[col[i]] : 0;
+    ok[i] = row[i] < rows && col[i] < cols && v[i] != 0.0f;
+    off[i] = ok[i] ? S.cro[row[i]] + S.cco[col[i]] : 0;
     sg[i] = 1.0f;
   }
   if (d.cmapped) {
     const OpndDesc& od = d.cmap;
-    const int32_t* rc = S.rc[row];
     for (int j = 0; j < od.ncomp; ++j) {
       const int32_t* mp = od.map[j];
       if (!mp) continue;
@@ -284,6 +301,7 @@ __device__ __forceinline__ void scatter(const TcSmem& S, int row, const int (&co
       int mv[NB];
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
+        const int32_t* rc = S.rc[row[i]];
         const int32_t* cc = S.cc[col[i]];
         const int i1 = r1 ? rc[ci1] : cc[ci1], i2 = r2 ? rc[ci2] : cc[ci2];
         mv[i] = ok[i] ? __ldg(mp + (int64_t)i2 * n1 + i1) : 1;
@@ -315,20 +333,18 @@ __device__ __forceinline__ void scatter(const TcSmem& S, int row, const int (&co
 // ---- GEMM ------------------------------------------------------------------
 __global__ void __launch_bounds__(TNT, 1)
     k_gemm_tc(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
-              double alpha, int* err) {
+              int64_t ntiles, double alpha, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const TileDesc td = tiles[blockIdx.x];
-  {
-    const int* src = reinterpret_cast<const int*>(descs + td.item);
-    int* dst = reinterpret_cast<int*>(&S.d);
-    for (int i = tid; i < (int)(sizeof(GemmDesc) / sizeof(int)); i += TNT) dst[i] = src[i];
-  }
   if (tid == 0) {
     for (int s = 0; s < NST; ++s) {
       mbar_init(smem_u32(&S.full[s]), 1);
       mbar_init(smem_u32(&S.empty[s]), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(smem_u32(&S.accf[a]), 1);
+      mbar_init(smem_u32(&S.acce[a]), kEpiWarps);
     }
     mbar_init(smem_u32(&S.done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -336,10 +352,10 @@ __global__ void __launch_bounds__(TNT, 1)
     S.issued = 0;
     S.consumed = 0;
   }
-  if (warp == 0) {  // TMEM: TBN f32 columns x 128 lanes
+  if (warp == 0) {  // TMEM: two accumulators of TBN f32 columns x 128 lanes
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(&S.tmem_base)), "r"((uint32_t)TBN)
+                 : "r"(smem_u32(&S.tmem_base)), "r"((uint32_t)(2 * TBN))
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -347,33 +363,38 @@ __global__ void __launch_bounds__(TNT, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
-  const GemmDesc& d = S.d;
-  const int64_t rows = d.M - td.m0, cols = d.N - td.n0;
-  const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
   volatile int* failed = &S.failed;
-  const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;  // stages of this tile
+  // tiles of this CTA: blockIdx.x + lt * gridDim.x (the grid is at most ntiles)
+  const int64_t nmine = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+  auto tile_of = [&](int64_t lt) { return tiles[blockIdx.x + lt * gridDim.x]; };
   if (warp == 0) {
     if (lane == 0) {  // producer: panel slices -> stage ring
-      const int64_t nsl = (d.K + SK - 1) / SK, g0 = td.k0 / BK;
-      const float* pa = g_tc_ws + d.pa + (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
-      const float* pb = g_tc_ws + d.pb + (int64_t)(td.n0 / TBN) * nsl * 2 * TBN * SK;
-      for (int64_t t = 0; t < nk; ++t) {
-        const int s = (int)(t % NST);
-        if (t >= NST &&
-            !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((t / NST - 1) & 1), failed)) {
-          *failed = 1;
-          break;
+      int64_t it = 0;
+      for (int64_t lt = 0; lt < nmine && !*failed; ++lt) {
+        const TileDesc td = tile_of(lt);
+        const GemmDesc* dg = descs + td.item;
+        const int64_t K = dg->K, nsl = (K + SK - 1) / SK, g0 = td.k0 / BK;
+        const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
+        const float* pa = g_tc_ws + dg->pa + (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
+        const float* pb = g_tc_ws + dg->pb + (int64_t)(td.n0 / TBN) * nsl * 2 * TBN * SK;
+        for (int64_t t = 0; t < nk; ++t, ++it) {
+          const int s = (int)(it % NST);
+          if (it >= NST &&
+              !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((it / NST - 1) & 1), failed)) {
+            *failed = 1;
+            break;
+          }
+          const int64_t g = g0 + t, sl = g / 2, half = g % 2;
+          const float* sa = pa + sl * 2 * TBM * SK + half * TBM * BK;
+          const float* sb = pb + sl * 2 * TBN * SK + half * TBN * BK;
+          const uint32_t bar = smem_u32(&S.full[s]);
+          mbar_expect_tx(bar, kStageBytes);
+          bulk_g2s(S.a[s][0], sa, TBM * BK * sizeof(float), bar);
+          bulk_g2s(S.a[s][1], sa + TBM * SK, TBM * BK * sizeof(float), bar);
+          bulk_g2s(S.b[s][0], sb, TBN * BK * sizeof(float), bar);
+          bulk_g2s(S.b[s][1], sb + TBN * SK, TBN * BK * sizeof(float), bar);
+          S.issued = it + 1;
         }
-        const int64_t g = g0 + t, sl = g / 2, half = g % 2;
-        const float* sa = pa + sl * 2 * TBM * SK + half * TBM * BK;
-        const float* sb = pb + sl * 2 * TBN * SK + half * TBN * BK;
-        const uint32_t bar = smem_u32(&S.full[s]);
-        mbar_expect_tx(bar, kStageBytes);
-        bulk_g2s(S.a[s][0], sa, TBM * BK * sizeof(float), bar);
-        bulk_g2s(S.a[s][1], sa + TBM * SK, TBM * BK * sizeof(float), bar);
-        bulk_g2s(S.b[s][0], sb, TBN * BK * sizeof(float), bar);
-        bulk_g2s(S.b[s][1], sb + TBN * SK, TBN * BK * sizeof(float), bar);
-        S.issued = t + 1;
       }
     }
     __syncwarp();
@@ -381,41 +402,131 @@ __global__ void __launch_bounds__(TNT, 1)
     if (lane == 0) {  // MMA issuer
       const uint32_t kIdesc = idesc_tf32<TBM, TBN>();
       constexpr uint32_t kA = TBM * 16, kB = TBN * 16;  // next core matrix along K
-      for (int64_t t = 0; t < nk; ++t) {
-        const int s = (int)(t % NST);
-        if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((t / NST) & 1), failed)) {
+      int64_t it = 0;
+      for (int64_t lt = 0; lt < nmine && !*failed; ++lt) {
+        const TileDesc td = tile_of(lt);
+        const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
+        const int acc = (int)(lt & 1);
+        if (lt >= 2 &&  // the epilogue has read this accumulator two tiles ago
+            !mbar_wait(smem_u32(&S.acce[acc]), (uint32_t)((lt / 2 - 1) & 1), failed)) {
           *failed = 1;
           break;
         }
         tc_fence_after();
-        const uint32_t ah = smem_u32(S.a[s][0]), al = smem_u32(S.a[s][1]);
-        const uint32_t bh = smem_u32(S.b[s][0]), bl = smem_u32(S.b[s][1]);
+        const uint32_t dacc = tmem + (uint32_t)(acc * TBN);
+        for (int64_t t = 0; t < nk; ++t, ++it) {
+          const int s = (int)(it % NST);
+          if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((it / NST) & 1), failed)) {
+            *failed = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t ah = smem_u32(S.a[s][0]), al = smem_u32(S.a[s][1]);
+          const uint32_t bh = smem_u32(S.b[s][0]), bl = smem_u32(S.b[s][1]);
 #pragma unroll
-        for (int j = 0; j < BK / 8; ++j) {  // K = 8 per MMA = two core matrices
-          const uint32_t oa = 2 * j * kA, ob = 2 * j * kB;
-          const uint64_t dah = smem_desc(ah + oa, kA, 128), dal = smem_desc(al + oa, kA, 128);
-          const uint64_t dbh = smem_desc(bh + ob, kB, 128), dbl = smem_desc(bl + ob, kB, 128);
-          mma_tf32(tmem, dah, dbh, kIdesc, (t > 0 || j > 0) ? 1u : 0u);
-          mma_tf32(tmem, dah, dbl, kIdesc, 1u);
-          mma_tf32(tmem, dal, dbh, kIdesc, 1u);
+          for (int j = 0; j < BK / 8; ++j) {  // K = 8 per MMA = two core matrices
+            const uint32_t oa = 2 * j * kA, ob = 2 * j * kB;
+            const uint64_t dah = smem_desc(ah + oa, kA, 128), dal = smem_desc(al + oa, kA, 128);
+            const uint64_t dbh = smem_desc(bh + ob, kB, 128), dbl = smem_desc(bl + ob, kB, 128);
+            mma_tf32(dacc, dah, dbh, kIdesc, (t > 0 || j > 0) ? 1u : 0u);
+            mma_tf32(dacc, dah, dbl, kIdesc, 1u);
+            mma_tf32(dacc, dal, dbh, kIdesc, 1u);
+          }
+          mma_commit(smem_u32(&S.empty[s]));
+          S.consumed = it + 1;
         }
-        mma_commit(smem_u32(&S.empty[s]));
-        S.consumed = t + 1;
+        if (*failed) break;
+        mma_commit(smem_u32(&S.accf[acc]));
       }
       mma_commit(smem_u32(&S.done));  // tracks every MMA this thread issued
     }
     __syncwarp();
-  } else {  // epilogue tables, loaded while the main loop runs
-    for (int i = tid - 64; i < TBM; i += TNT - 64)
-      if (i < rows) {
-        S.cro[i] = d.cro[td.m0 + i];
-        if (d.cmapped) decomp(d.rad[d.rowspace], d.nsp[d.rowspace], td.m0 + i, S.rc[i]);
+  } else if (warp >= kEpiWarp0) {
+    const int et = tid - 32 * kEpiWarp0, ew = warp - kEpiWarp0;
+    const int quarter = warp & 3, half = ew >> 2;  // TMEM lanes 32*quarter.., column half
+    for (int64_t lt = 0; lt < nmine; ++lt) {
+      const TileDesc td = tile_of(lt);
+      {  // descriptor and tables of the tile (the previous tile's are no longer read)
+        const int* src = reinterpret_cast<const int*>(descs + td.item);
+        int* dst = reinterpret_cast<int*>(&S.d);
+        for (int i = et; i < (int)(sizeof(GemmDesc) / sizeof(int)); i += kEpiThreads)
+          dst[i] = src[i];
       }
-    for (int i = tid - 64; i < TBN; i += TNT - 64)
-      if (i < cols) {
-        S.cco[i] = d.cco[td.n0 + i];
-        if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
+      epi_sync();
+      const GemmDesc& d = S.d;
+      const int64_t rows = d.M - td.m0, cols = d.N - td.n0;
+      const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
+      for (int i = et; i < TBM; i += kEpiThreads)
+        if (i < rows) {
+          S.cro[i] = d.cro[td.m0 + i];
+          if (d.cmapped) decomp(d.rad[d.rowspace], d.nsp[d.rowspace], td.m0 + i, S.rc[i]);
+        }
+      for (int i = et; i < TBN; i += kEpiThreads)
+        if (i < cols) {
+          S.cco[i] = d.cco[td.n0 + i];
+          if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
+        }
+      const int acc = (int)(lt & 1);
+      if (!mbar_wait(smem_u32(&S.accf[acc]), (uint32_t)((lt / 2) & 1), failed)) *failed = 1;
+      epi_sync();
+      if (*failed) break;  // the same in every epilogue thread after the barrier
+      tc_fence_after();
+      const uint32_t tacc = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * TBN);
+      const double f = alpha * d.fac;
+      // result elements adjacent in memory along the columns: lanes should
+      // run along columns, the transpose of TMEM's lane = row order
+      const bool colfast = rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
+                           S.cro[1] - S.cro[0] != 1;
+      if (colfast) {
+        // passes of kTcols columns: the four warps of the column half holding
+        // them stage the pass in shared memory, then every epilogue warp
+        // scatters rows ew, ew+8, .. with lanes on consecutive columns
+        for (int c0 = 0; c0 < TBN && c0 < cols; c0 += kTcols) {
+          if ((c0 / (TBN / 2)) == half) {
+            const int row = 32 * quarter + lane;
+#pragma unroll
+            for (int cb = 0; cb < kTcols; cb += 16) {
+              float v[16];
+              tmem_ld16(tacc + (uint32_t)(c0 + cb), v);
+#pragma unroll
+              for (int i = 0; i < 16; ++i) S.t[row][cb + i] = v[i];
+            }
+          }
+          epi_sync();
+          constexpr int kRows = TBM / kEpiWarps;
+          int rr[kRows], cc[kRows];
+          float v[kRows];
+#pragma unroll
+          for (int i = 0; i < kRows; ++i) {
+            rr[i] = ew + kEpiWarps * i;
+            cc[i] = c0 + lane;
+            v[i] = S.t[rr[i]][lane];
+          }
+          scatter<kRows>(S, rr, cc, v, rows, cols, f);
+          epi_sync();
+        }
+      } else {
+        const int row = 32 * quarter + lane;
+        const int c0 = half * (TBN / 2);
+        for (int cb = 0; cb < TBN / 2; cb += 16) {
+          if (c0 + cb >= cols) break;  // warp-uniform
+          float v[16];
+          tmem_ld16(tacc + (uint32_t)(c0 + cb), v);
+          int rr[16], cc[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            rr[i] = row;
+            cc[i] = c0 + cb + i;
+          }
+          scatter<16>(S, rr, cc, v, rows, cols, f);
+        }
       }
+      // accumulator read (tcgen05.ld waited in tmem_ld16): release it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&S.acce[acc]));
+      epi_sync();  // tables and descriptor free for the next tile
+    }
   }
   __syncthreads();
   if (!mbar_wait(smem_u32(&S.done), 0u, nullptr)) *failed = 1;  // all MMAs complete
@@ -425,73 +536,24 @@ __global__ void __launch_bounds__(TNT, 1)
         *failed = 1;
   }
   __syncthreads();
-  const bool ok = !*failed;  // the same in every thread
-  tc_fence_after();
-  if (!ok && (tid & 31) == 0) atomicExch(err, 1);
-  // result elements adjacent in memory along the columns: the warps' lanes
-  // should run along columns, the transpose of TMEM's lane = row order
-  const bool colfast = ok && rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
-                       S.cro[1] - S.cro[0] != 1;
-  const double f = alpha * d.fac;
-  if (colfast) {
-    // stage the tile (FP32, row pitch kTp floats) in the idle stage buffers,
-    // then scatter row by row with lanes on consecutive columns
-    constexpr int kTp = TBN + 1;
-    static_assert(TBM * kTp * sizeof(float) <= sizeof(S.a) + sizeof(S.b), "staging tile");
-    float* T = &S.a[0][0][0];
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    const int row = 32 * (warp & 3) + lane;
-    const int c0 = (warp >> 2) * (TBN / (NW / 4));
-    for (int cb = 0; cb < TBN / (NW / 4); cb += 16) {
-      if (c0 + cb >= cols) break;  // warp-uniform
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + cb), v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) T[row * kTp + c0 + cb + i] = v[i];
-    }
-    __syncthreads();
-    const int nr = (int)(rows < TBM ? rows : TBM);
-    for (int r = warp; r < nr; r += NW) {
-      int col[TBN / 32];
-      float v[TBN / 32];
-#pragma unroll
-      for (int i = 0; i < TBN / 32; ++i) {
-        col[i] = lane + 32 * i;
-        v[i] = T[r * kTp + col[i]];
-      }
-      scatter<TBN / 32>(S, r, col, v, cols, f);
-    }
-  } else if (ok) {
-    // warp w reads TMEM lanes 32(w%4).. (its rows) and column half w/4
-    const int row = 32 * (warp & 3) + lane;
-    const int c0 = (warp >> 2) * (TBN / (NW / 4));
-    for (int cb = 0; cb < TBN / (NW / 4); cb += 16) {
-      if (c0 + cb >= cols) break;  // warp-uniform
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + cb), v);
-      if (row >= rows) continue;
-      int col[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) col[i] = c0 + cb + i;
-      scatter<16>(S, row, col, v, cols, f);
-    }
-  }
+  if (*failed && tid == 0) atomicExch(err, 1);
   tc_fence_before();
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                  :
-                 : "r"(tmem), "r"((uint32_t)TBN)
+                 : "r"(tmem), "r"((uint32_t)(2 * TBN))
                  : "memory");
 }
 
-// one CTA per SM (the TMEM allocation of TBN <= 256 columns never waits)
+// one CTA per SM (the TMEM allocation of all 512 columns never waits)
 static_assert(sizeof(TcSmem) <= 227 * 1024, "tensor-core tile exceeds shared memory");
 static_assert(TBN <= 256 && TBN % 16 == 0, "UMMA N must be a multiple of 16 up to 256");
 static_assert(SK % BK == 0 && SK / BK == 2, "a stage is half a panel slice");
 static_assert((TBM * BK * sizeof(float)) % 16 == 0 && (TBN * BK * sizeof(float)) % 16 == 0,
               "bulk copies move multiples of 16 bytes");
-static_assert(TBN / (NW / 4) % 16 == 0, "epilogue column blocks of 16");
+static_assert(TBM % kEpiWarps == 0 && TBN % kTcols == 0 && (TBN / 2) % kTcols == 0,
+              "epilogue passes");
 
 }  // namespace
 
@@ -514,7 +576,15 @@ void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles
     cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = true;
   }
-  k_gemm_tc<<<(unsigned)ntiles, TNT, smem, s>>>(descs, tiles, alpha, err);
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const int64_t grid = ntiles < nsm ? ntiles : nsm;
+  k_gemm_tc<<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err);
 }
 
 }  // namespace gccu
