@@ -72,6 +72,7 @@ struct GemmDesc {
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update
+  int32_t tn;            // tensor-core items: tile width (columns, multiple of 32, <= 256)
   int32_t nsp[3];
   int32_t rad[3][kDevMaxComp];
   OpndDesc cmap;  // result operand (map lookups in the epilogue)
@@ -93,7 +94,7 @@ struct ReoItem {
 
 // Split of one operand of a tensor-core item into its TF32 panel: for the
 // row operand (op 0, tile rows TR = 128) and the column operand (op 1, TR =
-// 256) of descriptor `desc`, every (TR-row band, 32-index slice) of the
+// the item's tile width tn) of descriptor `desc`, every (TR-row band, 32-index slice) of the
 // operand is stored as two planes (hi, lo) of TR x 32 floats in the
 // tensor core's K-major core-matrix order, [k/4][row][k%4]:
 //   panel[((band * nslice + slice) * 2 + plane) * TR * 32 + (k/4) * TR * 4 + row * 4 + k%4]

@@ -655,14 +655,18 @@ class Engine {
     for (int kind = 0; kind < kGemmKinds; ++kind)
       for (auto& d : g[kind]) writers[d.c]++;
     for (int kind = 0; kind < kGemmKinds; ++kind) {
-      int TM, TN;
-      gemm_tile(kind, TM, TN);
+      int TM, TN0;
+      gemm_tile(kind, TM, TN0);
+      if (kind == kGemmTc)
+        for (auto& d : g[kind]) d.tn = tc_tile_n(d.N);
+      auto width = [&](const GemmDesc& d) { return kind == kGemmTc ? d.tn : TN0; };
       std::vector<TileDesc> tiles;
       int64_t total = 0;
-      for (auto& d : g[kind]) total += ((d.M + TM - 1) / TM) * ((d.N + TN - 1) / TN);
+      for (auto& d : g[kind]) total += ((d.M + TM - 1) / TM) * ((d.N + width(d) - 1) / width(d));
       const int64_t want = 2 * 148;
       for (size_t i = 0; i < g[kind].size(); ++i) {
         GemmDesc& d = g[kind][i];
+        const int TN = width(d);
         int64_t mt = (d.M + TM - 1) / TM, nt = (d.N + TN - 1) / TN;
         int64_t ks = 1;
         if (kind == kGemmSmall) {
@@ -711,11 +715,11 @@ class Engine {
           d.pa = off;
           off += tc_panel_floats(d.M, kGemmTcM, d.K);
           d.pb = off;
-          off += tc_panel_floats(d.N, kGemmTcN, d.K);
+          off += tc_panel_floats(d.N, d.tn, d.K);
           sj.push_back(SplitJob{(int32_t)i, 0, cs});
           cs += tc_split_chunks(d.M, kGemmTcM, d.K);
           sj.push_back(SplitJob{(int32_t)i, 1, cs});
-          cs += tc_split_chunks(d.N, kGemmTcN, d.K);
+          cs += tc_split_chunks(d.N, d.tn, d.K);
         }
         GCCU_REQUIRE(cs < INT32_MAX, "tensor-core operands too large for one split launch");
         dp.ws_floats = off;

@@ -50,7 +50,6 @@ constexpr int NST = 4;         // pipeline stages
 constexpr int TNT = 384;
 constexpr int kEpiWarp0 = 4, kEpiWarps = 8, kEpiThreads = 32 * kEpiWarps;
 constexpr long kWaitLimit = 1L << 22;
-constexpr uint32_t kStageBytes = 2u * (TBM + TBN) * BK * sizeof(float);
 constexpr int kTcols = 32;  // columns per pass of the column-major epilogue
 
 struct __align__(1024) TcSmem {
@@ -80,8 +79,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 }
 
 // instruction descriptor: D f32, A/B tf32, both K-major, M x N
-template <int M, int N>
-__device__ __forceinline__ uint32_t idesc_tf32() {
+__device__ __forceinline__ uint32_t idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
@@ -216,7 +214,7 @@ __global__ void __launch_bounds__(kSplitThreads)
   const GemmDesc& d = descs[J.desc];
   const bool row_op = J.op == 0;
   const int64_t R = row_op ? d.M : d.N, K = d.K;
-  const int TR = row_op ? TBM : TBN;
+  const int TR = row_op ? TBM : d.tn;
   const double* __restrict__ x = row_op ? d.a : d.b;
   const int64_t* rtab = row_op ? d.aro : d.bco;
   const int64_t* ktab = row_op ? d.ako : d.bko;
@@ -259,15 +257,19 @@ __global__ void __launch_bounds__(kSplitThreads)
     }
   }
   __syncthreads();
-  const int64_t band = r0 / TR, rr0 = r0 % TR;
-  float* __restrict__ dst =
-      g_tc_ws + (row_op ? d.pa : d.pb) + (band * nsl + c % nsl) * 2 * TR * SK;
+  // a 128-row chunk may span two row bands when TR is not a multiple of 128
+  const int64_t padded = (R + TR - 1) / TR * TR;
+  float* __restrict__ base = g_tc_ws + (row_op ? d.pa : d.pb) + (c % nsl) * 2 * TR * SK;
 #pragma unroll
   for (int i = 0; i < 2 * 8 * 128 / kSplitThreads; ++i) {
     const int u = tid + kSplitThreads * i;
     const int plane = u >> 10, kq = (u >> 7) & 7, r = u & 127;
+    const int64_t row = r0 + r;
+    if (row >= padded) continue;
+    const int64_t band = row / TR, rr = row % TR;
     const float4 v = *reinterpret_cast<const float4*>(&sh[plane][kq * kSplitPitch + 4 * r]);
-    *reinterpret_cast<float4*>(dst + plane * TR * SK + kq * TR * 4 + (rr0 + r) * 4) = v;
+    *reinterpret_cast<float4*>(base + band * nsl * 2 * TR * SK + plane * TR * SK + kq * TR * 4 +
+                               rr * 4) = v;
   }
 }
 
@@ -375,8 +377,10 @@ __global__ void __launch_bounds__(TNT, 1)
         const GemmDesc* dg = descs + td.item;
         const int64_t K = dg->K, nsl = (K + SK - 1) / SK, g0 = td.k0 / BK;
         const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
+        const int bn = dg->tn;
+        const uint32_t stage_bytes = 2u * (uint32_t)(TBM + bn) * BK * sizeof(float);
         const float* pa = g_tc_ws + dg->pa + (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
-        const float* pb = g_tc_ws + dg->pb + (int64_t)(td.n0 / TBN) * nsl * 2 * TBN * SK;
+        const float* pb = g_tc_ws + dg->pb + (int64_t)(td.n0 / bn) * nsl * 2 * bn * SK;
         for (int64_t t = 0; t < nk; ++t, ++it) {
           const int s = (int)(it % NST);
           if (it >= NST &&
@@ -386,13 +390,13 @@ __global__ void __launch_bounds__(TNT, 1)
           }
           const int64_t g = g0 + t, sl = g / 2, half = g % 2;
           const float* sa = pa + sl * 2 * TBM * SK + half * TBM * BK;
-          const float* sb = pb + sl * 2 * TBN * SK + half * TBN * BK;
+          const float* sb = pb + sl * 2 * bn * SK + half * bn * BK;
           const uint32_t bar = smem_u32(&S.full[s]);
-          mbar_expect_tx(bar, kStageBytes);
+          mbar_expect_tx(bar, stage_bytes);
           bulk_g2s(S.a[s][0], sa, TBM * BK * sizeof(float), bar);
           bulk_g2s(S.a[s][1], sa + TBM * SK, TBM * BK * sizeof(float), bar);
-          bulk_g2s(S.b[s][0], sb, TBN * BK * sizeof(float), bar);
-          bulk_g2s(S.b[s][1], sb + TBN * SK, TBN * BK * sizeof(float), bar);
+          bulk_g2s(S.b[s][0], sb, (uint32_t)bn * BK * sizeof(float), bar);
+          bulk_g2s(S.b[s][1], sb + bn * SK, (uint32_t)bn * BK * sizeof(float), bar);
           S.issued = it + 1;
         }
       }
@@ -400,12 +404,13 @@ __global__ void __launch_bounds__(TNT, 1)
     __syncwarp();
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      const uint32_t kIdesc = idesc_tf32<TBM, TBN>();
-      constexpr uint32_t kA = TBM * 16, kB = TBN * 16;  // next core matrix along K
+      constexpr uint32_t kA = TBM * 16;  // next core matrix along K (row operand)
       int64_t it = 0;
       for (int64_t lt = 0; lt < nmine && !*failed; ++lt) {
         const TileDesc td = tile_of(lt);
         const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
+        const int bn = descs[td.item].tn;
+        const uint32_t kIdesc = idesc_tf32(TBM, bn), kB = (uint32_t)bn * 16;
         const int acc = (int)(lt & 1);
         if (lt >= 2 &&  // the epilogue has read this accumulator two tiles ago
             !mbar_wait(smem_u32(&S.acce[acc]), (uint32_t)((lt / 2 - 1) & 1), failed)) {
@@ -454,7 +459,9 @@ __global__ void __launch_bounds__(TNT, 1)
       }
       epi_sync();
       const GemmDesc& d = S.d;
-      const int64_t rows = d.M - td.m0, cols = d.N - td.n0;
+      const int bn = d.tn;  // tile width
+      const int64_t rows = d.M - td.m0 < TBM ? d.M - td.m0 : TBM;
+      const int64_t cols = d.N - td.n0 < bn ? d.N - td.n0 : bn;
       const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
       for (int i = et; i < TBM; i += kEpiThreads)
         if (i < rows) {
@@ -478,11 +485,12 @@ __global__ void __launch_bounds__(TNT, 1)
       const bool colfast = rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
                            S.cro[1] - S.cro[0] != 1;
       if (colfast) {
-        // passes of kTcols columns: the four warps of the column half holding
-        // them stage the pass in shared memory, then every epilogue warp
-        // scatters rows ew, ew+8, .. with lanes on consecutive columns
-        for (int c0 = 0; c0 < TBN && c0 < cols; c0 += kTcols) {
-          if ((c0 / (TBN / 2)) == half) {
+        // passes of kTcols columns: four warps (one per lane quarter, the two
+        // sets taking turns) stage the pass in shared memory, then every
+        // epilogue warp scatters rows ew, ew+8, .. with lanes on consecutive
+        // columns
+        for (int c0 = 0; c0 < cols; c0 += kTcols) {
+          if (((c0 / kTcols) & 1) == half) {
             const int row = 32 * quarter + lane;
 #pragma unroll
             for (int cb = 0; cb < kTcols; cb += 16) {
@@ -507,8 +515,8 @@ __global__ void __launch_bounds__(TNT, 1)
         }
       } else {
         const int row = 32 * quarter + lane;
-        const int c0 = half * (TBN / 2);
-        for (int cb = 0; cb < TBN / 2; cb += 16) {
+        const int c0 = half * (bn / 2);
+        for (int cb = 0; cb < bn / 2; cb += 16) {
           if (c0 + cb >= cols) break;  // warp-uniform
           float v[16];
           tmem_ld16(tacc + (uint32_t)(c0 + cb), v);
@@ -552,8 +560,8 @@ static_assert(TBN <= 256 && TBN % 16 == 0, "UMMA N must be a multiple of 16 up t
 static_assert(SK % BK == 0 && SK / BK == 2, "a stage is half a panel slice");
 static_assert((TBM * BK * sizeof(float)) % 16 == 0 && (TBN * BK * sizeof(float)) % 16 == 0,
               "bulk copies move multiples of 16 bytes");
-static_assert(TBM % kEpiWarps == 0 && TBN % kTcols == 0 && (TBN / 2) % kTcols == 0,
-              "epilogue passes");
+static_assert(TBM % kEpiWarps == 0 && kTcols % 16 == 0 && TBN % 32 == 0,
+              "epilogue passes (tile widths are multiples of 32)");
 
 }  // namespace
 

@@ -61,7 +61,16 @@ inline int64_t tc_panel_floats(int64_t rows, int tile_rows, int64_t K) {
 }
 // number of 128-row x 32-index chunks of one operand's panel
 inline int64_t tc_split_chunks(int64_t rows, int tile_rows, int64_t K) {
-  return (rows + tile_rows - 1) / tile_rows * (tile_rows / 128) * ((K + kTcSlice - 1) / kTcSlice);
+  const int64_t padded = (rows + tile_rows - 1) / tile_rows * tile_rows;
+  return (padded + 127) / 128 * ((K + kTcSlice - 1) / kTcSlice);
+}
+// tile width of a tensor-core item with N columns: as many tiles as 256-wide
+// ones would need, each narrowed to the multiple of 32 that covers N
+inline int tc_tile_n(int64_t N) {
+  const int64_t nt = (N + kGemmTcN - 1) / kGemmTcN;
+  int64_t w = ((N + nt - 1) / nt + 31) / 32 * 32;
+  if (w < 32) w = 32;
+  return (int)(w < kGemmTcN ? w : kGemmTcN);
 }
 // split the operands of tensor-core items into their panels (jobs sorted by
 // cstart, nchunks = total chunks)
