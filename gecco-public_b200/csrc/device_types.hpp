@@ -99,10 +99,14 @@ struct ReoItem {
 // tensor core's K-major core-matrix order, [k/4][row][k%4]:
 //   panel[((band * nslice + slice) * 2 + plane) * TR * 32 + (k/4) * TR * 4 + row * 4 + k%4]
 // with rows and contraction indices outside the item set to zero.  The job's
-// blocks are 128-row x 32-index chunks numbered from cstart.
+// blocks are 128-row x 32-index chunks numbered from cstart.  An operand whose
+// strings merge an external and a contracted component is read through its
+// gather description (PackJob index `gather`, -1: through the descriptor's
+// offset tables).
 struct SplitJob {
   int32_t desc, op;
   int64_t cstart;
+  int32_t gather, pad;
 };
 
 // gather of one operand of one block contraction into a dense panel

@@ -61,6 +61,7 @@ struct DevPlan {
   // split-TF32 panels of the tensor-core items (workspace floats, jobs)
   SplitJob* d_split = nullptr;
   int64_t nsplit = 0, split_chunks = 0, ws_floats = 0;
+  PackJob* d_gather = nullptr;  // gather descriptions of map-addressed tensor-core operands
   int64_t* d_tabs = nullptr;
   double* scratch = nullptr;
   int64_t scratch_len = 0;
@@ -521,8 +522,14 @@ class Engine {
       // and epilogue only)
       if (precision == 1 && kind_of[i] == kGemmRegular && it.K >= kTcMinK) kind_of[i] = kGemmTc;
     }
-    // an operand whose strings need map lookups is packed into a dense panel
-    auto packed = [&](size_t i, int op) { return P.items[i].op[op].nmap > 0; };
+    // an operand whose strings need map lookups is packed into a dense panel,
+    // except for tensor-core items, whose split pre-pass reads it in place
+    // through the same gather description
+    auto maps_of = [&](size_t i, int op) { return P.items[i].op[op].nmap > 0; };
+    auto tcgather = [&](size_t i, int op) {
+      return maps_of(i, op) && kind_of[i] == kGemmTc && P.items[i].op[op].nmap <= kTcGatherMaps;
+    };
+    auto packed = [&](size_t i, int op) { return maps_of(i, op) && !tcgather(i, op); };
     struct PackTab { int64_t roff, koff, rmi, kmi; };
     std::vector<PackTab> ptab1(P.items.size()), ptab2(P.items.size());
     auto pack_tabs = [&](const ItemDesc& it, int op, PackTab& pt) {
@@ -537,9 +544,12 @@ class Engine {
     for (size_t i = 0; i < P.items.size(); ++i) {
       const ItemDesc& it = P.items[i];
       Tab& t = toff[i];
-      if (packed(i, 0)) pack_tabs(it, 0, ptab1[i]);
-      if (packed(i, 1)) pack_tabs(it, 1, ptab2[i]);
-      if (packed(i, 0)) {  // panel[k*M + r]
+      if (maps_of(i, 0)) pack_tabs(it, 0, ptab1[i]);
+      if (maps_of(i, 1)) pack_tabs(it, 1, ptab2[i]);
+      if (tcgather(i, 0)) {  // read in place by the split pre-pass
+        t.aro = ptab1[i].roff;
+        t.ako = ptab1[i].koff;
+      } else if (packed(i, 0)) {  // panel[k*M + r]
         pack_off1[i] = scratch;
         scratch += it.M * it.K;
         t.aro = put([&](std::vector<int64_t>& v) { for (int64_t r = 0; r < it.M; ++r) v.push_back(r); });
@@ -548,7 +558,10 @@ class Engine {
         t.aro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kEx1, it.M, v); });
         t.ako = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kCnt, it.K, v); });
       }
-      if (packed(i, 1)) {  // panel[k*N + c]
+      if (tcgather(i, 1)) {
+        t.bco = ptab2[i].roff;
+        t.bko = ptab2[i].koff;
+      } else if (packed(i, 1)) {  // panel[k*N + c]
         pack_off2[i] = scratch;
         scratch += it.N * it.K;
         t.bco = put([&](std::vector<int64_t>& v) { for (int64_t c = 0; c < it.N; ++c) v.push_back(c); });
@@ -566,6 +579,43 @@ class Engine {
     dp.scratch_len = scratch;
     std::vector<GemmDesc> g[kGemmKinds];
     std::vector<int32_t> group_of(P.items.size());
+    // gather description of operand op of item i (a k_pack job into dst, or
+    // read in place by the split pre-pass when dst is null)
+    auto job_of = [&](size_t i, int op, double* dst) {
+      const ItemDesc& it = P.items[i];
+      PackJob j{};
+      j.R = op == 0 ? it.M : it.N;
+      j.K = it.K;
+      j.src = op == 0 ? x1 + it.base1 : x2 + it.base2;
+      j.dst = dst;
+      const PackTab& pt = op == 0 ? ptab1[i] : ptab2[i];
+      j.roff = dp.d_tabs + pt.roff;
+      j.koff = dp.d_tabs + pt.koff;
+      j.rmi = dp.d_tabs + pt.rmi;
+      j.kmi = dp.d_tabs + pt.kmi;
+      const OpndDesc& od = it.op[op];
+      const int rsp = op == 0 ? kEx1 : kEx2;
+      j.nm = 0;
+      for (int c = 0; c < od.ncomp; ++c) {
+        if (!od.map[c]) continue;
+        GCCU_REQUIRE((od.sp1[c] == rsp && od.sp2[c] == kCnt) ||
+                         (od.sp1[c] == kCnt && od.sp2[c] == rsp),
+                     "string map of an operand must merge an external and a contracted string");
+        j.row_is_1[j.nm] = od.sp1[c] == rsp;
+        j.n1[j.nm] = od.n1[c];
+        j.ldim[j.nm] = od.ldim[c];
+        j.map[j.nm] = od.map[c];
+        ++j.nm;
+      }
+      GCCU_REQUIRE(j.R < INT32_MAX && j.K < INT32_MAX, "block too large for the pack kernel");
+      j.kfast = op == 0 ? it.kfast1 : it.kfast2;
+      const int64_t nf = j.kfast ? j.K : j.R;
+      j.F = 1;
+      while (j.F < 256 && j.F < nf) j.F *= 2;
+      return j;
+    };
+    std::vector<PackJob> gathers;
+    std::map<std::pair<size_t, int>, int32_t> gather_of;  // (index in g[kGemmTc], op) -> gather
     for (size_t i = 0; i < P.items.size(); ++i) {
       const ItemDesc& it = P.items[i];
       const Tab& t = toff[i];
@@ -608,37 +658,15 @@ class Engine {
       group_of[i] = kind;
       g[kind].push_back(d);
       for (int op = 0; op < 2; ++op) {
+        if (!tcgather(i, op)) continue;
+        GCCU_REQUIRE(!swapped[i], "tensor-core items keep their operand roles");
+        gather_of[{g[kind].size() - 1, op}] = (int32_t)gathers.size();
+        gathers.push_back(job_of(i, op, nullptr));
+      }
+      for (int op = 0; op < 2; ++op) {
         int64_t po = op == 0 ? pack_off1[i] : pack_off2[i];
         if (po < 0) continue;
-        PackJob j{};
-        j.R = op == 0 ? it.M : it.N;
-        j.K = it.K;
-        j.src = op == 0 ? x1 + it.base1 : x2 + it.base2;
-        j.dst = dp.scratch + po;
-        const PackTab& pt = op == 0 ? ptab1[i] : ptab2[i];
-        j.roff = dp.d_tabs + pt.roff;
-        j.koff = dp.d_tabs + pt.koff;
-        j.rmi = dp.d_tabs + pt.rmi;
-        j.kmi = dp.d_tabs + pt.kmi;
-        const OpndDesc& od = it.op[op];
-        const int rsp = op == 0 ? kEx1 : kEx2;
-        j.nm = 0;
-        for (int c = 0; c < od.ncomp; ++c) {
-          if (!od.map[c]) continue;
-          GCCU_REQUIRE((od.sp1[c] == rsp && od.sp2[c] == kCnt) ||
-                           (od.sp1[c] == kCnt && od.sp2[c] == rsp),
-                       "string map of an operand must merge an external and a contracted string");
-          j.row_is_1[j.nm] = od.sp1[c] == rsp;
-          j.n1[j.nm] = od.n1[c];
-          j.ldim[j.nm] = od.ldim[c];
-          j.map[j.nm] = od.map[c];
-          ++j.nm;
-        }
-        GCCU_REQUIRE(j.R < INT32_MAX && j.K < INT32_MAX, "block too large for the pack kernel");
-        j.kfast = op == 0 ? it.kfast1 : it.kfast2;
-        const int64_t nf = j.kfast ? j.K : j.R;
-        j.F = 1;
-        while (j.F < 256 && j.F < nf) j.F *= 2;
+        PackJob j = job_of(i, op, dp.scratch + po);
         int64_t gx, gy;
         pack_geometry(j, gx, gy);
         dp.pack_gx = std::max(dp.pack_gx, gx);
@@ -650,6 +678,7 @@ class Engine {
     GCCU_REQUIRE(dp.njobs <= 65535 && dp.pack_gy <= 65535 && dp.pack_gx < INT32_MAX,
                  "contraction has too many or too large map-addressed operand blocks");
     if (!jobs.empty()) dp.d_jobs = upload(jobs);
+    if (!gathers.empty()) dp.d_gather = upload(gathers);
     // result blocks written by more than one item need atomic updates
     std::map<const double*, int> writers;
     for (int kind = 0; kind < kGemmKinds; ++kind)
@@ -716,9 +745,13 @@ class Engine {
           off += tc_panel_floats(d.M, kGemmTcM, d.K);
           d.pb = off;
           off += tc_panel_floats(d.N, d.tn, d.K);
-          sj.push_back(SplitJob{(int32_t)i, 0, cs});
+          auto gat = [&](int op) {
+            auto f = gather_of.find({i, op});
+            return f == gather_of.end() ? -1 : f->second;
+          };
+          sj.push_back(SplitJob{(int32_t)i, 0, cs, gat(0), 0});
           cs += tc_split_chunks(d.M, kGemmTcM, d.K);
-          sj.push_back(SplitJob{(int32_t)i, 1, cs});
+          sj.push_back(SplitJob{(int32_t)i, 1, cs, gat(1), 0});
           cs += tc_split_chunks(d.N, d.tn, d.K);
         }
         GCCU_REQUIRE(cs < INT32_MAX, "tensor-core operands too large for one split launch");
@@ -1233,7 +1266,7 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       launch_rebase_descs(dp.d_desc[kind], descs, dp.ndesc_g[kind], dp.scratch, dp.scratch_len,
                           ss.panels, e.stream);
       if (kind == kGemmTc && dp.nsplit) {  // panels in the engine's existing workspace
-        launch_split_tc(descs, dp.d_split, dp.nsplit, dp.split_chunks, e.stream);
+        launch_split_tc(descs, dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather, e.stream);
         ++e.launches;
       }
       launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err, e.stream);
@@ -1305,7 +1338,8 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
       ++e.launches;
     }
     if (dp.nsplit) {  // operand split of the tensor-core items (after the pack it may read)
-      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, e.stream);
+      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather,
+                      e.stream);
       ++e.launches;
     }
     cudaEvent_t evp = nullptr;

@@ -192,16 +192,22 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 // kfast, else row), split, staged in shared memory in the panel order (each
 // k/4 plane padded by 4 floats so that neither read direction conflicts on
 // banks) and written out as 16-byte stores, consecutive threads on
-// consecutive rows.
+// consecutive rows.  A map-addressed operand is read through its gather
+// description (the signed string-map gather of collect_block_impr,
+// contract/collect_block_impr.f:397, without a dense FP64 panel): the chunk's
+// string indices of both sides are staged in shared memory, the element
+// offset adds (|map_m[i2 * n1 + i1]| - 1) * ldim_m per map component.
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
 
-__global__ void __launch_bounds__(kSplitThreads)
+__global__ void __launch_bounds__(kSplitThreads, 6)
     k_split_tc(const GemmDesc* __restrict__ descs, const SplitJob* __restrict__ jobs,
-               int64_t njobs) {
+               int64_t njobs, const PackJob* __restrict__ gathers) {
   __shared__ __align__(16) float sh[2][8 * kSplitPitch];
   __shared__ int64_t ro[128];
   __shared__ int64_t ko[SK];
+  __shared__ int32_t rmi_s[kTcGatherMaps][128], kmi_s[kTcGatherMaps][SK];
+  __shared__ PackJob G;
   const int tid = threadIdx.x;
   const int64_t blk = blockIdx.x;
   int64_t lo = 0, hi = njobs - 1;  // last job with cstart <= blk
@@ -213,49 +219,92 @@ __global__ void __launch_bounds__(kSplitThreads)
   const SplitJob J = jobs[lo];
   const GemmDesc& d = descs[J.desc];
   const bool row_op = J.op == 0;
+  const bool gat = J.gather >= 0;  // block-uniform
   const int64_t R = row_op ? d.M : d.N, K = d.K;
   const int TR = row_op ? TBM : d.tn;
-  const double* __restrict__ x = row_op ? d.a : d.b;
-  const int64_t* rtab = row_op ? d.aro : d.bco;
-  const int64_t* ktab = row_op ? d.ako : d.bko;
-  const int kfast = row_op ? d.afast : d.bfast;
+  const PackJob* gp = gat ? gathers + J.gather : nullptr;
+  const double* __restrict__ x = gat ? gp->src : row_op ? d.a : d.b;
+  const int64_t* rtab = gat ? gp->roff : row_op ? d.aro : d.bco;
+  const int64_t* ktab = gat ? gp->koff : row_op ? d.ako : d.bko;
+  const int kfast = gat ? gp->kfast : row_op ? d.afast : d.bfast;
   const int64_t nsl = (K + SK - 1) / SK;
   const int64_t c = blk - J.cstart;  // chunk = row chunk * nsl + slice
   const int64_t r0 = (c / nsl) * 128, k0 = (c % nsl) * SK;
   if (tid < 128) ro[tid] = r0 + tid < R ? __ldg(rtab + r0 + tid) : -1;
   else if (tid < 128 + SK) ko[tid - 128] = k0 + (tid - 128) < K ? __ldg(ktab + k0 + tid - 128) : -1;
-  __syncthreads();
-  if (kfast) {  // warp: 16 rows, lane: contraction index
-    const int warp = tid >> 5, lane = tid & 31;
-    const int64_t kof = ko[lane];
-#pragma unroll 8
-    for (int i = 0; i < 16; ++i) {
-      const int r = warp * 16 + i;
-      const int64_t rof = ro[r];
-      const double v = (kof >= 0 && rof >= 0) ? __ldg(x + rof + kof) : 0.0;
-      float h, l;
-      split_tf32(v, h, l);
-      sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
-      sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
+  if (gat) {
+    const int nw = (int)(sizeof(PackJob) / sizeof(int));
+    for (int i = tid; i < nw; i += kSplitThreads)
+      reinterpret_cast<int*>(&G)[i] = reinterpret_cast<const int*>(gp)[i];
+    const int nm = gp->nm;
+    for (int i = tid; i < nm * 128; i += kSplitThreads) {
+      const int m = i >> 7, r = i & 127;
+      if (r0 + r < R) rmi_s[m][r] = (int32_t)__ldg(gp->rmi + (int64_t)m * R + r0 + r);
     }
-  } else {  // thread: one row, 16 contraction indices
-    const int r = tid & 127, kh = tid >> 7;
-    const int64_t rof = ro[r];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float4 h4, l4;
-      float* hp = &h4.x;
-      float* lp = &l4.x;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int64_t kof = ko[16 * kh + 4 * q + e];
-        const double v = (kof >= 0 && rof >= 0) ? __ldg(x + rof + kof) : 0.0;
-        split_tf32(v, hp[e], lp[e]);
-      }
-      *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
-      *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+    for (int i = tid; i < nm * SK; i += kSplitThreads) {
+      const int m = i / SK, k = i % SK;
+      if (k0 + k < K) kmi_s[m][k] = (int32_t)__ldg(gp->kmi + (int64_t)m * K + k0 + k);
     }
   }
+  __syncthreads();
+  // element (local row r, local index k) of a direct operand
+  auto direct = [&](int r, int k) -> double {
+    const int64_t rof = ro[r], kof = ko[k];
+    return (rof >= 0 && kof >= 0) ? __ldg(x + rof + kof) : 0.0;
+  };
+  // element of a map-addressed operand
+  auto mapped_elem = [&](int r, int k) -> double {
+    const int64_t rof = ro[r], kof = ko[k];
+    if (rof < 0 || kof < 0) return 0.0;
+    int64_t off = rof + kof;
+    bool neg = false;
+    for (int m = 0; m < G.nm; ++m) {
+      const int32_t ir = rmi_s[m][r], ik = kmi_s[m][k];
+      const bool r1 = G.row_is_1[m] != 0;
+      int v = __ldg(G.map[m] + (int64_t)(r1 ? ik : ir) * G.n1[m] + (r1 ? ir : ik));
+      if (v == 0) return 0.0;
+      if (v < 0) {
+        neg = !neg;
+        v = -v;
+      }
+      off += (int64_t)(v - 1) * G.ldim[m];
+    }
+    const double val = __ldg(x + off);
+    return neg ? -val : val;
+  };
+  // staging of one chunk: thread mappings per read direction, the element
+  // function a template argument so that the direct path keeps its loads
+  // independent (no map branch between them)
+  auto stage = [&](auto&& elem) {
+    if (kfast) {  // warp: 16 rows, lane: contraction index
+      const int warp = tid >> 5, lane = tid & 31;
+#pragma unroll 8
+      for (int i = 0; i < 16; ++i) {
+        const int r = warp * 16 + i;
+        const double v = elem(r, lane);
+        float h, l;
+        split_tf32(v, h, l);
+        sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
+        sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
+      }
+    } else {  // thread: one row, 16 contraction indices
+      const int r = tid & 127, kh = tid >> 7;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 h4, l4;
+        float* hp = &h4.x;
+        float* lp = &l4.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) split_tf32(elem(r, 16 * kh + 4 * q + e), hp[e], lp[e]);
+        *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
+        *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+      }
+    }
+  };
+  if (gat)
+    stage(mapped_elem);
+  else
+    stage(direct);
   __syncthreads();
   // a 128-row chunk may span two row bands when TR is not a multiple of 128
   const int64_t padded = (R + TR - 1) / TR * TR;
@@ -570,9 +619,9 @@ cudaError_t set_tc_workspace(float* ws) {
 }
 
 void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
-                     cudaStream_t s) {
+                     const PackJob* gathers, cudaStream_t s) {
   if (njobs == 0 || nchunks == 0) return;
-  k_split_tc<<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs);
+  k_split_tc<<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
 }
 
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,

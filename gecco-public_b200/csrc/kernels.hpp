@@ -73,9 +73,11 @@ inline int tc_tile_n(int64_t N) {
   return (int)(w < kGemmTcN ? w : kGemmTcN);
 }
 // split the operands of tensor-core items into their panels (jobs sorted by
-// cstart, nchunks = total chunks)
+// cstart, nchunks = total chunks); gathers: descriptions of map-addressed
+// operands with at most kTcGatherMaps map components
+constexpr int kTcGatherMaps = 4;
 void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
-                     cudaStream_t s);
+                     const PackJob* gathers, cudaStream_t s);
 // device address of the split-TF32 workspace used by the two kernels above
 // (a device-side variable, so captured graphs follow a reallocation)
 cudaError_t set_tc_workspace(float* ws);
