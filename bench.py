@@ -362,7 +362,7 @@ def roofline(cfg, r, fp64_peak_tflops, mode):
         peak = bf16 / 2.0 / 3.0 if bf16 else None
         out.update(peak=peak,
                    traffic=profiled_traffic(cfg, "k_gemm_tc"),
-                   kernel=f"k_gemm_tc<256> split TF32 (tcgen05), launch of [CONTR] "
+                   kernel=f"k_gemm_tc split TF32 (tcgen05, persistent), launch of [CONTR] "
                           f"{ROOFLINE_CONTRACTION}",
                    peak_source="of measured: MEASURED_PEAKS.json bf16_tflops (burst) / 2 "
                                "(dense TF32 = half of dense BF16) / 3 (three TF32 products "
