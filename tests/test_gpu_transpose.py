@@ -1,12 +1,14 @@
 """GPU parity of contractions with operands used transposed (tra_op1 /
 tra_op2 / tra_op1op2): every case matches the oracle's route-2 kernel to
-1e-12 relative (FP64 path)."""
+1e-12 relative on the FP64 path, and to split-TF32 accuracy on a space whose
+blocks take the tensor-core path."""
 import numpy as np
 import pytest
 
 import gccu
 from binding import Oracle
-from cases import SPACES, TRANSPOSES, random_list, transpose_operands, transpose_variants
+from cases import (SPACES, TRANSPOSES, contractions_for, random_list, transpose_operands,
+                   transpose_variants)
 
 pytestmark = pytest.mark.gpu
 
@@ -48,3 +50,39 @@ def test_transposed_contractions_match_oracle(engine, space):
                 (case[0], sym, tra)
             nrun += 1
     assert nrun > 0
+
+
+RTOL_TC = 2e-5  # split TF32, FP32 accumulation over <= 4096 terms
+
+
+def test_transposed_contractions_tensor_cores(engine):
+    # 6 holes, 24 particles: the ladder- and ring-like blocks have hundreds of
+    # rows, columns and contraction indices and run on the tensor cores
+    nsym, norb = 1, [[6], [24], [0], [0]]
+    engine.register_orbinfo(nsym, norb)
+    diffs = []
+    for i, case in enumerate(contractions_for("c1_small")):
+        for j, tra in enumerate(TRANSPOSES):
+            sym = ((1, 0), (1, 0), (1, 0))
+            o = Oracle(nsym, norb)
+            ops_o = transpose_operands(o, case, sym, tra, True)
+            ops_e = transpose_operands(engine, case, sym, tra, False)
+            xs = [random_list(op[1], 41 * i + 5 * j + k) for k, op in enumerate(ops_o)]
+            for op, x in zip(ops_e, xs):
+                engine.upload(op[0], x)
+            ex1, ex2, cnt = case[4:7]
+            ref = np.zeros(ops_o[2][1])
+            o.contract(2, ops_o[0][0], 1, xs[0], ops_o[1][0], 1, xs[1], ops_o[2][0], 1, ref,
+                       ex1, ex2, cnt, 0.5, update=False, tra=tra)
+            scale = max(1.0, np.abs(ref).max())
+            got = {}
+            for mode in (1, 0):
+                engine.set_precision(mode)
+                engine.contract(*[(op[0], 1) for op in ops_e], ex1, ex2, cnt, fact=0.5,
+                                update=False, tra=tra)
+                got[mode] = engine.download(ops_e[2][0], ops_e[2][1])
+            engine.set_precision(0)
+            assert np.max(np.abs(got[1] - ref)) <= RTOL_TC * scale, (case[0], tra)
+            assert np.max(np.abs(got[0] - ref)) <= RTOL * scale, (case[0], tra)
+            diffs.append(np.max(np.abs(got[1] - got[0])) / scale)
+    assert max(diffs) > 1e-10, "no transposed contraction took the tensor-core path"

@@ -61,3 +61,28 @@ def test_noalloc_needs_a_plan(engine):
     (l1, _), (l2, _), (l12, _) = _lists(engine, case)
     with pytest.raises(gccu.GccuError, match="has not been planned"):
         engine.contract_noalloc((l1, 1), (l2, 1), (l12, 1), case[4], case[5], case[6])
+
+
+def test_noalloc_split_tf32(engine):
+    # precision mode 1: the tensor-core items' split panels live in the
+    # engine's workspace, which the first gccu_contract of the descriptor
+    # sized; the allocation-free call reuses it
+    nsym, norb = 1, [[6], [24], [0], [0]]
+    engine.register_orbinfo(nsym, norb)
+    engine.set_precision(1)
+    try:
+        for i, case in enumerate(contractions_for("c1_small")):
+            (l1, n1), (l2, n2), (l12, n12) = _lists(engine, case)
+            ex1, ex2, cnt = case[4], case[5], case[6]
+            args = ((l1, 1), (l2, 1), (l12, 1), ex1, ex2, cnt)
+            engine.upload(l1, random_list(n1, 7 * i))
+            engine.upload(l2, random_list(n2, 7 * i + 1))
+            engine.zero(l12)
+            engine.contract(*args, fact=0.5, update=False)
+            ref = engine.download(l12, n12)
+            engine.upload(l12, random_list(n12, 7 * i + 2))
+            engine.contract_noalloc(*args, fact=0.5, update=False)
+            got = engine.download(l12, n12)
+            assert _close(got, ref), case[0]
+    finally:
+        engine.set_precision(0)
