@@ -21,7 +21,10 @@ namespace gccu {
 namespace {
 
 constexpr int BK = 16;
-constexpr int PAD = 8;
+// row pitch of the staged tiles: BM + 4 doubles = 8 words mod 32, so the four
+// contraction rows of a 64-bit fragment load (one 16-lane phase: 4 rows x 4
+// doubles) fall on 32 distinct banks (BM + 8 put rows 0 and 2 on the same ones)
+constexpr int PAD = 4;
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
   asm volatile(
