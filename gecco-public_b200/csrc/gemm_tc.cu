@@ -8,14 +8,15 @@
 // scatter_block, contract/scatter_block.f:163), so the FP32 accumulation
 // error does not grow with the full contraction length.
 //
-// Two kernels.  k_split_tc reads each operand of each item once through the
-// item's offset tables (the gather of collect_block_impr,
-// contract/collect_block_impr.f:397, already done for map-addressed operands
-// by the pack kernel), splits it and writes both halves as panels in the
-// K-major core-matrix order the tensor core reads (8 rows x 16 bytes per core
-// matrix, no swizzle).  k_gemm_tc is persistent: one CTA per SM walks the
-// tiles (128 x 256 outputs, one contraction chunk) blockIdx.x, +gridDim.x, ...
-// with warp roles.  One thread streams the panel slices of its tiles into a
+// Two kernels.  k_split_tc reads each operand of each item once, through the
+// item's offset tables or, for an operand whose strings merge an external
+// and a contracted component, through its gather description (the signed
+// string-map gather of collect_block_impr, contract/collect_block_impr.f:397),
+// splits it and writes both halves as panels in the K-major core-matrix order
+// the tensor core reads (8 rows x 16 bytes per core matrix, no swizzle).
+// k_gemm_tc is persistent: one CTA per SM walks the tiles (128 rows x tn
+// columns, tn <= 256 chosen per item, one contraction chunk) blockIdx.x,
+// +gridDim.x, ... with warp roles.  One thread streams the panel slices of its tiles into a
 // 4-stage shared-memory ring with bulk asynchronous copies (cp.async.bulk,
 // completion counted in bytes on an mbarrier); one thread issues the MMAs of
 // each stage (2 K-steps x 3 products) into one of two TMEM accumulators and
@@ -41,7 +42,7 @@ __device__ float* g_tc_ws;
 namespace {
 
 constexpr int TBM = kGemmTcM;  // tile rows = TMEM lanes
-constexpr int TBN = kGemmTcN;  // tile columns = TMEM columns
+constexpr int TBN = kGemmTcN;  // widest tile (columns) = TMEM columns per accumulator
 constexpr int SK = (int)kTcSlice;  // contraction indices per panel slice
 constexpr int BK = 16;         // contraction indices per pipeline stage
 constexpr int NST = 4;         // pipeline stages
