@@ -361,27 +361,32 @@ def roofline(cfg, r, fp64_peak_tflops, mode):
         # the launch is timed in the profiled iteration right after the timed
         # loop, i.e. inside a long tensor-core run under the power cap: the
         # sustained BF16 figure is its denominator (the burst one beside it)
-        bf16 = measured_bf16_tflops("bf16_tflops_sustained")
-        burst = measured_bf16_tflops("bf16_tflops")
-        peak = bf16 / 2.0 / 3.0 if bf16 else None
+        bf16, src = measured_bf16_tflops("bf16_tflops_sustained")
+        burst, _ = measured_bf16_tflops("bf16_tflops")
+        peak = bf16 / 2.0 / 3.0
         out.update(peak=peak,
                    traffic=profiled_traffic(cfg, "k_gemm_tc"),
                    kernel=f"k_gemm_tc split TF32 (tcgen05, persistent), launch of [CONTR] "
                           f"{ROOFLINE_CONTRACTION}",
-                   peak_source="of measured: MEASURED_PEAKS.json bf16_tflops_sustained / 2 "
-                               "(dense TF32 = half of dense BF16) / 3 (three TF32 products "
-                               "per useful product)",
-                   frac_of_burst=(achieved / (burst / 6.0)) if burst else None)
+                   peak_source=f"of {src}: bf16_tflops_sustained / 2 (dense TF32 = half of "
+                               "dense BF16) / 3 (three TF32 products per useful product)",
+                   frac_of_burst=achieved / (burst / 6.0))
     out["frac"] = (achieved / out["peak"]) if out["peak"] else None
     return out
 
 
+# earlier measurement on this pool's B200s, used only when MEASURED_PEAKS.json
+# (written before each run) is absent
+FALLBACK_PEAKS = {"bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "hbm_gbs": 6650.0}
+
+
 def measured_bf16_tflops(key="bf16_tflops"):
+    """(value, "measured" from MEASURED_PEAKS.json | "fallback")"""
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
-        return float(json.load(open(path))[key])
+        return float(json.load(open(path))[key]), "measured"
     except (OSError, KeyError, ValueError):
-        return None
+        return FALLBACK_PEAKS[key], "fallback"
 
 
 def convergence(local):
