@@ -261,6 +261,20 @@ METRIC = {0: "s/CC-iteration (CCSD, plain FP64)",
 DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums"}
 
 
+def max_over_ranks(value, dist):
+    """the largest of every rank's value (the job's time is its slowest
+    rank's); NCCL reduces a device tensor, gloo a host one; without a process
+    group the value itself"""
+    if dist is None:
+        return value
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measure(args, cfg, eng, solver, local, dist, mode):
     """warm-up (plans every contraction in this precision mode), the timed
     graph-replayed iterations, one eagerly profiled iteration and the
@@ -307,11 +321,7 @@ def measure(args, cfg, eng, solver, local, dist, mode):
                         "block_contractions": int(r[3]), "tiles": int(r[4]),
                         "pack_ms": r[5] / max(r[1], 1)}
                        for n, r in zip(names, prof)], f, indent=1)
-    ms = ms_total / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms_total / args.steps, dist)
     # e2e: the same iteration through the public API with host buffers: the
     # amplitudes come from pinned host memory, the residual and energy go back
     nT = {a: solver.lists[a][1] for a in solver.amps}
