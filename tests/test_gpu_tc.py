@@ -6,7 +6,8 @@ tensor-core path (more than 32 rows and columns, at least 256 contraction
 indices), to FP32-level accuracy; switching back to FP64 restores the 1e-12
 agreement.  The large space adds a contraction whose result is contiguous
 along the column space (its creator string comes from the second operand),
-which the tensor-core epilogue scatters column-major.  The test also checks
+which the tensor-core epilogue scatters column-major, and the same
+contractions run under spin-flip symmetry (use_tr).  The tests also check
 that the tensor-core path ran: mode 1 must differ from mode 0 at the FP32
 level for some contraction of the large space."""
 import numpy as np
@@ -68,3 +69,43 @@ def test_split_tf32_contractions(engine, space):
         diffs.append(np.max(np.abs(got[1] - got[0])) / scale)
     if space == "c1_tc":
         assert max(diffs) > 1e-10, "no contraction of the large space took the tensor-core path"
+
+
+def test_split_tf32_with_spin_flip_symmetry(engine):
+    # use_tr on the tensor-core path: half of the Ms cases, doubled, then the
+    # spin-flip symmetrisation of the result, against the oracle's route 2
+    nsym, norb = TC_SPACES["c1_tc"]
+    engine.register_orbinfo(nsym, norb)
+    engine.set_precision(1)
+    diffs = []
+    try:
+        for i, case in enumerate(contractions_for("c1_small")[:5] + TC_EXTRA):
+            o = Oracle(nsym, norb)
+            name, op1, op2, res, ex1, ex2, cnt = case
+            ls = []
+            for occ in (op1, op2, res):
+                le, n = engine.register_list(engine.define_operator([occ]), absym=1)
+                lo, _ = o.define_list(o.define_op([occ]), absym=1)
+                ls.append((le, lo, n))
+            (l1, o1, n1), (l2, o2, n2), (l12, o12, n12) = ls
+            x1, x2 = random_list(n1, 5 * i), random_list(n2, 5 * i + 1)
+            o.sym_ab(o1, 1, x1)  # spin-symmetric inputs
+            o.sym_ab(o2, 1, x2)
+            engine.upload(l1, x1)
+            engine.upload(l2, x2)
+            ref = np.zeros(n12)
+            o.contract(2, o1, 1, x1, o2, 1, x2, o12, 1, ref, ex1, ex2, cnt, 1.0, use_tr=True)
+            scale = max(1.0, np.abs(ref).max())
+            got = {}
+            for mode in (1, 0):
+                engine.set_precision(mode)
+                engine.contract((l1, 1), (l2, 1), (l12, 1), ex1, ex2, cnt, fact=1.0,
+                                update=False, use_tr=True)
+                got[mode] = engine.download(l12, n12)
+            engine.set_precision(1)
+            assert np.max(np.abs(got[1] - ref)) <= RTOL_TC * scale, name
+            assert np.max(np.abs(got[0] - ref)) <= RTOL_FP64 * scale, name
+            diffs.append(np.max(np.abs(got[1] - got[0])) / scale)
+    finally:
+        engine.set_precision(0)
+    assert max(diffs) > 1e-10, "no spin-flip contraction took the tensor-core path"
