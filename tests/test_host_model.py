@@ -60,3 +60,23 @@ def test_plan_matches_oracle_enumeration(host_engine, space):
         nitems, st = host_engine.plan_info((l1, 1), (l2, 1), (l12, 1), ex1, ex2, cnt)
         _, sto = _run_case(Oracle(nsym, norb), case, 3, 11 + i)
         assert np.array_equal(st, sto), (name, st, sto)
+
+
+@pytest.mark.parametrize("space", ["c1_small", "c2v", "d2h"])
+def test_plan_items_agree_with_plan_info(host_engine, space):
+    # gccu_plan_items lists the same block contractions gccu_plan_info counts;
+    # their 2*M*N*K sums to the reference's dgemm flop accounting, and the
+    # map-component counts are those of the operands' string merges
+    nsym, norb = SPACES[space]
+    host_engine.register_orbinfo(nsym, norb)
+    for case in contractions_for(space):
+        name, op1, op2, res, ex1, ex2, cnt = case
+        ls = [host_engine.register_list(host_engine.define_operator([o]))[0]
+              for o in (op1, op2, res)]
+        args = [(l, 1) for l in ls] + [ex1, ex2, cnt]
+        nitems, st = host_engine.plan_info(*args)
+        rows = host_engine.plan_items(*args)
+        assert len(rows) == nitems, name
+        assert (rows[:, :3] > 0).all(), name
+        assert 2.0 * float(np.sum(rows[:, 0] * rows[:, 1] * rows[:, 2])) == st[7], name
+        assert ((rows[:, 3:6] >= 0) & (rows[:, 3:6] <= 8)).all(), name
