@@ -242,11 +242,10 @@ def sampling_report():
 
 
 def scaled_time(wall, rep):
-    """wall time of a sampled evaluation scaled to the full work: executed
-    short-operand gathers and long-operand batches scaled by their counts"""
-    other = wall - rep["t_short"] - rep["t_sampled"]
-    return (other + rep["t_short"] * rep["shorts"] / max(rep["shorts_done"], 1) +
-            rep["t_sampled"] * rep["batches"] / max(rep["done"], 1))
+    """wall time of a sampled evaluation scaled to the full work: the
+    executed long-operand batches scaled by their count (every short-operand
+    gather and everything outside route 3 runs in full)"""
+    return wall + rep["t_sampled"] * (rep["batches"] / max(rep["done"], 1) - 1.0)
 
 
 def add_opblk(xout, xin, fac, reset=False, typ=1):

@@ -916,7 +916,8 @@ typedef void (*dgemm_t)(const char*, const char*, const int64_t*, const int64_t*
 dgemm_t g_dgemm = nullptr;
 
 // timing sample: only every g_stride-th long-operand batch of route 3 is
-// executed (the CPU baseline times a bounded sample of a large workload)
+// executed (the CPU baseline times a bounded sample of a large workload);
+// the short-operand gathers always run
 int64_t g_stride = 1, g_batch = 0, g_batches_total = 0, g_batches_done = 0;
 int64_t g_short_total = 0, g_short_done = 0;
 double g_t_always = 0, g_t_sampled = 0;
@@ -959,20 +960,20 @@ void route3(const Blk& b, int64_t str_block, int64_t cnt_block, Stats* st) {
   for (int64_t c0 = 0; c0 < ncnt; c0 += mcnt) {
     int64_t nc = std::min(mcnt, ncnt - c0);
     // the short operand (all its ex strings) is gathered once per cnt batch,
-    // here on first use by an executed long-operand batch
-    bool have_short = false;
-    ++g_short_total;
+    // always, also when sampling skips every long-operand batch of it: its
+    // cost differs widely between block contractions, so it is measured, not
+    // extrapolated
+    {
+      double t0 = now_s();
+      gather(op1shorter, 0, nexs, c0, nc, ps);
+      g_t_always += now_s() - t0;
+      ++g_short_total;
+      ++g_short_done;
+    }
     for (int64_t l0 = 0; l0 < nexl; l0 += mexl) {
       ++g_batches_total;
       if ((g_batch++) % g_stride != 0) continue;
       ++g_batches_done;
-      if (!have_short) {
-        double t0 = now_s();
-        gather(op1shorter, 0, nexs, c0, nc, ps);
-        g_t_always += now_s() - t0;
-        ++g_short_done;
-        have_short = true;
-      }
       double t1 = now_s();
       int64_t nl = std::min(mexl, nexl - l0);
       gather(!op1shorter, l0, nl, c0, nc, pl);
