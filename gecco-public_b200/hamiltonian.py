@@ -107,11 +107,14 @@ class DenseIntegrals:
 
 
 def synthetic(nocc, nvir, naux, seed, nsym=1, occ_range=(-1.5, -0.3), vir_range=(0.1, 4.0),
-              gap=None, dtype=np.float64):
+              gap=None, dtype=np.float64, sigma=0.05):
     """seeded synthetic closed-shell Hamiltonian: canonical diagonal Fock with
     occupied energies U[occ_range], virtual energies U[vir_range] (or a
-    HOMO-LUMO gap), (pq|rs) = sum_P B_pq^P B_rs^P with B symmetric in pq and
-    N(0, 0.05^2) entries; with nsym > 1 irreps are assigned round-robin to
+    HOMO-LUMO gap), (pq|rs) = sum_P B_pq^P B_rs^P with B symmetric in pq:
+    the entries with p <= q are drawn from N(0, sigma^2) (sigma = 0.05 by
+    default) and mirrored to q > p, so every entry has that distribution.
+    The exchange-type integrals (pq|pq) = sum_P (B_pq^P)^2 are then about
+    naux * sigma^2 Eh.  With nsym > 1 irreps are assigned round-robin to
     orbitals and auxiliary functions and B_pq^P vanishes unless
     irrep(p) x irrep(q) = irrep(P), so every integral is totally symmetric.
     Returns (space, eps, B) with B of shape (norb, norb, naux)."""
@@ -125,8 +128,9 @@ def synthetic(nocc, nvir, naux, seed, nsym=1, occ_range=(-1.5, -0.3), vir_range=
         ev = np.sort(rng.uniform(*vir_range, size=nvir))
     eps = np.concatenate([eo, ev])
     sym = np.arange(n) % nsym + 1
-    B = rng.normal(0.0, 0.05, size=(n, n, naux)).astype(dtype)
-    B = 0.5 * (B + B.transpose(1, 0, 2))
+    B = rng.normal(0.0, sigma, size=(n, n, naux)).astype(dtype)
+    upper = np.arange(n)[:, None] <= np.arange(n)[None, :]
+    B = np.where(upper[:, :, None], B, B.transpose(1, 0, 2))
     if nsym > 1:
         psym = np.arange(naux) % nsym
         mask = ((sym[:, None] - 1) ^ (sym[None, :] - 1))[:, :, None] == psym[None, None, :]
