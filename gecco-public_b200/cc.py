@@ -193,13 +193,20 @@ class CCSolver:
     lists (solve_nleq with method=diis, solve/solve_nleq.f; diagonal step
     diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
 
-    def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0):
+    def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
+                 learned=None):
         self.e = engine
         self.ints = ints
         self.method = method
         self.use_tr = use_tr
         self.maxsub = maxsub
         self.shift = shift  # level shift of the diagonal preconditioner (diavc)
+        # learned correction of the diagonal step (weights loaded into the
+        # engine), used for a step only if the last step reduced the residual
+        # norm; plain diavc otherwise (counted in self.fallbacks)
+        self.learned = learned is not None
+        self.fallbacks = 0
+        self.recorder = None  # called with the solver before each step (sampling)
         sp = ints.space
         self.nsym = sp.nsym
         engine.register_orbinfo(sp.nsym, sp.norb)
@@ -215,15 +222,18 @@ class CCSolver:
             self.lists[name] = (lid, n, blocks)
         self.amps = ["T2"] if method == "mp2" else ["T1", "T2"]
         self.res = {"T1": "R1", "T2": "R2"}
-        # denominators, steps and DIIS subspace
+        # denominators, steps (the last one kept for the learned step's
+        # inputs) and DIIS subspace
         for a in self.amps:
             blocks = self.lists[a][2]
-            for extra in ("D" + a, "S" + a):
+            for extra in ("D" + a, "S" + a, "P" + a):
                 opid = engine.define_operator(blocks)
                 lid, n = engine.register_list(opid)
                 self.lists[extra] = (lid, n, blocks)
         self.graph = None
         self.history = []
+        if self.learned:
+            engine.lp_set_weights(learned)
 
     def lid(self, name):
         return self.lists[name][0]
@@ -250,6 +260,13 @@ class CCSolver:
             d = fill_denominators(self.view("D" + a), n, self.lists[a][2][0], self.ints)
             self.e.upload(self.lid("D" + a), d)
             self.e.zero(self.lid(a))
+        self.freeze_hamiltonian()
+
+    def freeze_hamiltonian(self, frozen=True):
+        """the Fock and two-electron lists are constant during the solve: the
+        engine may keep the operand panels it derives from them"""
+        for name in ("F", "V"):
+            self.e.freeze(self.lid(name), frozen)
 
     def load_hamiltonian_device(self, tints):
         """generate the Hamiltonian and denominator lists on the device
@@ -294,6 +311,7 @@ class CCSolver:
             torch.cuda.synchronize()
         for a in self.amps:
             self.e.zero(self.lid(a))
+        self.freeze_hamiltonian()
 
     def evaluate(self):
         """one formula evaluation (frm_sched2 over the item list)"""
@@ -323,11 +341,35 @@ class CCSolver:
         return float(np.sqrt(sum(self.e.dot(self.lid(self.res[a]), self.lid(self.res[a]))
                                  for a in self.amps)))
 
+    def use_learned_step(self):
+        """the learned step is taken while the residual norm decreases"""
+        if not self.learned:
+            return False
+        h = self.history
+        ok = len(h) < 2 or h[-1][2] < h[-2][2]
+        if not ok:
+            self.fallbacks += 1
+        return ok
+
+    def precondition(self, out, a, learned):
+        """out = -R/D (diavc) or its learned correction; the step is kept as
+        the previous step of the next call"""
+        if learned:
+            self.e.lp_precondition(out, self.lid(self.res[a]), self.lid("D" + a),
+                                   self.lid("P" + a), fac=-1.0, shift=self.shift)
+        else:
+            self.e.precondition(out, self.lid(self.res[a]), self.lid("D" + a), fac=-1.0,
+                                shift=self.shift)
+        if self.learned or self.recorder is not None:
+            self.e.add_block(1.0, out, 1, self.lid("P" + a), 1, reset=True)
+
     def step(self):
         """t <- t - R/D (diagonal preconditioner)"""
+        if self.recorder is not None:
+            self.recorder(self)
+        learned = self.use_learned_step()
         for a in self.amps:
-            self.e.precondition(self.lid("S" + a), self.lid(self.res[a]), self.lid("D" + a),
-                                fac=-1.0, shift=self.shift)
+            self.precondition(self.lid("S" + a), a, learned)
             self.e.add_block(1.0, self.lid("S" + a), 1, self.lid(a), 1)
 
     def _diis_lists(self):
@@ -355,9 +397,11 @@ class CCSolver:
         k = len(used) if len(used) < self.maxsub else used.pop(0)
         used.append(k)
         slot = d["slots"][k]
+        if self.recorder is not None:
+            self.recorder(self)
+        learned = self.use_learned_step()
         for a in self.amps:
-            self.e.precondition(slot[("e", a)], self.lid(self.res[a]), self.lid("D" + a), fac=-1.0,
-                                shift=self.shift)
+            self.precondition(slot[("e", a)], a, learned)
             self.e.add_block(1.0, self.lid(a), 1, slot[("t", a)], 1, reset=True)
             self.e.add_block(1.0, slot[("e", a)], 1, slot[("t", a)], 1)
         B = d["B"]

@@ -67,8 +67,10 @@ struct GemmDesc {
   // k offset tables that are affine, ako[k] = ako[0] + k * akstep (0: not affine)
   int64_t akstep, bkstep;
   // tensor-core items: float offsets of the split operand panels in the
-  // split-TF32 workspace (see SplitJob)
+  // split-TF32 workspace (see SplitJob), or, for an operand read from a
+  // frozen list, its persistent panel (pa_ptr / pb_ptr, else null)
   int64_t pa, pb;
+  float *pa_ptr, *pb_ptr;
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update

@@ -40,6 +40,10 @@ Occ to_occ(const int64_t* o) {
 struct DevList {
   ListLayout L;
   double* d = nullptr;
+  // frozen: the host has declared the data constant (gccu_freeze_list);
+  // plans may cache panels derived from it; epoch counts unfreezes
+  bool frozen = false;
+  int64_t epoch = 0;
 };
 
 struct DevGraph {
@@ -61,6 +65,15 @@ struct DevPlan {
   // split-TF32 panels of the tensor-core items (workspace floats, jobs)
   SplitJob* d_split = nullptr;
   int64_t nsplit = 0, split_chunks = 0, ws_floats = 0;
+  // operands read from lists that were frozen when the plan was made: their
+  // packed FP64 panels and split TF32 panels are made once and kept
+  PackJob* d_jobs_c = nullptr;
+  int64_t njobs_c = 0, pack_gx_c = 0, pack_gy_c = 0;
+  SplitJob* d_split_c = nullptr;
+  int64_t nsplit_c = 0, split_chunks_c = 0;
+  float* const_panels = nullptr;  // persistent split panels (floats)
+  std::vector<int> const_lists;   // the frozen lists behind them
+  bool const_stale = false;       // a list of const_lists was unfrozen since they were made
   PackJob* d_gather = nullptr;  // gather descriptions of map-addressed tensor-core operands
   int64_t* d_tabs = nullptr;
   double* scratch = nullptr;
@@ -103,6 +116,10 @@ class Engine {
   bool capturing = false;
   std::vector<cudaGraphExec_t> graphs;
   std::vector<int64_t> graph_kernels;  // kernel launches recorded in each graph
+  // (list, epoch) pairs whose cached panels a graph reads without re-making
+  // them: the graph is valid while each list stays frozen in that epoch
+  std::vector<std::vector<std::pair<int, int64_t>>> graph_deps;
+  std::vector<std::pair<int, int64_t>> capture_deps;
   int64_t capture_start = 0;
   cudaEvent_t slots[64] = {};
   bool profiling = false;
@@ -112,12 +129,41 @@ class Engine {
   float* tc_ws = nullptr;
   int64_t tc_ws_floats = 0;
   int* d_err = nullptr;  // set by kernels whose bounded pipeline waits ran out
+  int64_t wait_limit = kTcWaitLimitDefault;  // mbarrier polls per pipeline wait
   // fixed scratch of gccu_contract_noalloc, looked up on its first call
   bool have_static = false;
   StaticScratch static_ss;
   std::vector<cudaEvent_t> event_pool;
   std::vector<DevPlan*> plan_order;  // plans in first-use order (profile report)
   std::map<std::string, std::unique_ptr<DevReo>> reos;  // reorder plans per descriptor
+  // learned correction of the diagonal step: weights, Adam moments, sample
+  // set (rows and targets), gradient buffers
+  double *lp_w = nullptr, *lp_m = nullptr, *lp_v = nullptr;
+  int64_t lp_t = 0;
+  bool lp_have_w = false;
+  double *lp_rows = nullptr, *lp_tgt = nullptr;
+  int64_t lp_nrows = 0, lp_cap = 0;
+  double *lp_part = nullptr, *lp_grad = nullptr;
+  int64_t lp_part_rows = 0;
+  int64_t* lp_idx = nullptr;  // sampled element indices
+  double* lp_out = nullptr;   // sampled rows
+  int64_t lp_idx_cap = 0;
+
+  void lp_alloc_weights() {
+    if (lp_w) return;
+    lp_w = (double*)alloc(kLpWeights * sizeof(double));
+    lp_m = (double*)alloc(kLpWeights * sizeof(double));
+    lp_v = (double*)alloc(kLpWeights * sizeof(double));
+    lp_grad = (double*)alloc((kLpWeights + 1) * sizeof(double));
+  }
+  double* lp_partials(int64_t blocks) {
+    if (blocks > lp_part_rows) {
+      if (lp_part) release(lp_part, (size_t)lp_part_rows * (kLpWeights + 1) * sizeof(double));
+      lp_part = (double*)alloc((size_t)blocks * (kLpWeights + 1) * sizeof(double));
+      lp_part_rows = blocks;
+    }
+    return lp_part;
+  }
 
   cudaEvent_t get_event() {
     if (!event_pool.empty()) {
@@ -198,6 +244,42 @@ class Engine {
   DevList& list(int64_t id) {
     GCCU_REQUIRE(id >= 1 && id <= (int64_t)lists.size(), "invalid ME-list handle");
     return lists[id - 1];
+  }
+  // a list the call is about to write
+  DevList& wlist(int64_t id) {
+    DevList& l = list(id);
+    GCCU_REQUIRE(!l.frozen, "the ME list is frozen (gccu_freeze_list): unfreeze it before "
+                            "writing it");
+    return l;
+  }
+
+  // do the cached panels of a plan have to be (re)made by this call?
+  bool need_const(const DevPlan& dp) {
+    if (dp.const_stale) return true;
+    for (int l : dp.const_lists)
+      if (!list(l).frozen) return true;
+    return false;
+  }
+  // make the cached panels of a plan (packs before splits: a split may read
+  // a packed panel); during a capture, or else note what the graph relies on
+  void run_const(DevPlan& dp, bool force = false) {
+    if (dp.const_lists.empty()) return;
+    if (force || need_const(dp)) {
+      if (dp.njobs_c) {
+        launch_pack(dp.d_jobs_c, dp.njobs_c, dp.pack_gx_c, dp.pack_gy_c, stream);
+        ++launches;
+      }
+      if (dp.nsplit_c) {
+        launch_split_tc(dp.d_desc[kGemmTc], dp.d_split_c, dp.nsplit_c, dp.split_chunks_c,
+                        dp.d_gather, stream);
+        ++launches;
+      }
+      bool all_frozen = true;
+      for (int l : dp.const_lists) all_frozen = all_frozen && list(l).frozen;
+      if (all_frozen) dp.const_stale = false;
+    } else if (capturing) {
+      for (int l : dp.const_lists) capture_deps.push_back({l, list(l).epoch});
+    }
   }
 
   DevGraph& dgraph(int gid) {
@@ -486,8 +568,11 @@ class Engine {
     std::vector<int64_t> tabs;
     struct Tab { int64_t aro, ako, bco, bko, cro, cco; };
     std::vector<Tab> toff(P.items.size());
-    std::vector<PackJob> jobs;
+    std::vector<PackJob> jobs, jobs_c;
     std::vector<int64_t> pack_off1(P.items.size(), -1), pack_off2(P.items.size(), -1);
+    // operands of frozen lists: made once (plan time), kept with the plan
+    const bool frozen_op[2] = {list(dp.list1).frozen, list(dp.list2).frozen};
+    bool const_used[2] = {false, false};
     int64_t scratch = 0;
     dp.pack_gx = dp.pack_gy = 0;
     auto put = [&](auto&& fill) {
@@ -669,15 +754,25 @@ class Engine {
         PackJob j = job_of(i, op, dp.scratch + po);
         int64_t gx, gy;
         pack_geometry(j, gx, gy);
-        dp.pack_gx = std::max(dp.pack_gx, gx);
-        dp.pack_gy = std::max(dp.pack_gy, gy);
-        jobs.push_back(j);
+        if (frozen_op[op]) {
+          dp.pack_gx_c = std::max(dp.pack_gx_c, gx);
+          dp.pack_gy_c = std::max(dp.pack_gy_c, gy);
+          jobs_c.push_back(j);
+          const_used[op] = true;
+        } else {
+          dp.pack_gx = std::max(dp.pack_gx, gx);
+          dp.pack_gy = std::max(dp.pack_gy, gy);
+          jobs.push_back(j);
+        }
       }
     }
     dp.njobs = (int64_t)jobs.size();
-    GCCU_REQUIRE(dp.njobs <= 65535 && dp.pack_gy <= 65535 && dp.pack_gx < INT32_MAX,
+    dp.njobs_c = (int64_t)jobs_c.size();
+    GCCU_REQUIRE(dp.njobs <= 65535 && dp.pack_gy <= 65535 && dp.pack_gx < INT32_MAX &&
+                     dp.njobs_c <= 65535 && dp.pack_gy_c <= 65535 && dp.pack_gx_c < INT32_MAX,
                  "contraction has too many or too large map-addressed operand blocks");
     if (!jobs.empty()) dp.d_jobs = upload(jobs);
+    if (!jobs_c.empty()) dp.d_jobs_c = upload(jobs_c);
     if (!gathers.empty()) dp.d_gather = upload(gathers);
     // result blocks written by more than one item need atomic updates
     std::map<const double*, int> writers;
@@ -736,29 +831,53 @@ class Engine {
         }
       }
       if (kind == kGemmTc && !g[kind].empty()) {
-        // operand panels of every item, row operand then column operand
-        std::vector<SplitJob> sj;
-        int64_t off = 0, cs = 0;
+        // operand panels of every item, row operand then column operand: in
+        // the shared workspace, or, for an operand of a frozen list, in the
+        // plan's persistent panels (split once, at plan time)
+        std::vector<SplitJob> sj, sj_c;
+        int64_t off = 0, cs = 0, off_c = 0, cs_c = 0;
         for (size_t i = 0; i < g[kind].size(); ++i) {
           GemmDesc& d = g[kind][i];
-          d.pa = off;
-          off += tc_panel_floats(d.M, kGemmTcM, d.K);
-          d.pb = off;
-          off += tc_panel_floats(d.N, d.tn, d.K);
           auto gat = [&](int op) {
             auto f = gather_of.find({i, op});
             return f == gather_of.end() ? -1 : f->second;
           };
-          sj.push_back(SplitJob{(int32_t)i, 0, cs, gat(0), 0});
-          cs += tc_split_chunks(d.M, kGemmTcM, d.K);
-          sj.push_back(SplitJob{(int32_t)i, 1, cs, gat(1), 0});
-          cs += tc_split_chunks(d.N, d.tn, d.K);
+          for (int op = 0; op < 2; ++op) {
+            const int64_t rows = op == 0 ? d.M : d.N;
+            const int tr = op == 0 ? kGemmTcM : d.tn;
+            const int64_t fl = tc_panel_floats(rows, tr, d.K);
+            const int64_t ch = tc_split_chunks(rows, tr, d.K);
+            int64_t& po = op == 0 ? d.pa : d.pb;
+            if (frozen_op[op]) {
+              po = off_c;  // made absolute below
+              off_c += fl;
+              sj_c.push_back(SplitJob{(int32_t)i, op, cs_c, gat(op), 0});
+              cs_c += ch;
+              const_used[op] = true;
+            } else {
+              po = off;
+              off += fl;
+              sj.push_back(SplitJob{(int32_t)i, op, cs, gat(op), 0});
+              cs += ch;
+            }
+          }
         }
-        GCCU_REQUIRE(cs < INT32_MAX, "tensor-core operands too large for one split launch");
+        GCCU_REQUIRE(cs < INT32_MAX && cs_c < INT32_MAX,
+                     "tensor-core operands too large for one split launch");
+        if (off_c) {
+          dp.const_panels = (float*)alloc((size_t)off_c * sizeof(float));
+          for (auto& d : g[kind]) {
+            if (frozen_op[0]) d.pa_ptr = dp.const_panels + d.pa;
+            if (frozen_op[1]) d.pb_ptr = dp.const_panels + d.pb;
+          }
+        }
         dp.ws_floats = off;
         dp.nsplit = (int64_t)sj.size();
         dp.split_chunks = cs;
-        dp.d_split = upload(sj);
+        if (!sj.empty()) dp.d_split = upload(sj);
+        dp.nsplit_c = (int64_t)sj_c.size();
+        dp.split_chunks_c = cs_c;
+        if (!sj_c.empty()) dp.d_split_c = upload(sj_c);
         ensure_tc_ws(off);
       }
       dp.ntiles_g[kind] = (int64_t)tiles.size();
@@ -770,6 +889,9 @@ class Engine {
     }
     dp.ntiles = 0;
     for (int kind = 0; kind < kGemmKinds; ++kind) dp.ntiles += dp.ntiles_g[kind];
+    if (const_used[0]) dp.const_lists.push_back(dp.list1);
+    if (const_used[1] && dp.list2 != dp.list1) dp.const_lists.push_back(dp.list2);
+    run_const(dp, true);  // the cached panels, made once here
   }
 
   // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
@@ -1105,7 +1227,7 @@ int gccu_list_dists(int64_t list_id, int64_t* rows, int64_t maxrows, int64_t* nr
 int gccu_upload_list(int64_t list_id, const double* host, int64_t n) {
   return guarded([&] {
     Engine& e = eng();
-    DevList& dl = e.list(list_id);
+    DevList& dl = e.wlist(list_id);
     GCCU_REQUIRE(n == dl.L.len, "upload length differs from the list length");
     CUDA_OK(cudaMemcpyAsync(dl.d, host, n * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     CUDA_OK(cudaStreamSynchronize(e.stream));
@@ -1125,7 +1247,7 @@ int gccu_download_list(int64_t list_id, double* host, int64_t n) {
 int gccu_zero_list(int64_t list_id) {
   return guarded([&] {
     Engine& e = eng();
-    DevList& dl = e.list(list_id);
+    DevList& dl = e.wlist(list_id);
     CUDA_OK(cudaMemsetAsync(dl.d, 0, dl.L.len * sizeof(double), e.stream));
   });
 }
@@ -1144,7 +1266,7 @@ int gccu_reorder(const gccu_reo_desc* reo, double fac, int64_t sign_reo, int64_t
     GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
     DevReo& dr = e.reo_for(reo);
     DevList& lo = e.list(dr.list_ori);
-    DevList& lr = e.list(dr.list_reo);
+    DevList& lr = e.wlist(dr.list_reo);
     GCCU_REQUIRE(lo.d != lr.d, "reorder: original and reordered list must differ");
     if (!update)
       CUDA_OK(cudaMemsetAsync(lr.d + dr.reo_off, 0, dr.reo_len * sizeof(double), e.stream));
@@ -1177,7 +1299,7 @@ int gccu_trace(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t iblk_
     GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
     DevReo& dr = e.trace_for(list_op, iblk_op, list_res, iblk_res, occ_cnt);
     DevList& lo = e.list(dr.list_ori);
-    DevList& lr = e.list(dr.list_reo);
+    DevList& lr = e.wlist(dr.list_reo);
     GCCU_REQUIRE(lo.d != lr.d, "trace: operator and result list must differ");
     if (!update)
       CUDA_OK(cudaMemsetAsync(lr.d + dr.reo_off, 0, dr.reo_len * sizeof(double), e.stream));
@@ -1239,25 +1361,40 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
          << kStaticPanelDoubles * sizeof(double) / (1 << 20) << " MiB";
       throw Error(os.str());
     }
-    GCCU_REQUIRE(ndesc <= kStaticMaxDescs && dp.njobs <= kStaticMaxJobs,
+    GCCU_REQUIRE(ndesc <= kStaticMaxDescs && dp.njobs + dp.njobs_c <= kStaticMaxJobs,
                  "gccu_contract_noalloc: the contraction has more block contractions than the "
                  "fixed scratch holds descriptors for (16384)");
+    // the symbol look-up may load the module lazily, which a stream capture
+    // does not allow
+    GCCU_REQUIRE(!e.capturing || e.have_static,
+                 "gccu_contract_noalloc: the first call of an engine looks up the fixed "
+                 "scratch array and must come before any graph capture");
     if (!e.have_static) {  // once per engine (and so per device), with its device current
       CUDA_OK(cudaSetDevice(e.device));
       CUDA_OK(static_scratch(&e.static_ss));
       e.have_static = true;
     }
     const StaticScratch& ss = e.static_ss;
-    DevList& r = e.list(dp.list12);
+    DevList& r = e.wlist(dp.list12);
     if (!update) {
       CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
     }
+    // every packed panel, those of frozen operands included, is made in the
+    // fixed array (the descriptors are moved there); the split panels of
+    // frozen operands stay in the plan
     if (dp.njobs) {
       launch_rebase_jobs(dp.d_jobs, ss.jobs, dp.njobs, dp.scratch, dp.scratch_len, ss.panels,
                          e.stream);
       launch_pack(ss.jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
       e.launches += 2;
     }
+    if (dp.njobs_c) {
+      launch_rebase_jobs(dp.d_jobs_c, ss.jobs + dp.njobs, dp.njobs_c, dp.scratch,
+                         dp.scratch_len, ss.panels, e.stream);
+      launch_pack(ss.jobs + dp.njobs, dp.njobs_c, dp.pack_gx_c, dp.pack_gy_c, e.stream);
+      e.launches += 2;
+    }
+    const bool remake = e.need_const(dp);
     int64_t first = 0;
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
@@ -1265,11 +1402,17 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       first += dp.ndesc_g[kind];
       launch_rebase_descs(dp.d_desc[kind], descs, dp.ndesc_g[kind], dp.scratch, dp.scratch_len,
                           ss.panels, e.stream);
+      if (kind == kGemmTc && remake && dp.nsplit_c) {  // persistent panels, out of date
+        launch_split_tc(descs, dp.d_split_c, dp.nsplit_c, dp.split_chunks_c, dp.d_gather,
+                        e.stream);
+        ++e.launches;
+      }
       if (kind == kGemmTc && dp.nsplit) {  // panels in the engine's existing workspace
         launch_split_tc(descs, dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather, e.stream);
         ++e.launches;
       }
-      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err, e.stream);
+      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err,
+                  e.wait_limit, e.stream);
       e.launches += 2;
     }
     if (dp.plan.use_tr && dp.nflip) {
@@ -1277,6 +1420,13 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       ++e.launches;
     }
     CUDA_OK(cudaGetLastError());
+    if (remake) {
+      bool all_frozen = true;
+      for (int l : dp.const_lists) all_frozen = all_frozen && e.list(l).frozen;
+      if (all_frozen) dp.const_stale = false;
+    } else if (e.capturing) {
+      for (int l : dp.const_lists) e.capture_deps.push_back({l, e.list(l).epoch});
+    }
     for (int k = 0; k < 8; ++k) e.stats[k] += dp.plan.stats[k];
   });
 }
@@ -1321,8 +1471,8 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     GCCU_REQUIRE(!e.host_only, "gccu_contract needs a device");
     GCCU_REQUIRE(bc, "null contraction descriptor");
     GCCU_REQUIRE(!(e.capturing && type_xret != 0), "type_xret must be 0 inside a graph capture");
+    DevList& r = e.wlist(bc->list_res);
     DevPlan& dp = e.plan_for(bc, use_tr != 0);
-    DevList& r = e.list(dp.list12);
     if (!update) {
       CUDA_OK(cudaMemsetAsync(r.d + dp.res_off, 0, dp.res_len * sizeof(double), e.stream));
     }
@@ -1333,6 +1483,7 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
       ev1 = e.get_event();
       CUDA_OK(cudaEventRecord(ev0, e.stream));
     }
+    e.run_const(dp);  // cached panels of frozen operands, only when out of date
     if (dp.njobs) {
       launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
       ++e.launches;
@@ -1350,7 +1501,7 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
       launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err,
-                  e.stream);
+                  e.wait_limit, e.stream);
       ++e.launches;
     }
     if (timed) {
@@ -1380,7 +1531,7 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
 int gccu_put_vec(int64_t list_id, int64_t offset, const void* src, int64_t n) {
   return guarded([&] {
     Engine& e = eng();
-    DevList& dl = e.list(list_id);
+    DevList& dl = e.wlist(list_id);
     GCCU_REQUIRE(offset >= 0 && n >= 0 && offset + n <= dl.L.len, "put_vec out of range");
     CUDA_OK(cudaMemcpyAsync(dl.d + offset, src, n * sizeof(double), cudaMemcpyDefault, e.stream));
     CUDA_OK(cudaStreamSynchronize(e.stream));
@@ -1401,7 +1552,7 @@ int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_ou
                    int64_t iblk_out, int64_t reset, int64_t type, double* xnorm2) {
   return guarded([&] {
     Engine& e = eng();
-    DevList &a = e.list(list_in), &b = e.list(list_out);
+    DevList &a = e.list(list_in), &b = e.wlist(list_out);
     GCCU_REQUIRE(iblk_in >= 1 && iblk_in <= (int64_t)a.L.blk.size(), "invalid input class");
     GCCU_REQUIRE(iblk_out >= 1 && iblk_out <= (int64_t)b.L.blk.size(), "invalid output class");
     const LayoutBlock &Bi = a.L.blk[iblk_in - 1], &Bo = b.L.blk[iblk_out - 1];
@@ -1427,7 +1578,7 @@ int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_ou
 int gccu_scale_list(int64_t list_id, double fac) {
   return guarded([&] {
     Engine& e = eng();
-    DevList& l = e.list(list_id);
+    DevList& l = e.wlist(list_id);
     launch_scale(l.d, fac, l.L.len, e.stream);
     ++e.launches;
     CUDA_OK(cudaGetLastError());
@@ -1449,7 +1600,7 @@ int gccu_dot_lists(int64_t list_a, int64_t list_b, double* dot) {
 int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac) {
   return guarded([&] {
     Engine& e = eng();
-    DevList& l = e.list(list_id);
+    DevList& l = e.wlist(list_id);
     GCCU_REQUIRE(iblk >= 1 && iblk <= (int64_t)l.L.blk.size(), "invalid occupation class");
     int64_t maxlen = 0;
     std::vector<FlipDesc> v = e.flip_descs(l.L, (int)iblk, relfac, maxlen);
@@ -1465,7 +1616,7 @@ int gccu_precondition(int64_t list_out, int64_t list_in, int64_t list_diag, doub
                       double shift) {
   return guarded([&] {
     Engine& e = eng();
-    DevList &o = e.list(list_out), &i = e.list(list_in), &d = e.list(list_diag);
+    DevList &o = e.wlist(list_out), &i = e.list(list_in), &d = e.list(list_diag);
     GCCU_REQUIRE(o.L.len == i.L.len && i.L.len == d.L.len, "diavc: lists differ in length");
     launch_diavc(o.d, i.d, d.d, fac, shift, o.L.len, e.stream);
     ++e.launches;
@@ -1480,6 +1631,7 @@ int gccu_graph_begin(void) {
     CUDA_OK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
     e.capturing = true;
     e.capture_start = e.launches;
+    e.capture_deps.clear();
   });
 }
 
@@ -1495,6 +1647,7 @@ int gccu_graph_end(int64_t* graph_id) {
     cudaGraphDestroy(g);
     e.graphs.push_back(ex);
     e.graph_kernels.push_back(e.launches - e.capture_start);
+    e.graph_deps.push_back(e.capture_deps);
     e.launches = e.capture_start;
     *graph_id = (int64_t)e.graphs.size();
   });
@@ -1504,6 +1657,10 @@ int gccu_graph_launch(int64_t graph_id) {
   return guarded([&] {
     Engine& e = eng();
     GCCU_REQUIRE(graph_id >= 1 && graph_id <= (int64_t)e.graphs.size(), "invalid graph id");
+    for (auto& dep : e.graph_deps[graph_id - 1])
+      GCCU_REQUIRE(e.list(dep.first).frozen && e.list(dep.first).epoch == dep.second,
+                   "the graph reads panels cached from a list that has been unfrozen since it "
+                   "was captured: capture it again");
     CUDA_OK(cudaGraphLaunch(e.graphs[graph_id - 1], e.stream));
     e.launches += e.graph_kernels[graph_id - 1];
   });
@@ -1514,6 +1671,203 @@ int gccu_sync(void) {
     Engine& e = eng();
     CUDA_OK(cudaStreamSynchronize(e.stream));
     if (!e.host_only) e.check_err();
+  });
+}
+
+int gccu_freeze_list(int64_t list_id, int64_t frozen) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.capturing, "a list cannot be frozen or unfrozen during a graph capture");
+    DevList& l = e.list(list_id);
+    if (frozen) {
+      l.frozen = true;
+    } else if (l.frozen) {
+      l.frozen = false;
+      ++l.epoch;
+      for (auto& kv : e.plans)
+        for (int c : kv.second->const_lists)
+          if (c == (int)list_id) kv.second->const_stale = true;
+    }
+  });
+}
+
+int gccu_lp_set_weights(const double* w, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "the learned preconditioner needs a device");
+    GCCU_REQUIRE(w && n == kLpWeights, "learned preconditioner: wrong number of weights");
+    e.lp_alloc_weights();
+    CUDA_OK(cudaMemcpyAsync(e.lp_w, w, n * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    CUDA_OK(cudaMemsetAsync(e.lp_m, 0, n * sizeof(double), e.stream));
+    CUDA_OK(cudaMemsetAsync(e.lp_v, 0, n * sizeof(double), e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    e.lp_t = 0;
+    e.lp_have_w = true;
+  });
+}
+
+int gccu_lp_get_weights(double* w, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.lp_have_w, "learned preconditioner: no weights loaded");
+    GCCU_REQUIRE(w && n == kLpWeights, "learned preconditioner: wrong number of weights");
+    CUDA_OK(cudaMemcpyAsync(w, e.lp_w, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+  });
+}
+
+int gccu_lp_precondition(int64_t list_out, int64_t list_in, int64_t list_diag,
+                         int64_t list_prev, double fac, double shift) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.lp_have_w, "learned preconditioner: no weights loaded");
+    DevList &o = e.wlist(list_out), &i = e.list(list_in), &d = e.list(list_diag);
+    const double* prev = nullptr;
+    if (list_prev) {
+      DevList& p = e.list(list_prev);
+      GCCU_REQUIRE(p.L.len == o.L.len, "learned preconditioner: lists differ in length");
+      GCCU_REQUIRE(p.d != o.d, "learned preconditioner: previous step and output must differ");
+      prev = p.d;
+    }
+    GCCU_REQUIRE(o.L.len == i.L.len && i.L.len == d.L.len,
+                 "learned preconditioner: lists differ in length");
+    CUDA_OK(cudaMemsetAsync(e.d_red + 2, 0, 2 * sizeof(double), e.stream));
+    launch_lp_sums(i.d, d.d, prev, fac, shift, o.L.len, e.d_red + 2, e.stream);
+    launch_lp_apply(o.d, i.d, d.d, prev, fac, shift, o.L.len, e.d_red + 2, e.lp_w, e.stream);
+    e.launches += 2;
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_lp_rows(int64_t list_in, int64_t list_diag, int64_t list_prev, int64_t list_amp,
+                 double fac, double shift, const int64_t* idx, int64_t n, double* rows) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "the learned preconditioner needs a device");
+    GCCU_REQUIRE(!e.capturing, "learned preconditioner: sampling reads back to the host");
+    DevList &i = e.list(list_in), &d = e.list(list_diag);
+    GCCU_REQUIRE(i.L.len == d.L.len, "learned preconditioner: lists differ in length");
+    const double* prev = list_prev ? e.list(list_prev).d : nullptr;
+    const double* amp = list_amp ? e.list(list_amp).d : nullptr;
+    if (list_prev) GCCU_REQUIRE(e.list(list_prev).L.len == i.L.len, "lists differ in length");
+    if (list_amp) GCCU_REQUIRE(e.list(list_amp).L.len == i.L.len, "lists differ in length");
+    GCCU_REQUIRE(n >= 0 && (n == 0 || (idx && rows)), "null argument");
+    for (int64_t r = 0; r < n; ++r)
+      GCCU_REQUIRE(idx[r] >= 0 && idx[r] < i.L.len, "learned preconditioner: index out of range");
+    if (n == 0) return;
+    if (n > e.lp_idx_cap) {
+      if (e.lp_idx) e.release(e.lp_idx, (size_t)e.lp_idx_cap * sizeof(int64_t));
+      if (e.lp_out) e.release(e.lp_out, (size_t)e.lp_idx_cap * kLpRowLen * sizeof(double));
+      e.lp_idx = nullptr;
+      e.lp_out = nullptr;
+      e.lp_idx = (int64_t*)e.alloc((size_t)n * sizeof(int64_t));
+      e.lp_out = (double*)e.alloc((size_t)n * kLpRowLen * sizeof(double));
+      e.lp_idx_cap = n;
+    }
+    CUDA_OK(cudaMemcpyAsync(e.lp_idx, idx, n * sizeof(int64_t), cudaMemcpyHostToDevice, e.stream));
+    CUDA_OK(cudaMemsetAsync(e.d_red + 2, 0, 2 * sizeof(double), e.stream));
+    launch_lp_sums(i.d, d.d, prev, fac, shift, i.L.len, e.d_red + 2, e.stream);
+    launch_lp_rows(i.d, d.d, prev, amp, fac, shift, i.L.len, e.lp_idx, n, e.d_red + 2, e.lp_out,
+                   e.stream);
+    e.launches += 2;
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemcpyAsync(rows, e.lp_out, n * kLpRowLen * sizeof(double),
+                            cudaMemcpyDeviceToHost, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+  });
+}
+
+int gccu_lp_load_samples(const double* rows, const double* target, int64_t n) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "the learned preconditioner needs a device");
+    GCCU_REQUIRE(n >= 1 && rows && target, "learned preconditioner: empty sample set");
+    if (n > e.lp_cap) {
+      if (e.lp_rows) e.release(e.lp_rows, (size_t)e.lp_cap * kLpRowLen * sizeof(double));
+      if (e.lp_tgt) e.release(e.lp_tgt, (size_t)e.lp_cap * sizeof(double));
+      e.lp_rows = nullptr;
+      e.lp_tgt = nullptr;
+      e.lp_rows = (double*)e.alloc((size_t)n * kLpRowLen * sizeof(double));
+      e.lp_tgt = (double*)e.alloc((size_t)n * sizeof(double));
+      e.lp_cap = n;
+    }
+    CUDA_OK(cudaMemcpyAsync(e.lp_rows, rows, n * kLpRowLen * sizeof(double),
+                            cudaMemcpyHostToDevice, e.stream));
+    CUDA_OK(cudaMemcpyAsync(e.lp_tgt, target, n * sizeof(double), cudaMemcpyHostToDevice,
+                            e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    e.lp_nrows = n;
+  });
+}
+
+int gccu_lp_gradient(double* grad, double* loss) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.lp_have_w && e.lp_nrows > 0, "learned preconditioner: weights or samples missing");
+    GCCU_REQUIRE(grad && loss, "null argument");
+    double* part = e.lp_partials(lp_grad_blocks(e.lp_nrows));
+    launch_lp_grad(e.lp_rows, e.lp_tgt, e.lp_nrows, 0, 0, 0, e.lp_w, part, e.lp_grad, e.stream);
+    e.launches += 2;
+    CUDA_OK(cudaGetLastError());
+    std::vector<double> h(kLpWeights + 1);
+    CUDA_OK(cudaMemcpyAsync(h.data(), e.lp_grad, h.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    std::copy(h.begin(), h.begin() + kLpWeights, grad);
+    *loss = h[kLpWeights];
+  });
+}
+
+int gccu_lp_train(int64_t steps, int64_t batch, double lr, int64_t seed, double* loss) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.lp_have_w && e.lp_nrows > 0, "learned preconditioner: weights or samples missing");
+    GCCU_REQUIRE(steps >= 1 && batch >= 1 && lr > 0, "learned preconditioner: bad training parameters");
+    GCCU_REQUIRE(!e.capturing, "learned preconditioner: training is not captured");
+    double* part = e.lp_partials(lp_grad_blocks(batch));
+    for (int64_t k = 0; k < steps; ++k) {
+      launch_lp_grad(e.lp_rows, e.lp_tgt, e.lp_nrows, batch, (uint64_t)seed, (uint64_t)k, e.lp_w,
+                     part, e.lp_grad, e.stream);
+      launch_lp_adam(e.lp_w, e.lp_m, e.lp_v, e.lp_grad, lr, ++e.lp_t, e.stream);
+      e.launches += 3;
+    }
+    CUDA_OK(cudaGetLastError());
+    double l = 0;
+    CUDA_OK(cudaMemcpyAsync(&l, e.lp_grad + kLpWeights, sizeof(double), cudaMemcpyDeviceToHost,
+                            e.stream));
+    CUDA_OK(cudaStreamSynchronize(e.stream));
+    if (loss) *loss = l;
+  });
+}
+
+int gccu_set_wait_limit(int64_t polls) {
+  return guarded([&] {
+    eng().wait_limit = polls < 0 ? kTcWaitLimitDefault : polls;
+  });
+}
+
+int gccu_mem_info(int64_t* used_bytes, int64_t* cap_bytes) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(used_bytes && cap_bytes, "null argument");
+    *used_bytes = e.mem_used;
+    *cap_bytes = e.memmax;
+  });
+}
+
+int gccu_device_info(int64_t* info4) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_device_info needs a device");
+    GCCU_REQUIRE(info4, "null argument");
+    cudaDeviceProp prop;
+    CUDA_OK(cudaGetDeviceProperties(&prop, e.device));
+    cudaFuncAttributes attr;
+    CUDA_OK(tc_kernel_attributes(&attr));
+    info4[0] = 10 * prop.major + prop.minor;
+    info4[1] = prop.multiProcessorCount;
+    info4[2] = attr.binaryVersion;
+    info4[3] = attr.ptxVersion;
   });
 }
 

@@ -368,10 +368,10 @@ void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cud
 }
 
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
-                 double alpha, int* err, cudaStream_t s) {
+                 double alpha, int* err, int64_t wait_limit, cudaStream_t s) {
   if (ntiles == 0) return;
   if (kind == kGemmTc) {
-    launch_gemm_tc(descs, tiles, ntiles, alpha, err, s);
+    launch_gemm_tc(descs, tiles, ntiles, alpha, err, wait_limit, s);
     return;
   }
   if (kind == kGemmRegular)

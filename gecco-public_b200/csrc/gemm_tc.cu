@@ -26,9 +26,10 @@
 // and scatter it with the map signs while the MMAs of the next tile run in
 // the other accumulator.
 //
-// Every wait on an mbarrier is bounded; on time-out the kernel records the
-// failure in *err, stops issuing work, waits (bounded) for the copies and
-// MMAs it has issued, frees its TMEM and returns.
+// Every wait on an mbarrier is bounded (the pipeline waits by a runtime
+// limit, gccu_set_wait_limit); on time-out the kernel records the failure in
+// *err, stops issuing work, waits (bounded by the fixed default limit) for
+// the copies and MMAs it has issued, frees its TMEM and returns.
 #include <cstdio>
 
 #include "index.cuh"
@@ -50,7 +51,10 @@ constexpr int NST = 4;         // pipeline stages
 // epilogue (warp w reads TMEM lanes 32(w%4).., two warps per lane quarter)
 constexpr int TNT = 384;
 constexpr int kEpiWarp0 = 4, kEpiWarps = 8, kEpiThreads = 32 * kEpiWarps;
-constexpr long kWaitLimit = 1L << 22;
+// polls of one pipeline wait before it gives up: the default of the
+// runtime limit (gccu_set_wait_limit) and the fixed limit of the clean-up
+// waits at the end, which only wait for work already issued
+constexpr long kWaitLimit = kTcWaitLimitDefault;
 constexpr int kTcols = 32;  // columns per pass of the column-major epilogue
 
 struct __align__(1024) TcSmem {
@@ -133,11 +137,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// bounded wait for the completion of phase `parity`; false on time-out or
-// when another role of the CTA has failed
+// bounded wait for the completion of phase `parity`: at most `limit` polls;
+// false on time-out or when another role of the CTA has failed
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
-                                          const volatile int* failed) {
-  for (long it = 0; it < kWaitLimit; ++it) {
+                                          const volatile int* failed, long limit = kWaitLimit) {
+  for (long it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -309,7 +313,9 @@ __global__ void __launch_bounds__(kSplitThreads, 6)
   __syncthreads();
   // a 128-row chunk may span two row bands when TR is not a multiple of 128
   const int64_t padded = (R + TR - 1) / TR * TR;
-  float* __restrict__ base = g_tc_ws + (row_op ? d.pa : d.pb) + (c % nsl) * 2 * TR * SK;
+  float* const panel = row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa)
+                              : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb);
+  float* __restrict__ base = panel + (c % nsl) * 2 * TR * SK;
 #pragma unroll
   for (int i = 0; i < 2 * 8 * 128 / kSplitThreads; ++i) {
     const int u = tid + kSplitThreads * i;
@@ -385,7 +391,7 @@ __device__ __forceinline__ void scatter(const TcSmem& S, const int (&row)[NB],
 // ---- GEMM ------------------------------------------------------------------
 __global__ void __launch_bounds__(TNT, 1)
     k_gemm_tc(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
-              int64_t ntiles, double alpha, int* err) {
+              int64_t ntiles, double alpha, int* err, long wait_limit) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -429,12 +435,15 @@ __global__ void __launch_bounds__(TNT, 1)
         const int64_t nk = (td.k1 - td.k0 + BK - 1) / BK;
         const int bn = dg->tn;
         const uint32_t stage_bytes = 2u * (uint32_t)(TBM + bn) * BK * sizeof(float);
-        const float* pa = g_tc_ws + dg->pa + (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
-        const float* pb = g_tc_ws + dg->pb + (int64_t)(td.n0 / bn) * nsl * 2 * bn * SK;
+        const float* pa = (dg->pa_ptr ? dg->pa_ptr : g_tc_ws + dg->pa) +
+                          (int64_t)(td.m0 / TBM) * nsl * 2 * TBM * SK;
+        const float* pb = (dg->pb_ptr ? dg->pb_ptr : g_tc_ws + dg->pb) +
+                          (int64_t)(td.n0 / bn) * nsl * 2 * bn * SK;
         for (int64_t t = 0; t < nk; ++t, ++it) {
           const int s = (int)(it % NST);
           if (it >= NST &&
-              !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((it / NST - 1) & 1), failed)) {
+              !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((it / NST - 1) & 1), failed,
+                         wait_limit)) {
             *failed = 1;
             break;
           }
@@ -463,7 +472,8 @@ __global__ void __launch_bounds__(TNT, 1)
         const uint32_t kIdesc = idesc_tf32(TBM, bn), kB = (uint32_t)bn * 16;
         const int acc = (int)(lt & 1);
         if (lt >= 2 &&  // the epilogue has read this accumulator two tiles ago
-            !mbar_wait(smem_u32(&S.acce[acc]), (uint32_t)((lt / 2 - 1) & 1), failed)) {
+            !mbar_wait(smem_u32(&S.acce[acc]), (uint32_t)((lt / 2 - 1) & 1), failed,
+                       wait_limit)) {
           *failed = 1;
           break;
         }
@@ -471,7 +481,7 @@ __global__ void __launch_bounds__(TNT, 1)
         const uint32_t dacc = tmem + (uint32_t)(acc * TBN);
         for (int64_t t = 0; t < nk; ++t, ++it) {
           const int s = (int)(it % NST);
-          if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((it / NST) & 1), failed)) {
+          if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((it / NST) & 1), failed, wait_limit)) {
             *failed = 1;
             break;
           }
@@ -524,7 +534,8 @@ __global__ void __launch_bounds__(TNT, 1)
           if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
         }
       const int acc = (int)(lt & 1);
-      if (!mbar_wait(smem_u32(&S.accf[acc]), (uint32_t)((lt / 2) & 1), failed)) *failed = 1;
+      if (!mbar_wait(smem_u32(&S.accf[acc]), (uint32_t)((lt / 2) & 1), failed, wait_limit))
+        *failed = 1;
       epi_sync();
       if (*failed) break;  // the same in every epilogue thread after the barrier
       tc_fence_after();
@@ -626,7 +637,7 @@ void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
 }
 
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
-                    int* err, cudaStream_t s) {
+                    int* err, int64_t wait_limit, cudaStream_t s) {
   if (ntiles == 0) return;
   const size_t smem = sizeof(TcSmem);
   static bool configured = false;
@@ -642,7 +653,12 @@ void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles
     if (nsm <= 0) nsm = 148;
   }
   const int64_t grid = ntiles < nsm ? ntiles : nsm;
-  k_gemm_tc<<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err);
+  k_gemm_tc<<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err,
+                                                (long)wait_limit);
+}
+
+cudaError_t tc_kernel_attributes(cudaFuncAttributes* attr) {
+  return cudaFuncGetAttributes(attr, k_gemm_tc);
 }
 
 }  // namespace gccu

@@ -50,9 +50,12 @@ void pack_geometry(const PackJob& j, int64_t& gx, int64_t& gy);
 void launch_pack(const PackJob* jobs, int64_t njobs, int64_t gx, int64_t gy, cudaStream_t s);
 // split-TF32 tensor-core GEMM (tcgen05) over 128 x kGemmTcN tiles, reading
 // the split panels of its items from the workspace; *err is set if a
-// pipeline wait timed out
+// pipeline wait (at most wait_limit mbarrier polls) timed out
+constexpr int64_t kTcWaitLimitDefault = int64_t(1) << 22;
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
-                    int* err, cudaStream_t s);
+                    int* err, int64_t wait_limit, cudaStream_t s);
+// attributes of the tensor-core GEMM kernel (target architecture of the build)
+cudaError_t tc_kernel_attributes(cudaFuncAttributes* attr);
 // floats of the split panels of one tensor-core item (both operands)
 constexpr int64_t kTcSlice = 32;  // contraction indices per panel slice
 inline int64_t tc_panel_floats(int64_t rows, int tile_rows, int64_t K) {
@@ -81,10 +84,10 @@ void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
 // device address of the split-TF32 workspace used by the two kernels above
 // (a device-side variable, so captured graphs follow a reallocation)
 cudaError_t set_tc_workspace(float* ws);
-// grouped block-contraction GEMM over the tiles of one tile shape (err: see
-// launch_gemm_tc, used by kind kGemmTc)
+// grouped block-contraction GEMM over the tiles of one tile shape (err,
+// wait_limit: see launch_gemm_tc, used by kind kGemmTc)
 void launch_gemm(int kind, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
-                 double alpha, int* err, cudaStream_t s);
+                 double alpha, int* err, int64_t wait_limit, cudaStream_t s);
 
 // reorder of a joined operator class (nitems <= 65535 distribution cases,
 // maxlen = largest N0*NK); reo += alpha * signs * ori
@@ -117,6 +120,34 @@ struct FlipDesc {
 };
 void launch_sym_ab(const FlipDesc* d, int64_t n, double* x, double prefac, int64_t maxlen,
                    cudaStream_t s);
+
+// Learned correction of the diagonal step (learned.cu): a perceptron with
+// kLpInputs inputs, two tanh layers of kLpHidden and one output; weights
+// W1[hidden][inputs], b1, W2[hidden][hidden], b2, W3[hidden], b3 (FP64)
+constexpr int kLpInputs = 3, kLpHidden = 32;
+constexpr int kLpWeights = kLpHidden * kLpInputs + kLpHidden + kLpHidden * kLpHidden +
+                           kLpHidden + kLpHidden + 1;
+constexpr int kLpRowLen = 5;  // sample row: 3 inputs, plain step, amplitude
+// acc[0] += sum (fac*in/d)^2, acc[1] += sum prev^2 (acc zeroed by the caller)
+void launch_lp_sums(const double* in, const double* diag, const double* prev, double fac,
+                    double shift, int64_t n, double* acc, cudaStream_t s);
+// out = fac*in/d * (1 + tanh(mlp(inputs))), acc from launch_lp_sums
+void launch_lp_apply(double* out, const double* in, const double* diag, const double* prev,
+                     double fac, double shift, int64_t n, const double* acc,
+                     const double* weights, cudaStream_t s);
+// sample rows of the elements idx[0..nrows) (indices checked by the caller)
+void launch_lp_rows(const double* in, const double* diag, const double* prev, const double* amp,
+                    double fac, double shift, int64_t n, const int64_t* idx, int64_t nrows,
+                    const double* acc, double* rows, cudaStream_t s);
+// blocks (= partial-sum rows of kLpWeights + 1) of one gradient launch
+int64_t lp_grad_blocks(int64_t count);
+// grad[0..kLpWeights) = dL/dw, grad[kLpWeights] = L over all rows (batch 0)
+// or over `batch` rows drawn from (seed, step); part: lp_grad_blocks rows
+void launch_lp_grad(const double* rows, const double* target, int64_t nrows, int64_t batch,
+                    uint64_t seed, uint64_t step, const double* weights, double* part,
+                    double* grad, cudaStream_t s);
+void launch_lp_adam(double* w, double* m, double* v, const double* grad, double lr, int64_t t,
+                    cudaStream_t s);
 
 // Fixed scratch of the allocation-free contraction path (noalloc.cu): one
 // file-scope device array holding 64 MiB of operand panels and room for the

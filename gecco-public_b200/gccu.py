@@ -20,6 +20,7 @@ P64 = ctypes.POINTER(ctypes.c_int64)
 PD = ctypes.POINTER(ctypes.c_double)
 
 H, P, V, X = 0, 1, 2, 3  # hpvx types
+LP_NWEIGHTS = 1217  # weights of the learned preconditioner (GCCU_LP_NWEIGHTS)
 
 
 class BcDesc(ctypes.Structure):
@@ -56,6 +57,16 @@ _SIGS = {
     "gccu_reorder_info": [ctypes.POINTER(ReoDesc), P64, P64],
     "gccu_trace": [I64, I64, I64, I64, P64, ctypes.c_double, I64, I64, PD],
     "gccu_set_precision": [I64],
+    "gccu_set_wait_limit": [I64],
+    "gccu_lp_set_weights": [PD, I64],
+    "gccu_lp_get_weights": [PD, I64],
+    "gccu_lp_precondition": [I64, I64, I64, I64, ctypes.c_double, ctypes.c_double],
+    "gccu_lp_rows": [I64, I64, I64, I64, ctypes.c_double, ctypes.c_double, P64, I64, PD],
+    "gccu_lp_load_samples": [PD, PD, I64],
+    "gccu_lp_gradient": [PD, PD],
+    "gccu_lp_train": [I64, I64, ctypes.c_double, I64, PD],
+    "gccu_mem_info": [P64, P64],
+    "gccu_device_info": [P64],
     "gccu_trace_info": [I64, I64, I64, I64, P64, P64, P64],
     "gccu_register_list": [I64, I64, I64, I64, P64, P64],
     "gccu_list_block": [I64, I64, P64, P64],
@@ -64,6 +75,7 @@ _SIGS = {
     "gccu_download_list": [I64, PD, I64],
     "gccu_zero_list": [I64],
     "gccu_list_device_ptr": [I64, ctypes.POINTER(ctypes.c_void_p)],
+    "gccu_freeze_list": [I64, I64],
     "gccu_contract": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64, I64, PD],
     "gccu_plan_info": [ctypes.POINTER(BcDesc), I64, P64, PD],
     "gccu_plan_items": [ctypes.POINTER(BcDesc), I64, P64, I64, P64],
@@ -250,6 +262,61 @@ class Engine:
         """0 = FP64 (default), 1 = split TF32 on the tcgen05 tensor cores"""
         _call("gccu_set_precision", int(mode))
 
+    # ---- learned correction of the diagonal step
+    def lp_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        _call("gccu_lp_set_weights", _pd(w), w.size)
+
+    def lp_get_weights(self):
+        w = np.zeros(LP_NWEIGHTS)
+        _call("gccu_lp_get_weights", _pd(w), w.size)
+        return w
+
+    def lp_precondition(self, out, inp, diag, prev=0, fac=1.0, shift=0.0):
+        _call("gccu_lp_precondition", out, inp, diag, prev, fac, shift)
+
+    def lp_rows(self, inp, diag, prev, amp, idx, fac=1.0, shift=0.0):
+        """(x0, x1, x2, plain step, amplitude) of the elements idx"""
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        rows = np.zeros((max(idx.size, 1), 5))
+        _call("gccu_lp_rows", inp, diag, prev, amp, fac, shift, _p64(idx), idx.size, _pd(rows))
+        return rows[: idx.size]
+
+    def lp_load_samples(self, rows, target):
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        assert rows.shape == (target.size, 5)
+        _call("gccu_lp_load_samples", _pd(rows), _pd(target), target.size)
+
+    def lp_gradient(self):
+        g = np.zeros(LP_NWEIGHTS)
+        l = np.zeros(1)
+        _call("gccu_lp_gradient", _pd(g), _pd(l))
+        return g, float(l[0])
+
+    def lp_train(self, steps, batch, lr, seed=0):
+        l = np.zeros(1)
+        _call("gccu_lp_train", steps, batch, lr, seed, _pd(l))
+        return float(l[0])
+
+    def set_wait_limit(self, polls=-1):
+        """mbarrier polls per tensor-core pipeline wait (negative: default)"""
+        _call("gccu_set_wait_limit", int(polls))
+
+    def mem_info(self):
+        """(bytes of device memory the engine holds, its cap or 0)"""
+        u = np.zeros(1, np.int64)
+        c = np.zeros(1, np.int64)
+        _call("gccu_mem_info", _p64(u), _p64(c))
+        return int(u[0]), int(c[0])
+
+    def device_info(self):
+        """(compute capability, SMs, binary version and PTX version of the
+        tensor-core kernel)"""
+        r = np.zeros(4, np.int64)
+        _call("gccu_device_info", _p64(r))
+        return tuple(int(x) for x in r)
+
     def trace(self, op, res, cnt, fact=1.0, update=True, xret=0):
         """partial trace res(IC,IA) += fact * sum_J op(IC*J, IA*J); op/res =
         (list, iblk), cnt = occupation of J (creators = annihilators)"""
@@ -296,6 +363,11 @@ class Engine:
 
     def zero(self, lst):
         _call("gccu_zero_list", lst)
+
+    def freeze(self, lst, frozen=True):
+        """declare a list constant (contractions then cache the panels they
+        derive from it) or release it"""
+        _call("gccu_freeze_list", lst, int(frozen))
 
     def device_ptr(self, lst):
         p = ctypes.c_void_p()

@@ -3,7 +3,7 @@
  *
  * Drop-in boundary: the Fortran host (formula interpreter frm_sched2, solvers)
  * stays unchanged and calls these entry points through ISO_C_BINDING from a
- * thin shim.  Conventions follow the reference:
+ * thin bind(C) shim module.  Conventions follow the reference:
  *   - every integer is int64_t (the reference is built with 64-bit default
  *     INTEGER, config/x86_64-linux.conf:39,51), reals are double;
  *   - irreps, occupation-class indices and Ms indices are 1-based;
@@ -31,6 +31,15 @@ extern "C" {
  * layouts and contraction plans can be queried, nothing is executed. */
 int gccu_init(int64_t device, int64_t memmax_bytes);
 int gccu_finalize(void);
+/* device memory the engine holds (ME lists, maps, plans, workspaces) and its
+ * cap (0: none), in bytes; replaces mem_free_words (memman/mem_free_words.f:2-9),
+ * free = cap - used when a cap is set */
+int gccu_mem_info(int64_t* used_bytes, int64_t* cap_bytes);
+/* the device the engine runs on and the build of its kernels: info4 =
+ * (compute capability 10*major+minor, SM count, binary and PTX version of
+ * the tensor-core contraction kernel, 100 for sm_100a).  No counterpart in
+ * the reference (a host query, like the banner of gecco/gecco.f). */
+int gccu_device_info(int64_t* info4);
 /* copies the last error message (NUL-terminated, truncated to len) */
 int gccu_last_error(char* buf, int64_t len);
 
@@ -94,8 +103,19 @@ int gccu_zero_list(int64_t list_id);
  * host (pageable or pinned) or device pointers */
 int gccu_put_vec(int64_t list_id, int64_t offset, const void* src, int64_t n);
 int gccu_get_vec(int64_t list_id, int64_t offset, void* dst, int64_t n);
-/* raw device pointer of the list data (for callers that own device memory) */
+/* raw device pointer of the list data (for callers that own device memory;
+ * a frozen list must not be written through it) */
 int gccu_list_device_ptr(int64_t list_id, void** dptr);
+/* frozen != 0: the host declares the list's data constant until it is
+ * unfrozen (the Hamiltonian lists during a CC solve, which the reference's
+ * solver only reads, solve/solve_nleq.f).  Contractions planned while an
+ * operand's list is frozen make the panels they derive from it (gathered
+ * FP64 panels of map-addressed operands, split TF32 panels) once and keep
+ * them; every entry point that would write a frozen list fails.  frozen = 0:
+ * the cached panels are remade by the next contraction that reads them, and
+ * CUDA graphs captured while they were valid can no longer be launched.  No
+ * counterpart in the reference. */
+int gccu_freeze_list(int64_t list_id, int64_t frozen);
 
 /* ---- [CONTR] ------------------------------------------------------------------
  * replaces: contr_op1op2 case(2,3) (contract/contr_op1op2.f:112-173) ->
@@ -146,9 +166,11 @@ int gccu_plan_items(const gccu_bc_desc* bc, int64_t use_tr, int64_t* rows8, int6
  * memory owned by the contraction; larger contractions are rejected with an
  * error naming the size they need.  The contraction must have been run once
  * through gccu_contract with the same descriptor and use_tr, because
- * planning allocates; this call allocates nothing.  The first call of an
- * engine looks up the array's device address (set-up, no allocation) and
- * should come before any stream capture.  Every call uses the same array
+ * planning allocates; the plan, including the operand panels planning
+ * allocated for gccu_contract, stays allocated; this call allocates nothing
+ * further.  The first call of an engine looks up the array's device address
+ * (set-up, no allocation) and must come before any stream capture: inside
+ * a capture it is rejected with an error.  Every call uses the same array
  * and leaves its contents behind; calls that overlap in time (from other
  * host threads or on other streams) race on it. */
 int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, int64_t use_tr);
@@ -217,6 +239,37 @@ int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac);
 int gccu_precondition(int64_t list_out, int64_t list_in, int64_t list_diag, double fac,
                       double shift);
 
+/* ---- learned correction of the preconditioner (no counterpart in the
+ * reference, whose step is diavc, baserout/diavc.f:31-35, inside
+ * optc_diis_sbsp_add, solve/optc_diis_sbsp_add.f:125-145) -------------------
+ * A perceptron maps three inputs of every element to a factor m = 1 +
+ * tanh(o) of the plain step s = fac*in/d, d = diag+shift clamped as in diavc:
+ *   out = s * m,  inputs x0 = d/4, x1 = 1/max(|d|, 0.05),
+ *   x2 = clip(u*v, -10, 10), u = s/rms(s), v = prev/rms(prev)
+ * (prev = the previous step, list_prev; 0 = none, then v = 0);
+ * h1 = tanh(W1 x + b1), h2 = tanh(W2 h1 + b2), o = W3.h2 + b3, in FP64.
+ * Weights: GCCU_LP_NWEIGHTS doubles, W1[32][3], b1[32], W2[32][32], b2[32],
+ * W3[32], b3.  Training: sample rows (x0, x1, x2, s, amplitude) of chosen
+ * elements during earlier solves (gccu_lp_rows), targets = converged
+ * amplitude - sampled amplitude, loss L = mean over rows of
+ * (s*(1+tanh(o)) - target)^2, gradients and Adam on the device. */
+#define GCCU_LP_NWEIGHTS 1217
+int gccu_lp_set_weights(const double* w, int64_t n);
+int gccu_lp_get_weights(double* w, int64_t n);
+int gccu_lp_precondition(int64_t list_out, int64_t list_in, int64_t list_diag,
+                         int64_t list_prev, double fac, double shift);
+/* rows[5*r..] = (x0, x1, x2, s, amplitude) of element idx[r] (0-based) of
+ * lists in/diag/prev/amp (prev, amp: 0 = none) */
+int gccu_lp_rows(int64_t list_in, int64_t list_diag, int64_t list_prev, int64_t list_amp,
+                 double fac, double shift, const int64_t* idx, int64_t n, double* rows);
+/* the training set: n rows of 5 (the fifth entry is not read) and targets */
+int gccu_lp_load_samples(const double* rows, const double* target, int64_t n);
+/* dL/dw over the whole training set (grad[GCCU_LP_NWEIGHTS]) and L */
+int gccu_lp_gradient(double* grad, double* loss);
+/* `steps` Adam steps (learning rate lr), each on `batch` rows drawn from the
+ * set by a hash of (seed, step); *loss = the last minibatch's loss */
+int gccu_lp_train(int64_t steps, int64_t batch, double lr, int64_t seed, double* loss);
+
 /* ---- CUDA graphs -------------------------------------------------------------
  * Capture the device work of a sequence of calls (one formula evaluation,
  * contract/frm_sched.f:89-100) and replay it.  Calls inside a capture must not
@@ -238,6 +291,12 @@ int gccu_sync(void);
  * that times out inside a kernel is reported as an error by the next call
  * that synchronises (gccu_sync, norms, downloads). */
 int gccu_set_precision(int64_t mode);
+/* Polls of one pipeline wait of the tensor-core kernel before it gives up
+ * (polls < 0: the default, 4194304); on time-out the kernel stops, waits for
+ * the work it has issued, sets the engine's error flag and returns, and the
+ * next synchronising call reports the error.  No counterpart in the
+ * reference (failure detection of the device pipeline). */
+int gccu_set_wait_limit(int64_t polls);
 
 /* ---- statistics -----------------------------------------------------------
  * dgemm shape statistics in the reference's accounting

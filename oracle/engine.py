@@ -56,6 +56,9 @@ class OracleEngine:
     def zero(self, lid):
         self.data[lid][:] = 0.0
 
+    def freeze(self, lid, frozen=True):
+        pass  # host arrays: nothing is derived from a list
+
     def contract(self, op1, op2, res, ex1, ex2, cnt, fact=1.0, update=True, use_tr=False,
                  xret=0, desc=None):
         (l1, b1), (l2, b2), (l12, b12) = op1, op2, res

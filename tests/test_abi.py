@@ -28,10 +28,14 @@ def test_library_exports_all_symbols(built):
         assert re.search(r"\bT\s+" + name + r"\b", out), name
 
 
-def test_library_targets_sm100a(built):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", gccu.LIB_PATH],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_build_targets_sm100a():
+    # the engine is compiled for sm_100a only (the tcgen05 kernels need the
+    # architecture-specific target); the device-side check is in
+    # tests/test_gpu_device.py
+    text = open(os.path.join(ROOT, "gecco-public_b200", "Makefile")).read()
+    arch = re.search(r"^ARCH\s*:=\s*(.*)$", text, re.M).group(1).split()
+    assert arch == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert "$(ARCH)" in re.search(r"^NVFLAGS\s*:=.*(?:\n\s+.*)*", text, re.M).group(0)
 
 
 def test_errors_are_reported(built):

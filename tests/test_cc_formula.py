@@ -73,3 +73,18 @@ def test_ccsd_synthetic_c1(built):
     s.load_hamiltonian()
     eo = s.solve(maxiter=30, conv=1e-9)
     assert abs(ed - eo) < 1e-10
+
+
+def test_ccsd_spin_flip_symmetry_same_iterates(hf_ints):
+    # use_tr (calculate.routes.use_tr, the reference's default): every
+    # contraction computes half of its Ms cases into spin-symmetric lists,
+    # doubled, then symmetrised (sym_ab_blk); the iterates equal those of the
+    # plain evaluation
+    hist = []
+    for use_tr in (False, True):
+        s = cc.CCSolver(OracleEngine(route=3), hf_ints, method="ccsd", use_tr=use_tr)
+        s.load_hamiltonian()
+        s.solve(maxiter=6, conv=1e-14)
+        hist.append(s.history)
+    for (i, ea, ra), (_, eb, rb) in zip(*hist):
+        assert abs(ea - eb) < 1e-12 and abs(ra - rb) < 1e-11 * max(1.0, ra), (i, ea, eb)

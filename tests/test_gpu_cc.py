@@ -95,3 +95,27 @@ def test_device_fill_matches_host_fill(engine):
     assert np.allclose(engine.download(s.lid("V"), s.lists["V"][1]), xv, rtol=0, atol=1e-13)
     d2 = cc.fill_denominators(s.view("DT2"), s.lists["T2"][1], s.lists["T2"][2][0], ints)
     assert np.allclose(engine.download(s.lid("DT2"), s.lists["T2"][1]), d2, atol=1e-13)
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["fp64", "split_tf32"])
+def test_ccsd_spin_flip_symmetry_same_iterates(built, mode):
+    # the engine under use_tr (half of the Ms cases, doubled, sym_ab_blk) gives
+    # the iterates of the plain evaluation, replayed from CUDA graphs, on a
+    # synthetic system whose particle ladder reaches the tensor cores
+    from devfill import TorchIntegrals
+    sp, eps, B = hm.synthetic(6, 30, 60, seed=6030)
+    hist = []
+    for use_tr in (False, True):
+        e = gccu.Engine(0)
+        try:
+            e.set_precision(mode)
+            s = cc.CCSolver(e, hm.FactorizedIntegrals(sp, eps, B), method="ccsd", use_tr=use_tr)
+            s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+            s.solve(maxiter=8, conv=1e-14, use_graph=True)
+            hist.append(s.history)
+        finally:
+            e.close()
+    tol = 1e-10 if mode == 0 else 1e-6
+    for (i, ea, ra), (_, eb, rb) in zip(*hist):
+        assert abs(ea - eb) < tol * max(1.0, abs(ea)), (i, ea, eb)
+        assert abs(ra - rb) < tol * max(1.0, ra), (i, ra, rb)

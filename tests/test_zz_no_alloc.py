@@ -1,6 +1,8 @@
 """gccu_contract_noalloc (operand panels and launch descriptors in the
 library's fixed device array, no allocation) gives the same results as
-gccu_contract, on two calls in a row with different inputs."""
+gccu_contract, on two calls in a row with different inputs, leaves the
+engine's device memory and the device's free memory unchanged, and rejects a
+contraction whose panels do not fit the fixed array."""
 import numpy as np
 import pytest
 
@@ -34,6 +36,8 @@ def _close(got, ref):
 
 @pytest.mark.parametrize("space", list(SPACES))
 def test_noalloc_matches_contract(engine, space):
+    import torch
+
     nsym, norb = SPACES[space]
     engine.register_orbinfo(nsym, norb)
     for i, case in enumerate(contractions_for(space)):
@@ -49,9 +53,30 @@ def test_noalloc_matches_contract(engine, space):
             engine.contract(*args, fact=-0.75, update=update)  # plans on first use
             ref = engine.download(l12, n12)
             engine.upload(l12, x12)
+            engine.sync()
+            used = engine.mem_info()[0]
+            free = torch.cuda.mem_get_info(0)[0]
             engine.contract_noalloc(*args, fact=-0.75, update=update)
             got = engine.download(l12, n12)
             assert _close(got, ref), (case[0], call)
+            assert engine.mem_info()[0] == used, case[0]
+            if i > 0:  # after the first call, which may load the module
+                assert torch.cuda.mem_get_info(0)[0] == free, case[0]
+
+
+def test_noalloc_rejects_panels_beyond_the_fixed_array(engine):
+    # a three-body operator gathered for one contracted hole: 159 MiB of
+    # operand panels, more than the 64 MiB the fixed array holds
+    nsym, norb = 1, [[6], [40], [0], [0]]
+    engine.register_orbinfo(nsym, norb)
+    case = [c for c in contractions_for("c1_small") if c[0] == "t3_fhh"][0]
+    (l1, n1), (l2, n2), (l12, _) = _lists(engine, case)
+    engine.upload(l1, random_list(n1, 3))
+    engine.upload(l2, random_list(n2, 4))
+    args = ((l1, 1), (l2, 1), (l12, 1), case[4], case[5], case[6])
+    engine.contract(*args, update=False)
+    with pytest.raises(gccu.GccuError, match="MiB"):
+        engine.contract_noalloc(*args, update=False)
 
 
 def test_noalloc_needs_a_plan(engine):
