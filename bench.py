@@ -7,16 +7,25 @@ norm read back, DIIS update of the amplitudes.  Default workload: closed-shell
 CCSD, C1, n_occ=24, n_virt=200, n_aux=900 (the metric's headline size);
 --config 0 selects n_occ=8, n_virt=32, n_aux=160.
 
+The line's `value` is the split-TF32 (mixed) iteration, with `precision`
+giving its errors against FP64 from identical amplitudes and `fp64` the
+plain FP64 iteration measured in the same run; `use_tr` times both with the
+spin-flip symmetry the reference uses by default; `convergence` gives the
+time to |dE| < 1 uEh of FP64 and mixed at o24/v200 on a variant of the
+Hamiltonian whose CC iteration converges.
+
 --impl reference times the CPU restatement of the reference path (oracle/,
 route 3: gather, ILP64 OpenBLAS dgemm on all host cores, scatter) on the same
-workload, each step a bounded sample of the block contractions scaled to a
-full iteration.
+workload and metric, each step a bounded sample of the block contractions
+extrapolated to a full iteration (the line says so).
 
-Multi-GPU: replicas only (each rank runs the whole iteration); the value is
-the job's iterations per ... expressed as seconds per iteration of the job.
+Multi-GPU: replicas only (each rank runs its own whole solve; the path is
+not sharded); the value is one replica's seconds per iteration (max over
+ranks), `throughput` the job's iterations per second.
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -31,33 +40,39 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-# the contraction whose k_gemm<128,64> launch stands for the dominant kernel
+# the contraction whose GEMM launch stands for the dominant kernel
 ROOFLINE_CONTRACTION = "r2_ladder"
-PROFILES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles")
 
+# DRAM traffic of the roofline launch per algorithmic byte (operands read
+# once at 8 bytes per element, FP64 or split TF32 hi + lo, plus the result's
+# read-modify-write), measured by ncu on the same launch at the reduced size
+# o12/v100 (profiles/k_gemm_tc_ladder_ccsd_o12v100.md,
+# profiles/k_gemm_ladder_ccsd_o12v100.md: 1.2436 GB and 1.2470 GB against
+# 1.2423 GB of algorithmic bytes); the full-size traffic is this ratio times
+# the full-size algorithmic bytes
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"k_gemm_tc": 1.2436 / 1.2423, "k_gemm": 1.2470 / 1.2423}
 
-def profiled_traffic(cfg, kernel="k_gemm"):
-    """DRAM bytes (read + write) of one roofline launch at this workload, from
-    the ncu summary in profiles/ (a line 'traffic_bytes_per_launch: N'), or
-    None when no capture of this workload is committed"""
-    path = os.path.join(PROFILES, f"{kernel}_ladder_{cfg['tag']}.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
-            return float(line.split(":", 1)[1])
-    return None
-
-
+SIGMA_SPEC = 0.05
 CONFIGS = {
-    0: dict(nocc=8, nvir=32, naux=160, seed=1000, name="CCSD C1 o8 v32 naux160",
-            tag="ccsd_o8v32"),
-    2: dict(nocc=24, nvir=200, naux=900, seed=1002, name="CCSD C1 o24 v200 naux900",
-            tag="ccsd_o24v200"),
+    0: dict(nocc=8, nvir=32, naux=160, seed=1000, sigma=SIGMA_SPEC,
+            name="CCSD C1 o8 v32 naux160", tag="ccsd_o8v32"),
+    2: dict(nocc=24, nvir=200, naux=900, seed=1002, sigma=SIGMA_SPEC,
+            name="CCSD C1 o24 v200 naux900", tag="ccsd_o24v200"),
     # reduced size of the same family, used for kernel captures (a few GB)
-    10: dict(nocc=12, nvir=100, naux=450, seed=1010, name="CCSD C1 o12 v100 naux450",
-             tag="ccsd_o12v100"),
+    10: dict(nocc=12, nvir=100, naux=450, seed=1010, sigma=SIGMA_SPEC,
+             name="CCSD C1 o12 v100 naux450", tag="ccsd_o12v100"),
+    # the o24/v200 shape with B's standard deviation scaled so that the
+    # exchange integrals naux*sigma^2 equal those of o8/v32 naux160 (0.4 Eh);
+    # with sigma = 0.05 at naux = 900 they are 2.25 Eh, above most orbital
+    # gaps, and the CC iteration diverges
+    12: dict(nocc=24, nvir=200, naux=900, seed=1002, sigma=SIGMA_SPEC * math.sqrt(160 / 900),
+             name="CCSD C1 o24 v200 naux900, B std 0.0211", tag="ccsd_o24v200_conv"),
 }
+
+
+def metric_of(cfg):
+    """the metric string of both arms (same workload, same unit)"""
+    return f"s/CC-iteration ({cfg['name']})"
 
 
 def clocks_sampler(stop, out, index):
@@ -115,14 +130,20 @@ def fp64_peak():
 
 def setup_hamiltonian(cfg):
     import hamiltonian as hm
-    sp, eps, B = hm.synthetic(cfg["nocc"], cfg["nvir"], cfg["naux"], seed=cfg["seed"])
-    return sp, eps, B
+    return hm.synthetic(cfg["nocc"], cfg["nvir"], cfg["naux"], seed=cfg["seed"],
+                        sigma=cfg["sigma"])
 
 
-def cpu_baseline_oracle(solver_lists, sp, eps, B, target_s, cores, host_lists):
+def data_desc(cfg):
+    return (f"synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
+            f"B_pq (p<=q, mirrored)~N(0,{cfg['sigma']:.4g}^2))")
+
+
+def cpu_baseline_oracle(sp, eps, B, target_s, cores, host_lists):
     """the oracle (route 3, OpenBLAS on all host cores) on the same workload:
     every formula item, only every stride-th long-operand batch executed;
-    returns seconds per full iteration and the sample description"""
+    returns seconds per full iteration (extrapolated) and the sample
+    description"""
     import binding
     import cc
     from engine import OracleEngine
@@ -145,11 +166,46 @@ def cpu_baseline_oracle(solver_lists, sp, eps, B, target_s, cores, host_lists):
     wall = time.time() - t0
     rep = binding.sampling_report()
     scaled = binding.scaled_time(wall, rep)
+    binding.sampling(1)
     sample = (f"one CCSD iteration of the same workload through the oracle (route 3 gathers, "
               f"OpenBLAS dgemm, scatters) with every {stride}-th of {rep['batches']} "
               f"long-operand batches executed ({rep['done']} run, {wall:.1f} s wall), "
-              f"scaled by batch count")
+              f"extrapolated by batch count")
     return scaled, sample
+
+
+def evaluation_errors(eng, solver):
+    """one formula evaluation in split TF32 and one in FP64 from the same
+    amplitudes (the solver's current T1, T2): errors of the mixed
+    evaluation's energy, residuals and next Jacobi step against FP64"""
+    import torch
+    from devfill import list_tensor
+
+    def lists(names):
+        return {n: list_tensor(eng, solver.lid(n), solver.lists[n][1]).clone()
+                for n in names}
+
+    out = {}
+    for mode in (1, 0):
+        eng.set_precision(mode)
+        solver.evaluate()
+        eng.sync()
+        out[mode] = lists(["E", "R1", "R2"])
+    eng.set_precision(1)
+    d = {n: list_tensor(eng, solver.lid(n), solver.lists[n][1]) for n in ("DT1", "DT2")}
+    res = {"dE": abs(float(out[1]["E"][0] - out[0]["E"][0])), "E_fp64": float(out[0]["E"][0])}
+    num, den = 0.0, 0.0
+    for a, r in (("T1", "R1"), ("T2", "R2")):
+        x1, x0 = out[1][r], out[0][r]
+        res[f"d{r}_max_rel"] = float((x1 - x0).abs().max() / x0.abs().max().clamp_min(1e-300))
+        res[f"d{r}_norm_rel"] = float((x1 - x0).norm() / x0.norm().clamp_min(1e-300))
+        # the next diagonal step -R/D: the amplitude change the error reaches
+        dd = d["D" + a].abs().clamp_min(1e-10) * torch.sign(d["D" + a])
+        s1, s0 = -x1 / dd, -x0 / dd
+        num += float((s1 - s0).norm() ** 2)
+        den += float(s0.norm() ** 2)
+    res["step_norm_rel"] = math.sqrt(num / max(den, 1e-300))
+    return res
 
 
 def run_gpu(args, cfg):
@@ -157,7 +213,7 @@ def run_gpu(args, cfg):
 
     import cc
     import gccu
-    from devfill import TorchIntegrals, list_tensor
+    from devfill import TorchIntegrals
     import hamiltonian as hm
 
     rank = int(os.environ.get("RANK", 0))
@@ -193,18 +249,13 @@ def run_gpu(args, cfg):
     modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else [])
     results = {}
     for mode in modes:
-        if mode != modes[0]:  # fresh amplitudes and DIIS subspace for the next mode
-            for a in solver.amps:
-                eng.zero(solver.lid(a))
-            if hasattr(solver, "_diis"):
-                del solver._diis
-            solver.graph = None
+        reset_amplitudes(eng, solver)
         eng.set_precision(mode)
         results[mode] = measure(args, cfg, eng, solver, local, dist, mode)
     r = results[modes[0]]
     line = {
-        "metric": METRIC[modes[0]],
-        "value": (r["ms"] / 1e3) / world,
+        "metric": metric_of(cfg),
+        "value": r["ms"] / 1e3,
         "unit": "s",
         "n_gpus": world,
         "steps": args.steps,
@@ -214,41 +265,61 @@ def run_gpu(args, cfg):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": DTYPE[modes[0]],
-        "data": "synthetic (seeded Hamiltonian: eps_occ~U[-1.5,-0.3], eps_virt~U[0.1,4.0], "
-                "B~N(0,0.05^2)); inputs larger than L2 (two-electron list "
+        "data": data_desc(cfg) + "; inputs larger than L2 (two-electron list "
                 f"{8 * solver.lists['V'][1] / 1e9:.1f} GB)",
         "config": {"workload": cfg["name"], "method": "CCSD spin-orbital, DIIS maxsub 8",
                    "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
-                   "parallelism": f"replicas x{world}", "l2": "inputs > L2",
-                   "setup_s": round(setup_s, 2), "energy_last": r["energies"][-1]},
-        "roofline": roofline(cfg, r, peak, modes[0]),
+                   "sigma_B": cfg["sigma"], "use_tr": False,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs > L2", "setup_s": round(setup_s, 2),
+                   "energy_last": r["energies"][-1]},
+        "roofline": roofline(r, peak, modes[0], solver, eng),
         "clocks": clock_summary(r["samples"]),
         "e2e": r["e2e"],
         "gpu_launches": r["launches"],
     }
+    if world > 1:
+        line["throughput"] = {"value": world / line["value"], "unit": "CC iterations/s",
+                              "note": f"{world} independent replicas, one solve per GPU"}
     if 0 in results and modes[0] != 0:
         f = results[0]
-        line["fp64"] = {"metric": METRIC[0], "value": (f["ms"] / 1e3) / world,
+        line["fp64"] = {"metric": metric_of(cfg) + " plain FP64", "value": f["ms"] / 1e3,
                         "ms_per_step": f["ms"], "e2e": f["e2e"], "gpu_launches": f["launches"],
-                        "roofline": roofline(cfg, f, peak, 0),
+                        "roofline": roofline(f, peak, 0, solver, eng),
+                        "clocks": clock_summary(f["samples"]),
                         "energy_last": f["energies"][-1]}
+        # errors of one split-TF32 evaluation against FP64 from identical
+        # amplitudes: those after two plain Jacobi iterations from zero
+        reset_amplitudes(eng, solver)
+        eng.set_precision(0)
+        for _ in range(2):
+            solver.iterate()
+            solver.step()
+        line["precision"] = dict(
+            evaluation_errors(eng, solver),
+            amplitudes="after two FP64 Jacobi iterations from T=0",
+            note="mixed evaluation (split TF32, FP32 accumulation per 4096-index chunk, "
+                 "FP64 sums) minus FP64 evaluation; R*_max_rel relative to max|R|")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         host_lists = {}
-        for name in ("F", "V", "T1", "T2", "D" + "T1", "D" + "T2"):
+        for name in ("F", "V", "T1", "T2", "DT1", "DT2"):
             lid, n, _ = solver.lists[name]
             x = np.empty(n)
             eng.get_vec(lid, 0, x.ctypes.data, n)
             host_lists[name] = x
         cores = os.cpu_count()
-        val, sample = cpu_baseline_oracle(solver.lists, sp, eps, B, args.cpu_seconds, cores,
-                                          host_lists)
+        val, sample = cpu_baseline_oracle(sp, eps, B, args.cpu_seconds, cores, host_lists)
         line["cpu_baseline"] = {"value": val, "unit": "s", "cores": cores, "kind": "port",
                                 "sample": sample}
     eng.close()
     del solver
     torch.cuda.empty_cache()
+    if not args.no_use_tr:
+        line["use_tr"] = measure_use_tr(args, cfg, local, dist, modes,
+                                        {m: results[m]["energies"] for m in modes})
     if rank == 0 and world == 1 and not args.no_convergence:
-        line["convergence"] = convergence(local)
+        line["convergence"] = convergence(local, CONFIGS[args.conv_config])
+        line["convergence_small"] = convergence(local, CONFIGS[0])
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -256,9 +327,17 @@ def run_gpu(args, cfg):
         print(json.dumps(line), flush=True)
 
 
-METRIC = {0: "s/CC-iteration (CCSD, plain FP64)",
-          1: "s/CC-iteration (CCSD, split-TF32 tensor cores, FP64 accumulation)"}
+METRIC_MODE = {0: "plain FP64", 1: "split-TF32 tensor cores, FP64 accumulation"}
 DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums"}
+
+
+def reset_amplitudes(eng, solver):
+    """zero amplitudes, a fresh DIIS subspace and no captured graph"""
+    for a in solver.amps:
+        eng.zero(solver.lid(a))
+    if hasattr(solver, "_diis"):
+        del solver._diis
+    solver.graph = None
 
 
 def max_over_ranks(value, dist):
@@ -275,12 +354,13 @@ def max_over_ranks(value, dist):
     return float(t.item())
 
 
-def measure(args, cfg, eng, solver, local, dist, mode):
+def measure(args, cfg, eng, solver, local, dist, mode, steps=None, profile=True, e2e=True):
     """warm-up (plans every contraction in this precision mode), the timed
     graph-replayed iterations, one eagerly profiled iteration and the
     end-to-end iterations through host buffers"""
     import torch
 
+    steps = steps or args.steps
     energies = []
     for _ in range(args.warmup):
         en, rn = solver.iterate()
@@ -296,7 +376,7 @@ def measure(args, cfg, eng, solver, local, dist, mode):
     th.start()
     eng.reset_stats()
     eng.event_record(0)
-    for _ in range(args.steps):
+    for _ in range(steps):
         en, rn = solver.iterate()
         energies.append(en)
         solver.diis_step()
@@ -305,25 +385,40 @@ def measure(args, cfg, eng, solver, local, dist, mode):
     stop.set()
     th.join()
     _, launches = eng.stats()
-    # per-kernel times: one more iteration, launched eagerly with every [CONTR]
-    # kernel bracketed by events on the engine's stream (outside the timed loop)
-    eng.profile(True)
-    solver.evaluate()
-    prof = eng.profile_report()
-    eng.profile(False)
-    names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
-    if len(names) != len(prof):
-        raise RuntimeError(f"profile rows ({len(prof)}) do not match contractions ({len(names)})")
-    if args.profile_out and mode == args.precision and int(os.environ.get("RANK", 0)) == 0:
-        with open(args.profile_out, "w") as f:
-            json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
-                        "tflops": r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12 if r[2] else None,
-                        "block_contractions": int(r[3]), "tiles": int(r[4]),
-                        "pack_ms": r[5] / max(r[1], 1)}
-                       for n, r in zip(names, prof)], f, indent=1)
-    ms = max_over_ranks(ms_total / args.steps, dist)
-    # e2e: the same iteration through the public API with host buffers: the
-    # amplitudes come from pinned host memory, the residual and energy go back
+    ms = max_over_ranks(ms_total / steps, dist)
+    out = {"ms": ms, "launches": int(launches), "samples": samples, "energies": energies}
+    if profile:
+        # per-kernel times: one more iteration, launched eagerly with every
+        # [CONTR] kernel bracketed by events on the engine's stream (outside
+        # the timed loop)
+        eng.profile(True)
+        solver.evaluate()
+        prof = eng.profile_report()
+        eng.profile(False)
+        names = [it["name"] for it in solver.formula if it["kind"] == "CONTR"]
+        if len(names) != len(prof):
+            raise RuntimeError(f"profile rows ({len(prof)}) do not match contractions "
+                               f"({len(names)})")
+        if args.profile_out and mode == args.precision and int(os.environ.get("RANK", 0)) == 0:
+            with open(args.profile_out, "w") as f:
+                json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
+                            "tflops": (r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12
+                                       if r[2] else None),
+                            "block_contractions": int(r[3]), "tiles": int(r[4]),
+                            "pack_ms": r[5] / max(r[1], 1)}
+                           for n, r in zip(names, prof)], f, indent=1)
+        out.update(prof=prof, names=names)
+    if e2e:
+        out["e2e"] = measure_e2e(args, eng, solver)
+    return out
+
+
+def measure_e2e(args, eng, solver):
+    """the same iteration through the public API with host buffers: the
+    amplitudes come from pinned host memory, the residuals and the energy go
+    back"""
+    import torch
+
     nT = {a: solver.lists[a][1] for a in solver.amps}
     nR = {a: solver.lists[solver.res[a]][1] for a in solver.amps}
     host_t = {a: torch.empty(n, dtype=torch.float64, pin_memory=True) for a, n in nT.items()}
@@ -336,18 +431,62 @@ def measure(args, cfg, eng, solver, local, dist, mode):
     for _ in range(e2e_steps):
         for a in solver.amps:
             eng.put_vec(solver.lid(a), 0, host_t[a].data_ptr(), nT[a])
-        en, rn = solver.iterate()
+        solver.iterate()
         for a in solver.amps:
             eng.get_vec(solver.lid(solver.res[a]), 0, host_r[a].data_ptr(), nR[a])
     eng.sync()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    return {"ms": ms, "launches": int(launches), "samples": samples, "prof": prof,
-            "names": names, "energies": energies,
-            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * sum(nT.values()),
-                    "d2h_bytes_per_step": 8 * sum(nR.values()) + 8}}
+    return {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * sum(nT.values()),
+            "d2h_bytes_per_step": 8 * sum(nR.values()) + 8}
 
 
-def roofline(cfg, r, fp64_peak_tflops, mode):
+def measure_use_tr(args, cfg, local, dist, modes, plain_energies):
+    """seconds per iteration with spin-flip symmetry (calculate.routes.use_tr,
+    the reference's default): half of the Ms cases of every contraction into
+    a spin-symmetric list, doubled, then symmetrised (sym_ab_blk); the first
+    warm-up energies are compared with those of the plain evaluation (same
+    iterates from T = 0)"""
+    import torch
+
+    import cc
+    import gccu
+    from devfill import TorchIntegrals
+    import hamiltonian as hm
+
+    sp, eps, B = setup_hamiltonian(cfg)
+    eng = gccu.Engine(local)
+    out = {}
+    try:
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd", use_tr=True)
+        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+        for mode in modes:
+            reset_amplitudes(eng, s)
+            eng.set_precision(mode)
+            r = measure(args, cfg, eng, s, local, dist, mode, steps=max(2, args.steps // 2),
+                        profile=False, e2e=False)
+            ref = plain_energies[mode]
+            k = min(3, len(ref), len(r["energies"]))
+            out["fp64" if mode == 0 else "mixed"] = {
+                "value": r["ms"] / 1e3, "unit": "s", "gpu_launches": r["launches"],
+                "clocks": clock_summary(r["samples"]),
+                "dE_first_iterations_vs_plain": max(
+                    abs(a - b) for a, b in zip(r["energies"][:k], ref[:k]))}
+    finally:
+        eng.close()
+        torch.cuda.empty_cache()
+    return out
+
+
+def plan_rows(eng, solver, name):
+    it = [x for x in solver.formula if x.get("name") == name][0]
+    o1, o2, r = solver.blk(it["op1"]), solver.blk(it["op2"]), solver.blk(it["res"])
+    c = np.asarray(it["cnt"])
+    ex1 = np.asarray(it["op1"][1]) - c
+    ex2 = np.asarray(it["op2"][1]) - np.concatenate([c[4:], c[:4]])
+    return eng.plan_items(o1, o2, r, ex1, ex2, c)
+
+
+def roofline(r, fp64_peak_tflops, mode, solver, eng):
     """dominant kernel: the GEMM launch(es) of the pp-ladder contraction (the
     leading term; no operand gathers), timed with events in the profiled
     iteration: k_gemm<128,64> (FP64 DMMA) in mode 0, k_gemm_tc (split TF32 on
@@ -357,13 +496,21 @@ def roofline(cfg, r, fp64_peak_tflops, mode):
     dom_ms = (dom[2] - dom[5]) / dom[1]
     achieved = dom[0] / (dom_ms * 1e-3) / 1e12
     total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
+    rows = plan_rows(eng, solver, ROOFLINE_CONTRACTION).astype(float)
+    M, N, K = rows[:, 0], rows[:, 1], rows[:, 2]
+    alg_bytes = float(8 * np.sum(M * K + N * K) + 16 * np.sum(M * N))
     out = {"bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
            "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
            "iteration_flops": total_flops,
-           "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12}
+           "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12,
+           "algorithmic_bytes_per_launch": alg_bytes}
+    kern = "k_gemm" if mode == 0 else "k_gemm_tc"
+    out["traffic"] = TRAFFIC_PER_ALGORITHMIC_BYTE[kern] * alg_bytes
+    out["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same "
+                             "launch at o12/v100 per algorithmic byte, times this launch's "
+                             "algorithmic bytes")
     if mode == 0:
         out.update(peak=fp64_peak_tflops,
-                   traffic=profiled_traffic(cfg, "k_gemm"),
                    kernel=f"k_gemm<128,64> FP64 DMMA, launch of [CONTR] {ROOFLINE_CONTRACTION}",
                    peak_source="cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
                                "MEASURED_PEAKS.json)")
@@ -375,12 +522,13 @@ def roofline(cfg, r, fp64_peak_tflops, mode):
         burst, _ = measured_bf16_tflops("bf16_tflops")
         peak = bf16 / 2.0 / 3.0
         out.update(peak=peak,
-                   traffic=profiled_traffic(cfg, "k_gemm_tc"),
                    kernel=f"k_gemm_tc split TF32 (tcgen05, persistent), launch of [CONTR] "
                           f"{ROOFLINE_CONTRACTION}",
                    peak_source=f"of {src}: bf16_tflops_sustained / 2 (dense TF32 = half of "
                                "dense BF16) / 3 (three TF32 products per useful product)",
                    frac_of_burst=achieved / (burst / 6.0))
+        # the ladder end to end, its operand split included
+        out["ladder_with_split_tflops"] = dom[0] / (dom[2] / dom[1] * 1e-3) / 1e12
     out["frac"] = (achieved / out["peak"]) if out["peak"] else None
     return out
 
@@ -399,47 +547,56 @@ def measured_bf16_tflops(key="bf16_tflops"):
         return FALLBACK_PEAKS[key], "fallback"
 
 
-def convergence(local):
-    """time to |dE| < 1 uEh against the converged FP64 energy, plain FP64 and
-    mixed (split TF32 until the residual norm is below 1e-5, then FP64), on
-    the largest size of the synthetic family that converges under
-    diagonal+DIIS (o8 v32; o12 v100 and larger diverge with these integral
-    distributions).  Wall time of the solve loop (device work, energy and
-    residual reads, DIIS solves), graphs replayed after the first iteration
-    of each mode."""
+def convergence(local, cfg):
+    """time to |dE| < 1 uEh against the converged FP64 energy: plain FP64 and
+    mixed (split TF32 until the residual norm is below 1e-5, then FP64).
+    Wall time of the solve loop (device work, energy and residual reads,
+    DIIS solves), graphs replayed after the first iteration of each mode;
+    set-up excluded, planning of the first iteration included."""
     import cc
     import gccu
     import hamiltonian as hm
     from devfill import TorchIntegrals
 
-    cfg = CONFIGS[0]
     sp, eps, B = setup_hamiltonian(cfg)
-    out = {"workload": cfg["name"]}
+    out = {"workload": cfg["name"], "sigma_B": cfg["sigma"]}
     ref = None
+    ref_t = None
     for label in ("fp64", "mixed"):
         eng = gccu.Engine(local)
-        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
-        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
-        eng.sync()
-        hist = []
-        t0 = time.perf_counter()
+        try:
+            s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+            s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+            eng.sync()
+            hist = []
+            t0 = time.perf_counter()
 
-        def cb(it, en, rn):
-            hist.append((it, en, rn, time.perf_counter() - t0))
+            def cb(it, en, rn):
+                hist.append((it, en, rn, time.perf_counter() - t0))
 
-        if label == "fp64":
-            s.solve(maxiter=60, conv=1e-9, use_graph=True, callback=cb)
-        else:
-            s.solve_mixed(maxiter=60, conv=1e-9, switch=1e-5, callback=cb)
-        eng.close()
+            if label == "fp64":
+                s.solve(maxiter=80, conv=1e-9, use_graph=True, callback=cb)
+            else:
+                s.solve_mixed(maxiter=80, conv=1e-9, switch=1e-5, callback=cb)
+            t = {a: eng.download(s.lid(a), s.lists[a][1]) for a in s.amps}
+        finally:
+            eng.close()
         if ref is None:
             ref = hist[-1][1]
+            ref_t = t
         hit = next((h for h in hist if abs(h[1] - ref) < 1e-6), None)
         out[label] = {"iterations": hist[-1][0], "energy": hist[-1][1],
                       "residual": hist[-1][2], "s_total": hist[-1][3],
+                      "converged": hist[-1][2] < 1e-9,
                       "iterations_to_1uEh": hit[0] if hit else None,
                       "s_to_1uEh": hit[3] if hit else None}
-    out["dE_mixed_vs_fp64"] = out["mixed"]["energy"] - out["fp64"]["energy"]
+        if label != "fp64":
+            num = sum(float(np.sum((t[a] - ref_t[a]) ** 2)) for a in t)
+            den = sum(float(np.sum(ref_t[a] ** 2)) for a in t)
+            out[label]["dE_vs_fp64"] = hist[-1][1] - ref
+            out[label]["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
+    if out["mixed"]["s_to_1uEh"] and out["fp64"]["s_to_1uEh"]:
+        out["speedup_to_1uEh_mixed_vs_fp64"] = out["fp64"]["s_to_1uEh"] / out["mixed"]["s_to_1uEh"]
     return out
 
 
@@ -461,13 +618,7 @@ def run_reference(args, cfg):
     from devfill import TorchIntegrals
     s.load_hamiltonian_device(TorchIntegrals(sp, eps, B, device="cpu"))
     setup_s = time.time() - t0
-    # nonzero amplitudes so that no block is screened out (the reference skips
-    # blocks with norm^2 < 1e-28): T2 = MP2 guess -<ab||ij>/D, T1 small, seeded
-    oe.add_block(1.0, s.lid("V"), 7, s.lid("R2"), 1, reset=True)
-    oe.precondition(s.lid("T2"), s.lid("R2"), s.lid("DT2"), fac=-1.0)
-    rng = np.random.default_rng(cfg["seed"])
-    t1 = oe.data[s.lid("T1")]
-    t1[:] = 1e-3 * rng.standard_normal(t1.size)
+    seed_amplitudes(oe, s, cfg)
     stride = None
     times = []
     for i in range(1 + args.steps):
@@ -482,26 +633,73 @@ def run_reference(args, cfg):
         t0 = time.time()
         s.evaluate()
         scaled = binding.scaled_time(time.time() - t0, binding.sampling_report())
-        if i >= 1:
-            times.append(scaled)
+        times.append(scaled)
+    binding.sampling(1)
     val = float(np.mean(times)) if times else None
     line = {
         "impl": "reference",
-        "metric": "s/CC-iteration (CCSD, plain FP64)",
+        "metric": metric_of(cfg),
         "value": val, "unit": "s", "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3 if val else None,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (same seeded Hamiltonian as the GPU arm)",
+        "data": data_desc(cfg) + " (same seeded Hamiltonian as the GPU arm)",
         "config": {"workload": cfg["name"], "method": "CCSD spin-orbital",
                    "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
-                   "setup_s": round(setup_s, 1)},
+                   "sigma_B": cfg["sigma"], "use_tr": False, "setup_s": round(setup_s, 1)},
+        "extrapolated": True,
         "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
                          "sample": f"each step: one CCSD iteration through the oracle (route 3, "
                                    f"OpenBLAS dgemm on {cores} cores) with every {stride}-th "
-                                   f"long-operand batch executed, scaled by batch count"},
+                                   f"long-operand batch executed, extrapolated by batch count "
+                                   f"(validated against an unsampled iteration at o12/v100 "
+                                   f"with bench.py --validate-sampling)"},
         "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def seed_amplitudes(oe, s, cfg):
+    """nonzero amplitudes so that no block is screened out (the reference
+    skips blocks with norm^2 < 1e-28): T2 = MP2 guess -<ab||ij>/D, T1 small,
+    seeded"""
+    oe.add_block(1.0, s.lid("V"), 7, s.lid("R2"), 1, reset=True)
+    oe.precondition(s.lid("T2"), s.lid("R2"), s.lid("DT2"), fac=-1.0)
+    rng = np.random.default_rng(cfg["seed"])
+    t1 = oe.data[s.lid("T1")]
+    t1[:] = 1e-3 * rng.standard_normal(t1.size)
+
+
+def validate_sampling(args):
+    """the reference arm's extrapolation checked on a size where a full
+    iteration is affordable: one unsampled oracle iteration at o12/v100 next
+    to the sampled estimates at several strides"""
+    import binding
+    import cc
+    from devfill import TorchIntegrals
+    from engine import OracleEngine
+    import hamiltonian as hm
+    cfg = CONFIGS[10]
+    sp, eps, B = setup_hamiltonian(cfg)
+    cores = os.cpu_count()
+    binding.set_blas(cores)
+    oe = OracleEngine(route=3)
+    s = cc.CCSolver(oe, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+    s.load_hamiltonian_device(TorchIntegrals(sp, eps, B, device="cpu"))
+    seed_amplitudes(oe, s, cfg)
+    out = {"workload": cfg["name"], "cores": cores}
+    binding.sampling(1)
+    t0 = time.time()
+    s.evaluate()
+    out["unsampled_s"] = time.time() - t0
+    for stride in (4, 16, 64):
+        binding.sampling(stride)
+        t0 = time.time()
+        s.evaluate()
+        est = binding.scaled_time(time.time() - t0, binding.sampling_report())
+        out[f"stride_{stride}_estimate_s"] = est
+        out[f"stride_{stride}_ratio"] = est / out["unsampled_s"]
+    binding.sampling(1)
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -511,6 +709,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gecco-b200")
     ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--conv-config", type=int, default=12,
+                    help="workload of the time-to-convergence comparison")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -519,18 +719,25 @@ def main():
                          "path measured beside them; 0: FP64 only")
     ap.add_argument("--no-fp64", action="store_true",
                     help="with --precision 1, skip the FP64 measurement")
+    ap.add_argument("--no-use-tr", action="store_true",
+                    help="skip the timing with spin-flip symmetry")
     ap.add_argument("--no-convergence", action="store_true",
-                    help="skip the time-to-convergence comparison on o8 v32")
+                    help="skip the time-to-convergence comparisons")
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")
     ap.add_argument("--profile-out", default=None,
                     help="write per-contraction kernel times (JSON)")
+    ap.add_argument("--validate-sampling", action="store_true",
+                    help="compare the reference arm's sampled estimate with an unsampled "
+                         "oracle iteration at o12/v100 and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     cfg = CONFIGS[args.config]
-    if args.impl == "reference":
+    if args.validate_sampling:
+        validate_sampling(args)
+    elif args.impl == "reference":
         run_reference(args, cfg)
     else:
         run_gpu(args, cfg)
