@@ -89,6 +89,14 @@ struct DevPlan {
   double ms = 0, pack_ms = 0;
 };
 
+// transposed [ADD] of one class (add_opblk_transp), planned on first use
+struct DevTransp {
+  TranspDesc* d = nullptr;
+  int64_t n = 0, maxlen = 0;
+  int list_in = 0, list_out = 0;
+  int64_t off_out = 0, len_out = 0;
+};
+
 struct DevReo {
   ReoPlan plan;
   ReoItem* d_items = nullptr;
@@ -136,6 +144,7 @@ class Engine {
   std::vector<cudaEvent_t> event_pool;
   std::vector<DevPlan*> plan_order;  // plans in first-use order (profile report)
   std::map<std::string, std::unique_ptr<DevReo>> reos;  // reorder plans per descriptor
+  std::map<std::string, std::unique_ptr<DevTransp>> transps;  // transposed [ADD] plans
   // learned correction of the diagonal step: weights, Adam moments, sample
   // set (rows and targets), gradient buffers
   double *lp_w = nullptr, *lp_m = nullptr, *lp_v = nullptr;
@@ -410,6 +419,120 @@ class Engine {
       if (!P.items.empty()) dr->d_items = upload(P.items);
     }
     return *(reos[os.str()] = std::move(dr));
+  }
+
+  // leading dimensions of set_op_ldim_c (contract/set_op_ldim_c.f) over the
+  // components c, a with string counts lc, la: C before A per hpvx type, or
+  // with transpose A before C, the components of a type in reverse order
+  static void op_ldims(const std::vector<Comp>& c, const std::vector<Comp>& a,
+                       const std::vector<int64_t>& lc, const std::vector<int64_t>& la,
+                       bool transpose, int64_t* ldc, int64_t* lda) {
+    int64_t ld = 1;
+    for (int ih = 0; ih < 4; ++ih) {
+      const int t = kHpvxSeq[ih];
+      if (!transpose) {
+        for (size_t i = 0; i < c.size(); ++i)
+          if (c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
+        for (size_t i = 0; i < a.size(); ++i)
+          if (a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+      } else {
+        for (size_t i = a.size(); i-- > 0;)
+          if (a[i].hpvx == t) lda[i] = ld, ld *= la[i];
+        for (size_t i = c.size(); i-- > 0;)
+          if (c[i].hpvx == t) ldc[i] = ld, ld *= lc[i];
+      }
+    }
+  }
+
+  // plan of a transposed [ADD] (add_opblk_transp, contract/add_opblk_transp.f:
+  // 195-321): per distribution of the output class, the input distribution
+  // with C and A strings exchanged (at Ms(C), IRREP(C) of the output) and the
+  // leading dimensions of both over the output's components
+  DevTransp& transp_for(int64_t lin, int64_t ibin, int64_t lout, int64_t ibout, bool tra_in,
+                        bool tra_out) {
+    std::ostringstream os;
+    os << lin << ',' << ibin << ',' << lout << ',' << ibout << ',' << tra_in << tra_out;
+    auto it = transps.find(os.str());
+    if (it != transps.end()) return *it->second;
+    GCCU_REQUIRE(!capturing, "transposed add must be run once before it is captured in a graph");
+    GCCU_REQUIRE(tra_in != tra_out, "add_opblk_transp: exactly one side is transposed");
+    const ListLayout& Li = list(lin).L;
+    const ListLayout& Lo = list(lout).L;
+    GCCU_REQUIRE(model.ops.at(Li.op - 1).nj == 1 && model.ops.at(Lo.op - 1).nj == 1,
+                 "add_opblk_transp: operators of one vertex only in this engine version");
+    GCCU_REQUIRE(ibin >= 1 && ibin <= (int64_t)Li.blk.size() && ibout >= 1 &&
+                     ibout <= (int64_t)Lo.blk.size(),
+                 "add_opblk_transp: occupation class out of range");
+    const LayoutBlock& Bi = Li.blk[ibin - 1];
+    const LayoutBlock& Bo = Lo.blk[ibout - 1];
+    auto same = [](const std::vector<Comp>& x, const std::vector<Comp>& y) {
+      if (x.size() != y.size()) return false;
+      for (size_t i = 0; i < x.size(); ++i)
+        if (x[i].occ != y[i].occ || x[i].hpvx != y[i].hpvx) return false;
+      return true;
+    };
+    GCCU_REQUIRE(same(Bi.c, Bo.a) && same(Bi.a, Bo.c),
+                 "add_opblk_transp: input and output list do not have compatible operators");
+    GCCU_REQUIRE(Bo.c.size() <= (size_t)kDevMaxComp && Bo.a.size() <= (size_t)kDevMaxComp,
+                 "add_opblk_transp: too many components");
+    int msc_max = 0, msa_max = 0;
+    for (auto& x : Bo.c) msc_max += x.occ;
+    for (auto& x : Bo.a) msa_max += x.occ;
+    const int nsym = model.os.nsym;
+    auto dt = std::make_unique<DevTransp>();
+    std::vector<TranspDesc> v;
+    for (auto& kv : Bo.dis) {
+      const int gama = kv.first.second;
+      for (const Dist& d : kv.second) {
+        if (d.len <= 0) continue;
+        int msc = 0;
+        for (int m : d.msc) msc += m;
+        std::vector<int> ixc(Bo.c.size()), ixa(Bo.a.size());
+        std::vector<int64_t> lc(Bo.c.size()), la(Bo.a.size());
+        TranspDesc t{};
+        t.nc = (int32_t)Bo.c.size();
+        t.na = (int32_t)Bo.a.size();
+        t.lenc = t.lena = 1;
+        for (size_t i = 0; i < Bo.c.size(); ++i) {
+          ixc[i] = ms_index(Bo.c[i].occ, d.msc[i]);
+          lc[i] = model.G(Bo.c[i].graph).nstr(ixc[i], d.gc[i]);
+          t.lc[i] = (int32_t)lc[i];
+          t.lenc *= lc[i];
+        }
+        for (size_t i = 0; i < Bo.a.size(); ++i) {
+          ixa[i] = ms_index(Bo.a[i].occ, d.msa[i]);
+          la[i] = model.G(Bo.a[i].graph).nstr(ixa[i], d.ga[i]);
+          t.la[i] = (int32_t)la[i];
+          t.lena *= la[i];
+        }
+        if (t.lenc == 0 || t.lena == 0) continue;
+        const int ix_in = msa_to_idxms(msc, Li.mst, msc_max, msa_max);
+        const int gam_in = irrep_mult(gama, Lo.gamt);
+        auto f = Bi.dis.find({ix_in, gam_in});
+        GCCU_REQUIRE(f != Bi.dis.end(),
+                     "add_opblk_transp: the input list has no distribution for this case "
+                     "(total Ms or IRREP differ from the output's adjoint)");
+        const int64_t did = dist_id(Bi.c, ixa, d.ga, Bi.a, ixc, d.gc, nsym);
+        const Dist* src = nullptr;
+        for (const Dist& di : f->second)
+          if (di.did == did) src = &di;
+        GCCU_REQUIRE(src && src->len == d.len, "add_opblk_transp: distribution not found");
+        t.off_out = d.off;
+        t.off_in = src->off;
+        op_ldims(Bo.c, Bo.a, lc, la, tra_out, t.ldoc, t.ldoa);
+        op_ldims(Bo.c, Bo.a, lc, la, tra_in, t.ldic, t.ldia);
+        v.push_back(t);
+        dt->maxlen = std::max(dt->maxlen, t.lenc * t.lena);
+      }
+    }
+    GCCU_REQUIRE(v.size() <= 65535, "add_opblk_transp: too many distributions");
+    dt->n = (int64_t)v.size();
+    if (!v.empty() && !host_only) dt->d = upload(v);
+    dt->list_in = (int)lin;
+    dt->list_out = (int)lout;
+    dt->off_out = Bo.off;
+    dt->len_out = Bo.len;
+    return *(transps[os.str()] = std::move(dt));
   }
 
   // trace plan (same device form as a reorder), built on first use
@@ -1572,6 +1695,38 @@ int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_ou
       CUDA_OK(cudaStreamSynchronize(e.stream));
     }
     CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_add_block_transp(double fac, int64_t list_in, int64_t iblk_in, int64_t list_out,
+                          int64_t iblk_out, int64_t tra_in, int64_t tra_out, int64_t reset,
+                          int64_t type, double* xnorm2) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_add_block_transp needs a device");
+    DevList& b = e.wlist(list_out);
+    DevList& a = e.list(list_in);
+    GCCU_REQUIRE(a.d != b.d, "add_opblk_transp: input and output list must differ");
+    DevTransp& dt = e.transp_for(list_in, iblk_in, list_out, iblk_out, tra_in != 0, tra_out != 0);
+    if (reset)
+      CUDA_OK(cudaMemsetAsync(b.d + dt.off_out, 0, dt.len_out * sizeof(double), e.stream));
+    if (dt.n) {
+      launch_add_transp(dt.d, dt.n, a.d, b.d, fac, dt.maxlen, e.stream);
+      ++e.launches;
+    }
+    CUDA_OK(cudaGetLastError());
+    if (type == 1) {
+      GCCU_REQUIRE(!e.capturing, "type must be 0 inside a graph capture");
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, sizeof(double), e.stream));
+      launch_sumsq(b.d + dt.off_out, dt.len_out, e.d_red, e.stream);
+      ++e.launches;
+      *xnorm2 = e.read_red(0);
+    } else if (type == 2) {
+      GCCU_REQUIRE(!e.capturing, "type must be 0 inside a graph capture");
+      CUDA_OK(cudaMemcpyAsync(xnorm2, b.d + dt.off_out, sizeof(double), cudaMemcpyDeviceToHost,
+                              e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
   });
 }
 

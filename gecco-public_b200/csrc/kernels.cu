@@ -203,6 +203,39 @@ void launch_diavc(double* out, const double* in, const double* diag, double fac,
   if (n == 0) return;
   k_diavc<<<grid_for(n, 256), 256, 0, s>>>(out, in, diag, fac, shift, n);
 }
+// one output distribution per blockIdx.y; consecutive threads on
+// consecutive output C indices (the output's fastest creator component)
+__global__ void k_add_transp(const TranspDesc* __restrict__ ds, const double* __restrict__ in,
+                             double* __restrict__ out, double fac) {
+  const TranspDesc& d = ds[blockIdx.y];
+  const int64_t n = d.lenc * d.lena;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t ia = e / d.lenc, ic = e % d.lenc;
+    int64_t po = 0, pi = 0;
+    for (int k = 0; k < d.nc; ++k) {
+      const int64_t s = ic % d.lc[k];
+      ic /= d.lc[k];
+      po += s * d.ldoc[k];
+      pi += s * d.ldic[k];
+    }
+    for (int k = 0; k < d.na; ++k) {
+      const int64_t s = ia % d.la[k];
+      ia /= d.la[k];
+      po += s * d.ldoa[k];
+      pi += s * d.ldia[k];
+    }
+    out[d.off_out + po] += fac * in[d.off_in + pi];
+  }
+}
+
+void launch_add_transp(const TranspDesc* d, int64_t n, const double* in, double* out, double fac,
+                       int64_t maxlen, cudaStream_t s) {
+  if (n == 0 || maxlen == 0) return;
+  dim3 grid((unsigned)std::min<int64_t>((maxlen + 255) / 256, 4096), (unsigned)n);
+  k_add_transp<<<grid, 256, 0, s>>>(d, in, out, fac);
+}
+
 void launch_sym_ab(const FlipDesc* d, int64_t n, double* x, double prefac, int64_t maxlen,
                    cudaStream_t s) {
   if (n == 0 || maxlen == 0) return;

@@ -120,6 +120,18 @@ struct FlipDesc {
 };
 void launch_sym_ab(const FlipDesc* d, int64_t n, double* x, double prefac, int64_t maxlen,
                    cudaStream_t s);
+// transposed add of one output distribution (add_opblk_transp): for every
+// element (C strings ic, A strings ia) of the output distribution
+// out[off_out + pos(ldo)] += fac * in[off_in + pos(ldi)], pos summing the
+// component string indices times the leading dimensions
+struct TranspDesc {
+  int64_t off_out, off_in, lenc, lena;
+  int32_t nc, na;
+  int32_t lc[kDevMaxComp], la[kDevMaxComp];
+  int64_t ldoc[kDevMaxComp], ldoa[kDevMaxComp], ldic[kDevMaxComp], ldia[kDevMaxComp];
+};
+void launch_add_transp(const TranspDesc* d, int64_t n, const double* in, double* out, double fac,
+                       int64_t maxlen, cudaStream_t s);
 
 // Learned correction of the diagonal step (learned.cu): a perceptron with
 // kLpInputs inputs, two tanh layers of kLpHidden and one output; weights

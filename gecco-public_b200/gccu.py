@@ -82,6 +82,7 @@ _SIGS = {
     "gccu_contract_noalloc": [ctypes.POINTER(BcDesc), ctypes.c_double, I64, I64],
     "gccu_add_block": [ctypes.c_double, I64, I64, I64, I64, I64, I64, PD],
     "gccu_scale_list": [I64, ctypes.c_double],
+    "gccu_add_block_transp": [ctypes.c_double, I64, I64, I64, I64, I64, I64, I64, I64, PD],
     "gccu_dot_lists": [I64, I64, PD],
     "gccu_sym_ab": [I64, I64, ctypes.c_double, ctypes.c_double],
     "gccu_precondition": [I64, I64, I64, ctypes.c_double, ctypes.c_double],
@@ -425,6 +426,14 @@ class Engine:
     def add_block(self, fac, lin, iblk_in, lout, iblk_out, reset=False, typ=0):
         r = np.zeros(1)
         _call("gccu_add_block", fac, lin, iblk_in, lout, iblk_out, int(reset), typ, _pd(r))
+        return float(r[0])
+
+    def add_block_transp(self, fac, lin, iblk_in, lout, iblk_out, tra_in=True, tra_out=False,
+                         reset=False, typ=0):
+        """out(IC,IA) = (reset ? 0 : out) + fac*in(IA,IC) (add_opblk_transp)"""
+        r = np.zeros(1)
+        _call("gccu_add_block_transp", fac, lin, iblk_in, lout, iblk_out, int(tra_in),
+              int(tra_out), int(reset), typ, _pd(r))
         return float(r[0])
 
     def scale(self, lst, fac):

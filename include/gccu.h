@@ -223,6 +223,16 @@ int gccu_trace_info(int64_t list_op, int64_t iblk_op, int64_t list_res, int64_t 
  * the squared norm of the updated block, type 2 its first element. */
 int gccu_add_block(double fac, int64_t list_in, int64_t iblk_in, int64_t list_out,
                    int64_t iblk_out, int64_t reset, int64_t type, double* xnorm2);
+/* transposed [ADD] (fs_add_drv with tra_op != tra_res,
+ * contract/fs_add_drv.f:127-131 -> add_opblk_transp,
+ * contract/add_opblk_transp.f:2-355): out(IC,IA) = (reset ? 0 : out) +
+ * fac*in(IA,IC), the input class being the adjoint of the output class
+ * (total Ms negated, same IRREP); exactly one of tra_in, tra_out is set and
+ * selects set_op_ldim_c's A-C sequence for that side; type as for
+ * gccu_add_block.  Single-vertex operators. */
+int gccu_add_block_transp(double fac, int64_t list_in, int64_t iblk_in, int64_t list_out,
+                          int64_t iblk_out, int64_t tra_in, int64_t tra_out, int64_t reset,
+                          int64_t type, double* xnorm2);
 /* scale a whole list in place (scale_copy_op with one operand) */
 int gccu_scale_list(int64_t list_id, double fac);
 /* dot product of two lists of identical layout (DIIS subspace products) */

@@ -199,6 +199,19 @@ class Oracle:
         _chk(rc)
         return float(xret[0])
 
+    def add_transp(self, fac, lin, bin_, xin, lout, bout, xout, tra_in, tra_out, reset=False,
+                   typ=1):
+        """add_opblk_transp: out(IC,IA) += fac * in(IA,IC) (xout updated in place)"""
+        L = lib()
+        L.ora_add_opblk_transp.restype = ctypes.c_int
+        L.ora_add_opblk_transp.argtypes = [ctypes.c_void_p, PD, I64, ctypes.c_double, I64, I64,
+                                           PD, I64, I64, PD, I64, I64, I64]
+        xn = np.zeros(1)
+        _chk(L.ora_add_opblk_transp(self.ctx, _pd(xn), typ, fac, lin, bin_,
+                                    _pd(np.ascontiguousarray(xin)), lout, bout, _pd(xout),
+                                    int(tra_in), int(tra_out), int(reset)))
+        return float(xn[0])
+
     def sym_ab(self, lst, iblk, x, prefac=0.5, relfac=1.0):
         _chk(lib().ora_sym_ab_blk(self.ctx, lst, iblk, _pd(x), prefac, relfac))
 

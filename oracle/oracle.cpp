@@ -1881,6 +1881,84 @@ void sym_ab_blk(ora_ctx* cx, List& L, int iblk, double* buf, double prefac, doub
   }
 }
 
+// add_opblk_transp (contract/add_opblk_transp.f:195-321): OUT(IC,IA) +=
+// fac * IN(IA,IC) for a class of the output whose adjoint is the input class
+// (op_in^tra_in = op_out^tra_out).  Loops over the output's Ms(A), IRREP(A)
+// and distributions; the input distribution is the one with C and A strings
+// exchanged, looked up at (Ms(C), IRREP(C)) of the output (idx_msgmdst2
+// with C and A swapped); the element offsets inside the two distributions
+// use set_op_ldim_c over the output's components with tra_in and tra_out.
+// Single-vertex operators.
+void add_opblk_transp(ora_ctx* cx, List& Li, int iblk_in, const double* xin, List& Lo,
+                      int iblk_out, double* xout, double fac, bool tra_in, bool tra_out) {
+  CHECK(cx->ops[Li.op - 1].nj == 1 && cx->ops[Lo.op - 1].nj == 1,
+        "add_opblk_transp: single-vertex operators only");
+  ListBlock& Bo = Lo.blk.at(iblk_out - 1);
+  ListBlock& Bi = Li.blk.at(iblk_in - 1);
+  auto same = [](const std::vector<Comp>& x, const std::vector<Comp>& y) {
+    if (x.size() != y.size()) return false;
+    for (size_t i = 0; i < x.size(); ++i)
+      if (x[i].occ != y[i].occ || x[i].hpvx != y[i].hpvx) return false;
+    return true;
+  };
+  CHECK(same(Bi.c, Bo.a) && same(Bi.a, Bo.c),
+        "add_opblk_transp: input and output list do not have compatible operators");
+  int nsym = cx->oi.nsym;
+  int msc_max = sum_occ(Bo.c), msa_max = sum_occ(Bo.a);
+  std::vector<int> oc = occs(Bo.c), oa = occs(Bo.a);
+  int idxmsa = 0;
+  for (int msa = msa_max; msa >= -msa_max; msa -= 2) {
+    int msc = msa + Lo.mst;
+    if (std::abs(msc) > msc_max) continue;
+    ++idxmsa;
+    int idxmsc = (msc_max - msc) / 2 + 1;
+    for (int gama = 1; gama <= nsym; ++gama) {
+      int gamc = mult(gama, Lo.gamt);
+      auto itl = Bo.gm_len.find({idxmsa, gama});
+      if (itl == Bo.gm_len.end() || itl->second <= 0) continue;
+      const auto& dlo = Bo.dis.at({idxmsa, gama});
+      MsGamDist d;
+      bool first = true;
+      size_t idxdis = 0;
+      while (next_msgamdist2(first, d, oc, oa, msc, msa, gamc, gama, nsym)) {
+        first = false;
+        auto ixc = ixms(Bo.c, d.msc), ixa = ixms(Bo.a, d.msa);
+        auto lc = lens(cx, Bo.c, ixc, d.gc), la = lens(cx, Bo.a, ixa, d.ga);
+        int64_t lenc = prod(lc, 0, lc.size()), lena = prod(la, 0, la.size());
+        if (lenc == 0 || lena == 0) continue;
+        const int64_t off_out = dlo.at(idxdis++).off;
+        int64_t id_in = 0;
+        const auto& dli = Bi.dis.at({idxmsc, gamc});
+        if (dli.size() > 1)
+          id_in = find_dis(Bi, idxmsc, gamc, msgmdid2(Bi.c, ixa, d.ga, Bi.a, ixc, d.gc, nsym));
+        const int64_t off_in = dli[id_in].off;
+        std::vector<int64_t> ldic, ldia, ldoc, ldoa;
+        ldims(Bo.c, Bo.a, cat(lc, la), ldic, ldia, tra_in);
+        ldims(Bo.c, Bo.a, cat(lc, la), ldoc, ldoa, tra_out);
+        for (int64_t ic = 0; ic < lenc; ++ic) {
+          int64_t r = ic, pi = 0, po = 0;
+          for (size_t k = 0; k < Bo.c.size(); ++k) {
+            int64_t sidx = r % lc[k];
+            r /= lc[k];
+            pi += sidx * ldic[k];
+            po += sidx * ldoc[k];
+          }
+          for (int64_t ia = 0; ia < lena; ++ia) {
+            int64_t q = ia, qi = pi, qo = po;
+            for (size_t k = 0; k < Bo.a.size(); ++k) {
+              int64_t sidx = q % la[k];
+              q /= la[k];
+              qi += sidx * ldia[k];
+              qo += sidx * ldoa[k];
+            }
+            xout[off_out + qo] += fac * xin[off_in + qi];
+          }
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -2105,6 +2183,27 @@ int ora_add_opblk(double* xnorm2, int64_t type, double fac, const double* xin, d
     *xnorm2 = len > 0 ? xout[0] : 0.0;
   }
   return 0;
+}
+
+int ora_add_opblk_transp(ora_ctx* c, double* xnorm2, int64_t type, double fac, int64_t list_in,
+                         int64_t iblk_in, const double* xin, int64_t list_out, int64_t iblk_out,
+                         double* xout, int64_t tra_in, int64_t tra_out, int64_t reset) {
+  GUARD_BEGIN
+  CHECK((tra_in != 0) != (tra_out != 0), "add_opblk_transp: exactly one side is transposed");
+  List& Lo = c->lists.at(list_out - 1);
+  const ListBlock& Bo = Lo.blk.at(iblk_out - 1);
+  if (reset) std::fill(xout + Bo.off_occ, xout + Bo.off_occ + Bo.len_occ, 0.0);
+  add_opblk_transp(c, c->lists.at(list_in - 1), (int)iblk_in, xin, Lo, (int)iblk_out, xout, fac,
+                   tra_in != 0, tra_out != 0);
+  if (type == 1) {
+    double sq = 0;
+    for (int64_t i = 0; i < Bo.len_occ; ++i) sq += xout[Bo.off_occ + i] * xout[Bo.off_occ + i];
+    *xnorm2 = sq;
+  } else {
+    *xnorm2 = Bo.len_occ > 0 ? xout[Bo.off_occ] : 0.0;
+  }
+  return 0;
+  GUARD_END(-1)
 }
 
 int ora_set_blas(const char* path, int64_t nthreads) {

@@ -1,7 +1,9 @@
 """GPU parity of contractions with operands used transposed (tra_op1 /
 tra_op2 / tra_op1op2): every case matches the oracle's route-2 kernel to
 1e-12 relative on the FP64 path, and to split-TF32 accuracy on a space whose
-blocks take the tensor-core path."""
+blocks take the tensor-core path.  The transposed [ADD]
+(gccu_add_block_transp, add_opblk_transp) matches the oracle's restatement
+for input and output transposed in turn."""
 import numpy as np
 import pytest
 
@@ -86,3 +88,36 @@ def test_transposed_contractions_tensor_cores(engine):
             assert np.max(np.abs(got[0] - ref)) <= RTOL * scale, (case[0], tra)
             diffs.append(np.max(np.abs(got[1] - got[0])) / scale)
     assert max(diffs) > 1e-10, "no transposed contraction took the tensor-core path"
+
+
+@pytest.mark.parametrize("space", list(SPACES))
+def test_add_block_transp_matches_oracle(engine, space):
+    # gccu_add_block_transp (add_opblk_transp) against the oracle's
+    # restatement, both sides transposed in turn, with reset, update and the
+    # returned squared norm
+    from cases import cnt_dag
+    from test_transpose_host import add_transp_variants
+    nsym, norb = SPACES[space]
+    engine.register_orbinfo(nsym, norb)
+    nrun = 0
+    for i, (occ, (g, m)) in enumerate(add_transp_variants(space)):
+        o = Oracle(nsym, norb)
+        lo, no = engine.register_list(engine.define_operator([occ]), g, m)
+        li, ni = engine.register_list(engine.define_operator([cnt_dag(occ)]), g, -m)
+        olo, _ = o.define_list(o.define_op([occ]), g, m)
+        oli, _ = o.define_list(o.define_op([cnt_dag(occ)]), g, -m)
+        if no == 0:
+            continue
+        for tra_in, tra_out in ((1, 0), (0, 1)):
+            for reset in (False, True):
+                xin, xout = random_list(ni, 5 * i + reset), random_list(no, 5 * i + 2)
+                engine.upload(li, xin)
+                engine.upload(lo, xout)
+                xn = engine.add_block_transp(-0.4, li, 1, lo, 1, tra_in, tra_out, reset, typ=1)
+                got = engine.download(lo, no)
+                ref = xout.copy()
+                xr = o.add_transp(-0.4, oli, 1, xin, olo, 1, ref, tra_in, tra_out, reset=reset)
+                assert np.max(np.abs(got - ref)) <= 1e-14 * max(1.0, np.abs(ref).max())
+                assert xn == pytest.approx(xr, rel=1e-12)
+                nrun += 1
+    assert nrun > 0

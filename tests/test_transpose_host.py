@@ -57,3 +57,53 @@ def test_engine_plans_transposed_like_explicit_copy(built, space):
                 assert n_t == n_e and np.array_equal(st_t, st_e), (case[0], sym, tra)
     finally:
         e.close()
+
+
+# classes of transposed [ADD]s: (output occupation); the input class is its
+# adjoint
+ADD_CLASSES = [gccu.occ8({gccu.P: 1}, {gccu.H: 1}), gccu.occ8({gccu.P: 2}, {gccu.H: 2}),
+               gccu.occ8({gccu.P: 1, gccu.H: 1}, {gccu.P: 1, gccu.H: 1}),
+               gccu.occ8({gccu.P: 1}, {gccu.P: 1}), gccu.occ8({gccu.P: 2}, {gccu.P: 1, gccu.H: 1})]
+
+
+def add_transp_variants(space):
+    nsym = SPACES[space][0]
+    for occ in ADD_CLASSES:
+        yield occ, (1, 0)
+        if nsym > 1:
+            yield occ, (2, 0)
+        yield occ, (1, 2)
+
+
+def _pure_excitation(occ):
+    # no hpvx type among both the creators and the annihilators
+    return not any(occ[t] > 0 and occ[4 + t] > 0 for t in range(4))
+
+
+@pytest.mark.parametrize("space", list(SPACES))
+def test_oracle_add_transp_equals_explicit_copy(built, space):
+    # add_opblk_transp (contract/add_opblk_transp.f) with tra_in:
+    # out(IC,IA) += fac * in(IA,IC), against the explicitly transposed copy of
+    # the input list.  With tra_out the output is addressed in set_op_ldim_c's
+    # A-C sequence, which for pure (de)excitation classes is the C-A one
+    # (contract/set_op_ldim_c.f:24-25): the same result there
+    from cases import cnt_dag
+    nsym, norb = SPACES[space]
+    nrun = 0
+    for i, (occ, (g, m)) in enumerate(add_transp_variants(space)):
+        for tra_in, tra_out in ((1, 0), (0, 1)):
+            if tra_out and not _pure_excitation(occ):
+                continue
+            o = Oracle(nsym, norb)
+            lo, no = o.define_list(o.define_op([occ]), g, m)
+            li, ni = o.define_list(o.define_op([cnt_dag(occ)]), g, -m)
+            if no == 0:
+                continue
+            xin, xout = random_list(ni, 3 * i), random_list(no, 3 * i + 1)
+            ref = xout + 0.6 * transpose_list(o, li, cnt_dag(occ), xin, lo, no, nsym)
+            got = xout.copy()
+            xn = o.add_transp(0.6, li, 1, xin, lo, 1, got, tra_in, tra_out)
+            assert np.max(np.abs(got - ref)) <= 1e-14 * max(1.0, np.abs(ref).max())
+            assert xn == pytest.approx(float(ref @ ref), rel=1e-12)
+            nrun += 1
+    assert nrun > 0
