@@ -19,9 +19,12 @@ route 3: gather, ILP64 OpenBLAS dgemm on all host cores, scatter) on the same
 workload and metric, each step a bounded sample of the block contractions
 extrapolated to a full iteration (the line says so).
 
-Multi-GPU: replicas only (each rank runs its own whole solve; the path is
-not sharded); the value is one replica's seconds per iteration (max over
-ranks), `throughput` the job's iterations per second.
+Multi-GPU (torchrun, one rank per GPU): one solve sharded over the ranks
+(cc.Shard, owner-computes: every rank runs its share of the output tiles of
+the residual and energy contractions, intermediates and amplitudes are
+replicated, the residuals are summed by an NCCL all-reduce per iteration);
+the value is the seconds per iteration of that solve, max over ranks
+(strong scaling).
 """
 import argparse
 import json
@@ -229,7 +232,8 @@ def run_gpu(args, cfg):
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
     eng.set_precision(args.precision)
-    solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+    solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd",
+                         shard=cc.Shard(dist) if dist else None)
     t0 = time.time()
     solver.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
     setup_s = time.time() - t0
@@ -262,7 +266,7 @@ def run_gpu(args, cfg):
         "warmup": args.warmup,
         "ms_per_step": r["ms"],
         "higher_is_better": False,
-        "scaling": "weak",
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None,
         "dtype": DTYPE[modes[0]],
         "data": data_desc(cfg) + "; inputs larger than L2 (two-electron list "
@@ -270,7 +274,8 @@ def run_gpu(args, cfg):
         "config": {"workload": cfg["name"], "method": "CCSD spin-orbital, DIIS maxsub 8",
                    "nocc": cfg["nocc"], "nvirt": cfg["nvir"], "naux": cfg["naux"],
                    "sigma_B": cfg["sigma"], "use_tr": False,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "parallelism": (f"owner-computes sharding x{world}, NCCL all-reduce of "
+                                   "the residuals" if world > 1 else "single GPU"),
                    "l2": "inputs > L2", "setup_s": round(setup_s, 2),
                    "energy_last": r["energies"][-1]},
         "roofline": roofline(r, peak, modes[0], solver, eng),
@@ -278,9 +283,6 @@ def run_gpu(args, cfg):
         "e2e": r["e2e"],
         "gpu_launches": r["launches"],
     }
-    if world > 1:
-        line["throughput"] = {"value": world / line["value"], "unit": "CC iterations/s",
-                              "note": f"{world} independent replicas, one solve per GPU"}
     if 0 in results and modes[0] != 0:
         f = results[0]
         line["fp64"] = {"metric": metric_of(cfg) + " plain FP64", "value": f["ms"] / 1e3,
@@ -288,6 +290,7 @@ def run_gpu(args, cfg):
                         "roofline": roofline(f, peak, 0, solver, eng),
                         "clocks": clock_summary(f["samples"]),
                         "energy_last": f["energies"][-1]}
+    if 0 in results and modes[0] != 0 and world == 1:
         # errors of one split-TF32 evaluation against FP64 from identical
         # amplitudes: those after two plain Jacobi iterations from zero
         reset_amplitudes(eng, solver)
@@ -314,12 +317,15 @@ def run_gpu(args, cfg):
     eng.close()
     del solver
     torch.cuda.empty_cache()
-    if not args.no_use_tr:
+    if not args.no_use_tr and world == 1:
         line["use_tr"] = measure_use_tr(args, cfg, local, dist, modes,
                                         {m: results[m]["energies"] for m in modes})
+    weights = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned"], weights = learned_stream(local, args.c4_train, args.c4_test)
     if rank == 0 and world == 1 and not args.no_convergence:
-        line["convergence"] = convergence(local, CONFIGS[args.conv_config])
-        line["convergence_small"] = convergence(local, CONFIGS[0])
+        line["convergence"] = convergence(local, CONFIGS[args.conv_config], weights)
+        line["convergence_small"] = convergence(local, CONFIGS[0], weights)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -547,12 +553,13 @@ def measured_bf16_tflops(key="bf16_tflops"):
         return FALLBACK_PEAKS[key], "fallback"
 
 
-def convergence(local, cfg):
-    """time to |dE| < 1 uEh against the converged FP64 energy: plain FP64 and
-    mixed (split TF32 until the residual norm is below 1e-5, then FP64).
-    Wall time of the solve loop (device work, energy and residual reads,
-    DIIS solves), graphs replayed after the first iteration of each mode;
-    set-up excluded, planning of the first iteration included."""
+def convergence(local, cfg, weights=None):
+    """time to |dE| < 1 uEh against the converged FP64 energy: plain FP64,
+    mixed (split TF32 until the residual norm is below 1e-5, then FP64) and,
+    given weights, mixed with the learned step.  Wall time of the solve loop
+    (device work, energy and residual reads, DIIS solves), graphs replayed
+    after the first iteration of each mode; set-up excluded, planning of the
+    first iteration included."""
     import cc
     import gccu
     import hamiltonian as hm
@@ -562,10 +569,12 @@ def convergence(local, cfg):
     out = {"workload": cfg["name"], "sigma_B": cfg["sigma"]}
     ref = None
     ref_t = None
-    for label in ("fp64", "mixed"):
+    labels = ("fp64", "mixed") + (("mixed_learned",) if weights is not None else ())
+    for label in labels:
         eng = gccu.Engine(local)
         try:
-            s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+            s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd",
+                            learned=weights if label == "mixed_learned" else None)
             s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
             eng.sync()
             hist = []
@@ -595,9 +604,94 @@ def convergence(local, cfg):
             den = sum(float(np.sum(ref_t[a] ** 2)) for a in t)
             out[label]["dE_vs_fp64"] = hist[-1][1] - ref
             out[label]["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
-    if out["mixed"]["s_to_1uEh"] and out["fp64"]["s_to_1uEh"]:
-        out["speedup_to_1uEh_mixed_vs_fp64"] = out["fp64"]["s_to_1uEh"] / out["mixed"]["s_to_1uEh"]
+        if label == "mixed_learned":
+            out[label]["fallbacks"] = s.fallbacks
+    for label in labels[1:]:
+        if out[label]["s_to_1uEh"] and out["fp64"]["s_to_1uEh"]:
+            out[f"speedup_to_1uEh_{label}_vs_fp64"] = (out["fp64"]["s_to_1uEh"] /
+                                                       out[label]["s_to_1uEh"])
     return out
+
+
+def learned_stream(local, ntrain, ntest, seed=4000):
+    """the learned preconditioner on the instance stream (n_occ ~ U[6,16],
+    n_virt ~ U[30,120], gap ~ U[0.2,0.8] Eh, n_aux 160): the first `ntrain`
+    instances are solved with plain diagonal + DIIS (FP64) while their steps
+    are sampled, the perceptron is trained on the device, and the next
+    `ntest` instances are solved plain and with the learned step; iterations
+    and wall time to |dE| < 1 uEh against each instance's plain converged
+    energy.  Returns (report, weights)."""
+    import gccu
+    import learned
+
+    insts = learned.stream(ntrain + ntest, seed)
+    rows, tg = [], []
+    t0 = time.perf_counter()
+    for inst in insts[:ntrain]:
+        eng = gccu.Engine(local)
+        try:
+            smp = learned.Sampler(seed=inst["seed"])
+            s = learned.solve(eng, inst, sampler=smp)
+            if s.history[-1][2] < 1e-8:
+                r, t = smp.targets(s)
+                rows.append(r)
+                tg.append(t)
+        finally:
+            eng.close()
+    t_collect = time.perf_counter() - t0
+    eng = gccu.Engine(local)
+    try:
+        t0 = time.perf_counter()
+        w, l0, l1 = learned.train(eng, np.concatenate(rows), np.concatenate(tg))
+        t_train = time.perf_counter() - t0
+    finally:
+        eng.close()
+    per = []
+    for inst in insts[ntrain:]:
+        res = {}
+        for label, weights in (("plain", None), ("learned", w)):
+            eng = gccu.Engine(local)
+            try:
+                stamps = []
+                t0 = time.perf_counter()
+                s = learned.solve(eng, inst, weights=weights,
+                                  callback=lambda it, en, rn: stamps.append(
+                                      time.perf_counter() - t0))
+                res[label] = (s.history, stamps, s.fallbacks)
+            finally:
+                eng.close()
+        e_ref = res["plain"][0][-1][1]
+        row = {"nocc": inst["nocc"], "nvirt": inst["nvir"], "gap": round(inst["gap"], 3)}
+        for label, (hist, stamps, fb) in res.items():
+            it = learned.iterations_to(hist, e_ref)
+            row[label] = {"iterations_to_1uEh": it,
+                          "s_to_1uEh": stamps[it - 1] if it else None,
+                          "converged": hist[-1][2] < 1e-9}
+            if label == "learned":
+                row[label]["fallbacks"] = fb
+                row[label]["dE_vs_plain"] = hist[-1][1] - e_ref
+        per.append(row)
+
+    def mean(label, key):
+        v = [r[label][key] for r in per if r[label][key] is not None]
+        return float(np.mean(v)) if v else None
+
+    report = {
+        "stream": f"{ntrain} training + {ntest} held-out instances, seed {seed}",
+        "training_rows": int(sum(len(t) for t in tg)), "train_solves_converged": len(rows),
+        "s_collect": t_collect, "s_train": t_train, "loss_before": l0, "loss_after": l1,
+        "mean_iterations_to_1uEh": {"plain": mean("plain", "iterations_to_1uEh"),
+                                    "learned": mean("learned", "iterations_to_1uEh")},
+        "mean_s_to_1uEh": {"plain": mean("plain", "s_to_1uEh"),
+                           "learned": mean("learned", "s_to_1uEh")},
+        "fallbacks_total": int(sum(r["learned"]["fallbacks"] for r in per)),
+        "held_out_not_reaching_1uEh": {
+            lab: int(sum(r[lab]["iterations_to_1uEh"] is None for r in per))
+            for lab in ("plain", "learned")},
+        "max_abs_dE_learned_vs_plain": float(max(abs(r["learned"]["dE_vs_plain"]) for r in per)),
+        "instances": per,
+    }
+    return report, w
 
 
 def run_reference(args, cfg):
@@ -723,6 +817,13 @@ def main():
                     help="skip the timing with spin-flip symmetry")
     ap.add_argument("--no-convergence", action="store_true",
                     help="skip the time-to-convergence comparisons")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned preconditioner's instance stream")
+    ap.add_argument("--c4-train", type=int, default=32,
+                    help="training instances of the learned preconditioner's stream (64: the "
+                         "full stream)")
+    ap.add_argument("--c4-test", type=int, default=16,
+                    help="held-out instances of the stream (192: the full stream)")
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")

@@ -188,14 +188,50 @@ def fill_denominators(view, n, occ, ints):
 
 # ---- solver -------------------------------------------------------------------
 
+class Shard:
+    """owner-computes evaluation over the ranks of a process group: the
+    contractions into the residual and energy lists run only this rank's
+    share of their output tiles (gccu_set_shard), [ADD]s into them count on
+    rank 0 only, the intermediates are computed in full on every rank, and
+    after each evaluation the residual and energy lists are summed over the
+    ranks; amplitudes, DIIS and the step stay replicated.  `dist` is
+    torch.distributed with an initialised group (NCCL for device lists, gloo
+    for host lists)."""
+
+    LISTS = ("R1", "R2", "E")
+
+    def __init__(self, dist):
+        self.dist = dist
+        self.rank = dist.get_rank()
+        self.n = dist.get_world_size()
+
+    def reduce(self, solver):
+        import torch
+        e = solver.e
+        e.sync()
+        for name in self.LISTS:
+            if name not in solver.lists:
+                continue
+            lid, n, _ = solver.lists[name]
+            if hasattr(e, "data"):  # host lists (the CPU oracle)
+                t = torch.from_numpy(e.data[lid])
+            else:
+                from devfill import list_tensor
+                t = list_tensor(e, lid, n)
+            self.dist.all_reduce(t)
+        if not hasattr(e, "data"):
+            torch.cuda.synchronize()
+
+
 class CCSolver:
     """Jacobi/DIIS solution of the CC amplitude equations with device-resident
     lists (solve_nleq with method=diis, solve/solve_nleq.f; diagonal step
     diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
 
     def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
-                 learned=None):
+                 learned=None, shard=None):
         self.e = engine
+        self.shard = shard  # Shard: residual contractions split over ranks
         self.ints = ints
         self.method = method
         self.use_tr = use_tr
@@ -320,19 +356,30 @@ class CCSolver:
 
     def run_item(self, it):
         """one [ADD] or [CONTR] item of the formula"""
+        sharded = self.shard is not None and it["res"][0] in Shard.LISTS
         if it["kind"] == "ADD":
             (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
-            self.e.add_block(it["fac"], li, bi, lo, bo, reset=it["reset"])
+            fac = it["fac"] if not sharded or self.shard.rank == 0 else 0.0
+            self.e.add_block(fac, li, bi, lo, bo, reset=it["reset"])
+        elif sharded:
+            self.e.set_shard(self.shard.rank, self.shard.n)
+            try:
+                self._contract(it)
+            finally:
+                self.e.set_shard(0, 1)
         else:
-            o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
-            c = np.asarray(it["cnt"])
-            occ1 = np.asarray(it["op1"][1])
-            occ2 = np.asarray(it["op2"][1])
-            ex1 = occ1 - c
-            ex2 = occ2 - np.concatenate([c[4:], c[:4]])
-            use_tr = self.use_tr and it["res"][0] not in ("E",)
-            self.e.contract(o1, o2, r, ex1, ex2, c, fact=it["fac"], update=it["update"],
-                            use_tr=use_tr)
+            self._contract(it)
+
+    def _contract(self, it):
+        o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
+        c = np.asarray(it["cnt"])
+        occ1 = np.asarray(it["op1"][1])
+        occ2 = np.asarray(it["op2"][1])
+        ex1 = occ1 - c
+        ex2 = occ2 - np.concatenate([c[4:], c[:4]])
+        use_tr = self.use_tr and it["res"][0] not in ("E",)
+        self.e.contract(o1, o2, r, ex1, ex2, c, fact=it["fac"], update=it["update"],
+                        use_tr=use_tr)
 
     def energy(self):
         return float(self.e.download(self.lid("E"), 1)[0])
@@ -428,12 +475,14 @@ class CCSolver:
         return c
 
     def iterate(self, diis=True):
-        """one CC iteration: formula evaluation, energy and residual norm,
-        amplitude update"""
+        """one CC iteration: formula evaluation (summed over the ranks when
+        sharded), energy and residual norm"""
         if self.graph is not None:
             self.e.graph_launch(self.graph)
         else:
             self.evaluate()
+        if self.shard is not None:
+            self.shard.reduce(self)
         en = self.energy()
         rn = self.residual_norm()
         return en, rn

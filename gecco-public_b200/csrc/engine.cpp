@@ -138,6 +138,13 @@ class Engine {
   int64_t tc_ws_floats = 0;
   int* d_err = nullptr;  // set by kernels whose bounded pipeline waits ran out
   int64_t wait_limit = kTcWaitLimitDefault;  // mbarrier polls per pipeline wait
+  // contractions run the tiles [ntiles*rank/nranks, ntiles*(rank+1)/nranks)
+  // of every tile list (gccu_set_shard); 0 of 1: all
+  int64_t shard_rank = 0, shard_n = 1;
+  void shard_range(int64_t ntiles, int64_t& lo, int64_t& hi) const {
+    lo = ntiles * shard_rank / shard_n;
+    hi = ntiles * (shard_rank + 1) / shard_n;
+  }
   // fixed scratch of gccu_contract_noalloc, looked up on its first call
   bool have_static = false;
   StaticScratch static_ss;
@@ -1534,8 +1541,11 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
         launch_split_tc(descs, dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather, e.stream);
         ++e.launches;
       }
-      launch_gemm(kind, descs, dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err,
-                  e.wait_limit, e.stream);
+      int64_t lo, hi;
+      e.shard_range(dp.ntiles_g[kind], lo, hi);
+      if (hi > lo)
+        launch_gemm(kind, descs, dp.d_tiles_g[kind] + lo, hi - lo, fact, e.d_err, e.wait_limit,
+                    e.stream);
       e.launches += 2;
     }
     if (dp.plan.use_tr && dp.nflip) {
@@ -1623,7 +1633,10 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
     }
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
-      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind], dp.ntiles_g[kind], fact, e.d_err,
+      int64_t lo, hi;
+      e.shard_range(dp.ntiles_g[kind], lo, hi);
+      if (hi <= lo) continue;
+      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind] + lo, hi - lo, fact, e.d_err,
                   e.wait_limit, e.stream);
       ++e.launches;
     }
@@ -1992,6 +2005,15 @@ int gccu_lp_train(int64_t steps, int64_t batch, double lr, int64_t seed, double*
                             e.stream));
     CUDA_OK(cudaStreamSynchronize(e.stream));
     if (loss) *loss = l;
+  });
+}
+
+int gccu_set_shard(int64_t rank, int64_t nranks) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(nranks >= 1 && rank >= 0 && rank < nranks, "shard: need 0 <= rank < nranks");
+    e.shard_rank = rank;
+    e.shard_n = nranks;
   });
 }
 

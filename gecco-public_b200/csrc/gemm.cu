@@ -159,16 +159,13 @@ __device__ __forceinline__ void store_tile(double (*S)[R + PAD], int fastk, int 
 template <int NT, int BN>
 constexpr int kGemmMinBlocks = NT >= 256 ? 2 : BN <= 8 ? 4 : 3;
 
+// one output tile of the grouped GEMM (a block contraction's rows m0..,
+// columns n0.., contraction range k0..k1), with the CTA's shared memory S
 template <int BM, int BN, int WARPS_M, int WARPS_N>
-__global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT,
-                                  kGemmMinBlocks<Cfg<BM, BN, WARPS_M, WARPS_N>::NT, BN>)
-    k_gemm(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
-           double alpha) {
+__device__ __forceinline__ void gemm_tile(GemmSmem<BM, BN>& S, const GemmDesc* __restrict__ descs,
+                                          const TileDesc td, double alpha) {
   using C = Cfg<BM, BN, WARPS_M, WARPS_N>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  GemmSmem<BM, BN>& S = *reinterpret_cast<GemmSmem<BM, BN>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const TileDesc td = tiles[blockIdx.x];
   {
     const int* src = reinterpret_cast<const int*>(descs + td.item);
     int* dst = reinterpret_cast<int*>(&S.d);
@@ -288,6 +285,21 @@ __global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT,
       }
 }
 
+// Persistent grouped GEMM: CTA b walks the tiles b, b + gridDim.x, ... of the
+// device work list (the tile list of one tile shape of a [CONTR])
+template <int BM, int BN, int WARPS_M, int WARPS_N>
+__global__ void __launch_bounds__(Cfg<BM, BN, WARPS_M, WARPS_N>::NT,
+                                  kGemmMinBlocks<Cfg<BM, BN, WARPS_M, WARPS_N>::NT, BN>)
+    k_gemm(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
+           int64_t ntiles, double alpha) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GemmSmem<BM, BN>& S = *reinterpret_cast<GemmSmem<BM, BN>*>(smem_raw);
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    gemm_tile<BM, BN, WARPS_M, WARPS_N>(S, descs, tiles[t], alpha);
+    __syncthreads();  // the next tile overwrites the descriptor and tables
+  }
+}
+
 // Items with at most 16 result elements (energies, thin intermediates): a
 // block reduces a chunk of the contraction index for all M*N elements.
 constexpr int kSmallThreads = 256;
@@ -343,13 +355,18 @@ void launch_gemm_cfg(const GemmDesc* descs, const TileDesc* tiles, int64_t ntile
                      cudaStream_t s) {
   using C = Cfg<BM, BN, WM, WN>;
   const size_t smem = sizeof(GemmSmem<BM, BN>);
-  static bool configured = false;
-  if (!configured) {
+  static int64_t resident = 0;  // CTAs of this shape the GPU holds at once
+  if (!resident) {
     cudaFuncSetAttribute(k_gemm<BM, BN, WM, WN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    configured = true;
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm<BM, BN, WM, WN>, C::NT, smem);
+    resident = (int64_t)std::max(nsm, 1) * std::max(per_sm, 1);
   }
-  k_gemm<BM, BN, WM, WN><<<(unsigned)ntiles, C::NT, smem, s>>>(descs, tiles, alpha);
+  const int64_t grid = std::min(ntiles, resident);
+  k_gemm<BM, BN, WM, WN><<<(unsigned)grid, C::NT, smem, s>>>(descs, tiles, ntiles, alpha);
 }
 
 }  // namespace

@@ -58,6 +58,7 @@ _SIGS = {
     "gccu_trace": [I64, I64, I64, I64, P64, ctypes.c_double, I64, I64, PD],
     "gccu_set_precision": [I64],
     "gccu_set_wait_limit": [I64],
+    "gccu_set_shard": [I64, I64],
     "gccu_lp_set_weights": [PD, I64],
     "gccu_lp_get_weights": [PD, I64],
     "gccu_lp_precondition": [I64, I64, I64, I64, ctypes.c_double, ctypes.c_double],
@@ -299,6 +300,10 @@ class Engine:
         l = np.zeros(1)
         _call("gccu_lp_train", steps, batch, lr, seed, _pd(l))
         return float(l[0])
+
+    def set_shard(self, rank=0, nranks=1):
+        """run only this rank's share of every contraction's output tiles"""
+        _call("gccu_set_shard", int(rank), int(nranks))
 
     def set_wait_limit(self, polls=-1):
         """mbarrier polls per tensor-core pipeline wait (negative: default)"""

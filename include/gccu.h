@@ -301,6 +301,14 @@ int gccu_sync(void);
  * that times out inside a kernel is reported as an error by the next call
  * that synchronises (gccu_sync, norms, downloads). */
 int gccu_set_precision(int64_t mode);
+/* Owner-computes sharding of contractions over nranks devices (one engine
+ * per rank, no counterpart in the reference): contractions run after this
+ * call execute only this rank's share of their output tiles, the contiguous
+ * range [n*rank/nranks, n*(rank+1)/nranks) of each tile list n (operand
+ * gathers and splits run in full); the host sums the partial results of the
+ * ranks (an all-reduce of the residual lists) and keeps everything else
+ * replicated.  (0, 1) restores whole contractions. */
+int gccu_set_shard(int64_t rank, int64_t nranks);
 /* Polls of one pipeline wait of the tensor-core kernel before it gives up
  * (polls < 0: the default, 4194304); on time-out the kernel stops, waits for
  * the work it has issued, sets the engine's error flag and returns, and the

@@ -237,6 +237,14 @@ def set_blas(nthreads=0, path=None):
     return path
 
 
+def set_shard(rank, nranks):
+    """each contraction computes only the block contractions dealt to this rank"""
+    L = lib()
+    L.ora_set_shard.argtypes = [I64, I64]
+    L.ora_set_shard.restype = None
+    L.ora_set_shard(rank, nranks)
+
+
 def sampling(stride):
     L = lib()
     L.ora_sampling.argtypes = [I64]

@@ -56,6 +56,10 @@ class OracleEngine:
     def zero(self, lid):
         self.data[lid][:] = 0.0
 
+    def set_shard(self, rank=0, nranks=1):
+        from binding import set_shard
+        set_shard(rank, nranks)
+
     def freeze(self, lid, frozen=True):
         pass  # host arrays: nothing is derived from a list
 

@@ -921,6 +921,8 @@ dgemm_t g_dgemm = nullptr;
 int64_t g_stride = 1, g_batch = 0, g_batches_total = 0, g_batches_done = 0;
 int64_t g_short_total = 0, g_short_done = 0;
 double g_t_always = 0, g_t_sampled = 0;
+// sharding of the block contractions over ranks (ora_set_shard)
+int64_t g_shard_rank = 0, g_shard_n = 1, g_shard_item = 0;
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
@@ -1315,6 +1317,10 @@ void contract(ora_ctx* cx, int route, int l1, int ib1, const double* x1, int l2,
                 }
                 int64_t len2 = prod(cat(lo2c, lo2a), 0, lo2c.size() + lo2a.size());
                 if (ddot_blk(xop2 + idxop2, len2) < 1e-28) continue;
+                // sharded evaluation: block contractions dealt round-robin
+                // to the ranks, each rank computes its own (the ranks' partial
+                // results sum to the whole)
+                if ((g_shard_item++) % g_shard_n != g_shard_rank) continue;
                 Blk b;
                 b.xfac = fact * fac_scal;
                 b.x1 = xop1 + idxop1;
@@ -2218,6 +2224,12 @@ int ora_set_blas(const char* path, int64_t nthreads) {
   if (nt && nthreads > 0) nt((int)nthreads);
   return 0;
   GUARD_END(-1)
+}
+
+void ora_set_shard(int64_t rank, int64_t nranks) {
+  g_shard_n = nranks > 0 ? nranks : 1;
+  g_shard_rank = (rank >= 0 && rank < g_shard_n) ? rank : 0;
+  g_shard_item = 0;
 }
 
 void ora_sampling(int64_t stride) {
