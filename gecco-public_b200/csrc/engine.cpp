@@ -52,8 +52,42 @@ struct DevGraph {
   std::map<int, int32_t*> tables;  // (idxms-1)*nsym+gam-1 -> device string table
 };
 
+// Tile shapes and routing of a contraction's block contractions: the fixed
+// rule (candidate 0) or one of the alternatives the autotuner times
+struct TilePolicy {
+  int medium_max = kGemmMediumN;  // at most this many columns (rows): the 128 x 32 FP64 tile
+  int64_t tc_min_k = kTcMinK;     // shortest contraction sent to the tensor cores
+  bool tc_thin = false;           // 9..medium_max columns go to the tensor cores too
+  bool ksplit = true;             // split contractions over CTAs when a launch has few tiles
+};
+
+// candidates per precision mode; candidate 0 is the fixed rule
+inline std::vector<TilePolicy> tile_policies(int precision) {
+  std::vector<TilePolicy> v(1);
+  if (precision == 0) {
+    TilePolicy a;
+    a.medium_max = 64;
+    v.push_back(a);
+    TilePolicy b;
+    b.ksplit = false;
+    v.push_back(b);
+  } else {
+    TilePolicy a;
+    a.tc_min_k = 128;
+    v.push_back(a);
+    TilePolicy b;
+    b.tc_min_k = 512;
+    v.push_back(b);
+    TilePolicy c;
+    c.tc_thin = true;
+    v.push_back(c);
+  }
+  return v;
+}
+
 struct DevPlan {
   Plan plan;
+  int policy = 0;  // candidate of tile_policies(precision) the plan was built with
   // grouped GEMM launches (regular / thin tiles), pack jobs, tables, scratch
   GemmDesc* d_desc[kGemmKinds] = {};
   TileDesc* d_tiles_g[kGemmKinds] = {};
@@ -194,6 +228,17 @@ class Engine {
 
   bool host_only = false;  // no device: model, layout and planning queries only
 
+  // autotuner: 0 fixed rule, 1 time the candidates at a contraction's first
+  // call (cached by block-shape histogram), 2 force candidate tune_forced
+  int tune = 0, tune_forced = 0;
+  std::map<std::string, int> tuned;  // (precision, histogram) -> chosen candidate
+  struct TuneRecord {
+    int64_t items;
+    int chosen;
+    std::vector<double> ms;  // per candidate
+  };
+  std::vector<TuneRecord> tune_log;
+
   explicit Engine(int dev, int64_t mm) : device(dev), memmax(mm), host_only(dev < 0) {
     if (host_only) return;
     CUDA_OK(cudaSetDevice(dev));
@@ -215,6 +260,10 @@ class Engine {
     if (stream) cudaStreamDestroy(stream);
   }
 
+  // allocations made while set are also recorded here (plans built on trial
+  // by the autotuner, released afterwards)
+  std::vector<std::pair<void*, size_t>>* track = nullptr;
+
   void* alloc(size_t bytes) {
     GCCU_REQUIRE(!host_only, "engine was initialised without a device (host-only mode)");
     GCCU_REQUIRE(!capturing, "device allocation requested while capturing a CUDA graph");
@@ -223,6 +272,7 @@ class Engine {
     void* p = nullptr;
     CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
     allocs.push_back(p);
+    if (track) track->push_back({p, bytes});
     mem_used += (int64_t)bytes;
     return p;
   }
@@ -583,7 +633,8 @@ class Engine {
   std::string plan_key(const gccu_bc_desc* bc, bool use_tr) const {
     std::ostringstream os;
     os << bc->list_op1 << ',' << bc->iblk_op1 << ',' << bc->list_op2 << ',' << bc->iblk_op2 << ','
-       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision << ",t"
+       << bc->list_res << ',' << bc->iblk_res << ',' << use_tr << ",p" << precision
+       << ",u" << tune << (tune == 2 ? "." + std::to_string(tune_forced) : std::string()) << ",t"
        << (bc->tra_op1 != 0) << (bc->tra_op2 != 0) << (bc->tra_res != 0);
     for (int k = 0; k < 8; ++k) os << ',' << bc->occ_ex1[k] << ',' << bc->occ_ex2[k] << ','
                                    << bc->occ_cnt[k];
@@ -632,10 +683,122 @@ class Engine {
     Plan& P = dp->plan;
     if (host_only) return *(plans[key] = std::move(dp));
     for (auto& r : P.maps) P.items[r.item].op[r.opnd].map[r.comp] = strmap(r.key);
-    build_gemm(*dp);
+    dp->policy = tune == 2 ? tune_forced : tune == 1 ? autotune(*dp) : 0;
+    build_gemm(*dp, tile_policies(precision).at(dp->policy));
     if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);
     plan_order.push_back(dp.get());
     return *(plans[key] = std::move(dp));
+  }
+
+  // the kernels of one contraction after the result's reset: cached panels
+  // (when out of date), packs, splits, the GEMMs of every tile shape (this
+  // rank's share), the spin-flip symmetrisation; evp (optional) is recorded
+  // after the packs and splits
+  void launch_plan(DevPlan& dp, double fact, cudaEvent_t evp = nullptr, bool flip = true) {
+    run_const(dp);
+    if (dp.njobs) {
+      launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, stream);
+      ++launches;
+    }
+    if (dp.nsplit) {  // operand split of the tensor-core items (after the pack it may read)
+      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather,
+                      stream);
+      ++launches;
+    }
+    if (evp) CUDA_OK(cudaEventRecord(evp, stream));
+    for (int kind = 0; kind < kGemmKinds; ++kind) {
+      if (!dp.ntiles_g[kind]) continue;
+      int64_t lo, hi;
+      shard_range(dp.ntiles_g[kind], lo, hi);
+      if (hi <= lo) continue;
+      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind] + lo, hi - lo, fact, d_err,
+                  wait_limit, stream);
+      ++launches;
+    }
+    if (flip && dp.plan.use_tr && dp.nflip) {
+      launch_sym_ab(dp.d_flip, dp.nflip, list(dp.list12).d, 0.5, dp.flip_maxlen, stream);
+      ++launches;
+    }
+  }
+
+  // block-shape histogram of a plan: per item the binary orders of M, N, K
+  // and which operands need map lookups, counted
+  static std::string histogram_key(int precision, const Plan& P) {
+    std::map<std::array<int, 6>, int> h;
+    auto lg = [](int64_t x) {
+      int b = 0;
+      while ((int64_t(1) << b) < x) ++b;
+      return b;
+    };
+    for (const auto& it : P.items)
+      h[{lg(it.M), lg(it.N), lg(it.K), it.op[0].nmap > 0, it.op[1].nmap > 0,
+         it.op[2].nmap > 0}]++;
+    std::ostringstream os;
+    os << "p" << precision;
+    for (auto& kv : h) {
+      os << ';';
+      for (int v : kv.first) os << v << ',';
+      os << kv.second;
+    }
+    return os.str();
+  }
+
+  // the candidate tile policy for a new plan: the cached choice of its
+  // histogram, else each candidate built on trial and timed on the actual
+  // lists (best of two launches, the result block restored around them)
+  int autotune(DevPlan& dp) {
+    const std::string key = histogram_key(precision, dp.plan);
+    auto f = tuned.find(key);
+    if (f != tuned.end()) return f->second;
+    const auto cands = tile_policies(precision);
+    if (cands.size() == 1) return tuned[key] = 0;
+    DevList& r = list(dp.list12);
+    double* snap = (double*)alloc(std::max<int64_t>(dp.res_len, 1) * sizeof(double));
+    CUDA_OK(cudaMemcpyAsync(snap, r.d + dp.res_off, dp.res_len * sizeof(double),
+                            cudaMemcpyDeviceToDevice, stream));
+    cudaEvent_t e0 = get_event(), e1 = get_event();
+    TuneRecord rec{(int64_t)dp.plan.items.size(), 0, {}};
+    for (size_t c = 0; c < cands.size(); ++c) {
+      std::vector<std::pair<void*, size_t>> owned;
+      auto trial = std::make_unique<DevPlan>();
+      trial->plan = dp.plan;
+      trial->list1 = dp.list1;
+      trial->list2 = dp.list2;
+      trial->list12 = dp.list12;
+      trial->res_off = dp.res_off;
+      trial->res_len = dp.res_len;
+      track = &owned;
+      double best = 1e30;
+      try {
+        build_gemm(*trial, cands[c]);
+        for (int rep = 0; rep < 2; ++rep) {
+          CUDA_OK(cudaEventRecord(e0, stream));
+          launch_plan(*trial, 1.0, nullptr, false);
+          CUDA_OK(cudaEventRecord(e1, stream));
+          CUDA_OK(cudaEventSynchronize(e1));
+          float ms = 0;
+          CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+          best = std::min(best, (double)ms);
+        }
+      } catch (...) {
+        track = nullptr;
+        throw;
+      }
+      track = nullptr;
+      CUDA_OK(cudaStreamSynchronize(stream));
+      for (auto& pr : owned) release(pr.first, pr.second);
+      rec.ms.push_back(best);
+      if (best < rec.ms[rec.chosen]) rec.chosen = (int)c;
+      CUDA_OK(cudaMemcpyAsync(r.d + dp.res_off, snap, dp.res_len * sizeof(double),
+                              cudaMemcpyDeviceToDevice, stream));
+    }
+    event_pool.push_back(e0);
+    event_pool.push_back(e1);
+    CUDA_OK(cudaStreamSynchronize(stream));
+    release(snap, std::max<int64_t>(dp.res_len, 1) * sizeof(double));
+    check_err();
+    tune_log.push_back(rec);
+    return tuned[key] = rec.chosen;
   }
 
   // offsets of the single-source components of operand od that belong to
@@ -690,7 +853,7 @@ class Engine {
   }
 
   // GEMM descriptors, offset tables, pack jobs and tiles of one plan
-  void build_gemm(DevPlan& dp) {
+  void build_gemm(DevPlan& dp, const TilePolicy& pol) {
     Plan& P = dp.plan;
     const double* x1 = list(dp.list1).d;
     const double* x2 = list(dp.list2).d;
@@ -724,9 +887,9 @@ class Engine {
       } else if (it.M <= kGemmSkinnyN) {
         kind_of[i] = kGemmSkinny;
         swapped[i] = 1;
-      } else if (it.N <= kGemmMediumN) {
+      } else if (it.N <= pol.medium_max) {
         kind_of[i] = kGemmMedium;
-      } else if (it.M <= kGemmMediumN) {
+      } else if (it.M <= pol.medium_max) {
         kind_of[i] = kGemmMedium;
         swapped[i] = 1;
       }
@@ -735,7 +898,12 @@ class Engine {
       // wastes less than a 256-wide tensor-core tile; items with fewer than
       // kTcMinK contraction indices keep FP64, their tiles would be set-up
       // and epilogue only)
-      if (precision == 1 && kind_of[i] == kGemmRegular && it.K >= kTcMinK) kind_of[i] = kGemmTc;
+      if (precision == 1 && it.K >= pol.tc_min_k &&
+          (kind_of[i] == kGemmRegular ||
+           (pol.tc_thin && kind_of[i] == kGemmMedium && !swapped[i] && it.M > kGemmMediumN))) {
+        kind_of[i] = kGemmTc;
+        swapped[i] = 0;
+      }
     }
     // an operand whose strings need map lookups is packed into a dense panel,
     // except for tensor-core items, whose split pre-pass reads it in place
@@ -927,7 +1095,7 @@ class Engine {
           ks = std::max<int64_t>(1, (d.K + kSmallChunk - 1) / kSmallChunk);
         } else if (kind == kGemmTc) {  // FP32 accumulation over at most kTcChunk indices
           ks = std::max<int64_t>(1, (d.K + kTcChunk - 1) / kTcChunk);
-        } else if (total < want && d.K > 4 * kGemmK) {
+        } else if (pol.ksplit && total < want && d.K > 4 * kGemmK) {
           ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
           ks = std::max<int64_t>(ks, 1);
         }
@@ -1616,35 +1784,13 @@ int gccu_contract(const gccu_bc_desc* bc, double fact, int64_t update, int64_t u
       ev1 = e.get_event();
       CUDA_OK(cudaEventRecord(ev0, e.stream));
     }
-    e.run_const(dp);  // cached panels of frozen operands, only when out of date
-    if (dp.njobs) {
-      launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, e.stream);
-      ++e.launches;
-    }
-    if (dp.nsplit) {  // operand split of the tensor-core items (after the pack it may read)
-      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather,
-                      e.stream);
-      ++e.launches;
-    }
-    cudaEvent_t evp = nullptr;
-    if (timed) {
-      evp = e.get_event();
-      CUDA_OK(cudaEventRecord(evp, e.stream));
-    }
-    for (int kind = 0; kind < kGemmKinds; ++kind) {
-      if (!dp.ntiles_g[kind]) continue;
-      int64_t lo, hi;
-      e.shard_range(dp.ntiles_g[kind], lo, hi);
-      if (hi <= lo) continue;
-      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind] + lo, hi - lo, fact, e.d_err,
-                  e.wait_limit, e.stream);
-      ++e.launches;
-    }
+    cudaEvent_t evp = timed ? e.get_event() : nullptr;
+    e.launch_plan(dp, fact, evp, false);
     if (timed) {
       CUDA_OK(cudaEventRecord(ev1, e.stream));
       dp.pending.push_back({ev0, evp, ev1});
+      ++dp.calls;
     }
-    if (timed) ++dp.calls;
     if (dp.plan.use_tr && dp.nflip) {
       launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);
       ++e.launches;
@@ -2014,6 +2160,34 @@ int gccu_set_shard(int64_t rank, int64_t nranks) {
     GCCU_REQUIRE(nranks >= 1 && rank >= 0 && rank < nranks, "shard: need 0 <= rank < nranks");
     e.shard_rank = rank;
     e.shard_n = nranks;
+  });
+}
+
+int gccu_set_tuning(int64_t mode, int64_t candidate) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(mode >= 0 && mode <= 2, "tuning mode must be 0, 1 or 2");
+    if (mode == 2)
+      GCCU_REQUIRE(candidate >= 0 && candidate < (int64_t)tile_policies(e.precision).size(),
+                   "no such tile-policy candidate for the current precision mode");
+    e.tune = (int)mode;
+    e.tune_forced = (int)candidate;
+  });
+}
+
+int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(nrows, "null argument");
+    *nrows = (int64_t)e.tune_log.size();
+    for (int64_t i = 0; i < std::min<int64_t>(maxrows, *nrows); ++i) {
+      const auto& t = e.tune_log[i];
+      double* r = rows + 8 * i;
+      for (int k = 0; k < 8; ++k) r[k] = -1.0;
+      r[0] = (double)t.items;
+      r[1] = (double)t.chosen;
+      for (size_t c = 0; c < t.ms.size() && c < 6; ++c) r[2 + c] = t.ms[c];
+    }
   });
 }
 

@@ -59,6 +59,8 @@ _SIGS = {
     "gccu_set_precision": [I64],
     "gccu_set_wait_limit": [I64],
     "gccu_set_shard": [I64, I64],
+    "gccu_set_tuning": [I64, I64],
+    "gccu_tuning_report": [PD, I64, P64],
     "gccu_lp_set_weights": [PD, I64],
     "gccu_lp_get_weights": [PD, I64],
     "gccu_lp_precondition": [I64, I64, I64, I64, ctypes.c_double, ctypes.c_double],
@@ -300,6 +302,17 @@ class Engine:
         l = np.zeros(1)
         _call("gccu_lp_train", steps, batch, lr, seed, _pd(l))
         return float(l[0])
+
+    def set_tuning(self, mode, candidate=0):
+        """0 fixed tile rule, 1 autotune at first call, 2 force a candidate"""
+        _call("gccu_set_tuning", int(mode), int(candidate))
+
+    def tuning_report(self):
+        """rows (block contractions, chosen candidate, ms per candidate...)"""
+        n = np.zeros(1, np.int64)
+        rows = np.zeros((256, 8))
+        _call("gccu_tuning_report", _pd(rows), 256, _p64(n))
+        return rows[: min(int(n[0]), 256)]
 
     def set_shard(self, rank=0, nranks=1):
         """run only this rank's share of every contraction's output tiles"""

@@ -316,6 +316,23 @@ int gccu_set_shard(int64_t rank, int64_t nranks);
  * reference (failure detection of the device pipeline). */
 int gccu_set_wait_limit(int64_t polls);
 
+/* Tile shapes and routing of the block contractions of contractions planned
+ * after this call (no counterpart in the reference, whose route-3 batching is
+ * fixed by str_block): mode 0 = the fixed rule (default); 1 = autotune: at a
+ * contraction's first call each candidate policy of the current precision
+ * mode (FP64: the fixed rule, the 128 x 32 tile up to 64 columns, no
+ * contraction splitting; split TF32: the fixed rule, tensor cores from 128 or
+ * from 512 contraction indices, 9..32-column blocks on the tensor cores) is
+ * built and timed on the actual lists (result restored between the trials)
+ * and the fastest is kept; the choice is cached by the plan's block-shape
+ * histogram (per block contraction the binary orders of M, N, K and which
+ * operands need map lookups) and reused for every plan with the same
+ * histogram; 2 = always the candidate `candidate` (tests). */
+int gccu_set_tuning(int64_t mode, int64_t candidate);
+/* one row of 8 per tuned histogram: (block contractions, chosen candidate,
+ * ms of candidates 0..5, -1 where there is none) */
+int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows);
+
 /* ---- statistics -----------------------------------------------------------
  * dgemm shape statistics in the reference's accounting
  * (contract/contr_blk1blk2_blocked_mm.f:454-460): [calls, sum dim1,
