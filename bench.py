@@ -232,6 +232,7 @@ def run_gpu(args, cfg):
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
     eng.set_precision(args.precision)
+    eng.set_tuning(args.tune)
     solver = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd",
                          shard=cc.Shard(dist) if dist else None)
     t0 = time.time()
@@ -303,6 +304,15 @@ def run_gpu(args, cfg):
             amplitudes="after two FP64 Jacobi iterations from T=0",
             note="mixed evaluation (split TF32, FP32 accumulation per 4096-index chunk, "
                  "FP64 sums) minus FP64 evaluation; R*_max_rel relative to max|R|")
+    if args.tune:
+        rows = eng.tuning_report()
+        line["tuning"] = {
+            "mode": "autotuned at each contraction's first call (warm-up), cached per "
+                    "block-shape histogram",
+            "histograms": len(rows),
+            "non_default_choices": int(sum(r[1] != 0 for r in rows)),
+            "rows": [{"block_contractions": int(r[0]), "chosen": int(r[1]),
+                      "ms": [round(x, 4) for x in r[2:] if x >= 0]} for r in rows]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         host_lists = {}
         for name in ("F", "V", "T1", "T2", "DT1", "DT2"):
@@ -317,6 +327,8 @@ def run_gpu(args, cfg):
     eng.close()
     del solver
     torch.cuda.empty_cache()
+    if args.tune and world == 1 and not args.no_fixed_rule:
+        line["tuning"]["fixed_rule"] = measure_fixed_rule(args, cfg, local, modes[0])
     if not args.no_use_tr and world == 1:
         line["use_tr"] = measure_use_tr(args, cfg, local, dist, modes,
                                         {m: results[m]["energies"] for m in modes})
@@ -481,6 +493,31 @@ def measure_use_tr(args, cfg, local, dist, modes, plain_energies):
         eng.close()
         torch.cuda.empty_cache()
     return out
+
+
+def measure_fixed_rule(args, cfg, local, mode):
+    """seconds per iteration of the headline mode with the fixed tile rule
+    (no autotuning), in a fresh engine on the same Hamiltonian"""
+    import torch
+
+    import cc
+    import gccu
+    from devfill import TorchIntegrals
+    import hamiltonian as hm
+
+    sp, eps, B = setup_hamiltonian(cfg)
+    eng = gccu.Engine(local)
+    try:
+        eng.set_precision(mode)
+        eng.set_tuning(0)
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+        r = measure(args, cfg, eng, s, local, None, mode, steps=max(2, args.steps // 2),
+                    profile=False, e2e=False)
+        return {"value": r["ms"] / 1e3, "unit": "s", "clocks": clock_summary(r["samples"])}
+    finally:
+        eng.close()
+        torch.cuda.empty_cache()
 
 
 def plan_rows(eng, solver, name):
@@ -817,6 +854,10 @@ def main():
                     help="skip the timing with spin-flip symmetry")
     ap.add_argument("--no-convergence", action="store_true",
                     help="skip the time-to-convergence comparisons")
+    ap.add_argument("--tune", type=int, default=1,
+                    help="1 (default): autotuned tile policies; 0: the fixed rule")
+    ap.add_argument("--no-fixed-rule", action="store_true",
+                    help="skip the fixed-rule comparison of the autotuned iteration")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned preconditioner's instance stream")
     ap.add_argument("--c4-train", type=int, default=32,
