@@ -59,6 +59,11 @@ SIGMA_SPEC = 0.05
 CONFIGS = {
     0: dict(nocc=8, nvir=32, naux=160, seed=1000, sigma=SIGMA_SPEC,
             name="CCSD C1 o8 v32 naux160", tag="ccsd_o8v32"),
+    # the sizes and point group of the CCSDT configuration (D2h, irreps
+    # round-robin), run with the CCSD formula: thousands of uneven
+    # symmetry / spin blocks per iteration
+    1: dict(nocc=6, nvir=48, naux=300, seed=1001, sigma=SIGMA_SPEC, nsym=8,
+            name="CCSD D2h o6 v48 naux300", tag="ccsd_d2h_o6v48"),
     2: dict(nocc=24, nvir=200, naux=900, seed=1002, sigma=SIGMA_SPEC,
             name="CCSD C1 o24 v200 naux900", tag="ccsd_o24v200"),
     # reduced size of the same family, used for kernel captures (a few GB)
@@ -134,7 +139,7 @@ def fp64_peak():
 def setup_hamiltonian(cfg):
     import hamiltonian as hm
     return hm.synthetic(cfg["nocc"], cfg["nvir"], cfg["naux"], seed=cfg["seed"],
-                        sigma=cfg["sigma"])
+                        sigma=cfg["sigma"], nsym=cfg.get("nsym", 1))
 
 
 def data_desc(cfg):
@@ -329,6 +334,8 @@ def run_gpu(args, cfg):
     torch.cuda.empty_cache()
     if args.tune and world == 1 and not args.no_fixed_rule:
         line["tuning"]["fixed_rule"] = measure_fixed_rule(args, cfg, local, modes[0])
+    if not args.no_d2h and world == 1:
+        line["d2h"] = measure_d2h(args, local)
     if not args.no_use_tr and world == 1:
         line["use_tr"] = measure_use_tr(args, cfg, local, dist, modes,
                                         {m: results[m]["energies"] for m in modes})
@@ -518,6 +525,43 @@ def measure_fixed_rule(args, cfg, local, mode):
     finally:
         eng.close()
         torch.cuda.empty_cache()
+
+
+def measure_d2h(args, local):
+    """the CCSD iteration on the D2h workload (the CCSDT configuration's sizes
+    and point group) in split TF32, with the fixed tile rule and autotuned:
+    seconds per iteration, block contractions and kernel launches per
+    iteration"""
+    import torch
+
+    import cc
+    import gccu
+    from devfill import TorchIntegrals
+    import hamiltonian as hm
+
+    cfg = CONFIGS[1]
+    sp, eps, B = setup_hamiltonian(cfg)
+    out = {"workload": cfg["name"], "precision": "split TF32"}
+    for tune in (0, 1):
+        eng = gccu.Engine(local)
+        try:
+            eng.set_precision(1)
+            eng.set_tuning(tune)
+            s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+            s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+            r = measure(args, cfg, eng, s, local, None, 1, steps=args.steps, profile=True,
+                        e2e=False)
+            items = int(np.sum(r["prof"][:, 3]))
+            out["autotuned" if tune else "fixed_rule"] = {
+                "value": r["ms"] / 1e3, "unit": "s", "block_contractions": items,
+                "launches_per_iteration": r["launches"] / max(args.steps, 1),
+                "energy_last": r["energies"][-1]}
+            if tune:
+                out["histograms_tuned"] = len(eng.tuning_report())
+        finally:
+            eng.close()
+            torch.cuda.empty_cache()
+    return out
 
 
 def plan_rows(eng, solver, name):
@@ -858,6 +902,8 @@ def main():
                     help="1 (default): autotuned tile policies; 0: the fixed rule")
     ap.add_argument("--no-fixed-rule", action="store_true",
                     help="skip the fixed-rule comparison of the autotuned iteration")
+    ap.add_argument("--no-d2h", action="store_true",
+                    help="skip the D2h CCSD workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned preconditioner's instance stream")
     ap.add_argument("--c4-train", type=int, default=32,

@@ -81,6 +81,10 @@ inline std::vector<TilePolicy> tile_policies(int precision) {
     TilePolicy c;
     c.tc_thin = true;
     v.push_back(c);
+    TilePolicy d;
+    d.tc_thin = true;
+    d.tc_min_k = 128;
+    v.push_back(d);
   }
   return v;
 }

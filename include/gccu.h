@@ -322,7 +322,8 @@ int gccu_set_wait_limit(int64_t polls);
  * contraction's first call each candidate policy of the current precision
  * mode (FP64: the fixed rule, the 128 x 32 tile up to 64 columns, no
  * contraction splitting; split TF32: the fixed rule, tensor cores from 128 or
- * from 512 contraction indices, 9..32-column blocks on the tensor cores) is
+ * from 512 contraction indices, 9..32-column blocks on the tensor cores from
+ * 256 or from 128 contraction indices) is
  * built and timed on the actual lists (result restored between the trials)
  * and the fastest is kept; the choice is cached by the plan's block-shape
  * histogram (per block contraction the binary orders of M, N, K and which

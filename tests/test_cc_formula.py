@@ -88,3 +88,19 @@ def test_ccsd_spin_flip_symmetry_same_iterates(hf_ints):
         hist.append(s.history)
     for (i, ea, ra), (_, eb, rb) in zip(*hist):
         assert abs(ea - eb) < 1e-12 and abs(ra - rb) < 1e-11 * max(1.0, ra), (i, ea, eb)
+
+
+def test_ccsd_synthetic_d2h(built):
+    # the benchmark family in D2h (irreps round-robin over orbitals and
+    # auxiliary functions, integrals not totally symmetric zeroed): the
+    # symmetry-blocked lists give the dense CCSD energy
+    sp, eps, B = hm.synthetic(4, 8, 24, seed=8, nsym=8)
+    assert sp.nsym == 8
+    ints = hm.FactorizedIntegrals(sp, eps, B)
+    dense = hm.DenseIntegrals(sp, np.diag(eps), ints.dense_eri())
+    F, W, no = dense_cc.spin_orbital(sp, dense.f, dense.eri_elems)
+    ed, hd = dense_cc.ccsd(F, W, no, maxiter=40, conv=1e-9)
+    s = cc.CCSolver(OracleEngine(route=3), ints, method="ccsd")
+    s.load_hamiltonian()
+    eo = s.solve(maxiter=40, conv=1e-9)
+    assert abs(ed - eo) < 1e-10
