@@ -243,6 +243,25 @@ def run_gpu(args, cfg):
     t0 = time.time()
     solver.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
     setup_s = time.time() - t0
+    if args.trace_learned:
+        # the learned step once on the doubles lists (the command profilers
+        # capture): random residual and previous step, the denominators
+        import learned
+        for name, seed in (("R2", 1), ("PT2", 2)):
+            lid, n, _ = solver.lists[name]
+            x = np.random.default_rng(seed).standard_normal(n) * 1e-3
+            eng.upload(lid, x)
+        eng.lp_set_weights(learned.initial_weights(3))
+        eng.event_record(0)
+        eng.lp_precondition(solver.lid("ST2"), solver.lid("R2"), solver.lid("DT2"),
+                            solver.lid("PT2"), fac=-1.0)
+        eng.event_record(1)
+        ms = eng.event_elapsed(0, 1)
+        n = solver.lists["T2"][1]
+        eng.close()
+        print(json.dumps({"trace": "learned step", "workload": cfg["name"], "elements": n,
+                          "ms": ms, "GB_per_s": 32.0 * n / (ms * 1e-3) / 1e9}), flush=True)
+        return
     if args.trace_contraction:
         # one formula item, run once eagerly (the command profilers capture)
         items = [it for it in solver.formula if it.get("name") == args.trace_contraction]
@@ -914,6 +933,9 @@ def main():
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")
+    ap.add_argument("--trace-learned", action="store_true",
+                    help="set up, run the learned preconditioner step once on the doubles "
+                         "lists and exit (the command the ncu captures in profiles/ run)")
     ap.add_argument("--profile-out", default=None,
                     help="write per-contraction kernel times (JSON)")
     ap.add_argument("--validate-sampling", action="store_true",
