@@ -621,18 +621,17 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
                    peak_source="cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
                                "MEASURED_PEAKS.json)")
     else:
-        # the launch is timed in the profiled iteration right after the timed
-        # loop, i.e. inside a long tensor-core run under the power cap: the
-        # sustained BF16 figure is its denominator (the burst one beside it)
-        bf16, src = measured_bf16_tflops("bf16_tflops_sustained")
-        burst, _ = measured_bf16_tflops("bf16_tflops")
-        peak = bf16 / 2.0 / 3.0
-        out.update(peak=peak,
+        # the launch is timed on its own (events around it in an eager
+        # iteration), so the burst BF16 figure is the denominator; the
+        # fraction of the sustained (power-capped) figure is given beside it
+        burst, src = measured_bf16_tflops("bf16_tflops")
+        sustained, _ = measured_bf16_tflops("bf16_tflops_sustained")
+        out.update(peak=burst / 6.0,
                    kernel=f"k_gemm_tc split TF32 (tcgen05, persistent), launch of [CONTR] "
                           f"{ROOFLINE_CONTRACTION}",
-                   peak_source=f"of {src}: bf16_tflops_sustained / 2 (dense TF32 = half of "
-                               "dense BF16) / 3 (three TF32 products per useful product)",
-                   frac_of_burst=achieved / (burst / 6.0))
+                   peak_source=f"of {src}: bf16_tflops / 2 (dense TF32 = half of dense BF16) "
+                               "/ 3 (three TF32 products per useful product)",
+                   frac_of_sustained=achieved / (sustained / 6.0))
         # the ladder end to end, its operand split included
         out["ladder_with_split_tflops"] = dom[0] / (dom[2] / dom[1] * 1e-3) / 1e12
     out["frac"] = (achieved / out["peak"]) if out["peak"] else None
