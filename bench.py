@@ -714,7 +714,9 @@ def convergence(local, cfg, weights=None):
 
 def learned_stream(local, ntrain, ntest, seed=4000):
     """the learned preconditioner on the instance stream (n_occ ~ U[6,16],
-    n_virt ~ U[30,120], gap ~ U[0.2,0.8] Eh, n_aux 160): the first `ntrain`
+    n_virt ~ U[30,120], gap ~ U[0.2,0.8] Eh, n_aux 160, B's standard deviation
+    scaled with the size so that plain diagonal + DIIS converges, see
+    learned.stream): the first `ntrain`
     instances are solved with plain diagonal + DIIS (FP64) while their steps
     are sampled, the perceptron is trained on the device, and the next
     `ntest` instances are solved plain and with the learned step; iterations
@@ -723,7 +725,7 @@ def learned_stream(local, ntrain, ntest, seed=4000):
     import gccu
     import learned
 
-    insts = learned.stream(ntrain + ntest, seed)
+    insts = learned.stream(ntrain + ntest, seed, scale_sigma=True)
     rows, tg = [], []
     t0 = time.perf_counter()
     for inst in insts[:ntrain]:
@@ -738,6 +740,9 @@ def learned_stream(local, ntrain, ntest, seed=4000):
         finally:
             eng.close()
     t_collect = time.perf_counter() - t0
+    if not rows:
+        return {"stream": f"{ntrain} training instances, seed {seed}",
+                "error": "no training solve converged"}, None
     eng = gccu.Engine(local)
     try:
         t0 = time.perf_counter()
@@ -776,7 +781,8 @@ def learned_stream(local, ntrain, ntest, seed=4000):
         return float(np.mean(v)) if v else None
 
     report = {
-        "stream": f"{ntrain} training + {ntest} held-out instances, seed {seed}",
+        "stream": f"{ntrain} training + {ntest} held-out instances, seed {seed}, "
+                  "sigma_B = 0.035 (180/(n_occ n_virt))^(1/4)",
         "training_rows": int(sum(len(t) for t in tg)), "train_solves_converged": len(rows),
         "s_collect": t_collect, "s_train": t_train, "loss_before": l0, "loss_after": l1,
         "mean_iterations_to_1uEh": {"plain": mean("plain", "iterations_to_1uEh"),

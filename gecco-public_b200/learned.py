@@ -15,6 +15,11 @@ loss, the gradient and the Adam steps run on the device.
 Instance stream: seeded synthetic closed-shell CCSD Hamiltonians with
 n_occ ~ U[6,16], n_virt ~ U[30,120], a HOMO-LUMO gap ~ U[0.2,0.8] Eh and the
 integral distribution of the benchmark family (n_aux = 160, B ~ N(0, 0.05^2)).
+With that distribution the doubles coupling grows like sqrt(n_occ n_virt)
+against fixed gaps and plain diagonal + DIIS stalls or diverges from about
+n_virt = 60 on; scale_sigma draws B with the standard deviation
+0.035 (180 / (n_occ n_virt))^(1/4) instead, which keeps every size of the
+stream convergent.
 """
 import numpy as np
 
@@ -25,20 +30,23 @@ LP_SAMPLES = 2048  # sampled elements per amplitude list and step
 TRAIN = dict(steps=3000, batch=8192, lr=3e-3)
 
 
-def stream(n, seed=4000, nocc=(6, 16), nvir=(30, 120), gap=(0.2, 0.8), naux=160):
-    """instance parameters (nocc, nvir, naux, gap, seed), seeded"""
+def stream(n, seed=4000, nocc=(6, 16), nvir=(30, 120), gap=(0.2, 0.8), naux=160,
+           sigma=0.05, scale_sigma=False):
+    """instance parameters (nocc, nvir, naux, gap, sigma, seed), seeded"""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n):
-        out.append(dict(nocc=int(rng.integers(nocc[0], nocc[1] + 1)),
-                        nvir=int(rng.integers(nvir[0], nvir[1] + 1)),
-                        naux=naux, gap=float(rng.uniform(*gap)), seed=seed + 1 + k))
+        o = int(rng.integers(nocc[0], nocc[1] + 1))
+        v = int(rng.integers(nvir[0], nvir[1] + 1))
+        sg = 0.035 * (180.0 / (o * v)) ** 0.25 if scale_sigma else sigma
+        out.append(dict(nocc=o, nvir=v, naux=naux, gap=float(rng.uniform(*gap)), sigma=sg,
+                        seed=seed + 1 + k))
     return out
 
 
 def hamiltonian(inst):
     return hm.synthetic(inst["nocc"], inst["nvir"], inst["naux"], seed=inst["seed"],
-                        gap=inst["gap"])
+                        gap=inst["gap"], sigma=inst.get("sigma", 0.05))
 
 
 class Sampler:
