@@ -233,7 +233,8 @@ def run_gpu(args, cfg):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    peak = fp64_peak() if rank == 0 and not args.trace_contraction else None
+    tracing = args.trace_contraction or args.trace_learned
+    peak = fp64_peak() if rank == 0 and not tracing else None
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
     eng.set_precision(args.precision)
