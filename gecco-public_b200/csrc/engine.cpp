@@ -294,10 +294,15 @@ class Engine {
     if (floats <= tc_ws_floats) return;
     GCCU_REQUIRE(!capturing, "split-TF32 workspace must grow outside a graph capture");
     CUDA_OK(cudaStreamSynchronize(stream));  // earlier launches may still read it
+    // the workspace belongs to the engine, not to the plan being built: it is
+    // never recorded for release with a trial plan of the autotuner
+    auto* saved = track;
+    track = nullptr;
     if (tc_ws) release(tc_ws, (size_t)tc_ws_floats * sizeof(float));
     tc_ws = nullptr;
     tc_ws_floats = 0;
     tc_ws = (float*)alloc((size_t)floats * sizeof(float));
+    track = saved;
     tc_ws_floats = floats;
     CUDA_OK(set_tc_workspace(tc_ws));
   }
