@@ -233,6 +233,13 @@ def run_gpu(args, cfg):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.only_convergence:
+        cfgc = dict(CONFIGS[args.conv_config])
+        if args.conv_sigma:
+            cfgc["sigma"] = args.conv_sigma
+            cfgc["name"] += f" (B std {args.conv_sigma})"
+        print(json.dumps({"convergence": convergence(local, cfgc)}), flush=True)
+        return
     tracing = args.trace_contraction or args.trace_learned
     peak = fp64_peak() if rank == 0 and not tracing else None
     sp, eps, B = setup_hamiltonian(cfg)
@@ -911,6 +918,10 @@ def main():
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--conv-config", type=int, default=12,
                     help="workload of the time-to-convergence comparison")
+    ap.add_argument("--conv-sigma", type=float, default=None,
+                    help="standard deviation of B for the convergence workload (override)")
+    ap.add_argument("--only-convergence", action="store_true",
+                    help="run only the time-to-convergence comparison and exit")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -19,8 +19,10 @@
 // shared memory), k_lp_rows (inputs of sampled elements), k_lp_grad (forward
 // and backward of 128 rows per block, per-block gradient sums reduced in
 // shared memory), k_lp_reduce (block sums -> gradient and loss), k_lp_adam
-// (Adam update).  Everything in FP64, so the gradients equal a CPU
-// restatement to rounding.
+// (Adam update).  Training is FP64, so the gradients equal a CPU
+// restatement to rounding; the step applied in the solve runs the
+// perceptron in FP32 (its factor to about 1e-6 relative; the inputs, the
+// plain step and the product stay FP64).
 #include <cstdint>
 
 #include "kernels.hpp"
@@ -72,25 +74,25 @@ __device__ __forceinline__ double forward(const double* __restrict__ w, const do
   return o;
 }
 
-// o = MLP(x) without keeping the second hidden layer (inference); the first
-// hidden layer goes to the thread's row h1 of shared memory, so that few
-// values stay live across the FP64 tanh evaluations
-__device__ __forceinline__ double forward_o(const double* __restrict__ w, const double (&x)[NI],
-                                            double* __restrict__ h1) {
-#pragma unroll 4
-  for (int j = 0; j < NH; ++j) {
-    double a = w[OB1 + j];
+// o = MLP(x) in FP32 for inference (weights in shared memory as floats,
+// the first hidden layer in registers): the factor 1 + tanh(o) to about
+// 1e-6 relative, at the FP32 pipe's rate
+__device__ __forceinline__ float forward_f32(const float* __restrict__ w, const float (&x)[NI]) {
+  float h1[NH];
 #pragma unroll
-    for (int i = 0; i < NI; ++i) a = fma(w[OW1 + j * NI + i], x[i], a);
-    h1[j] = tanh(a);
+  for (int j = 0; j < NH; ++j) {
+    float a = w[OB1 + j];
+#pragma unroll
+    for (int i = 0; i < NI; ++i) a = fmaf(w[OW1 + j * NI + i], x[i], a);
+    h1[j] = tanhf(a);
   }
-  double o = w[OB3];
+  float o = w[OB3];
 #pragma unroll 1
   for (int j = 0; j < NH; ++j) {
-    double a = w[OB2 + j];
-#pragma unroll 8
-    for (int k = 0; k < NH; ++k) a = fma(w[OW2 + j * NH + k], h1[k], a);
-    o = fma(w[OW3 + j], tanh(a), o);
+    float a = w[OB2 + j];
+#pragma unroll
+    for (int k = 0; k < NH; ++k) a = fmaf(w[OW2 + j * NH + k], h1[k], a);
+    o = fmaf(w[OW3 + j], tanhf(a), o);
   }
   return o;
 }
@@ -132,20 +134,18 @@ __device__ __forceinline__ void inv_rms(const double* acc, int64_t n, double& is
   ip = mp > 0.0 ? rsqrt(mp) : 0.0;
 }
 
-constexpr int kApplyThreads = 128;
+constexpr int kApplyThreads = 256;
 
-// out[i] = s_i * (1 + tanh(o_i))
-__global__ void __launch_bounds__(kApplyThreads)
+// out[i] = s_i * (1 + tanh(o_i)); inputs and the plain step in FP64, the
+// perceptron in FP32
+__global__ void __launch_bounds__(kApplyThreads, 2)
     k_lp_apply(double* __restrict__ out, const double* __restrict__ in,
                const double* __restrict__ diag, const double* __restrict__ prev, double fac,
                double shift, int64_t n, const double* __restrict__ acc,
                const double* __restrict__ weights) {
-  __shared__ double w[kLpWeights];
-  // per thread a row of NH + 1 doubles (odd stride: rows on distinct banks)
-  __shared__ double hs[kApplyThreads * (NH + 1)];
-  for (int i = threadIdx.x; i < kLpWeights; i += blockDim.x) w[i] = weights[i];
+  __shared__ float w[kLpWeights];
+  for (int i = threadIdx.x; i < kLpWeights; i += blockDim.x) w[i] = (float)weights[i];
   __syncthreads();
-  double* h1 = hs + threadIdx.x * (NH + 1);
   double is, ip;
   inv_rms(acc, n, is, ip);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -154,7 +154,8 @@ __global__ void __launch_bounds__(kApplyThreads)
     const double s = fac * in[i] / d;
     double x[NI];
     inputs(d, s, prev ? prev[i] : 0.0, is, ip, x);
-    out[i] = s * (1.0 + tanh(forward_o(w, x, h1)));
+    const float xf[NI] = {(float)x[0], (float)x[1], (float)x[2]};
+    out[i] = s * (double)(1.0f + tanhf(forward_f32(w, xf)));
   }
 }
 

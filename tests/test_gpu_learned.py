@@ -1,6 +1,7 @@
 """The learned correction of the diagonal step (gccu_lp_*): its device
 kernels against the CPU restatement in oracle/mlp.py (loss and gradient over
-a training set at 1e-10 relative, corrected step and sampled rows at 1e-12),
+a training set at 1e-10 relative, sampled rows at 1e-12, the corrected step,
+whose perceptron runs in FP32, at 1e-5),
 training lowers the loss, and on held-out instances of a small stream of
 synthetic CCSD Hamiltonians the learned step reaches |dE| < 1 uEh in fewer
 iterations than plain diagonal + DIIS, at the same converged energy."""
@@ -79,7 +80,8 @@ def test_step_and_rows_match_cpu(engine):
         engine.lp_precondition(lo, li, ld, prev, fac=-1.0, shift=0.05)
         got = engine.download(lo, n)
         ref = mlp.step(w, r, d, pv, fac=-1.0, shift=0.05)
-        assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+        # the perceptron runs in FP32 in the solve's step: its factor to ~1e-6
+        assert np.max(np.abs(got - ref)) <= 1e-5 * np.max(np.abs(ref))
     idx = np.random.default_rng(9).choice(n, 50, replace=False)
     rows = engine.lp_rows(li, ld, lp, la, idx, fac=-1.0, shift=0.05)
     x, s = mlp.inputs(r, d, p, fac=-1.0, shift=0.05)
