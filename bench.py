@@ -288,7 +288,7 @@ def run_gpu(args, cfg):
     for mode in modes:
         reset_amplitudes(eng, solver)
         eng.set_precision(mode)
-        results[mode] = measure(args, cfg, eng, solver, local, dist, mode)
+        results[mode] = measure(args, cfg, eng, solver, local, dist, mode, main=True)
     r = results[modes[0]]
     line = {
         "metric": metric_of(cfg),
@@ -406,7 +406,8 @@ def max_over_ranks(value, dist):
     return float(t.item())
 
 
-def measure(args, cfg, eng, solver, local, dist, mode, steps=None, profile=True, e2e=True):
+def measure(args, cfg, eng, solver, local, dist, mode, steps=None, profile=True, e2e=True,
+            main=False):
     """warm-up (plans every contraction in this precision mode), the timed
     graph-replayed iterations, one eagerly profiled iteration and the
     end-to-end iterations through host buffers"""
@@ -451,7 +452,8 @@ def measure(args, cfg, eng, solver, local, dist, mode, steps=None, profile=True,
         if len(names) != len(prof):
             raise RuntimeError(f"profile rows ({len(prof)}) do not match contractions "
                                f"({len(names)})")
-        if args.profile_out and mode == args.precision and int(os.environ.get("RANK", 0)) == 0:
+        if (args.profile_out and main and mode == args.precision and
+                int(os.environ.get("RANK", 0)) == 0):
             with open(args.profile_out, "w") as f:
                 json.dump([{"item": n, "gflop": r[0] / 1e9, "ms": r[2] / max(r[1], 1),
                             "tflops": (r[0] / (r[2] / max(r[1], 1) * 1e-3) / 1e12
