@@ -205,7 +205,7 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
 
-__global__ void __launch_bounds__(kSplitThreads, 6)
+__global__ void __launch_bounds__(kSplitThreads, 4)
     k_split_tc(const GemmDesc* __restrict__ descs, const SplitJob* __restrict__ jobs,
                int64_t njobs, const PackJob* __restrict__ gathers) {
   __shared__ __align__(16) float sh[2][8 * kSplitPitch];
@@ -257,29 +257,9 @@ __global__ void __launch_bounds__(kSplitThreads, 6)
     const int64_t rof = ro[r], kof = ko[k];
     return (rof >= 0 && kof >= 0) ? __ldg(x + rof + kof) : 0.0;
   };
-  // element of a map-addressed operand
-  auto mapped_elem = [&](int r, int k) -> double {
-    const int64_t rof = ro[r], kof = ko[k];
-    if (rof < 0 || kof < 0) return 0.0;
-    int64_t off = rof + kof;
-    bool neg = false;
-    for (int m = 0; m < G.nm; ++m) {
-      const int32_t ir = rmi_s[m][r], ik = kmi_s[m][k];
-      const bool r1 = G.row_is_1[m] != 0;
-      int v = __ldg(G.map[m] + (int64_t)(r1 ? ik : ir) * G.n1[m] + (r1 ? ir : ik));
-      if (v == 0) return 0.0;
-      if (v < 0) {
-        neg = !neg;
-        v = -v;
-      }
-      off += (int64_t)(v - 1) * G.ldim[m];
-    }
-    const double val = __ldg(x + off);
-    return neg ? -val : val;
-  };
-  // staging of one chunk: thread mappings per read direction, the element
-  // function a template argument so that the direct path keeps its loads
-  // independent (no map branch between them)
+  // staging of one chunk of a direct operand: thread mappings per read
+  // direction, the element function a template argument so that the loads
+  // stay independent (no map branch between them)
   auto stage = [&](auto&& elem) {
     if (kfast) {  // warp: 16 rows, lane: contraction index
       const int warp = tid >> 5, lane = tid & 31;
@@ -306,8 +286,95 @@ __global__ void __launch_bounds__(kSplitThreads, 6)
       }
     }
   };
+  // map-addressed operand: eight elements at a time, their map lookups of
+  // each component issued together, then their value loads, so that the
+  // dependent loads of different elements overlap (rows or indices outside
+  // the block have ro / ko < 0 and load nothing)
+  auto gather8 = [&](const int (&rr)[8], const int (&kk)[8], double (&val)[8]) {
+    int64_t off[8];
+    bool ok[8], neg[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int64_t rof = ro[rr[e]], kof = ko[kk[e]];
+      ok[e] = rof >= 0 && kof >= 0;
+      off[e] = ok[e] ? rof + kof : 0;
+      neg[e] = false;
+    }
+    for (int m = 0; m < G.nm; ++m) {
+      const bool r1 = G.row_is_1[m] != 0;
+      const int32_t* __restrict__ mp = G.map[m];
+      const int64_t n1 = G.n1[m], ld = G.ldim[m];
+      int v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int32_t ir = rmi_s[m][rr[e]], ik = kmi_s[m][kk[e]];
+        v[e] = ok[e] ? __ldg(mp + (int64_t)(r1 ? ik : ir) * n1 + (r1 ? ir : ik)) : 1;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        int w = v[e];
+        if (w == 0) ok[e] = false;
+        if (w < 0) {
+          neg[e] = !neg[e];
+          w = -w;
+        }
+        off[e] += (int64_t)(w - 1) * ld;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const double x0 = ok[e] ? __ldg(x + off[e]) : 0.0;
+      val[e] = neg[e] ? -x0 : x0;
+    }
+  };
+  auto stage_mapped = [&]() {
+    if (kfast) {  // warp: 16 rows, lane: contraction index
+      const int warp = tid >> 5, lane = tid & 31;
+#pragma unroll 1
+      for (int i0 = 0; i0 < 16; i0 += 8) {
+        int rr[8], kk[8];
+        double v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          rr[e] = warp * 16 + i0 + e;
+          kk[e] = lane;
+        }
+        gather8(rr, kk, v);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          float h, l;
+          split_tf32(v[e], h, l);
+          sh[0][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = h;
+          sh[1][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = l;
+        }
+      }
+    } else {  // thread: one row, 16 contraction indices
+      const int r = tid & 127, kh = tid >> 7;
+#pragma unroll 1
+      for (int q0 = 0; q0 < 4; q0 += 2) {
+        int rr[8], kk[8];
+        double v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          rr[e] = r;
+          kk[e] = 16 * kh + 4 * q0 + e;
+        }
+        gather8(rr, kk, v);
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {
+          float4 h4, l4;
+          float* hp = &h4.x;
+          float* lp = &l4.x;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) split_tf32(v[4 * qq + e], hp[e], lp[e]);
+          *reinterpret_cast<float4*>(&sh[0][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = h4;
+          *reinterpret_cast<float4*>(&sh[1][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = l4;
+        }
+      }
+    }
+  };
   if (gat)
-    stage(mapped_elem);
+    stage_mapped();
   else
     stage(direct);
   __syncthreads();

@@ -34,6 +34,7 @@ constexpr int NH = kLpHidden, NI = kLpInputs;
 constexpr int OW1 = 0, OB1 = OW1 + NH * NI, OW2 = OB1 + NH, OB2 = OW2 + NH * NH,
               OW3 = OB2 + NH, OB3 = OW3 + NH;
 static_assert(OB3 + 1 == kLpWeights, "weight layout");
+static_assert(OW2 % 4 == 0 && NH % 4 == 0, "rows of W2 start on 16-byte boundaries");
 
 __device__ __forceinline__ double clampd(double x, double lo, double hi) {
   return x < lo ? lo : (x > hi ? hi : x);
@@ -74,27 +75,48 @@ __device__ __forceinline__ double forward(const double* __restrict__ w, const do
   return o;
 }
 
-// o = MLP(x) in FP32 for inference (weights in shared memory as floats,
-// the first hidden layer in registers): the factor 1 + tanh(o) to about
-// 1e-6 relative, at the FP32 pipe's rate
-__device__ __forceinline__ float forward_f32(const float* __restrict__ w, const float (&x)[NI]) {
-  float h1[NH];
+// o = MLP(x) in FP32 for inference of two elements at once (weights in
+// shared memory as floats, the first hidden layer of both in registers):
+// every weight read from shared memory (four at a time) feeds both
+// elements, so the shared-memory pipe is not the bound; the factor
+// 1 + tanh(o) to about 1e-6 relative
+__device__ __forceinline__ void forward_f32x2(const float* __restrict__ w,
+                                              const float (&xa)[NI], const float (&xb)[NI],
+                                              float& oa, float& ob) {
+  float ha[NH], hb[NH];
 #pragma unroll
   for (int j = 0; j < NH; ++j) {
-    float a = w[OB1 + j];
+    float a = w[OB1 + j], b = a;
 #pragma unroll
-    for (int i = 0; i < NI; ++i) a = fmaf(w[OW1 + j * NI + i], x[i], a);
-    h1[j] = tanhf(a);
+    for (int i = 0; i < NI; ++i) {
+      const float wi = w[OW1 + j * NI + i];
+      a = fmaf(wi, xa[i], a);
+      b = fmaf(wi, xb[i], b);
+    }
+    ha[j] = tanhf(a);
+    hb[j] = tanhf(b);
   }
-  float o = w[OB3];
+  oa = ob = w[OB3];
 #pragma unroll 1
   for (int j = 0; j < NH; ++j) {
-    float a = w[OB2 + j];
+    float a = w[OB2 + j], b = a;
+    const float4* w4 = reinterpret_cast<const float4*>(w + OW2 + j * NH);
 #pragma unroll
-    for (int k = 0; k < NH; ++k) a = fmaf(w[OW2 + j * NH + k], h1[k], a);
-    o = fmaf(w[OW3 + j], tanhf(a), o);
+    for (int k = 0; k < NH; k += 4) {
+      const float4 v = w4[k / 4];
+      a = fmaf(v.x, ha[k], a);
+      b = fmaf(v.x, hb[k], b);
+      a = fmaf(v.y, ha[k + 1], a);
+      b = fmaf(v.y, hb[k + 1], b);
+      a = fmaf(v.z, ha[k + 2], a);
+      b = fmaf(v.z, hb[k + 2], b);
+      a = fmaf(v.w, ha[k + 3], a);
+      b = fmaf(v.w, hb[k + 3], b);
+    }
+    const float w3 = w[OW3 + j];
+    oa = fmaf(w3, tanhf(a), oa);
+    ob = fmaf(w3, tanhf(b), ob);
   }
-  return o;
 }
 
 constexpr int kRedThreads = 256;
@@ -143,19 +165,28 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
                const double* __restrict__ diag, const double* __restrict__ prev, double fac,
                double shift, int64_t n, const double* __restrict__ acc,
                const double* __restrict__ weights) {
-  __shared__ float w[kLpWeights];
+  __shared__ __align__(16) float w[kLpWeights + 3];
   for (int i = threadIdx.x; i < kLpWeights; i += blockDim.x) w[i] = (float)weights[i];
   __syncthreads();
   double is, ip;
   inv_rms(acc, n, is, ip);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double d = denom(diag[i], shift);
-    const double s = fac * in[i] / d;
-    double x[NI];
-    inputs(d, s, prev ? prev[i] : 0.0, is, ip, x);
-    const float xf[NI] = {(float)x[0], (float)x[1], (float)x[2]};
-    out[i] = s * (double)(1.0f + tanhf(forward_f32(w, xf)));
+  // elements i and i + blockDim.x of each pass of 2 * blockDim.x (coalesced)
+  const int64_t pass = 2 * (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = 2 * (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += pass) {
+    const int64_t i1 = i0 + blockDim.x;
+    const bool has1 = i1 < n;
+    const double d0 = denom(diag[i0], shift), s0 = fac * in[i0] / d0;
+    const double d1 = has1 ? denom(diag[i1], shift) : 1.0;
+    const double s1 = has1 ? fac * in[i1] / d1 : 0.0;
+    double x0[NI], x1[NI];
+    inputs(d0, s0, prev ? prev[i0] : 0.0, is, ip, x0);
+    inputs(d1, s1, prev && has1 ? prev[i1] : 0.0, is, ip, x1);
+    const float xa[NI] = {(float)x0[0], (float)x0[1], (float)x0[2]};
+    const float xb[NI] = {(float)x1[0], (float)x1[1], (float)x1[2]};
+    float oa, ob;
+    forward_f32x2(w, xa, xb, oa, ob);
+    out[i0] = s0 * (double)(1.0f + tanhf(oa));
+    if (has1) out[i1] = s1 * (double)(1.0f + tanhf(ob));
   }
 }
 
@@ -328,8 +359,9 @@ void launch_lp_apply(double* out, const double* in, const double* diag, const do
                      double fac, double shift, int64_t n, const double* acc,
                      const double* weights, cudaStream_t s) {
   if (n == 0) return;
-  k_lp_apply<<<grid_for(n, kApplyThreads), kApplyThreads, 0, s>>>(out, in, diag, prev, fac,
-                                                                   shift, n, acc, weights);
+  // two elements per thread
+  k_lp_apply<<<grid_for((n + 1) / 2, kApplyThreads), kApplyThreads, 0, s>>>(
+      out, in, diag, prev, fac, shift, n, acc, weights);
 }
 
 void launch_lp_rows(const double* in, const double* diag, const double* prev, const double* amp,
