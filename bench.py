@@ -69,12 +69,14 @@ CONFIGS = {
     # reduced size of the same family, used for kernel captures (a few GB)
     10: dict(nocc=12, nvir=100, naux=450, seed=1010, sigma=SIGMA_SPEC,
              name="CCSD C1 o12 v100 naux450", tag="ccsd_o12v100"),
-    # the o24/v200 shape with B's standard deviation scaled so that the
-    # exchange integrals naux*sigma^2 equal those of o8/v32 naux160 (0.4 Eh);
-    # with sigma = 0.05 at naux = 900 they are 2.25 Eh, above most orbital
-    # gaps, and the CC iteration diverges
-    12: dict(nocc=24, nvir=200, naux=900, seed=1002, sigma=SIGMA_SPEC * math.sqrt(160 / 900),
-             name="CCSD C1 o24 v200 naux900, B std 0.0211", tag="ccsd_o24v200_conv"),
+    # the o24/v200 shape with a smaller standard deviation of B: with
+    # sigma = 0.05 at naux = 900 the exchange integrals naux*sigma^2 are
+    # 2.25 Eh, above most orbital gaps, and the CC iteration diverges, as it
+    # does at 0.0211 (the o8/v32 value of naux*sigma^2) and at 0.013; at
+    # 0.007 plain FP64 diagonal + DIIS converges to a residual norm of 1e-9
+    # in about 40 iterations
+    12: dict(nocc=24, nvir=200, naux=900, seed=1002, sigma=0.007,
+             name="CCSD C1 o24 v200 naux900, B std 0.007", tag="ccsd_o24v200_conv"),
 }
 
 
@@ -238,8 +240,9 @@ def run_gpu(args, cfg):
         if args.conv_sigma:
             cfgc["sigma"] = args.conv_sigma
             cfgc["name"] += f" (B std {args.conv_sigma})"
-        print(json.dumps({"convergence": convergence(local, cfgc, maxiter=args.conv_maxiter)}),
-              flush=True)
+        variants = json.loads(args.conv_variants) if args.conv_variants else None
+        print(json.dumps({"convergence": convergence(local, cfgc, maxiter=args.conv_maxiter,
+                                                     variants=variants)}), flush=True)
         return
     tracing = args.trace_contraction or args.trace_learned
     peak = fp64_peak() if rank == 0 and not tracing else None
@@ -668,13 +671,18 @@ def measured_bf16_tflops(key="bf16_tflops"):
         return FALLBACK_PEAKS[key], "fallback"
 
 
-def convergence(local, cfg, weights=None, maxiter=80):
+def convergence(local, cfg, weights=None, maxiter=80, mixed_opts=None, variants=None):
     """time to |dE| < 1 uEh against the converged FP64 energy: plain FP64,
-    mixed (split TF32 until the residual norm is below 1e-5, then FP64) and,
-    given weights, mixed with the learned step.  Wall time of the solve loop
-    (device work, energy and residual reads, DIIS solves), graphs replayed
-    after the first iteration of each mode; set-up excluded, planning of the
-    first iteration included."""
+    mixed (split TF32 until the residual norm is below 1e-5 or stops
+    falling, then FP64; options of CCSolver.solve_mixed in `mixed_opts`)
+    and, given weights, mixed with the learned step; `variants` maps further
+    labels to solve_mixed options.  Wall time of the solve loop (device work,
+    energy and residual reads, DIIS solves), graphs replayed after the first
+    iteration of each mode; set-up excluded, planning of the first iteration
+    included."""
+    opts = dict(switch=1e-5, stall=1.0)
+    opts.update(mixed_opts or {})
+    variants = dict(variants or {})
     import cc
     import gccu
     import hamiltonian as hm
@@ -684,7 +692,8 @@ def convergence(local, cfg, weights=None, maxiter=80):
     out = {"workload": cfg["name"], "sigma_B": cfg["sigma"]}
     ref = None
     ref_t = None
-    labels = ("fp64", "mixed") + (("mixed_learned",) if weights is not None else ())
+    labels = ("fp64", "mixed") + (("mixed_learned",) if weights is not None else ()) + \
+        tuple(variants)
     for label in labels:
         eng = gccu.Engine(local)
         try:
@@ -701,7 +710,8 @@ def convergence(local, cfg, weights=None, maxiter=80):
             if label == "fp64":
                 s.solve(maxiter=maxiter, conv=1e-9, use_graph=True, callback=cb)
             else:
-                s.solve_mixed(maxiter=maxiter, conv=1e-9, switch=1e-5, callback=cb)
+                s.solve_mixed(maxiter=maxiter, conv=1e-9, callback=cb,
+                              **dict(opts, **variants.get(label, {})))
             t = {a: eng.download(s.lid(a), s.lists[a][1]) for a in s.amps}
         finally:
             eng.close()
@@ -720,6 +730,9 @@ def convergence(local, cfg, weights=None, maxiter=80):
             den = sum(float(np.sum(ref_t[a] ** 2)) for a in t)
             out[label]["dE_vs_fp64"] = hist[-1][1] - ref
             out[label]["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
+        out[label]["s_first_iteration"] = hist[0][3]
+        if label != "fp64":
+            out[label]["switched_at"] = s.switched_at
         if label == "mixed_learned":
             out[label]["fallbacks"] = s.fallbacks
     for label in labels[1:]:
@@ -930,6 +943,9 @@ def main():
     ap.add_argument("--conv-sigma", type=float, default=None,
                     help="standard deviation of B for the convergence workload (override)")
     ap.add_argument("--conv-maxiter", type=int, default=80)
+    ap.add_argument("--conv-variants", default=None,
+                    help="JSON object: label -> options of CCSolver.solve_mixed, solved "
+                         "after the default variants (with --only-convergence)")
     ap.add_argument("--only-convergence", action="store_true",
                     help="run only the time-to-convergence comparison and exit")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)

@@ -493,19 +493,26 @@ class CCSolver:
         self.evaluate()
         self.graph = self.e.graph_end()
 
-    def solve_mixed(self, maxiter=60, conv=1e-8, switch=1e-5, callback=None, stop=None):
+    def solve_mixed(self, maxiter=60, conv=1e-8, switch=1e-5, callback=None, stop=None,
+                    stall=None, reset_diis=False, final=0):
         """Mixed-precision solve: the contractions run in split TF32 on the
         tensor cores (engine precision 1) while the residual norm is above
-        `switch`, in FP64 after that; the CC fixed-point iteration corrects
-        the errors of the cheaper iterations, the DIIS subspace, residuals,
-        energies and amplitude updates stay FP64 throughout.  Each mode's
-        evaluation runs once eagerly (planning) and is then replayed from its
-        own CUDA graph.  stop(it, energy, residual) may end the solve early.
-        Returns the last energy."""
+        `switch`, and in precision `final` (0 = FP64) after that; the CC
+        fixed-point iteration corrects the errors of the cheaper iterations,
+        the DIIS subspace, residuals, energies and amplitude updates stay FP64
+        throughout.  With `stall`, the solve also switches once a split-TF32
+        residual norm is above `stall` times the previous one (the residual
+        has reached the split-TF32 error floor); `reset_diis` empties the DIIS
+        subspace at the switch.  Each mode's evaluation runs once eagerly
+        (planning) and is then replayed from its own CUDA graph.
+        stop(it, energy, residual) may end the solve early.  Returns the last
+        energy."""
         graphs, planned = {}, set()
         mode = 1
         self.e.set_precision(mode)
         en = None
+        self.switched_at = None
+        prev = None
         for it in range(1, maxiter + 1):
             if mode not in graphs and mode in planned:
                 self.capture()
@@ -518,9 +525,14 @@ class CCSolver:
                 callback(it, en, rn)
             if rn < conv or (stop is not None and stop(it, en, rn)):
                 break
-            if mode == 1 and rn < switch:
-                mode = 0
+            if mode == 1 and (rn < switch or (stall is not None and prev is not None and
+                                              rn > stall * prev)):
+                mode = final
                 self.e.set_precision(mode)
+                self.switched_at = it
+                if reset_diis and hasattr(self, "_diis"):
+                    self._diis["used"].clear()
+            prev = rn
             self.diis_step()
         self.e.set_precision(0)
         self.graph = None

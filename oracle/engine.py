@@ -63,6 +63,9 @@ class OracleEngine:
     def freeze(self, lid, frozen=True):
         pass  # host arrays: nothing is derived from a list
 
+    def set_precision(self, mode):
+        pass  # the oracle computes in FP64 only
+
     def contract(self, op1, op2, res, ex1, ex2, cnt, fact=1.0, update=True, use_tr=False,
                  xret=0, desc=None):
         (l1, b1), (l2, b2), (l12, b12) = op1, op2, res
