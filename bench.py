@@ -385,7 +385,8 @@ def run_gpu(args, cfg):
 
 
 METRIC_MODE = {0: "plain FP64", 1: "split-TF32 tensor cores, FP64 accumulation"}
-DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums"}
+DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums",
+         2: "s8 slices x5 (15 products), s32 exact accumulate, f64 combine"}
 
 
 def reset_amplitudes(eng, solver):
@@ -629,12 +630,27 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
            "iteration_flops": total_flops,
            "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12,
            "algorithmic_bytes_per_launch": alg_bytes}
-    kern = "k_gemm" if mode == 0 else "k_gemm_tc"
-    out["traffic"] = TRAFFIC_PER_ALGORITHMIC_BYTE[kern] * alg_bytes
-    out["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same "
-                             "launch at o12/v100 per algorithmic byte, times this launch's "
-                             "algorithmic bytes")
-    if mode == 0:
+    kern = {0: "k_gemm", 1: "k_gemm_tc", 2: "k_gemm_i8"}[mode]
+    if kern in TRAFFIC_PER_ALGORITHMIC_BYTE:
+        out["traffic"] = TRAFFIC_PER_ALGORITHMIC_BYTE[kern] * alg_bytes
+        out["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                 "same launch at o12/v100 per algorithmic byte, times this "
+                                 "launch's algorithmic bytes")
+    else:
+        out["traffic"] = None
+    if mode == 2:
+        # int8 dense peak = 2 x dense BF16 on B200; 15 slice products per
+        # useful FP64 product
+        burst, src = measured_bf16_tflops("bf16_tflops")
+        sustained, _ = measured_bf16_tflops("bf16_tflops_sustained")
+        out.update(peak=burst * 2.0 / 15.0,
+                   kernel=f"k_gemm_i8 int8 slices (tcgen05 kind::i8, persistent), launch of "
+                          f"[CONTR] {ROOFLINE_CONTRACTION}",
+                   peak_source=f"of {src}: bf16_tflops x 2 (dense int8 = twice dense BF16) "
+                               "/ 15 (slice products per useful product)",
+                   frac_of_sustained=achieved / (sustained * 2.0 / 15.0))
+        out["ladder_with_split_tflops"] = dom[0] / (dom[2] / dom[1] * 1e-3) / 1e12
+    elif mode == 0:
         out.update(peak=fp64_peak_tflops,
                    kernel=f"k_gemm<128,64> FP64 DMMA, launch of [CONTR] {ROOFLINE_CONTRACTION}",
                    peak_source="cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
@@ -707,11 +723,12 @@ def convergence(local, cfg, weights=None, maxiter=80, mixed_opts=None, variants=
             def cb(it, en, rn):
                 hist.append((it, en, rn, time.perf_counter() - t0))
 
-            if label == "fp64":
+            vopts = variants.get(label, {})
+            if label == "fp64" or "plain" in vopts:  # one precision throughout
+                eng.set_precision(vopts.get("plain", 0))
                 s.solve(maxiter=maxiter, conv=1e-9, use_graph=True, callback=cb)
             else:
-                s.solve_mixed(maxiter=maxiter, conv=1e-9, callback=cb,
-                              **dict(opts, **variants.get(label, {})))
+                s.solve_mixed(maxiter=maxiter, conv=1e-9, callback=cb, **dict(opts, **vopts))
             t = {a: eng.download(s.lid(a), s.lists[a][1]) for a in s.amps}
         finally:
             eng.close()
@@ -732,7 +749,7 @@ def convergence(local, cfg, weights=None, maxiter=80, mixed_opts=None, variants=
             out[label]["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
         out[label]["s_first_iteration"] = hist[0][3]
         if label != "fp64":
-            out[label]["switched_at"] = s.switched_at
+            out[label]["switched_at"] = getattr(s, "switched_at", None)
         if label == "mixed_learned":
             out[label]["fallbacks"] = s.fallbacks
     for label in labels[1:]:
@@ -953,7 +970,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", type=int, default=1,
                     help="1 (default): split-TF32 tensor-core contractions, with the FP64 "
-                         "path measured beside them; 0: FP64 only")
+                         "path measured beside them; 2: FP64 emulated with int8 slices on "
+                         "the tensor cores; 0: FP64 only")
     ap.add_argument("--no-fp64", action="store_true",
                     help="with --precision 1, skip the FP64 measurement")
     ap.add_argument("--no-use-tr", action="store_true",

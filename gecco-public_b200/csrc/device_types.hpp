@@ -71,6 +71,12 @@ struct GemmDesc {
   // frozen list, its persistent panel (pa_ptr / pb_ptr, else null)
   int64_t pa, pb;
   float *pa_ptr, *pb_ptr;
+  // precision mode 2: float offsets of the panels' row maxima in the
+  // workspace (or, for a frozen operand, their persistent arrays)
+  int64_t ma, mb;
+  double *ma_ptr, *mb_ptr;
+  int32_t i8;            // the tensor-core item runs on the int8 slices (mode 2)
+  int32_t pad2;
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update

@@ -61,6 +61,10 @@ struct TilePolicy {
   bool ksplit = true;             // split contractions over CTAs when a launch has few tiles
 };
 
+// an autotuned alternative must take at most this fraction of the fixed
+// rule's time to be chosen
+constexpr double kTuneMargin = 0.97;
+
 // candidates per precision mode; candidate 0 is the fixed rule
 inline std::vector<TilePolicy> tile_policies(int precision) {
   std::vector<TilePolicy> v(1);
@@ -110,6 +114,10 @@ struct DevPlan {
   SplitJob* d_split_c = nullptr;
   int64_t nsplit_c = 0, split_chunks_c = 0;
   float* const_panels = nullptr;  // persistent split panels (floats)
+  // precision mode 2 (int8 slices): the panels' row maxima, zeroed before
+  // each slicing (workspace float range; the persistent panels' range)
+  bool i8 = false;
+  int64_t max_off = 0, max_floats = 0, max_off_c = 0, max_floats_c = 0;
   std::vector<int> const_lists;   // the frozen lists behind them
   bool const_stale = false;       // a list of const_lists was unfrozen since they were made
   PackJob* d_gather = nullptr;  // gather descriptions of map-addressed tensor-core operands
@@ -169,7 +177,8 @@ class Engine {
   int64_t capture_start = 0;
   cudaEvent_t slots[64] = {};
   bool profiling = false;
-  int precision = 0;     // 0: FP64 DMMA, 1: split TF32 on tcgen05 for regular/medium items
+  int precision = 0;     // 0: FP64 DMMA, 1: split TF32 on tcgen05 for regular/medium items,
+                         // 2: FP64 emulated with int8 slices on tcgen05 for the same items
   // split-TF32 operand panels, shared by all plans (one stream orders them);
   // grown to the largest plan's need, never while a graph is being captured
   float* tc_ws = nullptr;
@@ -335,6 +344,34 @@ class Engine {
       if (!list(l).frozen) return true;
     return false;
   }
+  // operand panels of a plan's tensor-core items over a split job list:
+  // split TF32 (mode 1), or row maxima then int8 slices (mode 2), in the
+  // workspace or (cached) in the plan's persistent panels
+  void run_split(const DevPlan& dp, const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
+                 int64_t nchunks, bool cached) {
+    if (!dp.i8) {
+      launch_split_tc(descs, jobs, njobs, nchunks, dp.d_gather, stream);
+      ++launches;
+      return;
+    }
+    if (cached)
+      launch_zero_tc(dp.const_panels, dp.max_off_c, dp.max_floats_c, stream);
+    else
+      launch_zero_tc(nullptr, dp.max_off, dp.max_floats, stream);
+    launch_slice_i8(0, descs, jobs, njobs, nchunks, dp.d_gather, stream);
+    launch_slice_i8(1, descs, jobs, njobs, nchunks, dp.d_gather, stream);
+    launches += 3;
+  }
+  // the GEMM launch of one tile kind (the int8-slice kernel for the
+  // tensor-core tiles of a mode-2 plan)
+  void run_gemm(const DevPlan& dp, int kind, const GemmDesc* descs, const TileDesc* tiles,
+                int64_t ntiles, double fact) {
+    if (kind == kGemmTc && dp.i8)
+      launch_gemm_i8(descs, tiles, ntiles, fact, d_err, wait_limit, stream);
+    else
+      launch_gemm(kind, descs, tiles, ntiles, fact, d_err, wait_limit, stream);
+    ++launches;
+  }
   // make the cached panels of a plan (packs before splits: a split may read
   // a packed panel); during a capture, or else note what the graph relies on
   void run_const(DevPlan& dp, bool force = false) {
@@ -344,11 +381,8 @@ class Engine {
         launch_pack(dp.d_jobs_c, dp.njobs_c, dp.pack_gx_c, dp.pack_gy_c, stream);
         ++launches;
       }
-      if (dp.nsplit_c) {
-        launch_split_tc(dp.d_desc[kGemmTc], dp.d_split_c, dp.nsplit_c, dp.split_chunks_c,
-                        dp.d_gather, stream);
-        ++launches;
-      }
+      if (dp.nsplit_c)
+        run_split(dp, dp.d_desc[kGemmTc], dp.d_split_c, dp.nsplit_c, dp.split_chunks_c, true);
       bool all_frozen = true;
       for (int l : dp.const_lists) all_frozen = all_frozen && list(l).frozen;
       if (all_frozen) dp.const_stale = false;
@@ -709,20 +743,15 @@ class Engine {
       launch_pack(dp.d_jobs, dp.njobs, dp.pack_gx, dp.pack_gy, stream);
       ++launches;
     }
-    if (dp.nsplit) {  // operand split of the tensor-core items (after the pack it may read)
-      launch_split_tc(dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, dp.d_gather,
-                      stream);
-      ++launches;
-    }
+    if (dp.nsplit)  // operand split of the tensor-core items (after the pack it may read)
+      run_split(dp, dp.d_desc[kGemmTc], dp.d_split, dp.nsplit, dp.split_chunks, false);
     if (evp) CUDA_OK(cudaEventRecord(evp, stream));
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       if (!dp.ntiles_g[kind]) continue;
       int64_t lo, hi;
       shard_range(dp.ntiles_g[kind], lo, hi);
       if (hi <= lo) continue;
-      launch_gemm(kind, dp.d_desc[kind], dp.d_tiles_g[kind] + lo, hi - lo, fact, d_err,
-                  wait_limit, stream);
-      ++launches;
+      run_gemm(dp, kind, dp.d_desc[kind], dp.d_tiles_g[kind] + lo, hi - lo, fact);
     }
     if (flip && dp.plan.use_tr && dp.nflip) {
       launch_sym_ab(dp.d_flip, dp.nflip, list(dp.list12).d, 0.5, dp.flip_maxlen, stream);
@@ -801,6 +830,9 @@ class Engine {
       CUDA_OK(cudaMemcpyAsync(r.d + dp.res_off, snap, dp.res_len * sizeof(double),
                               cudaMemcpyDeviceToDevice, stream));
     }
+    // an alternative replaces the fixed rule only when it is clearly faster
+    // (differences of a few percent are within the timing noise of two runs)
+    if (rec.chosen != 0 && rec.ms[rec.chosen] > kTuneMargin * rec.ms[0]) rec.chosen = 0;
     event_pool.push_back(e0);
     event_pool.push_back(e1);
     CUDA_OK(cudaStreamSynchronize(stream));
@@ -907,7 +939,7 @@ class Engine {
       // wastes less than a 256-wide tensor-core tile; items with fewer than
       // kTcMinK contraction indices keep FP64, their tiles would be set-up
       // and epilogue only)
-      if (precision == 1 && it.K >= pol.tc_min_k &&
+      if (precision >= 1 && it.K >= pol.tc_min_k &&
           (kind_of[i] == kGemmRegular ||
            (pol.tc_thin && kind_of[i] == kGemmMedium && !swapped[i] && it.M > kGemmMediumN))) {
         kind_of[i] = kGemmTc;
@@ -1088,8 +1120,13 @@ class Engine {
     for (int kind = 0; kind < kGemmKinds; ++kind) {
       int TM, TN0;
       gemm_tile(kind, TM, TN0);
-      if (kind == kGemmTc)
-        for (auto& d : g[kind]) d.tn = tc_tile_n(d.N);
+      if (kind == kGemmTc) {
+        dp.i8 = precision == 2;
+        for (auto& d : g[kind]) {
+          d.tn = dp.i8 ? tc_tile_n(d.N, kI8N) : tc_tile_n(d.N);
+          d.i8 = dp.i8;
+        }
+      }
       auto width = [&](const GemmDesc& d) { return kind == kGemmTc ? d.tn : TN0; };
       std::vector<TileDesc> tiles;
       int64_t total = 0;
@@ -1102,8 +1139,9 @@ class Engine {
         int64_t ks = 1;
         if (kind == kGemmSmall) {
           ks = std::max<int64_t>(1, (d.K + kSmallChunk - 1) / kSmallChunk);
-        } else if (kind == kGemmTc) {  // FP32 accumulation over at most kTcChunk indices
-          ks = std::max<int64_t>(1, (d.K + kTcChunk - 1) / kTcChunk);
+        } else if (kind == kGemmTc) {  // FP32 (int32) accumulation over at most kTcChunk
+          const int64_t ch = dp.i8 ? kI8Chunk : kTcChunk;  // (kI8Chunk) indices
+          ks = std::max<int64_t>(1, (d.K + ch - 1) / ch);
         } else if (pol.ksplit && total < want && d.K > 4 * kGemmK) {
           ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
           ks = std::max<int64_t>(ks, 1);
@@ -1152,7 +1190,7 @@ class Engine {
           for (int op = 0; op < 2; ++op) {
             const int64_t rows = op == 0 ? d.M : d.N;
             const int tr = op == 0 ? kGemmTcM : d.tn;
-            const int64_t fl = tc_panel_floats(rows, tr, d.K);
+            const int64_t fl = dp.i8 ? i8_panel_floats(rows, tr, d.K) : tc_panel_floats(rows, tr, d.K);
             const int64_t ch = tc_split_chunks(rows, tr, d.K);
             int64_t& po = op == 0 ? d.pa : d.pb;
             if (frozen_op[op]) {
@@ -1171,11 +1209,27 @@ class Engine {
         }
         GCCU_REQUIRE(cs < INT32_MAX && cs_c < INT32_MAX,
                      "tensor-core operands too large for one split launch");
+        if (dp.i8) {  // row maxima of every panel, after the panels (one range each)
+          dp.max_off = off;
+          dp.max_off_c = off_c;
+          for (auto& d : g[kind])
+            for (int op = 0; op < 2; ++op) {
+              const int64_t fl = i8_max_floats(op == 0 ? d.M : d.N, op == 0 ? kGemmTcM : d.tn);
+              int64_t& mo = op == 0 ? d.ma : d.mb;
+              int64_t& end = frozen_op[op] ? off_c : off;
+              mo = end;
+              end += fl;
+            }
+          dp.max_floats = off - dp.max_off;
+          dp.max_floats_c = off_c - dp.max_off_c;
+        }
         if (off_c) {
           dp.const_panels = (float*)alloc((size_t)off_c * sizeof(float));
           for (auto& d : g[kind]) {
             if (frozen_op[0]) d.pa_ptr = dp.const_panels + d.pa;
             if (frozen_op[1]) d.pb_ptr = dp.const_panels + d.pb;
+            if (dp.i8 && frozen_op[0]) d.ma_ptr = reinterpret_cast<double*>(dp.const_panels + d.ma);
+            if (dp.i8 && frozen_op[1]) d.mb_ptr = reinterpret_cast<double*>(dp.const_panels + d.mb);
           }
         }
         dp.ws_floats = off;
@@ -1661,6 +1715,8 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
     DevPlan& dp = *pp;
     int64_t ndesc = 0;
     for (int kind = 0; kind < kGemmKinds; ++kind) ndesc += dp.ndesc_g[kind];
+    GCCU_REQUIRE(!dp.i8, "gccu_contract_noalloc: precision mode 2 (int8 slices) is not "
+                         "supported by the allocation-free entry point");
     if (dp.scratch_len > kStaticPanelDoubles) {
       std::ostringstream os;
       os << "gccu_contract_noalloc: the operand panels of this contraction need "
@@ -2233,7 +2289,8 @@ int gccu_device_info(int64_t* info4) {
 
 int gccu_set_precision(int64_t mode) {
   return guarded([&] {
-    GCCU_REQUIRE(mode == 0 || mode == 1, "precision mode must be 0 (FP64) or 1 (split TF32)");
+    GCCU_REQUIRE(mode >= 0 && mode <= 2,
+                 "precision mode must be 0 (FP64), 1 (split TF32) or 2 (int8 slices)");
     eng().precision = (int)mode;
   });
 }

@@ -202,13 +202,34 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 // contract/collect_block_impr.f:397, without a dense FP64 panel): the chunk's
 // string indices of both sides are staged in shared memory, the element
 // offset adds (|map_m[i2 * n1 + i1]| - 1) * ldim_m per map component.
+//
+// The same kernel makes the int8-slice panels of precision mode 2 in two
+// launches over the same chunks: OUT = 1 stages the chunk's values and
+// raises the rows' maxima of |x| (atomic maximum on the FP64 bit pattern,
+// which orders non-negative values like the values), OUT = 2 cuts every
+// element into its kI8Slices bytes under its row's scale 127 / m and writes
+// 16-byte vectors (16 contraction indices of one row and slice).
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
+constexpr int kValPitch = SK + 1;         // doubles per row of a staged chunk (OUT > 0)
+union SplitStage {
+  float sh[2][8 * kSplitPitch];  // split-TF32 planes (OUT = 0)
+  double v[128][kValPitch];      // values (OUT = 1, 2)
+};
 
+// row maxima of an operand panel (precision mode 2)
+__device__ __forceinline__ double* panel_max(const GemmDesc& d, bool row_op) {
+  return row_op ? (d.ma_ptr ? d.ma_ptr : reinterpret_cast<double*>(g_tc_ws + d.ma))
+                : (d.mb_ptr ? d.mb_ptr : reinterpret_cast<double*>(g_tc_ws + d.mb));
+}
+
+template <int OUT>
 __global__ void __launch_bounds__(kSplitThreads, 4)
     k_split_tc(const GemmDesc* __restrict__ descs, const SplitJob* __restrict__ jobs,
                int64_t njobs, const PackJob* __restrict__ gathers) {
-  __shared__ __align__(16) float sh[2][8 * kSplitPitch];
+  __shared__ __align__(16) SplitStage U;
+  float(&sh)[2][8 * kSplitPitch] = U.sh;
+  __shared__ double inv_s[128];  // OUT = 2: 127 / row maximum (0 for a zero row)
   __shared__ int64_t ro[128];
   __shared__ int64_t ko[SK];
   __shared__ int32_t rmi_s[kTcGatherMaps][128], kmi_s[kTcGatherMaps][SK];
@@ -237,6 +258,12 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
   const int64_t r0 = (c / nsl) * 128, k0 = (c % nsl) * SK;
   if (tid < 128) ro[tid] = r0 + tid < R ? __ldg(rtab + r0 + tid) : -1;
   else if (tid < 128 + SK) ko[tid - 128] = k0 + (tid - 128) < K ? __ldg(ktab + k0 + tid - 128) : -1;
+  if constexpr (OUT == 2) {
+    if (tid < 128) {
+      const double m = r0 + tid < R ? panel_max(d, row_op)[r0 + tid] : 0.0;
+      inv_s[tid] = m > 0.0 ? 127.0 / m : 0.0;
+    }
+  }
   if (gat) {
     const int nw = (int)(sizeof(PackJob) / sizeof(int));
     for (int i = tid; i < nw; i += kSplitThreads)
@@ -267,22 +294,31 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
       for (int i = 0; i < 16; ++i) {
         const int r = warp * 16 + i;
         const double v = elem(r, lane);
-        float h, l;
-        split_tf32(v, h, l);
-        sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
-        sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
+        if constexpr (OUT == 0) {
+          float h, l;
+          split_tf32(v, h, l);
+          sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
+          sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
+        } else {
+          U.v[r][lane] = v;
+        }
       }
     } else {  // thread: one row, 16 contraction indices
       const int r = tid & 127, kh = tid >> 7;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        float4 h4, l4;
-        float* hp = &h4.x;
-        float* lp = &l4.x;
+        if constexpr (OUT == 0) {
+          float4 h4, l4;
+          float* hp = &h4.x;
+          float* lp = &l4.x;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) split_tf32(elem(r, 16 * kh + 4 * q + e), hp[e], lp[e]);
-        *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
-        *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+          for (int e = 0; e < 4; ++e) split_tf32(elem(r, 16 * kh + 4 * q + e), hp[e], lp[e]);
+          *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
+          *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) U.v[r][16 * kh + 4 * q + e] = elem(r, 16 * kh + 4 * q + e);
+        }
       }
     }
   };
@@ -342,10 +378,14 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
         gather8(rr, kk, v);
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-          float h, l;
-          split_tf32(v[e], h, l);
-          sh[0][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = h;
-          sh[1][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = l;
+          if constexpr (OUT == 0) {
+            float h, l;
+            split_tf32(v[e], h, l);
+            sh[0][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = h;
+            sh[1][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = l;
+          } else {
+            U.v[rr[e]][lane] = v[e];
+          }
         }
       }
     } else {  // thread: one row, 16 contraction indices
@@ -360,15 +400,20 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
           kk[e] = 16 * kh + 4 * q0 + e;
         }
         gather8(rr, kk, v);
+        if constexpr (OUT == 0) {
 #pragma unroll
-        for (int qq = 0; qq < 2; ++qq) {
-          float4 h4, l4;
-          float* hp = &h4.x;
-          float* lp = &l4.x;
+          for (int qq = 0; qq < 2; ++qq) {
+            float4 h4, l4;
+            float* hp = &h4.x;
+            float* lp = &l4.x;
 #pragma unroll
-          for (int e = 0; e < 4; ++e) split_tf32(v[4 * qq + e], hp[e], lp[e]);
-          *reinterpret_cast<float4*>(&sh[0][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = h4;
-          *reinterpret_cast<float4*>(&sh[1][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = l4;
+            for (int e = 0; e < 4; ++e) split_tf32(v[4 * qq + e], hp[e], lp[e]);
+            *reinterpret_cast<float4*>(&sh[0][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = h4;
+            *reinterpret_cast<float4*>(&sh[1][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = l4;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) U.v[r][kk[e]] = v[e];
         }
       }
     }
@@ -380,6 +425,45 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
   __syncthreads();
   // a 128-row chunk may span two row bands when TR is not a multiple of 128
   const int64_t padded = (R + TR - 1) / TR * TR;
+  if constexpr (OUT == 1) {  // rows' maxima: each thread half a row of the chunk
+    const int r = tid & 127, kh = tid >> 7;
+    double m = 0.0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) m = fmax(m, fabs(U.v[r][16 * kh + j]));
+    if (m > 0.0 && r0 + r < R)
+      atomicMax(reinterpret_cast<unsigned long long*>(panel_max(d, row_op) + r0 + r),
+                (unsigned long long)__double_as_longlong(m));
+    return;
+  } else if constexpr (OUT == 2) {  // slices: thread = one row x 16 indices (one plane)
+    const int r = tid & 127, kh = tid >> 7;
+    const int64_t row = r0 + r;
+    if (row >= padded) return;
+    const double inv = inv_s[r];
+    uint32_t w[kI8Slices][4];
+#pragma unroll
+    for (int s = 0; s < kI8Slices; ++s)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      double u = U.v[r][16 * kh + j] * inv;  // |u| <= 127
+#pragma unroll
+      for (int s = 0; s < kI8Slices; ++s) {
+        const int a = __double2int_rn(u);  // |a| <= 127, then <= 64
+        w[s][j >> 2] |= (uint32_t)(a & 0xff) << (8 * (j & 3));
+        u = (u - (double)a) * 128.0;  // exact
+      }
+    }
+    uint8_t* const panel = reinterpret_cast<uint8_t*>(
+        row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa) : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb));
+    const int64_t band = row / TR, rr = row % TR, slice = c % nsl;
+    uint8_t* base = panel + ((band * nsl + slice) * kI8Slices * 2 + kh) * TR * 16 + rr * 16;
+#pragma unroll
+    for (int s = 0; s < kI8Slices; ++s)
+      *reinterpret_cast<uint4*>(base + (int64_t)s * 2 * TR * 16) =
+          make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+    return;
+  }
   float* const panel = row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa)
                               : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb);
   float* __restrict__ base = panel + (c % nsl) * 2 * TR * SK;
@@ -401,9 +485,9 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
 // tables plus the string-map lookups of mapped result components, issued for
 // all NB elements together (one batch of independent loads per component),
 // then the updates.
-template <int NB>
-__device__ __forceinline__ void scatter(const TcSmem& S, const int (&row)[NB],
-                                        const int (&col)[NB], const float (&v)[NB],
+template <int NB, typename Smem, typename T>
+__device__ __forceinline__ void scatter(const Smem& S, const int (&row)[NB],
+                                        const int (&col)[NB], const T (&v)[NB],
                                         int64_t rows, int64_t cols, double f) {
   const GemmDesc& d = S.d;
   int64_t off[NB];
@@ -411,7 +495,7 @@ __device__ __forceinline__ void scatter(const TcSmem& S, const int (&row)[NB],
   bool ok[NB];
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
-    ok[i] = row[i] < rows && col[i] < cols && v[i] != 0.0f;
+    ok[i] = row[i] < rows && col[i] < cols && v[i] != T(0);
     off[i] = ok[i] ? S.cro[row[i]] + S.cco[col[i]] : 0;
     sg[i] = 1.0f;
   }
@@ -691,6 +775,306 @@ static_assert((TBM * BK * sizeof(float)) % 16 == 0 && (TBN * BK * sizeof(float))
 static_assert(TBM % kEpiWarps == 0 && kTcols % 16 == 0 && TBN % 32 == 0,
               "epilogue passes (tile widths are multiples of 32)");
 
+
+// ---- int8-slice GEMM (precision mode 2) -------------------------------------
+// The structure of k_gemm_tc (persistent, producer / MMA / epilogue warps,
+// bounded waits), with the slices: a stage is one 32-index slice of all
+// kI8Slices row-operand and column-operand slices (one bulk copy each); the
+// MMA thread issues, per stage, the products of slices (s, t) with
+// s + t < kI8Slices into accumulator s + t (kind::i8, int32, K = 32 per
+// instruction).  The kI8Slices accumulators of a tile take kI8Slices * tn
+// TMEM columns, so there is one set: the epilogue reads it into registers
+// (FP64, sum over s + t of 2^(-7(s+t)) times the accumulator, exact before
+// the last rounding), releases it to the MMAs of the next tile and then
+// scales by the rows' and columns' m / 127 and scatters from the registers.
+constexpr int IS = kI8Slices;
+constexpr int IBN = kI8N;  // widest int8 tile
+constexpr int INST = 4;    // pipeline stages
+constexpr int kI8StageA = IS * 2 * TBM * 16;      // bytes of one stage of the row operand
+constexpr int kI8StageBMax = IS * 2 * IBN * 16;   // ... of the column operand, widest tile
+
+struct __align__(1024) I8Smem {
+  uint8_t a[INST][kI8StageA];  // [stage][slice s][k/16][row][k%16]
+  uint8_t b[INST][kI8StageBMax];
+  double t[TBM][kTcols + 1];   // column-major epilogue staging
+  int64_t cro[TBM], cco[IBN];
+  double rs[TBM], cs[IBN];     // row / column scales m / 127
+  int32_t rc[TBM][kDevMaxComp];
+  int32_t cc[IBN][kDevMaxComp];
+  GemmDesc d;
+  alignas(8) uint64_t full[INST], empty[INST], accf, acce, done;
+  int64_t issued, consumed;
+  uint32_t tmem_base;
+  int failed;
+};
+
+// instruction descriptor: D s32, A/B signed 8-bit, both K-major, M x N
+__device__ __forceinline__ uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// 8 consecutive int32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld8_s32(uint32_t taddr, int (&v)[8]) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = (int)r[i];
+}
+
+__global__ void __launch_bounds__(TNT, 1)
+    k_gemm_i8(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
+              int64_t ntiles, double alpha, int* err, long wait_limit) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  I8Smem& S = *reinterpret_cast<I8Smem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    for (int s = 0; s < INST; ++s) {
+      mbar_init(smem_u32(&S.full[s]), 1);
+      mbar_init(smem_u32(&S.empty[s]), 1);
+    }
+    mbar_init(smem_u32(&S.accf), 1);
+    mbar_init(smem_u32(&S.acce), kEpiWarps);
+    mbar_init(smem_u32(&S.done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.failed = 0;
+    S.issued = 0;
+    S.consumed = 0;
+  }
+  if (warp == 0) {  // TMEM: all 512 columns (the kI8Slices accumulators of one tile)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(&S.tmem_base)), "r"(512u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  volatile int* failed = &S.failed;
+  const int64_t nmine = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+  auto tile_of = [&](int64_t lt) { return tiles[blockIdx.x + lt * gridDim.x]; };
+  if (warp == 0) {
+    if (lane == 0) {  // producer: one 32-index slice of all slices per stage
+      int64_t it = 0;
+      for (int64_t lt = 0; lt < nmine && !*failed; ++lt) {
+        const TileDesc td = tile_of(lt);
+        const GemmDesc* dg = descs + td.item;
+        const int64_t K = dg->K, nsl = (K + SK - 1) / SK, g0 = td.k0 / SK;
+        const int64_t nk = (td.k1 - td.k0 + SK - 1) / SK;
+        const int bn = dg->tn;
+        const uint32_t sb = (uint32_t)(IS * 2 * bn * 16);
+        const uint8_t* pa =
+            reinterpret_cast<const uint8_t*>(dg->pa_ptr ? dg->pa_ptr : g_tc_ws + dg->pa) +
+            (int64_t)(td.m0 / TBM) * nsl * kI8StageA;
+        const uint8_t* pb =
+            reinterpret_cast<const uint8_t*>(dg->pb_ptr ? dg->pb_ptr : g_tc_ws + dg->pb) +
+            (int64_t)(td.n0 / bn) * nsl * sb;
+        for (int64_t t = 0; t < nk; ++t, ++it) {
+          const int s = (int)(it % INST);
+          if (it >= INST &&
+              !mbar_wait(smem_u32(&S.empty[s]), (uint32_t)((it / INST - 1) & 1), failed,
+                         wait_limit)) {
+            *failed = 1;
+            break;
+          }
+          const uint32_t bar = smem_u32(&S.full[s]);
+          mbar_expect_tx(bar, (uint32_t)kI8StageA + sb);
+          bulk_g2s(S.a[s], pa + (g0 + t) * kI8StageA, (uint32_t)kI8StageA, bar);
+          bulk_g2s(S.b[s], pb + (g0 + t) * sb, sb, bar);
+          S.issued = it + 1;
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t kA = TBM * 16;  // next core matrix along K (row operand)
+      int64_t it = 0;
+      for (int64_t lt = 0; lt < nmine && !*failed; ++lt) {
+        const TileDesc td = tile_of(lt);
+        const int64_t nk = (td.k1 - td.k0 + SK - 1) / SK;
+        const int bn = descs[td.item].tn;
+        const uint32_t idesc = idesc_i8(TBM, bn), kB = (uint32_t)bn * 16;
+        if (lt >= 1 &&  // the epilogue has read the previous tile's accumulators
+            !mbar_wait(smem_u32(&S.acce), (uint32_t)((lt - 1) & 1), failed, wait_limit)) {
+          *failed = 1;
+          break;
+        }
+        tc_fence_after();
+        for (int64_t t = 0; t < nk; ++t, ++it) {
+          const int s = (int)(it % INST);
+          if (!mbar_wait(smem_u32(&S.full[s]), (uint32_t)((it / INST) & 1), failed, wait_limit)) {
+            *failed = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
+#pragma unroll
+          for (int dd = 0; dd < IS; ++dd)
+#pragma unroll
+            for (int sa = 0; sa <= dd; ++sa) {
+              const uint64_t da = smem_desc(a0 + (uint32_t)sa * 2 * kA, kA, 128);
+              const uint64_t db = smem_desc(b0 + (uint32_t)(dd - sa) * 2 * kB, kB, 128);
+              mma_i8(tmem + (uint32_t)(dd * bn), da, db, idesc, (t > 0 || sa > 0) ? 1u : 0u);
+            }
+          mma_commit(smem_u32(&S.empty[s]));
+          S.consumed = it + 1;
+        }
+        if (*failed) break;
+        mma_commit(smem_u32(&S.accf));
+      }
+      mma_commit(smem_u32(&S.done));  // tracks every MMA this thread issued
+    }
+    __syncwarp();
+  } else if (warp >= kEpiWarp0) {
+    const int et = tid - 32 * kEpiWarp0, ew = warp - kEpiWarp0;
+    const int quarter = warp & 3, half = ew >> 2;  // TMEM lanes 32*quarter.., column half
+    for (int64_t lt = 0; lt < nmine; ++lt) {
+      const TileDesc td = tile_of(lt);
+      {
+        const int* src = reinterpret_cast<const int*>(descs + td.item);
+        int* dst = reinterpret_cast<int*>(&S.d);
+        for (int i = et; i < (int)(sizeof(GemmDesc) / sizeof(int)); i += kEpiThreads)
+          dst[i] = src[i];
+      }
+      epi_sync();
+      const GemmDesc& d = S.d;
+      const int bn = d.tn;
+      const int64_t rows = d.M - td.m0 < TBM ? d.M - td.m0 : TBM;
+      const int64_t cols = d.N - td.n0 < bn ? d.N - td.n0 : bn;
+      const int colspace = d.rowspace == kEx1 ? kEx2 : kEx1;
+      const double* mr = panel_max(d, true);
+      const double* mc = panel_max(d, false);
+      for (int i = et; i < TBM; i += kEpiThreads)
+        if (i < rows) {
+          S.cro[i] = d.cro[td.m0 + i];
+          S.rs[i] = mr[td.m0 + i] * (1.0 / 127.0);
+          if (d.cmapped) decomp(d.rad[d.rowspace], d.nsp[d.rowspace], td.m0 + i, S.rc[i]);
+        }
+      for (int i = et; i < IBN; i += kEpiThreads)
+        if (i < cols) {
+          S.cco[i] = d.cco[td.n0 + i];
+          S.cs[i] = mc[td.n0 + i] * (1.0 / 127.0);
+          if (d.cmapped) decomp(d.rad[colspace], d.nsp[colspace], td.n0 + i, S.cc[i]);
+        }
+      if (!mbar_wait(smem_u32(&S.accf), (uint32_t)(lt & 1), failed, wait_limit)) *failed = 1;
+      epi_sync();
+      if (*failed) break;  // the same in every epilogue thread after the barrier
+      tc_fence_after();
+      // this thread: row 32*quarter + lane, columns c0 .. c0 + bn/2 - 1
+      const int row = 32 * quarter + lane;
+      const int c0 = half * (bn / 2);
+      const uint32_t tl = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)c0;
+      double v[IBN / 2];
+#pragma unroll
+      for (int cb = 0; cb < IBN / 2; cb += 8) {
+        if (cb < bn / 2) {  // warp-uniform
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[cb + j] = 0.0;
+#pragma unroll
+          for (int dd = IS - 1; dd >= 0; --dd) {  // smallest terms first
+            int q[8];
+            tmem_ld8_s32(tl + (uint32_t)(dd * bn + cb), q);
+            const double w = ldexp(1.0, -7 * dd);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[cb + j] += w * (double)q[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[cb + j] = 0.0;
+        }
+      }
+      // accumulators read (tcgen05.ld waited): release them to the next tile
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&S.acce));
+      const double f = alpha * d.fac;
+      const double rsc = row < rows ? S.rs[row] : 0.0;
+      const bool colfast = rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
+                           S.cro[1] - S.cro[0] != 1;
+      if (colfast) {
+        // passes of kTcols columns through shared memory, then every epilogue
+        // warp scatters rows ew, ew+8, .. with lanes on consecutive columns
+        for (int p0 = 0; p0 < cols; p0 += kTcols) {
+#pragma unroll
+          for (int j = 0; j < IBN / 2; ++j) {
+            const int col = c0 + j;
+            if (j < bn / 2 && col >= p0 && col < p0 + kTcols)
+              S.t[row][col - p0] = col < cols ? v[j] * rsc * S.cs[col] : 0.0;
+          }
+          epi_sync();
+          constexpr int kRows = TBM / kEpiWarps, kBatch = 8;
+#pragma unroll
+          for (int i0 = 0; i0 < kRows; i0 += kBatch) {
+            int rr[kBatch], cc[kBatch];
+            double y[kBatch];
+#pragma unroll
+            for (int i = 0; i < kBatch; ++i) {
+              rr[i] = ew + kEpiWarps * (i0 + i);
+              cc[i] = p0 + lane;
+              y[i] = S.t[rr[i]][lane];
+            }
+            scatter<kBatch>(S, rr, cc, y, rows, cols, f);
+          }
+          epi_sync();
+        }
+      } else {
+#pragma unroll
+        for (int cb = 0; cb < IBN / 2; cb += 8) {
+          if (cb >= bn / 2 || c0 + cb >= cols) break;  // warp-uniform
+          int rr[8], cc[8];
+          double y[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            rr[i] = row;
+            cc[i] = c0 + cb + i;
+            y[i] = cc[i] < cols ? v[cb + i] * rsc * S.cs[cc[i]] : 0.0;
+          }
+          scatter<8>(S, rr, cc, y, rows, cols, f);
+        }
+      }
+      epi_sync();  // tables and descriptor free for the next tile
+    }
+  }
+  __syncthreads();
+  if (!mbar_wait(smem_u32(&S.done), 0u, nullptr)) *failed = 1;  // all MMAs complete
+  if (tid == 0) {  // copies issued but never consumed (only after a failure)
+    for (int64_t t = S.consumed; t < S.issued; ++t)
+      if (!mbar_wait(smem_u32(&S.full[t % INST]), (uint32_t)((t / INST) & 1), nullptr))
+        *failed = 1;
+  }
+  __syncthreads();
+  if (*failed && tid == 0) atomicExch(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :
+                 : "r"(tmem), "r"(512u)
+                 : "memory");
+}
+
+static_assert(sizeof(I8Smem) <= 227 * 1024, "int8 tile exceeds shared memory");
+static_assert(IBN % 32 == 0 && IBN / 2 % 16 == 0, "int8 tile width: epilogue column groups");
+static_assert(kI8StageA % 16 == 0 && kI8StageBMax % 16 == 0, "bulk copies move multiples of 16 bytes");
+
 }  // namespace
 
 cudaError_t set_tc_workspace(float* ws) {
@@ -700,7 +1084,29 @@ cudaError_t set_tc_workspace(float* ws) {
 void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
                      const PackJob* gathers, cudaStream_t s) {
   if (njobs == 0 || nchunks == 0) return;
-  k_split_tc<<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
+  k_split_tc<0><<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
+}
+
+__global__ void k_zero_tc(float* base, int64_t off, int64_t n) {
+  float* p = (base ? base : g_tc_ws) + off;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0.0f;
+}
+
+void launch_zero_tc(float* base, int64_t off, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + 255) / 256;
+  k_zero_tc<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, s>>>(base, off, n);
+}
+
+void launch_slice_i8(int phase, const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
+                     int64_t nchunks, const PackJob* gathers, cudaStream_t s) {
+  if (njobs == 0 || nchunks == 0) return;
+  if (phase == 0)
+    k_split_tc<1><<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
+  else
+    k_split_tc<2><<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
 }
 
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
@@ -726,6 +1132,31 @@ void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles
 
 cudaError_t tc_kernel_attributes(cudaFuncAttributes* attr) {
   return cudaFuncGetAttributes(attr, k_gemm_tc);
+}
+
+void launch_gemm_i8(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
+                    int* err, int64_t wait_limit, cudaStream_t s) {
+  if (ntiles == 0) return;
+  const size_t smem = sizeof(I8Smem);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = true;
+  }
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const int64_t grid = ntiles < nsm ? ntiles : nsm;
+  k_gemm_i8<<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err,
+                                                (long)wait_limit);
+}
+
+cudaError_t i8_kernel_attributes(cudaFuncAttributes* attr) {
+  return cudaFuncGetAttributes(attr, k_gemm_i8);
 }
 
 }  // namespace gccu

@@ -67,13 +67,46 @@ inline int64_t tc_split_chunks(int64_t rows, int tile_rows, int64_t K) {
   const int64_t padded = (rows + tile_rows - 1) / tile_rows * tile_rows;
   return (padded + 127) / 128 * ((K + kTcSlice - 1) / kTcSlice);
 }
-// tile width of a tensor-core item with N columns: as many tiles as 256-wide
-// ones would need, each narrowed to the multiple of 32 that covers N
-inline int tc_tile_n(int64_t N) {
-  const int64_t nt = (N + kGemmTcN - 1) / kGemmTcN;
+// tile width of a tensor-core item with N columns: as many tiles as
+// widest-wide ones would need, each narrowed to the multiple of 32 that
+// covers N
+inline int tc_tile_n(int64_t N, int widest = kGemmTcN) {
+  const int64_t nt = (N + widest - 1) / widest;
   int64_t w = ((N + nt - 1) / nt + 31) / 32 * 32;
   if (w < 32) w = 32;
-  return (int)(w < kGemmTcN ? w : kGemmTcN);
+  return (int)(w < widest ? w : widest);
+}
+
+// FP64 emulation on the int8 tensor cores (precision mode 2, the slicing
+// scheme of Ozaki et al.): an operand row x (row of the row operand, column
+// of the column operand) with m = max |x_k| is cut into kI8Slices signed
+// bytes per element, x_k ~ (m / 127) * sum_s a_s,k 2^(-7 s), |a_0| <= 127 and
+// |a_s| <= 64 after it (each slice the rounded remainder of the one before);
+// the products of slices s and t with s + t < kI8Slices are summed over the
+// contraction in int32 (exactly, for contraction ranges up to kI8Chunk), one
+// TMEM accumulator per s + t, and combined in FP64 in the epilogue.  The
+// panels use the split-TF32 chunk geometry (128-row x 32-index chunks); per
+// 32-index slice, a band of TR rows holds kI8Slices x 2 core-matrix planes
+// of TR x 16 bytes:
+//   panel[(((band * nslice + slice) * kI8Slices + s) * 2 + k/16) * TR * 16 + row * 16 + k%16]
+// and every panel has an array of its rows' maxima m (FP64, padded rows).
+constexpr int kI8Slices = 5;
+constexpr int kI8N = 96;             // widest tile: kI8Slices accumulators of kI8N columns
+constexpr int64_t kI8Chunk = 65536;  // contraction range of one int32 accumulation
+static_assert(kI8Slices * kI8N <= 512, "the accumulators fill at most the 512 TMEM columns");
+static_assert(kI8Slices <= 6 && (2 * 127 * 64 + (kI8Slices - 2) * 64 * 64) * kI8Chunk < (1ll << 31),
+              "an int32 accumulator must not overflow over one contraction chunk");
+inline int64_t i8_padded_rows(int64_t rows, int tile_rows) {
+  return (rows + tile_rows - 1) / tile_rows * tile_rows;
+}
+// floats of one operand's slice panel (bytes / 4)
+inline int64_t i8_panel_floats(int64_t rows, int tile_rows, int64_t K) {
+  return i8_padded_rows(rows, tile_rows) * ((K + kTcSlice - 1) / kTcSlice) * kTcSlice *
+         kI8Slices / 4;
+}
+// floats of one operand's row maxima (one double per padded row)
+inline int64_t i8_max_floats(int64_t rows, int tile_rows) {
+  return i8_padded_rows(rows, tile_rows) * 2;
 }
 // split the operands of tensor-core items into their panels (jobs sorted by
 // cstart, nchunks = total chunks); gathers: descriptions of map-addressed
@@ -81,6 +114,16 @@ inline int tc_tile_n(int64_t N) {
 constexpr int kTcGatherMaps = 4;
 void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs, int64_t nchunks,
                      const PackJob* gathers, cudaStream_t s);
+// precision mode 2: the row maxima of the panels (phase 0; the maxima must be
+// zero before it), then the slices (phase 1), same jobs and chunks as the split
+void launch_slice_i8(int phase, const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
+                     int64_t nchunks, const PackJob* gathers, cudaStream_t s);
+// zero n floats at base + off (base null: the tensor-core workspace)
+void launch_zero_tc(float* base, int64_t off, int64_t n, cudaStream_t s);
+// the int8-slice GEMM over 128 x kI8N tiles (err, wait_limit: as launch_gemm_tc)
+void launch_gemm_i8(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
+                    int* err, int64_t wait_limit, cudaStream_t s);
+cudaError_t i8_kernel_attributes(cudaFuncAttributes* attr);
 // device address of the split-TF32 workspace used by the two kernels above
 // (a device-side variable, so captured graphs follow a reallocation)
 cudaError_t set_tc_workspace(float* ws);

@@ -263,7 +263,8 @@ class Engine:
         return int(n[0]), int(m[0])
 
     def set_precision(self, mode):
-        """0 = FP64 (default), 1 = split TF32 on the tcgen05 tensor cores"""
+        """0 = FP64 (default), 1 = split TF32 on the tcgen05 tensor cores,
+        2 = FP64 emulated with int8 slices on the tcgen05 tensor cores"""
         _call("gccu_set_precision", int(mode))
 
     # ---- learned correction of the diagonal step

@@ -296,8 +296,13 @@ int gccu_sync(void);
  * three products accumulate in FP32 over at most 4096 contraction indices,
  * and the partial results are added in FP64 (about FP32 accuracy per
  * product; items with at most 32 rows or columns or fewer than 256
- * contraction indices stay FP64).  Plans are kept per mode, so a
- * solver can switch back to FP64 for its final iterations.  A pipeline wait
+ * contraction indices stay FP64); 2 = FP64 emulated on the int8 tensor
+ * cores for the same block contractions: each operand row is cut into five
+ * signed 8-bit slices under the row's scale (maximum / 127), the slice
+ * products of order s + t < 5 are summed exactly in int32 and combined in
+ * FP64 (about 35 bits of each operand relative to its row maximum; not
+ * supported by gccu_contract_noalloc).  Plans are kept per mode, so a
+ * solver can switch precision for its final iterations.  A pipeline wait
  * that times out inside a kernel is reported as an error by the next call
  * that synchronises (gccu_sync, norms, downloads). */
 int gccu_set_precision(int64_t mode);

@@ -69,7 +69,15 @@ def test_autotune_matches_oracle_and_caches(built):
         rows = e.tuning_report()
         assert len(rows) >= 1
         assert all(0 <= r[1] < NCAND[1] for r in rows)
-        assert all(r[2 + int(r[1])] == min(x for x in r[2:2 + NCAND[1]]) for r in rows)
+        # the fastest candidate, or the fixed rule when no alternative beats
+        # it by more than 3%
+        for r in rows:
+            ms = list(r[2:2 + NCAND[1]])
+            best = min(ms)
+            if best >= 0.97 * ms[0]:
+                assert int(r[1]) == 0 or ms[int(r[1])] == best
+            else:
+                assert ms[int(r[1])] == best
         # the same contractions on new lists: same histograms, no new timing
         for i, case in enumerate(cases):
             _run(e, o, case, 7 * i + 1000, 1)
