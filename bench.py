@@ -184,10 +184,10 @@ def cpu_baseline_oracle(sp, eps, B, target_s, cores, host_lists):
     return scaled, sample
 
 
-def evaluation_errors(eng, solver):
-    """one formula evaluation in split TF32 and one in FP64 from the same
-    amplitudes (the solver's current T1, T2): errors of the mixed
-    evaluation's energy, residuals and next Jacobi step against FP64"""
+def evaluation_errors(eng, solver, mode=1):
+    """one formula evaluation in precision `mode` and one in FP64 from the
+    same amplitudes (the solver's current T1, T2): errors of the mode's
+    energy, residuals and next Jacobi step against FP64"""
     import torch
     from devfill import list_tensor
 
@@ -196,17 +196,17 @@ def evaluation_errors(eng, solver):
                 for n in names}
 
     out = {}
-    for mode in (1, 0):
-        eng.set_precision(mode)
+    for m in (mode, 0):
+        eng.set_precision(m)
         solver.evaluate()
         eng.sync()
-        out[mode] = lists(["E", "R1", "R2"])
-    eng.set_precision(1)
+        out[m] = lists(["E", "R1", "R2"])
+    eng.set_precision(mode)
     d = {n: list_tensor(eng, solver.lid(n), solver.lists[n][1]) for n in ("DT1", "DT2")}
-    res = {"dE": abs(float(out[1]["E"][0] - out[0]["E"][0])), "E_fp64": float(out[0]["E"][0])}
+    res = {"dE": abs(float(out[mode]["E"][0] - out[0]["E"][0])), "E_fp64": float(out[0]["E"][0])}
     num, den = 0.0, 0.0
     for a, r in (("T1", "R1"), ("T2", "R2")):
-        x1, x0 = out[1][r], out[0][r]
+        x1, x0 = out[mode][r], out[0][r]
         res[f"d{r}_max_rel"] = float((x1 - x0).abs().max() / x0.abs().max().clamp_min(1e-300))
         res[f"d{r}_norm_rel"] = float((x1 - x0).norm() / x0.norm().clamp_min(1e-300))
         # the next diagonal step -R/D: the amplitude change the error reaches
@@ -287,7 +287,8 @@ def run_gpu(args, cfg):
         print(json.dumps({"trace": args.trace_contraction, "workload": cfg["name"],
                           "ms_including_planning": ms}), flush=True)
         return
-    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else [])
+    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else []) + \
+        ([2] if args.precision == 1 and not args.no_i8 else [])
     results = {}
     for mode in modes:
         reset_amplitudes(eng, solver)
@@ -327,19 +328,32 @@ def run_gpu(args, cfg):
                         "roofline": roofline(f, peak, 0, solver, eng),
                         "clocks": clock_summary(f["samples"]),
                         "energy_last": f["energies"][-1]}
+    if 2 in results and modes[0] != 2:
+        f = results[2]
+        line["i8"] = {"metric": metric_of(cfg) + " FP64 emulated with int8 slices",
+                      "value": f["ms"] / 1e3, "ms_per_step": f["ms"], "e2e": f["e2e"],
+                      "gpu_launches": f["launches"], "dtype": DTYPE[2],
+                      "roofline": roofline(f, peak, 2, solver, eng),
+                      "clocks": clock_summary(f["samples"]),
+                      "energy_last": f["energies"][-1]}
     if 0 in results and modes[0] != 0 and world == 1:
-        # errors of one split-TF32 evaluation against FP64 from identical
-        # amplitudes: those after two plain Jacobi iterations from zero
+        # errors of one evaluation in the tensor-core modes against FP64 from
+        # identical amplitudes: those after two plain Jacobi iterations from zero
         reset_amplitudes(eng, solver)
         eng.set_precision(0)
         for _ in range(2):
             solver.iterate()
             solver.step()
         line["precision"] = dict(
-            evaluation_errors(eng, solver),
+            evaluation_errors(eng, solver, modes[0]),
             amplitudes="after two FP64 Jacobi iterations from T=0",
             note="mixed evaluation (split TF32, FP32 accumulation per 4096-index chunk, "
                  "FP64 sums) minus FP64 evaluation; R*_max_rel relative to max|R|")
+        if 2 in results:
+            line["precision_i8"] = dict(
+                evaluation_errors(eng, solver, 2),
+                amplitudes="after two FP64 Jacobi iterations from T=0",
+                note="evaluation with FP64 emulated by int8 slices minus FP64 evaluation")
     if args.tune:
         rows = eng.tuning_report()
         line["tuning"] = {
@@ -687,75 +701,97 @@ def measured_bf16_tflops(key="bf16_tflops"):
         return FALLBACK_PEAKS[key], "fallback"
 
 
-def convergence(local, cfg, weights=None, maxiter=80, mixed_opts=None, variants=None):
-    """time to |dE| < 1 uEh against the converged FP64 energy: plain FP64,
-    mixed (split TF32 until the residual norm is below 1e-5 or stops
-    falling, then FP64; options of CCSolver.solve_mixed in `mixed_opts`)
-    and, given weights, mixed with the learned step; `variants` maps further
-    labels to solve_mixed options.  Wall time of the solve loop (device work,
-    energy and residual reads, DIIS solves), graphs replayed after the first
-    iteration of each mode; set-up excluded, planning of the first iteration
-    included."""
-    opts = dict(switch=1e-5, stall=1.0)
-    opts.update(mixed_opts or {})
-    variants = dict(variants or {})
+def convergence(local, cfg, weights=None, maxiter=80, variants=None):
+    """time to |dE| < 1 uEh against the converged FP64 energy, per solve
+    variant: plain FP64 ("fp64"), FP64 emulated with int8 slices throughout
+    ("i8"), split TF32 until the residual norm is below 1e-4 and the int8
+    emulation after it ("mixed") and, given weights, the same with the
+    learned step ("mixed_learned"); `variants` adds labels: options of
+    CCSolver.solve_mixed, or {"plain": mode} for one precision throughout.
+    Each variant is solved twice on one engine: from its first call, with
+    every contraction planned and autotuned during the first iteration of
+    each precision mode ("s_to_1uEh"), then again from zero amplitudes with
+    the plans made ("s_to_1uEh_planned").  Wall time of the solve loop
+    (device work, energy and residual reads, DIIS solves), graphs replayed
+    after the first iteration of each mode; Hamiltonian set-up excluded."""
     import cc
     import gccu
     import hamiltonian as hm
     from devfill import TorchIntegrals
 
+    mixed = {"switch": 1e-4, "stall": None, "final": 2}
+    runs = {"fp64": {"plain": 0}, "i8": {"plain": 2}, "mixed": dict(mixed)}
+    if weights is not None:
+        runs["mixed_learned"] = dict(mixed, learned=True)
+    runs.update(variants or {})
     sp, eps, B = setup_hamiltonian(cfg)
-    out = {"workload": cfg["name"], "sigma_B": cfg["sigma"]}
+    out = {"workload": cfg["name"], "sigma_B": cfg["sigma"],
+           "variants": {k: {o: v for o, v in opts.items()} for k, opts in runs.items()}}
     ref = None
     ref_t = None
-    labels = ("fp64", "mixed") + (("mixed_learned",) if weights is not None else ()) + \
-        tuple(variants)
-    for label in labels:
+
+    def solve(s, eng, opts):
+        hist = []
+        t0 = time.perf_counter()
+
+        def cb(it, en, rn):
+            hist.append((it, en, rn, time.perf_counter() - t0))
+
+        if "plain" in opts:
+            eng.set_precision(opts["plain"])
+            s.solve(maxiter=maxiter, conv=1e-9, use_graph=True, callback=cb)
+        else:
+            s.solve_mixed(maxiter=maxiter, conv=1e-9, callback=cb,
+                          **{o: v for o, v in opts.items() if o != "learned"})
+        eng.set_precision(0)
+        return hist
+
+    def hit(hist):
+        return next((h for h in hist if abs(h[1] - ref) < 1e-6), None) if ref is not None else None
+
+    for label, opts in runs.items():
         eng = gccu.Engine(local)
         try:
             s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd",
-                            learned=weights if label == "mixed_learned" else None)
+                            learned=weights if opts.get("learned") else None)
             s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
             eng.sync()
-            hist = []
-            t0 = time.perf_counter()
-
-            def cb(it, en, rn):
-                hist.append((it, en, rn, time.perf_counter() - t0))
-
-            vopts = variants.get(label, {})
-            if label == "fp64" or "plain" in vopts:  # one precision throughout
-                eng.set_precision(vopts.get("plain", 0))
-                s.solve(maxiter=maxiter, conv=1e-9, use_graph=True, callback=cb)
-            else:
-                s.solve_mixed(maxiter=maxiter, conv=1e-9, callback=cb, **dict(opts, **vopts))
+            hist = solve(s, eng, opts)
             t = {a: eng.download(s.lid(a), s.lists[a][1]) for a in s.amps}
+            switched = getattr(s, "switched_at", None)
+            fallbacks = getattr(s, "fallbacks", None)
+            if ref is None:
+                ref = hist[-1][1]
+                ref_t = t
+            reset_amplitudes(eng, s)
+            s.history = []
+            hist_p = solve(s, eng, opts)
         finally:
             eng.close()
-        if ref is None:
-            ref = hist[-1][1]
-            ref_t = t
-        hit = next((h for h in hist if abs(h[1] - ref) < 1e-6), None)
-        out[label] = {"iterations": hist[-1][0], "energy": hist[-1][1],
-                      "residual": hist[-1][2], "s_total": hist[-1][3],
-                      "converged": hist[-1][2] < 1e-9,
-                      "iterations_to_1uEh": hit[0] if hit else None,
-                      "s_to_1uEh": hit[3] if hit else None,
-                      "residual_every_5": [float(f"{h[2]:.2e}") for h in hist[4::5]]}
+        h, hp = hit(hist), hit(hist_p)
+        r = {"iterations": hist[-1][0], "energy": hist[-1][1], "residual": hist[-1][2],
+             "s_total": hist[-1][3], "converged": hist[-1][2] < 1e-9,
+             "iterations_to_1uEh": h[0] if h else None, "s_to_1uEh": h[3] if h else None,
+             "s_first_iteration": hist[0][3],
+             "s_to_1uEh_planned": hp[3] if hp else None,
+             "s_total_planned": hist_p[-1][3], "iterations_planned": hist_p[-1][0],
+             "s_per_iteration_planned": (hist_p[-1][3] - hist_p[0][3]) /
+                                        max(len(hist_p) - 1, 1),
+             "residual_every_5": [float(f"{x[2]:.2e}") for x in hist[4::5]]}
         if label != "fp64":
             num = sum(float(np.sum((t[a] - ref_t[a]) ** 2)) for a in t)
             den = sum(float(np.sum(ref_t[a] ** 2)) for a in t)
-            out[label]["dE_vs_fp64"] = hist[-1][1] - ref
-            out[label]["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
-        out[label]["s_first_iteration"] = hist[0][3]
-        if label != "fp64":
-            out[label]["switched_at"] = getattr(s, "switched_at", None)
-        if label == "mixed_learned":
-            out[label]["fallbacks"] = s.fallbacks
-    for label in labels[1:]:
-        if out[label]["s_to_1uEh"] and out["fp64"]["s_to_1uEh"]:
-            out[f"speedup_to_1uEh_{label}_vs_fp64"] = (out["fp64"]["s_to_1uEh"] /
-                                                       out[label]["s_to_1uEh"])
+            r["dE_vs_fp64"] = hist[-1][1] - ref
+            r["amplitude_norm_error_rel"] = math.sqrt(num / max(den, 1e-300))
+            r["switched_at"] = switched
+        if opts.get("learned"):
+            r["fallbacks"] = fallbacks
+        out[label] = r
+    for label in list(runs)[1:]:
+        for key, sfx in (("s_to_1uEh", ""), ("s_to_1uEh_planned", "_planned")):
+            if out[label][key] and out["fp64"][key]:
+                out[f"speedup_to_1uEh_{label}_vs_fp64{sfx}"] = (out["fp64"][key] /
+                                                               out[label][key])
     return out
 
 
@@ -972,6 +1008,8 @@ def main():
                     help="1 (default): split-TF32 tensor-core contractions, with the FP64 "
                          "path measured beside them; 2: FP64 emulated with int8 slices on "
                          "the tensor cores; 0: FP64 only")
+    ap.add_argument("--no-i8", action="store_true",
+                    help="skip the s/iteration of FP64 emulated with int8 slices")
     ap.add_argument("--no-fp64", action="store_true",
                     help="with --precision 1, skip the FP64 measurement")
     ap.add_argument("--no-use-tr", action="store_true",

@@ -761,7 +761,60 @@ class Engine {
 
   // block-shape histogram of a plan: per item the binary orders of M, N, K
   // and which operands need map lookups, counted
-  static std::string histogram_key(int precision, const Plan& P) {
+  // kernel kind per item of a plan under a tile policy (and whether its
+  // operands are swapped)
+  static void route_items(const Plan& P, const TilePolicy& pol, int precision,
+                          std::vector<int>& kind_of, std::vector<char>& swapped) {
+    // kernel kind per item: small result, skinny or medium (thin ex2, or thin
+    // ex1 with the operands swapped), else regular
+    kind_of.assign(P.items.size(), kGemmRegular);
+    swapped.assign(P.items.size(), 0);
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const ItemDesc& it = P.items[i];
+      kind_of[i] = kGemmRegular;
+      if (it.M * it.N <= 16) {
+        kind_of[i] = kGemmSmall;
+      } else if (it.N <= kGemmSkinnyN) {
+        kind_of[i] = kGemmSkinny;
+      } else if (it.M <= kGemmSkinnyN) {
+        kind_of[i] = kGemmSkinny;
+        swapped[i] = 1;
+      } else if (it.N <= pol.medium_max) {
+        kind_of[i] = kGemmMedium;
+      } else if (it.M <= pol.medium_max) {
+        kind_of[i] = kGemmMedium;
+        swapped[i] = 1;
+      }
+      // split-TF32 mode: the GEMM-sized items go to the tensor-core kernel
+      // (items with at most 32 columns keep the FP64 128 x 32 tile, which
+      // wastes less than a 256-wide tensor-core tile; items with fewer than
+      // kTcMinK contraction indices keep FP64, their tiles would be set-up
+      // and epilogue only)
+      if (precision >= 1 && it.K >= pol.tc_min_k &&
+          (kind_of[i] == kGemmRegular ||
+           (pol.tc_thin && kind_of[i] == kGemmMedium && !swapped[i] && it.M > kGemmMediumN))) {
+        kind_of[i] = kGemmTc;
+        swapped[i] = 0;
+      }
+    }
+  }
+
+  // what a tile policy changes in a plan: the kind and operand order of
+  // every item, and for FP64 launches whether contractions may be split
+  static std::string routing_signature(const Plan& P, const TilePolicy& pol, int precision) {
+    std::vector<int> kind_of;
+    std::vector<char> swapped;
+    route_items(P, pol, precision, kind_of, swapped);
+    std::string sig(kind_of.size() * 2 + 1, ' ');
+    for (size_t i = 0; i < kind_of.size(); ++i) {
+      sig[2 * i] = (char)('0' + kind_of[i]);
+      sig[2 * i + 1] = swapped[i] ? 's' : '-';
+    }
+    sig.back() = pol.ksplit ? 'k' : '-';
+    return sig;
+  }
+
+  static std::string histogram_key(int precision, const Plan& P, bool frozen1, bool frozen2) {
     std::map<std::array<int, 6>, int> h;
     auto lg = [](int64_t x) {
       int b = 0;
@@ -772,7 +825,7 @@ class Engine {
       h[{lg(it.M), lg(it.N), lg(it.K), it.op[0].nmap > 0, it.op[1].nmap > 0,
          it.op[2].nmap > 0}]++;
     std::ostringstream os;
-    os << "p" << precision;
+    os << "p" << precision << "f" << frozen1 << frozen2;  // cached operand panels
     for (auto& kv : h) {
       os << ';';
       for (int v : kv.first) os << v << ',';
@@ -785,7 +838,8 @@ class Engine {
   // histogram, else each candidate built on trial and timed on the actual
   // lists (best of two launches, the result block restored around them)
   int autotune(DevPlan& dp) {
-    const std::string key = histogram_key(precision, dp.plan);
+    const std::string key =
+        histogram_key(precision, dp.plan, list(dp.list1).frozen, list(dp.list2).frozen);
     auto f = tuned.find(key);
     if (f != tuned.end()) return f->second;
     const auto cands = tile_policies(precision);
@@ -796,7 +850,16 @@ class Engine {
                             cudaMemcpyDeviceToDevice, stream));
     cudaEvent_t e0 = get_event(), e1 = get_event();
     TuneRecord rec{(int64_t)dp.plan.items.size(), 0, {}};
+    std::vector<std::string> sigs;
     for (size_t c = 0; c < cands.size(); ++c) {
+      // a candidate that routes every item as an earlier one would build the
+      // same plan: it takes that candidate's time without a trial
+      sigs.push_back(routing_signature(dp.plan, cands[c], precision));
+      const size_t same = std::find(sigs.begin(), sigs.end(), sigs.back()) - sigs.begin();
+      if (same < c) {
+        rec.ms.push_back(rec.ms[same]);
+        continue;
+      }
       std::vector<std::pair<void*, size_t>> owned;
       auto trial = std::make_unique<DevPlan>();
       trial->plan = dp.plan;
@@ -914,38 +977,9 @@ class Engine {
       fill(tabs);
       return o;
     };
-    // kernel kind per item: small result, skinny or medium (thin ex2, or thin
-    // ex1 with the operands swapped), else regular
-    std::vector<int> kind_of(P.items.size());
-    std::vector<char> swapped(P.items.size(), 0);
-    for (size_t i = 0; i < P.items.size(); ++i) {
-      const ItemDesc& it = P.items[i];
-      kind_of[i] = kGemmRegular;
-      if (it.M * it.N <= 16) {
-        kind_of[i] = kGemmSmall;
-      } else if (it.N <= kGemmSkinnyN) {
-        kind_of[i] = kGemmSkinny;
-      } else if (it.M <= kGemmSkinnyN) {
-        kind_of[i] = kGemmSkinny;
-        swapped[i] = 1;
-      } else if (it.N <= pol.medium_max) {
-        kind_of[i] = kGemmMedium;
-      } else if (it.M <= pol.medium_max) {
-        kind_of[i] = kGemmMedium;
-        swapped[i] = 1;
-      }
-      // split-TF32 mode: the GEMM-sized items go to the tensor-core kernel
-      // (items with at most 32 columns keep the FP64 128 x 32 tile, which
-      // wastes less than a 256-wide tensor-core tile; items with fewer than
-      // kTcMinK contraction indices keep FP64, their tiles would be set-up
-      // and epilogue only)
-      if (precision >= 1 && it.K >= pol.tc_min_k &&
-          (kind_of[i] == kGemmRegular ||
-           (pol.tc_thin && kind_of[i] == kGemmMedium && !swapped[i] && it.M > kGemmMediumN))) {
-        kind_of[i] = kGemmTc;
-        swapped[i] = 0;
-      }
-    }
+    std::vector<int> kind_of;
+    std::vector<char> swapped;
+    route_items(P, pol, precision, kind_of, swapped);
     // an operand whose strings need map lookups is packed into a dense panel,
     // except for tensor-core items, whose split pre-pass reads it in place
     // through the same gather description

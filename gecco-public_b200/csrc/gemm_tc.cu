@@ -824,17 +824,17 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t a, uint64_t b, ui
       : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
-// 8 consecutive int32 accumulator columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_ld8_s32(uint32_t taddr, int (&v)[8]) {
-  uint32_t r[8];
+// 8 consecutive 32-bit accumulator columns of this thread's TMEM lane,
+// without waiting (tmem_wait_ld before the registers are used)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = (int)r[i];
 }
 
 __global__ void __launch_bounds__(TNT, 1)
@@ -986,15 +986,17 @@ __global__ void __launch_bounds__(TNT, 1)
 #pragma unroll
       for (int cb = 0; cb < IBN / 2; cb += 8) {
         if (cb < bn / 2) {  // warp-uniform
+          uint32_t q[IS][8];  // the column group of every accumulator, one wait
 #pragma unroll
-          for (int j = 0; j < 8; ++j) v[cb + j] = 0.0;
+          for (int dd = 0; dd < IS; ++dd) tmem_ld8(tl + (uint32_t)(dd * bn + cb), q[dd]);
+          tmem_wait_ld();
 #pragma unroll
-          for (int dd = IS - 1; dd >= 0; --dd) {  // smallest terms first
-            int q[8];
-            tmem_ld8_s32(tl + (uint32_t)(dd * bn + cb), q);
-            const double w = ldexp(1.0, -7 * dd);
+          for (int j = 0; j < 8; ++j) {
+            double x = 0.0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[cb + j] += w * (double)q[j];
+            for (int dd = IS - 1; dd >= 0; --dd)  // smallest terms first
+              x += ldexp(1.0, -7 * dd) * (double)(int)q[dd][j];
+            v[cb + j] = x;
           }
         } else {
 #pragma unroll
