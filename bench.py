@@ -287,8 +287,7 @@ def run_gpu(args, cfg):
         print(json.dumps({"trace": args.trace_contraction, "workload": cfg["name"],
                           "ms_including_planning": ms}), flush=True)
         return
-    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else []) + \
-        ([2] if args.precision == 1 and not args.no_i8 else [])
+    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else [])
     results = {}
     for mode in modes:
         reset_amplitudes(eng, solver)
@@ -328,14 +327,6 @@ def run_gpu(args, cfg):
                         "roofline": roofline(f, peak, 0, solver, eng),
                         "clocks": clock_summary(f["samples"]),
                         "energy_last": f["energies"][-1]}
-    if 2 in results and modes[0] != 2:
-        f = results[2]
-        line["i8"] = {"metric": metric_of(cfg) + " FP64 emulated with int8 slices",
-                      "value": f["ms"] / 1e3, "ms_per_step": f["ms"], "e2e": f["e2e"],
-                      "gpu_launches": f["launches"], "dtype": DTYPE[2],
-                      "roofline": roofline(f, peak, 2, solver, eng),
-                      "clocks": clock_summary(f["samples"]),
-                      "energy_last": f["energies"][-1]}
     if 0 in results and modes[0] != 0 and world == 1:
         # errors of one evaluation in the tensor-core modes against FP64 from
         # identical amplitudes: those after two plain Jacobi iterations from zero
@@ -349,11 +340,7 @@ def run_gpu(args, cfg):
             amplitudes="after two FP64 Jacobi iterations from T=0",
             note="mixed evaluation (split TF32, FP32 accumulation per 4096-index chunk, "
                  "FP64 sums) minus FP64 evaluation; R*_max_rel relative to max|R|")
-        if 2 in results:
-            line["precision_i8"] = dict(
-                evaluation_errors(eng, solver, 2),
-                amplitudes="after two FP64 Jacobi iterations from T=0",
-                note="evaluation with FP64 emulated by int8 slices minus FP64 evaluation")
+
     if args.tune:
         rows = eng.tuning_report()
         line["tuning"] = {
@@ -377,6 +364,8 @@ def run_gpu(args, cfg):
     eng.close()
     del solver
     torch.cuda.empty_cache()
+    if args.precision == 1 and not args.no_i8:
+        line["i8"] = measure_i8(args, cfg, local, dist, peak)
     if args.tune and world == 1 and not args.no_fixed_rule:
         line["tuning"]["fixed_rule"] = measure_fixed_rule(args, cfg, local, modes[0])
     if not args.no_d2h and world == 1:
@@ -518,6 +507,50 @@ def measure_e2e(args, eng, solver):
             "d2h_bytes_per_step": 8 * sum(nR.values()) + 8}
 
 
+def measure_i8(args, cfg, local, dist, peak):
+    """seconds per iteration with FP64 emulated by int8 slices (precision
+    mode 2) on an engine of its own (the plans and cached operand panels of
+    three precision modes do not fit one device together), its roofline
+    launch, and the errors of one evaluation against FP64 from identical
+    amplitudes"""
+    import torch
+
+    import cc
+    import gccu
+    from devfill import TorchIntegrals
+    import hamiltonian as hm
+
+    sp, eps, B = setup_hamiltonian(cfg)
+    eng = gccu.Engine(local)
+    try:
+        eng.set_tuning(args.tune)
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+        eng.set_precision(2)
+        f = measure(args, cfg, eng, s, local, dist, 2, main=True)
+        out = {"metric": metric_of(cfg) + " FP64 emulated with int8 slices",
+               "value": f["ms"] / 1e3, "unit": "s", "ms_per_step": f["ms"], "e2e": f["e2e"],
+               "gpu_launches": f["launches"], "dtype": DTYPE[2],
+               "roofline": roofline(f, peak, 2, s, eng),
+               "clocks": clock_summary(f["samples"]),
+               "energy_last": f["energies"][-1]}
+        if dist is None:
+            reset_amplitudes(eng, s)
+            eng.set_precision(0)
+            for _ in range(2):
+                s.iterate()
+                s.step()
+            out["precision"] = dict(
+                evaluation_errors(eng, s, 2),
+                amplitudes="after two FP64 Jacobi iterations from T=0",
+                note="evaluation with FP64 emulated by int8 slices minus FP64 evaluation; "
+                     "R*_max_rel relative to max|R|")
+    finally:
+        eng.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def measure_use_tr(args, cfg, local, dist, modes, plain_energies):
     """seconds per iteration with spin-flip symmetry (calculate.routes.use_tr,
     the reference's default): half of the Ms cases of every contraction into
@@ -544,7 +577,7 @@ def measure_use_tr(args, cfg, local, dist, modes, plain_energies):
                         profile=False, e2e=False)
             ref = plain_energies[mode]
             k = min(3, len(ref), len(r["energies"]))
-            out["fp64" if mode == 0 else "mixed"] = {
+            out[{0: "fp64", 1: "mixed", 2: "i8"}[mode]] = {
                 "value": r["ms"] / 1e3, "unit": "s", "gpu_launches": r["launches"],
                 "clocks": clock_summary(r["samples"]),
                 "dE_first_iterations_vs_plain": max(
