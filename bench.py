@@ -793,6 +793,7 @@ def convergence(local, cfg, weights=None, maxiter=80, variants=None):
             t = {a: eng.download(s.lid(a), s.lists[a][1]) for a in s.amps}
             switched = getattr(s, "switched_at", None)
             fallbacks = getattr(s, "fallbacks", None)
+            planning = eng.plan_stats()
             if ref is None:
                 ref = hist[-1][1]
                 ref_t = t
@@ -810,7 +811,9 @@ def convergence(local, cfg, weights=None, maxiter=80, variants=None):
              "s_total_planned": hist_p[-1][3], "iterations_planned": hist_p[-1][0],
              "s_per_iteration_planned": (hist_p[-1][3] - hist_p[0][3]) /
                                         max(len(hist_p) - 1, 1),
-             "residual_every_5": [float(f"{x[2]:.2e}") for x in hist[4::5]]}
+             "residual_every_5": [float(f"{x[2]:.2e}") for x in hist[4::5]],
+             "planning": {k: (round(v, 3) if isinstance(v, float) else v)
+                          for k, v in planning.items()}}
         if label != "fp64":
             num = sum(float(np.sum((t[a] - ref_t[a]) ** 2)) for a in t)
             den = sum(float(np.sum(ref_t[a] ** 2)) for a in t)

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -245,6 +246,12 @@ class Engine {
   // call (cached by block-shape histogram), 2 force candidate tune_forced
   int tune = 0, tune_forced = 0;
   std::map<std::string, int> tuned;  // (precision, histogram) -> chosen candidate
+  // seconds spent making contraction plans: host planner, string maps,
+  // autotuner trials, plan build (tables, packs and splits of cached panels)
+  struct PlanStats {
+    double host_s = 0, maps_s = 0, tune_s = 0, build_s = 0;
+    int64_t plans = 0;
+  } pstats;
   struct TuneRecord {
     int64_t items;
     int chosen;
@@ -716,6 +723,7 @@ class Engine {
     s.tra2 = bc->tra_op2 != 0;
     s.tra12 = bc->tra_res != 0;
     auto dp = std::make_unique<DevPlan>();
+    const auto t0 = std::chrono::steady_clock::now();
     dp->plan = plan_contraction(model, s);
     dp->list1 = (int)bc->list_op1;
     dp->list2 = (int)bc->list_op2;
@@ -725,10 +733,23 @@ class Engine {
     dp->res_len = B12.len;
     Plan& P = dp->plan;
     if (host_only) return *(plans[key] = std::move(dp));
+    // planning time by stage (device work of each stage waited for)
+    auto lap = [&](double& acc, std::chrono::steady_clock::time_point& t) {
+      CUDA_OK(cudaStreamSynchronize(stream));
+      const auto now = std::chrono::steady_clock::now();
+      acc += std::chrono::duration<double>(now - t).count();
+      t = now;
+    };
+    auto t = t0;
+    lap(pstats.host_s, t);
     for (auto& r : P.maps) P.items[r.item].op[r.opnd].map[r.comp] = strmap(r.key);
+    lap(pstats.maps_s, t);
     dp->policy = tune == 2 ? tune_forced : tune == 1 ? autotune(*dp) : 0;
+    lap(pstats.tune_s, t);
     build_gemm(*dp, tile_policies(precision).at(dp->policy));
     if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);
+    lap(pstats.build_s, t);
+    ++pstats.plans;
     plan_order.push_back(dp.get());
     return *(plans[key] = std::move(dp));
   }
@@ -2287,6 +2308,18 @@ int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows) {
       r[1] = (double)t.chosen;
       for (size_t c = 0; c < t.ms.size() && c < 6; ++c) r[2 + c] = t.ms[c];
     }
+  });
+}
+
+int gccu_plan_stats(double* out) {
+  return guarded([&] {
+    GCCU_REQUIRE(out, "null argument");
+    const Engine& e = eng();
+    out[0] = (double)e.pstats.plans;
+    out[1] = e.pstats.host_s;
+    out[2] = e.pstats.maps_s;
+    out[3] = e.pstats.tune_s;
+    out[4] = e.pstats.build_s;
   });
 }
 

@@ -61,6 +61,7 @@ _SIGS = {
     "gccu_set_shard": [I64, I64],
     "gccu_set_tuning": [I64, I64],
     "gccu_tuning_report": [PD, I64, P64],
+    "gccu_plan_stats": [PD],
     "gccu_lp_set_weights": [PD, I64],
     "gccu_lp_get_weights": [PD, I64],
     "gccu_lp_precondition": [I64, I64, I64, I64, ctypes.c_double, ctypes.c_double],
@@ -314,6 +315,14 @@ class Engine:
         rows = np.zeros((256, 8))
         _call("gccu_tuning_report", _pd(rows), 256, _p64(n))
         return rows[: min(int(n[0]), 256)]
+
+    def plan_stats(self):
+        """{"plans", "host_s", "maps_s", "tune_s", "build_s"}: time spent
+        making contraction plans, by stage"""
+        out = np.zeros(5)
+        _call("gccu_plan_stats", _pd(out))
+        return {"plans": int(out[0]), "host_s": float(out[1]), "maps_s": float(out[2]),
+                "tune_s": float(out[3]), "build_s": float(out[4])}
 
     def set_shard(self, rank=0, nranks=1):
         """run only this rank's share of every contraction's output tiles"""

@@ -338,6 +338,12 @@ int gccu_set_tuning(int64_t mode, int64_t candidate);
 /* one row of 8 per tuned histogram: (block contractions, chosen candidate,
  * ms of candidates 0..5, -1 where there is none) */
 int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows);
+/* time spent making contraction plans since the engine started (no
+ * counterpart in the reference): out[0] plans made, out[1..4] seconds in the
+ * host planner, the string maps, the autotuner's trials and the plan builds
+ * (tables, uploads, cached operand panels); each stage's device work is
+ * waited for. */
+int gccu_plan_stats(double* out);
 
 /* ---- statistics -----------------------------------------------------------
  * dgemm shape statistics in the reference's accounting
