@@ -365,7 +365,8 @@ def run_gpu(args, cfg):
     del solver
     torch.cuda.empty_cache()
     if args.precision == 1 and not args.no_i8:
-        line["i8"] = measure_i8(args, cfg, local, dist, peak)
+        line["i8"] = measure_i8(args, cfg, local, dist, peak, 2)
+        line["i8_fast"] = measure_i8(args, cfg, local, dist, peak, 3)
     if args.tune and world == 1 and not args.no_fixed_rule:
         line["tuning"]["fixed_rule"] = measure_fixed_rule(args, cfg, local, modes[0])
     if not args.no_d2h and world == 1:
@@ -389,7 +390,9 @@ def run_gpu(args, cfg):
 
 METRIC_MODE = {0: "plain FP64", 1: "split-TF32 tensor cores, FP64 accumulation"}
 DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums",
-         2: "s8 slices x5 (15 products), s32 exact accumulate, f64 combine"}
+         2: "s8 slices x5 (15 products), s32 exact accumulate, f64 combine",
+         3: "s8 slices x4 (10 products), s32 exact accumulate, f64 combine"}
+SLICE_PRODUCTS = {2: 15, 3: 10}
 
 
 def reset_amplitudes(eng, solver):
@@ -507,12 +510,12 @@ def measure_e2e(args, eng, solver):
             "d2h_bytes_per_step": 8 * sum(nR.values()) + 8}
 
 
-def measure_i8(args, cfg, local, dist, peak):
+def measure_i8(args, cfg, local, dist, peak, mode):
     """seconds per iteration with FP64 emulated by int8 slices (precision
-    mode 2) on an engine of its own (the plans and cached operand panels of
-    three precision modes do not fit one device together), its roofline
-    launch, and the errors of one evaluation against FP64 from identical
-    amplitudes"""
+    mode 2: five slices, 3: four) on an engine of its own (the plans and
+    cached operand panels of three precision modes do not fit one device
+    together), its roofline launch, and the errors of one evaluation against
+    FP64 from identical amplitudes"""
     import torch
 
     import cc
@@ -526,12 +529,13 @@ def measure_i8(args, cfg, local, dist, peak):
         eng.set_tuning(args.tune)
         s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
         s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
-        eng.set_precision(2)
-        f = measure(args, cfg, eng, s, local, dist, 2, main=True)
-        out = {"metric": metric_of(cfg) + " FP64 emulated with int8 slices",
+        eng.set_precision(mode)
+        f = measure(args, cfg, eng, s, local, dist, mode, main=True)
+        out = {"metric": metric_of(cfg) + f" FP64 emulated with {SLICE_PRODUCTS[mode]} int8 "
+                                          "slice products",
                "value": f["ms"] / 1e3, "unit": "s", "ms_per_step": f["ms"], "e2e": f["e2e"],
-               "gpu_launches": f["launches"], "dtype": DTYPE[2],
-               "roofline": roofline(f, peak, 2, s, eng),
+               "gpu_launches": f["launches"], "dtype": DTYPE[mode],
+               "roofline": roofline(f, peak, mode, s, eng),
                "clocks": clock_summary(f["samples"]),
                "energy_last": f["energies"][-1]}
         if dist is None:
@@ -541,7 +545,7 @@ def measure_i8(args, cfg, local, dist, peak):
                 s.iterate()
                 s.step()
             out["precision"] = dict(
-                evaluation_errors(eng, s, 2),
+                evaluation_errors(eng, s, mode),
                 amplitudes="after two FP64 Jacobi iterations from T=0",
                 note="evaluation with FP64 emulated by int8 slices minus FP64 evaluation; "
                      "R*_max_rel relative to max|R|")
@@ -677,7 +681,7 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
            "iteration_flops": total_flops,
            "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12,
            "algorithmic_bytes_per_launch": alg_bytes}
-    kern = {0: "k_gemm", 1: "k_gemm_tc", 2: "k_gemm_i8"}[mode]
+    kern = {0: "k_gemm", 1: "k_gemm_tc", 2: "k_gemm_i8", 3: "k_gemm_i8"}[mode]
     if kern in TRAFFIC_PER_ALGORITHMIC_BYTE:
         out["traffic"] = TRAFFIC_PER_ALGORITHMIC_BYTE[kern] * alg_bytes
         out["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
@@ -685,17 +689,18 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
                                  "launch's algorithmic bytes")
     else:
         out["traffic"] = None
-    if mode == 2:
-        # int8 dense peak = 2 x dense BF16 on B200; 15 slice products per
-        # useful FP64 product
+    if mode in SLICE_PRODUCTS:
+        # int8 dense peak = 2 x dense BF16 on B200; 15 (10) slice products per
+        # useful FP64 product with five (four) slices
+        npr = SLICE_PRODUCTS[mode]
         burst, src = measured_bf16_tflops("bf16_tflops")
         sustained, _ = measured_bf16_tflops("bf16_tflops_sustained")
-        out.update(peak=burst * 2.0 / 15.0,
-                   kernel=f"k_gemm_i8 int8 slices (tcgen05 kind::i8, persistent), launch of "
-                          f"[CONTR] {ROOFLINE_CONTRACTION}",
+        out.update(peak=burst * 2.0 / npr,
+                   kernel=f"k_gemm_i8 {npr} int8 slice products (tcgen05 kind::i8, "
+                          f"persistent), launch of [CONTR] {ROOFLINE_CONTRACTION}",
                    peak_source=f"of {src}: bf16_tflops x 2 (dense int8 = twice dense BF16) "
-                               "/ 15 (slice products per useful product)",
-                   frac_of_sustained=achieved / (sustained * 2.0 / 15.0))
+                               f"/ {npr} (slice products per useful product)",
+                   frac_of_sustained=achieved / (sustained * 2.0 / npr))
         out["ladder_with_split_tflops"] = dom[0] / (dom[2] / dom[1] * 1e-3) / 1e12
     elif mode == 0:
         out.update(peak=fp64_peak_tflops,
@@ -736,10 +741,11 @@ def measured_bf16_tflops(key="bf16_tflops"):
 
 def convergence(local, cfg, weights=None, maxiter=80, variants=None):
     """time to |dE| < 1 uEh against the converged FP64 energy, per solve
-    variant: plain FP64 ("fp64"), FP64 emulated with int8 slices throughout
-    ("i8"), split TF32 until the residual norm is below 1e-4 and the int8
-    emulation after it ("mixed") and, given weights, the same with the
-    learned step ("mixed_learned"); `variants` adds labels: options of
+    variant: plain FP64 ("fp64"), FP64 emulated with five int8 slices
+    throughout ("i8"), four slices until the residual norm is below 1e-7 and
+    five after it ("mixed"), split TF32 until 1e-4 and five slices after it
+    ("mixed_tf32") and, given weights, "mixed" with the learned step
+    ("mixed_learned"); `variants` adds labels: options of
     CCSolver.solve_mixed, or {"plain": mode} for one precision throughout.
     Each variant is solved twice on one engine: from its first call, with
     every contraction planned and autotuned during the first iteration of
@@ -752,8 +758,9 @@ def convergence(local, cfg, weights=None, maxiter=80, variants=None):
     import hamiltonian as hm
     from devfill import TorchIntegrals
 
-    mixed = {"switch": 1e-4, "stall": None, "final": 2}
-    runs = {"fp64": {"plain": 0}, "i8": {"plain": 2}, "mixed": dict(mixed)}
+    mixed = {"schedule": [(3, 1e-7), (2, None)]}
+    runs = {"fp64": {"plain": 0}, "i8": {"plain": 2}, "mixed": dict(mixed),
+            "mixed_tf32": {"schedule": [(1, 1e-4), (2, None)]}}
     if weights is not None:
         runs["mixed_learned"] = dict(mixed, learned=True)
     runs.update(variants or {})

@@ -494,24 +494,31 @@ class CCSolver:
         self.graph = self.e.graph_end()
 
     def solve_mixed(self, maxiter=60, conv=1e-8, switch=1e-5, callback=None, stop=None,
-                    stall=None, reset_diis=False, final=0):
+                    stall=None, reset_diis=False, final=0, schedule=None):
         """Mixed-precision solve: the contractions run in split TF32 on the
         tensor cores (engine precision 1) while the residual norm is above
-        `switch`, and in precision `final` (0 = FP64) after that; the CC
-        fixed-point iteration corrects the errors of the cheaper iterations,
-        the DIIS subspace, residuals, energies and amplitude updates stay FP64
-        throughout.  With `stall`, the solve also switches once a split-TF32
-        residual norm is above `stall` times the previous one (the residual
-        has reached the split-TF32 error floor); `reset_diis` empties the DIIS
-        subspace at the switch.  Each mode's evaluation runs once eagerly
-        (planning) and is then replayed from its own CUDA graph.
-        stop(it, energy, residual) may end the solve early.  Returns the last
-        energy."""
-        graphs, planned = {}, set()
-        mode = 1
+        `switch`, and in precision `final` (0 = FP64, 2 = FP64 emulated with
+        int8 slices) after that; `schedule`, a list of (precision, residual
+        norm below which the next entry takes over; None for the last), sets
+        any sequence of precisions instead.  The CC fixed-point iteration
+        corrects the errors of the cheaper iterations; the DIIS subspace,
+        residuals, energies and amplitude updates stay FP64 throughout.  With
+        `stall`, the solve also moves on once a residual norm is above `stall`
+        times the previous one (the residual has reached the precision's error
+        floor); `reset_diis` empties the DIIS subspace at each switch.  Each
+        precision's evaluation runs once eagerly (planning) and is then
+        replayed from its own CUDA graph.  stop(it, energy, residual) may end
+        the solve early.  Returns the last energy; switched_at lists the
+        iterations after which the precision changed."""
+        if schedule is None:
+            schedule = [(1, switch), (final, None)]
+        stage = 0
+        mode = schedule[0][0]
         self.e.set_precision(mode)
+        graphs, planned = {}, set()
         en = None
         self.switched_at = None
+        switches = []
         prev = None
         for it in range(1, maxiter + 1):
             if mode not in graphs and mode in planned:
@@ -525,15 +532,18 @@ class CCSolver:
                 callback(it, en, rn)
             if rn < conv or (stop is not None and stop(it, en, rn)):
                 break
-            if mode == 1 and (rn < switch or (stall is not None and prev is not None and
-                                              rn > stall * prev)):
-                mode = final
+            limit = schedule[stage][1]
+            if limit is not None and (rn < limit or (stall is not None and prev is not None and
+                                                     rn > stall * prev)):
+                stage += 1
+                mode = schedule[stage][0]
                 self.e.set_precision(mode)
-                self.switched_at = it
+                switches.append(it)
                 if reset_diis and hasattr(self, "_diis"):
                     self._diis["used"].clear()
             prev = rn
             self.diis_step()
+        self.switched_at = switches[0] if len(switches) == 1 else (switches or None)
         self.e.set_precision(0)
         self.graph = None
         return en

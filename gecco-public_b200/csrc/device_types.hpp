@@ -75,7 +75,7 @@ struct GemmDesc {
   // workspace (or, for a frozen operand, their persistent arrays)
   int64_t ma, mb;
   double *ma_ptr, *mb_ptr;
-  int32_t i8;            // the tensor-core item runs on the int8 slices (mode 2)
+  int32_t i8;            // int8 slices per element of a tensor-core item (modes 2, 3), else 0
   int32_t pad2;
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups

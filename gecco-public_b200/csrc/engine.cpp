@@ -117,7 +117,7 @@ struct DevPlan {
   float* const_panels = nullptr;  // persistent split panels (floats)
   // precision mode 2 (int8 slices): the panels' row maxima, zeroed before
   // each slicing (workspace float range; the persistent panels' range)
-  bool i8 = false;
+  int i8 = 0;  // int8 slices per element (precision modes 2, 3), else 0
   int64_t max_off = 0, max_floats = 0, max_off_c = 0, max_floats_c = 0;
   std::vector<int> const_lists;   // the frozen lists behind them
   bool const_stale = false;       // a list of const_lists was unfrozen since they were made
@@ -179,7 +179,8 @@ class Engine {
   cudaEvent_t slots[64] = {};
   bool profiling = false;
   int precision = 0;     // 0: FP64 DMMA, 1: split TF32 on tcgen05 for regular/medium items,
-                         // 2: FP64 emulated with int8 slices on tcgen05 for the same items
+                         // 2, 3: FP64 emulated with 5 / 4 int8 slices on tcgen05 for the
+                         // same items
   // split-TF32 operand panels, shared by all plans (one stream orders them);
   // grown to the largest plan's need, never while a graph is being captured
   float* tc_ws = nullptr;
@@ -365,8 +366,8 @@ class Engine {
       launch_zero_tc(dp.const_panels, dp.max_off_c, dp.max_floats_c, stream);
     else
       launch_zero_tc(nullptr, dp.max_off, dp.max_floats, stream);
-    launch_slice_i8(0, descs, jobs, njobs, nchunks, dp.d_gather, stream);
-    launch_slice_i8(1, descs, jobs, njobs, nchunks, dp.d_gather, stream);
+    launch_slice_i8(0, dp.i8, descs, jobs, njobs, nchunks, dp.d_gather, stream);
+    launch_slice_i8(1, dp.i8, descs, jobs, njobs, nchunks, dp.d_gather, stream);
     launches += 3;
   }
   // the GEMM launch of one tile kind (the int8-slice kernel for the
@@ -374,7 +375,7 @@ class Engine {
   void run_gemm(const DevPlan& dp, int kind, const GemmDesc* descs, const TileDesc* tiles,
                 int64_t ntiles, double fact) {
     if (kind == kGemmTc && dp.i8)
-      launch_gemm_i8(descs, tiles, ntiles, fact, d_err, wait_limit, stream);
+      launch_gemm_i8(dp.i8, descs, tiles, ntiles, fact, d_err, wait_limit, stream);
     else
       launch_gemm(kind, descs, tiles, ntiles, fact, d_err, wait_limit, stream);
     ++launches;
@@ -1176,9 +1177,9 @@ class Engine {
       int TM, TN0;
       gemm_tile(kind, TM, TN0);
       if (kind == kGemmTc) {
-        dp.i8 = precision == 2;
+        dp.i8 = precision >= 2 ? i8_slices(precision) : 0;
         for (auto& d : g[kind]) {
-          d.tn = dp.i8 ? tc_tile_n(d.N, kI8N) : tc_tile_n(d.N);
+          d.tn = dp.i8 ? tc_tile_n(d.N, i8_widest(precision)) : tc_tile_n(d.N);
           d.i8 = dp.i8;
         }
       }
@@ -1245,7 +1246,8 @@ class Engine {
           for (int op = 0; op < 2; ++op) {
             const int64_t rows = op == 0 ? d.M : d.N;
             const int tr = op == 0 ? kGemmTcM : d.tn;
-            const int64_t fl = dp.i8 ? i8_panel_floats(rows, tr, d.K) : tc_panel_floats(rows, tr, d.K);
+            const int64_t fl =
+                dp.i8 ? i8_panel_floats(rows, tr, d.K, dp.i8) : tc_panel_floats(rows, tr, d.K);
             const int64_t ch = tc_split_chunks(rows, tr, d.K);
             int64_t& po = op == 0 ? d.pa : d.pb;
             if (frozen_op[op]) {
@@ -1770,8 +1772,8 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
     DevPlan& dp = *pp;
     int64_t ndesc = 0;
     for (int kind = 0; kind < kGemmKinds; ++kind) ndesc += dp.ndesc_g[kind];
-    GCCU_REQUIRE(!dp.i8, "gccu_contract_noalloc: precision mode 2 (int8 slices) is not "
-                         "supported by the allocation-free entry point");
+    GCCU_REQUIRE(!dp.i8, "gccu_contract_noalloc: precision modes 2 and 3 (int8 slices) are "
+                         "not supported by the allocation-free entry point");
     if (dp.scratch_len > kStaticPanelDoubles) {
       std::ostringstream os;
       os << "gccu_contract_noalloc: the operand panels of this contraction need "
@@ -2356,8 +2358,9 @@ int gccu_device_info(int64_t* info4) {
 
 int gccu_set_precision(int64_t mode) {
   return guarded([&] {
-    GCCU_REQUIRE(mode >= 0 && mode <= 2,
-                 "precision mode must be 0 (FP64), 1 (split TF32) or 2 (int8 slices)");
+    GCCU_REQUIRE(mode >= 0 && mode <= 3,
+                 "precision mode must be 0 (FP64), 1 (split TF32), 2 (five int8 slices) or 3 "
+                 "(four int8 slices)");
     eng().precision = (int)mode;
   });
 }

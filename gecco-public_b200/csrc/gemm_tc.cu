@@ -207,8 +207,8 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 // launches over the same chunks: OUT = 1 stages the chunk's values and
 // raises the rows' maxima of |x| (atomic maximum on the FP64 bit pattern,
 // which orders non-negative values like the values), OUT = 2 cuts every
-// element into its kI8Slices bytes under its row's scale 127 / m and writes
-// 16-byte vectors (16 contraction indices of one row and slice).
+// element into its IS bytes under its row's scale 127 / m and writes 16-byte
+// vectors (16 contraction indices of one row and slice).
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
 constexpr int kValPitch = SK + 1;         // doubles per row of a staged chunk (OUT > 0)
@@ -223,7 +223,7 @@ __device__ __forceinline__ double* panel_max(const GemmDesc& d, bool row_op) {
                 : (d.mb_ptr ? d.mb_ptr : reinterpret_cast<double*>(g_tc_ws + d.mb));
 }
 
-template <int OUT>
+template <int OUT, int IS = 1>
 __global__ void __launch_bounds__(kSplitThreads, 4)
     k_split_tc(const GemmDesc* __restrict__ descs, const SplitJob* __restrict__ jobs,
                int64_t njobs, const PackJob* __restrict__ gathers) {
@@ -439,16 +439,16 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
     const int64_t row = r0 + r;
     if (row >= padded) return;
     const double inv = inv_s[r];
-    uint32_t w[kI8Slices][4];
+    uint32_t w[IS][4];
 #pragma unroll
-    for (int s = 0; s < kI8Slices; ++s)
+    for (int s = 0; s < IS; ++s)
 #pragma unroll
       for (int q = 0; q < 4; ++q) w[s][q] = 0u;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       double u = U.v[r][16 * kh + j] * inv;  // |u| <= 127
 #pragma unroll
-      for (int s = 0; s < kI8Slices; ++s) {
+      for (int s = 0; s < IS; ++s) {
         const int a = __double2int_rn(u);  // |a| <= 127, then <= 64
         w[s][j >> 2] |= (uint32_t)(a & 0xff) << (8 * (j & 3));
         u = (u - (double)a) * 128.0;  // exact
@@ -457,9 +457,9 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
     uint8_t* const panel = reinterpret_cast<uint8_t*>(
         row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa) : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb));
     const int64_t band = row / TR, rr = row % TR, slice = c % nsl;
-    uint8_t* base = panel + ((band * nsl + slice) * kI8Slices * 2 + kh) * TR * 16 + rr * 16;
+    uint8_t* base = panel + ((band * nsl + slice) * IS * 2 + kh) * TR * 16 + rr * 16;
 #pragma unroll
-    for (int s = 0; s < kI8Slices; ++s)
+    for (int s = 0; s < IS; ++s)
       *reinterpret_cast<uint4*>(base + (int64_t)s * 2 * TR * 16) =
           make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
     return;
@@ -776,29 +776,31 @@ static_assert(TBM % kEpiWarps == 0 && kTcols % 16 == 0 && TBN % 32 == 0,
               "epilogue passes (tile widths are multiples of 32)");
 
 
-// ---- int8-slice GEMM (precision mode 2) -------------------------------------
+// ---- int8-slice GEMM (precision modes 2 and 3) -----------------------------
 // The structure of k_gemm_tc (persistent, producer / MMA / epilogue warps,
-// bounded waits), with the slices: a stage is one 32-index slice of all
-// kI8Slices row-operand and column-operand slices (one bulk copy each); the
-// MMA thread issues, per stage, the products of slices (s, t) with
-// s + t < kI8Slices into accumulator s + t (kind::i8, int32, K = 32 per
-// instruction).  The kI8Slices accumulators of a tile take kI8Slices * tn
-// TMEM columns, so there is one set: the epilogue reads it into registers
-// (FP64, sum over s + t of 2^(-7(s+t)) times the accumulator, exact before
-// the last rounding), releases it to the MMAs of the next tile and then
-// scales by the rows' and columns' m / 127 and scatters from the registers.
-constexpr int IS = kI8Slices;
-constexpr int IBN = kI8N;  // widest int8 tile
-constexpr int INST = 4;    // pipeline stages
-constexpr int kI8StageA = IS * 2 * TBM * 16;      // bytes of one stage of the row operand
-constexpr int kI8StageBMax = IS * 2 * IBN * 16;   // ... of the column operand, widest tile
+// bounded waits), with the slices: a stage is one 32-index slice of all IS
+// row-operand and column-operand slices (one bulk copy each); the MMA thread
+// issues, per stage, the products of slices (s, t) with s + t < IS into
+// accumulator s + t (kind::i8, int32, K = 32 per instruction).  The IS
+// accumulators of a tile take IS * tn TMEM columns, so there is one set.
+// With tiles up to 96 columns (IS = 5) the epilogue reads the set into
+// registers (FP64, sum over s + t of 2^(-7(s+t)) times the accumulator, exact
+// before the last rounding), releases it to the MMAs of the next tile and
+// then scales by the rows' and columns' m / 127 and scatters from the
+// registers; with 128-column tiles (IS = 4) a thread's 64 values do not fit
+// its registers, so the epilogue combines, scales and scatters column group
+// by column group from TMEM and releases the set at the end of the tile.
+constexpr int INST = 4;  // pipeline stages
 
+template <int IS, int IBN>
 struct __align__(1024) I8Smem {
-  uint8_t a[INST][kI8StageA];  // [stage][slice s][k/16][row][k%16]
-  uint8_t b[INST][kI8StageBMax];
-  double t[TBM][kTcols + 1];   // column-major epilogue staging
+  static constexpr int kStageA = IS * 2 * TBM * 16;  // bytes of one stage, row operand
+  static constexpr int kStageB = IS * 2 * IBN * 16;  // ... column operand, widest tile
+  uint8_t a[INST][kStageA];  // [stage][slice s][k/16][row][k%16]
+  uint8_t b[INST][kStageB];
+  double t[TBM][kTcols + 1];  // column-major epilogue staging
   int64_t cro[TBM], cco[IBN];
-  double rs[TBM], cs[IBN];     // row / column scales m / 127
+  double rs[TBM], cs[IBN];  // row / column scales m / 127
   int32_t rc[TBM][kDevMaxComp];
   int32_t cc[IBN][kDevMaxComp];
   GemmDesc d;
@@ -837,11 +839,33 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// the FP64 values of 8 consecutive columns of this thread's TMEM lane:
+// sum over the IS accumulators (one per slice order d, d * bn columns on)
+// of 2^(-7d) times the int32 sum, smallest orders first
+template <int IS>
+__device__ __forceinline__ void i8_combine8(uint32_t taddr, int bn, double (&x)[8]) {
+  uint32_t q[IS][8];
+#pragma unroll
+  for (int dd = 0; dd < IS; ++dd) tmem_ld8(taddr + (uint32_t)(dd * bn), q[dd]);
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    double v = 0.0;
+#pragma unroll
+    for (int dd = IS - 1; dd >= 0; --dd) v += ldexp(1.0, -7 * dd) * (double)(int)q[dd][j];
+    x[j] = v;
+  }
+}
+
+template <int IS, int IBN>
 __global__ void __launch_bounds__(TNT, 1)
     k_gemm_i8(const GemmDesc* __restrict__ descs, const TileDesc* __restrict__ tiles,
               int64_t ntiles, double alpha, int* err, long wait_limit) {
+  using Sm = I8Smem<IS, IBN>;
+  constexpr int kStageA = Sm::kStageA;
+  constexpr bool kEarly = IBN <= 96;  // release TMEM before the scatter (values in registers)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  I8Smem& S = *reinterpret_cast<I8Smem*>(smem_raw);
+  Sm& S = *reinterpret_cast<Sm*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     for (int s = 0; s < INST; ++s) {
@@ -856,7 +880,7 @@ __global__ void __launch_bounds__(TNT, 1)
     S.issued = 0;
     S.consumed = 0;
   }
-  if (warp == 0) {  // TMEM: all 512 columns (the kI8Slices accumulators of one tile)
+  if (warp == 0) {  // TMEM: all 512 columns (the IS accumulators of one tile)
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
                  : "r"(smem_u32(&S.tmem_base)), "r"(512u)
@@ -882,7 +906,7 @@ __global__ void __launch_bounds__(TNT, 1)
         const uint32_t sb = (uint32_t)(IS * 2 * bn * 16);
         const uint8_t* pa =
             reinterpret_cast<const uint8_t*>(dg->pa_ptr ? dg->pa_ptr : g_tc_ws + dg->pa) +
-            (int64_t)(td.m0 / TBM) * nsl * kI8StageA;
+            (int64_t)(td.m0 / TBM) * nsl * kStageA;
         const uint8_t* pb =
             reinterpret_cast<const uint8_t*>(dg->pb_ptr ? dg->pb_ptr : g_tc_ws + dg->pb) +
             (int64_t)(td.n0 / bn) * nsl * sb;
@@ -895,8 +919,8 @@ __global__ void __launch_bounds__(TNT, 1)
             break;
           }
           const uint32_t bar = smem_u32(&S.full[s]);
-          mbar_expect_tx(bar, (uint32_t)kI8StageA + sb);
-          bulk_g2s(S.a[s], pa + (g0 + t) * kI8StageA, (uint32_t)kI8StageA, bar);
+          mbar_expect_tx(bar, (uint32_t)kStageA + sb);
+          bulk_g2s(S.a[s], pa + (g0 + t) * kStageA, (uint32_t)kStageA, bar);
           bulk_g2s(S.b[s], pb + (g0 + t) * sb, sb, bar);
           S.issued = it + 1;
         }
@@ -978,79 +1002,117 @@ __global__ void __launch_bounds__(TNT, 1)
       epi_sync();
       if (*failed) break;  // the same in every epilogue thread after the barrier
       tc_fence_after();
-      // this thread: row 32*quarter + lane, columns c0 .. c0 + bn/2 - 1
       const int row = 32 * quarter + lane;
-      const int c0 = half * (bn / 2);
-      const uint32_t tl = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)c0;
-      double v[IBN / 2];
-#pragma unroll
-      for (int cb = 0; cb < IBN / 2; cb += 8) {
-        if (cb < bn / 2) {  // warp-uniform
-          uint32_t q[IS][8];  // the column group of every accumulator, one wait
-#pragma unroll
-          for (int dd = 0; dd < IS; ++dd) tmem_ld8(tl + (uint32_t)(dd * bn + cb), q[dd]);
-          tmem_wait_ld();
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            double x = 0.0;
-#pragma unroll
-            for (int dd = IS - 1; dd >= 0; --dd)  // smallest terms first
-              x += ldexp(1.0, -7 * dd) * (double)(int)q[dd][j];
-            v[cb + j] = x;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) v[cb + j] = 0.0;
-        }
-      }
-      // accumulators read (tcgen05.ld waited): release them to the next tile
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&S.acce));
+      const uint32_t tq = tmem + ((uint32_t)(32 * quarter) << 16);  // this warp's lanes
       const double f = alpha * d.fac;
       const double rsc = row < rows ? S.rs[row] : 0.0;
       const bool colfast = rows > 1 && cols > 1 && S.cco[1] - S.cco[0] == 1 &&
                            S.cro[1] - S.cro[0] != 1;
-      if (colfast) {
-        // passes of kTcols columns through shared memory, then every epilogue
-        // warp scatters rows ew, ew+8, .. with lanes on consecutive columns
-        for (int p0 = 0; p0 < cols; p0 += kTcols) {
+      constexpr int kRows = TBM / kEpiWarps, kBatch = 8;
+      // one staged pass of kTcols columns: every epilogue warp scatters rows
+      // ew, ew+8, .. with lanes on consecutive columns
+      auto scatter_pass = [&](int p0) {
 #pragma unroll
-          for (int j = 0; j < IBN / 2; ++j) {
-            const int col = c0 + j;
-            if (j < bn / 2 && col >= p0 && col < p0 + kTcols)
-              S.t[row][col - p0] = col < cols ? v[j] * rsc * S.cs[col] : 0.0;
+        for (int i0 = 0; i0 < kRows; i0 += kBatch) {
+          int rr[kBatch], cc[kBatch];
+          double y[kBatch];
+#pragma unroll
+          for (int i = 0; i < kBatch; ++i) {
+            rr[i] = ew + kEpiWarps * (i0 + i);
+            cc[i] = p0 + lane;
+            y[i] = S.t[rr[i]][lane];
           }
-          epi_sync();
-          constexpr int kRows = TBM / kEpiWarps, kBatch = 8;
-#pragma unroll
-          for (int i0 = 0; i0 < kRows; i0 += kBatch) {
-            int rr[kBatch], cc[kBatch];
-            double y[kBatch];
-#pragma unroll
-            for (int i = 0; i < kBatch; ++i) {
-              rr[i] = ew + kEpiWarps * (i0 + i);
-              cc[i] = p0 + lane;
-              y[i] = S.t[rr[i]][lane];
-            }
-            scatter<kBatch>(S, rr, cc, y, rows, cols, f);
-          }
-          epi_sync();
+          scatter<kBatch>(S, rr, cc, y, rows, cols, f);
         }
-      } else {
+      };
+      if constexpr (kEarly) {
+        // this thread: columns c0 .. c0 + bn/2 - 1 of its row, into registers
+        const int c0 = half * (bn / 2);
+        double v[IBN / 2];
 #pragma unroll
         for (int cb = 0; cb < IBN / 2; cb += 8) {
-          if (cb >= bn / 2 || c0 + cb >= cols) break;  // warp-uniform
-          int rr[8], cc[8];
-          double y[8];
+          double x[8];
+          if (cb < bn / 2) {  // warp-uniform
+            i8_combine8<IS>(tq + (uint32_t)(c0 + cb), bn, x);
+          } else {
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            rr[i] = row;
-            cc[i] = c0 + cb + i;
-            y[i] = cc[i] < cols ? v[cb + i] * rsc * S.cs[cc[i]] : 0.0;
+            for (int j = 0; j < 8; ++j) x[j] = 0.0;
           }
-          scatter<8>(S, rr, cc, y, rows, cols, f);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[cb + j] = x[j];
         }
+        // accumulators read (tcgen05.ld waited): release them to the next tile
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&S.acce));
+        if (colfast) {
+          for (int p0 = 0; p0 < cols; p0 += kTcols) {
+#pragma unroll
+            for (int j = 0; j < IBN / 2; ++j) {
+              const int col = c0 + j;
+              if (j < bn / 2 && col >= p0 && col < p0 + kTcols)
+                S.t[row][col - p0] = col < cols ? v[j] * rsc * S.cs[col] : 0.0;
+            }
+            epi_sync();
+            scatter_pass(p0);
+            epi_sync();
+          }
+        } else {
+#pragma unroll
+          for (int cb = 0; cb < IBN / 2; cb += 8) {
+            if (cb >= bn / 2 || c0 + cb >= cols) break;  // warp-uniform
+            int rr[8], cc[8];
+            double y[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              rr[i] = row;
+              cc[i] = c0 + cb + i;
+              y[i] = cc[i] < cols ? v[cb + i] * rsc * S.cs[cc[i]] : 0.0;
+            }
+            scatter<8>(S, rr, cc, y, rows, cols, f);
+          }
+        }
+      } else {
+        // combined, scaled and scattered from TMEM column group by column
+        // group; the accumulators are released at the end of the tile
+        if (colfast) {
+          for (int p0 = 0; p0 < cols; p0 += kTcols) {
+            if (((p0 / kTcols) & 1) == half) {  // the warps of one half stage the pass
+#pragma unroll
+              for (int cb = 0; cb < kTcols; cb += 8) {
+                double x[8];
+                i8_combine8<IS>(tq + (uint32_t)(p0 + cb), bn, x);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                  const int col = p0 + cb + j;
+                  S.t[row][cb + j] = col < cols ? x[j] * rsc * S.cs[col] : 0.0;
+                }
+              }
+            }
+            epi_sync();
+            scatter_pass(p0);
+            epi_sync();
+          }
+        } else {
+          const int c0 = half * (bn / 2);
+          for (int cb = 0; cb < bn / 2; cb += 8) {
+            if (c0 + cb >= cols) break;  // warp-uniform
+            double x[8];
+            i8_combine8<IS>(tq + (uint32_t)(c0 + cb), bn, x);
+            int rr[8], cc[8];
+            double y[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              rr[i] = row;
+              cc[i] = c0 + cb + i;
+              y[i] = cc[i] < cols ? x[i] * rsc * S.cs[cc[i]] : 0.0;
+            }
+            scatter<8>(S, rr, cc, y, rows, cols, f);
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&S.acce));
       }
       epi_sync();  // tables and descriptor free for the next tile
     }
@@ -1073,9 +1135,12 @@ __global__ void __launch_bounds__(TNT, 1)
                  : "memory");
 }
 
-static_assert(sizeof(I8Smem) <= 227 * 1024, "int8 tile exceeds shared memory");
-static_assert(IBN % 32 == 0 && IBN / 2 % 16 == 0, "int8 tile width: epilogue column groups");
-static_assert(kI8StageA % 16 == 0 && kI8StageBMax % 16 == 0, "bulk copies move multiples of 16 bytes");
+static_assert(sizeof(I8Smem<kI8SlicesFine, kI8NFine>) <= 227 * 1024 &&
+                  sizeof(I8Smem<kI8SlicesFast, kI8NFast>) <= 227 * 1024,
+              "int8 tile exceeds shared memory");
+static_assert(kI8NFine % 32 == 0 && kI8NFast % 32 == 0 && kI8NFine / 2 % 8 == 0,
+              "int8 tile widths: epilogue column groups");
+
 
 }  // namespace
 
@@ -1102,13 +1167,17 @@ void launch_zero_tc(float* base, int64_t off, int64_t n, cudaStream_t s) {
   k_zero_tc<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, s>>>(base, off, n);
 }
 
-void launch_slice_i8(int phase, const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
-                     int64_t nchunks, const PackJob* gathers, cudaStream_t s) {
+void launch_slice_i8(int phase, int slices, const GemmDesc* descs, const SplitJob* jobs,
+                     int64_t njobs, int64_t nchunks, const PackJob* gathers, cudaStream_t s) {
   if (njobs == 0 || nchunks == 0) return;
   if (phase == 0)
     k_split_tc<1><<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
+  else if (slices == kI8SlicesFast)
+    k_split_tc<2, kI8SlicesFast>
+        <<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
   else
-    k_split_tc<2><<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
+    k_split_tc<2, kI8SlicesFine>
+        <<<(unsigned)nchunks, kSplitThreads, 0, s>>>(descs, jobs, njobs, gathers);
 }
 
 void launch_gemm_tc(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
@@ -1136,13 +1205,14 @@ cudaError_t tc_kernel_attributes(cudaFuncAttributes* attr) {
   return cudaFuncGetAttributes(attr, k_gemm_tc);
 }
 
-void launch_gemm_i8(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
-                    int* err, int64_t wait_limit, cudaStream_t s) {
-  if (ntiles == 0) return;
-  const size_t smem = sizeof(I8Smem);
+template <int IS, int IBN>
+static void launch_gemm_i8_t(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
+                             double alpha, int* err, int64_t wait_limit, cudaStream_t s) {
+  const size_t smem = sizeof(I8Smem<IS, IBN>);
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_gemm_i8<IS, IBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     configured = true;
   }
   static int nsm = 0;
@@ -1153,12 +1223,21 @@ void launch_gemm_i8(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles
     if (nsm <= 0) nsm = 148;
   }
   const int64_t grid = ntiles < nsm ? ntiles : nsm;
-  k_gemm_i8<<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err,
-                                                (long)wait_limit);
+  k_gemm_i8<IS, IBN><<<(unsigned)grid, TNT, smem, s>>>(descs, tiles, ntiles, alpha, err,
+                                                         (long)wait_limit);
+}
+
+void launch_gemm_i8(int slices, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
+                    double alpha, int* err, int64_t wait_limit, cudaStream_t s) {
+  if (ntiles == 0) return;
+  if (slices == kI8SlicesFast)
+    launch_gemm_i8_t<kI8SlicesFast, kI8NFast>(descs, tiles, ntiles, alpha, err, wait_limit, s);
+  else
+    launch_gemm_i8_t<kI8SlicesFine, kI8NFine>(descs, tiles, ntiles, alpha, err, wait_limit, s);
 }
 
 cudaError_t i8_kernel_attributes(cudaFuncAttributes* attr) {
-  return cudaFuncGetAttributes(attr, k_gemm_i8);
+  return cudaFuncGetAttributes(attr, k_gemm_i8<kI8SlicesFine, kI8NFine>);
 }
 
 }  // namespace gccu

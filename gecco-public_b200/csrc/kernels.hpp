@@ -77,32 +77,41 @@ inline int tc_tile_n(int64_t N, int widest = kGemmTcN) {
   return (int)(w < widest ? w : widest);
 }
 
-// FP64 emulation on the int8 tensor cores (precision mode 2, the slicing
-// scheme of Ozaki et al.): an operand row x (row of the row operand, column
-// of the column operand) with m = max |x_k| is cut into kI8Slices signed
+// FP64 emulation on the int8 tensor cores (precision modes 2 and 3, the
+// slicing scheme of Ozaki et al.): an operand row x (row of the row operand,
+// column of the column operand) with m = max |x_k| is cut into S signed
 // bytes per element, x_k ~ (m / 127) * sum_s a_s,k 2^(-7 s), |a_0| <= 127 and
 // |a_s| <= 64 after it (each slice the rounded remainder of the one before);
-// the products of slices s and t with s + t < kI8Slices are summed over the
+// the products of slices s and t with s + t < S are summed over the
 // contraction in int32 (exactly, for contraction ranges up to kI8Chunk), one
-// TMEM accumulator per s + t, and combined in FP64 in the epilogue.  The
-// panels use the split-TF32 chunk geometry (128-row x 32-index chunks); per
-// 32-index slice, a band of TR rows holds kI8Slices x 2 core-matrix planes
-// of TR x 16 bytes:
-//   panel[(((band * nslice + slice) * kI8Slices + s) * 2 + k/16) * TR * 16 + row * 16 + k%16]
+// TMEM accumulator per s + t, and combined in FP64 in the epilogue.  Mode 2
+// keeps S = 5 slices (about 35 bits of each element relative to its row
+// maximum; 15 products, tiles up to 96 columns), mode 3 S = 4 (28 bits; 10
+// products, tiles up to 128 columns).  The panels use the split-TF32 chunk
+// geometry (128-row x 32-index chunks); per 32-index slice, a band of TR
+// rows holds S x 2 core-matrix planes of TR x 16 bytes:
+//   panel[(((band * nslice + slice) * S + s) * 2 + k/16) * TR * 16 + row * 16 + k%16]
 // and every panel has an array of its rows' maxima m (FP64, padded rows).
-constexpr int kI8Slices = 5;
-constexpr int kI8N = 96;             // widest tile: kI8Slices accumulators of kI8N columns
+constexpr int kI8SlicesFine = 5, kI8NFine = 96;   // precision mode 2
+constexpr int kI8SlicesFast = 4, kI8NFast = 128;  // precision mode 3
 constexpr int64_t kI8Chunk = 65536;  // contraction range of one int32 accumulation
-static_assert(kI8Slices * kI8N <= 512, "the accumulators fill at most the 512 TMEM columns");
-static_assert(kI8Slices <= 6 && (2 * 127 * 64 + (kI8Slices - 2) * 64 * 64) * kI8Chunk < (1ll << 31),
+inline int i8_slices(int precision) { return precision == 3 ? kI8SlicesFast : kI8SlicesFine; }
+inline int i8_widest(int precision) { return precision == 3 ? kI8NFast : kI8NFine; }
+// the largest |sum over s + t = d of a_s b_t| per contraction index, d < S
+constexpr int64_t i8_term_bound(int S) { return 2 * 127 * 64 + (S - 2) * 64 * 64; }
+static_assert(kI8SlicesFine * kI8NFine <= 512 && kI8SlicesFast * kI8NFast <= 512,
+              "the accumulators fill at most the 512 TMEM columns");
+static_assert(i8_term_bound(kI8SlicesFine) * kI8Chunk < (1ll << 31) &&
+                  i8_term_bound(kI8SlicesFast) * kI8Chunk < (1ll << 31) &&
+                  127 * 127 * kI8Chunk < (1ll << 31),
               "an int32 accumulator must not overflow over one contraction chunk");
 inline int64_t i8_padded_rows(int64_t rows, int tile_rows) {
   return (rows + tile_rows - 1) / tile_rows * tile_rows;
 }
 // floats of one operand's slice panel (bytes / 4)
-inline int64_t i8_panel_floats(int64_t rows, int tile_rows, int64_t K) {
+inline int64_t i8_panel_floats(int64_t rows, int tile_rows, int64_t K, int slices) {
   return i8_padded_rows(rows, tile_rows) * ((K + kTcSlice - 1) / kTcSlice) * kTcSlice *
-         kI8Slices / 4;
+         slices / 4;
 }
 // floats of one operand's row maxima (one double per padded row)
 inline int64_t i8_max_floats(int64_t rows, int tile_rows) {
@@ -116,13 +125,14 @@ void launch_split_tc(const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
                      const PackJob* gathers, cudaStream_t s);
 // precision mode 2: the row maxima of the panels (phase 0; the maxima must be
 // zero before it), then the slices (phase 1), same jobs and chunks as the split
-void launch_slice_i8(int phase, const GemmDesc* descs, const SplitJob* jobs, int64_t njobs,
-                     int64_t nchunks, const PackJob* gathers, cudaStream_t s);
+void launch_slice_i8(int phase, int slices, const GemmDesc* descs, const SplitJob* jobs,
+                     int64_t njobs, int64_t nchunks, const PackJob* gathers, cudaStream_t s);
 // zero n floats at base + off (base null: the tensor-core workspace)
 void launch_zero_tc(float* base, int64_t off, int64_t n, cudaStream_t s);
-// the int8-slice GEMM over 128 x kI8N tiles (err, wait_limit: as launch_gemm_tc)
-void launch_gemm_i8(const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles, double alpha,
-                    int* err, int64_t wait_limit, cudaStream_t s);
+// the int8-slice GEMM over 128 x i8_widest tiles with `slices` slices
+// (err, wait_limit: as launch_gemm_tc)
+void launch_gemm_i8(int slices, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
+                    double alpha, int* err, int64_t wait_limit, cudaStream_t s);
 cudaError_t i8_kernel_attributes(cudaFuncAttributes* attr);
 // device address of the split-TF32 workspace used by the two kernels above
 // (a device-side variable, so captured graphs follow a reallocation)

@@ -265,7 +265,8 @@ class Engine:
 
     def set_precision(self, mode):
         """0 = FP64 (default), 1 = split TF32 on the tcgen05 tensor cores,
-        2 = FP64 emulated with int8 slices on the tcgen05 tensor cores"""
+        2 = FP64 emulated with five int8 slices on the tcgen05 tensor
+        cores, 3 = the same with four slices"""
         _call("gccu_set_precision", int(mode))
 
     # ---- learned correction of the diagonal step

@@ -300,8 +300,10 @@ int gccu_sync(void);
  * cores for the same block contractions: each operand row is cut into five
  * signed 8-bit slices under the row's scale (maximum / 127), the slice
  * products of order s + t < 5 are summed exactly in int32 and combined in
- * FP64 (about 35 bits of each operand relative to its row maximum; not
- * supported by gccu_contract_noalloc).  Plans are kept per mode, so a
+ * FP64 (about 35 bits of each operand relative to its row maximum); 3 = the
+ * same with four slices (10 products, 28 bits, tiles up to 128 columns);
+ * modes 2 and 3 are not supported by gccu_contract_noalloc.  Plans are kept
+ * per mode, so a
  * solver can switch precision for its final iterations.  A pipeline wait
  * that times out inside a kernel is reported as an error by the next call
  * that synchronises (gccu_sync, norms, downloads). */
