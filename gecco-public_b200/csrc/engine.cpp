@@ -251,8 +251,17 @@ class Engine {
   // autotuner trials, plan build (tables, packs and splits of cached panels)
   struct PlanStats {
     double host_s = 0, maps_s = 0, tune_s = 0, build_s = 0;
+    // parts of build_s: host tables, their upload, cached operand panels
+    double tables_s = 0, upload_s = 0, const_s = 0;
     int64_t plans = 0;
   } pstats;
+  std::chrono::steady_clock::time_point bt;  // stage clock inside build_gemm
+  void blap(double& acc) {
+    CUDA_OK(cudaStreamSynchronize(stream));
+    const auto now = std::chrono::steady_clock::now();
+    acc += std::chrono::duration<double>(now - bt).count();
+    bt = now;
+  }
   struct TuneRecord {
     int64_t items;
     int chosen;
@@ -980,6 +989,7 @@ class Engine {
 
   // GEMM descriptors, offset tables, pack jobs and tiles of one plan
   void build_gemm(DevPlan& dp, const TilePolicy& pol) {
+    bt = std::chrono::steady_clock::now();
     Plan& P = dp.plan;
     const double* x1 = list(dp.list1).d;
     const double* x2 = list(dp.list2).d;
@@ -1054,7 +1064,9 @@ class Engine {
       t.cco = put([&](std::vector<int64_t>& v) { part_table(it, it.op[2], kEx2, it.N, v); });
     }
     if (tabs.empty()) tabs.push_back(0);
+    blap(pstats.tables_s);
     dp.d_tabs = upload(tabs);
+    blap(pstats.upload_s);
     dp.scratch = scratch ? (double*)alloc(scratch * sizeof(double)) : nullptr;
     dp.scratch_len = scratch;
     std::vector<GemmDesc> g[kGemmKinds];
@@ -1309,7 +1321,9 @@ class Engine {
     for (int kind = 0; kind < kGemmKinds; ++kind) dp.ntiles += dp.ntiles_g[kind];
     if (const_used[0]) dp.const_lists.push_back(dp.list1);
     if (const_used[1] && dp.list2 != dp.list1) dp.const_lists.push_back(dp.list2);
+    blap(pstats.tables_s);
     run_const(dp, true);  // the cached panels, made once here
+    blap(pstats.const_s);
   }
 
   // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
@@ -2322,6 +2336,9 @@ int gccu_plan_stats(double* out) {
     out[2] = e.pstats.maps_s;
     out[3] = e.pstats.tune_s;
     out[4] = e.pstats.build_s;
+    out[5] = e.pstats.tables_s;
+    out[6] = e.pstats.upload_s;
+    out[7] = e.pstats.const_s;
   });
 }
 

@@ -320,10 +320,11 @@ class Engine:
     def plan_stats(self):
         """{"plans", "host_s", "maps_s", "tune_s", "build_s"}: time spent
         making contraction plans, by stage"""
-        out = np.zeros(5)
+        out = np.zeros(8)
         _call("gccu_plan_stats", _pd(out))
         return {"plans": int(out[0]), "host_s": float(out[1]), "maps_s": float(out[2]),
-                "tune_s": float(out[3]), "build_s": float(out[4])}
+                "tune_s": float(out[3]), "build_s": float(out[4]), "tables_s": float(out[5]),
+                "upload_s": float(out[6]), "const_s": float(out[7])}
 
     def set_shard(self, rank=0, nranks=1):
         """run only this rank's share of every contraction's output tiles"""

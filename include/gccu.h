@@ -343,8 +343,11 @@ int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows);
 /* time spent making contraction plans since the engine started (no
  * counterpart in the reference): out[0] plans made, out[1..4] seconds in the
  * host planner, the string maps, the autotuner's trials and the plan builds
- * (tables, uploads, cached operand panels); each stage's device work is
- * waited for. */
+ * (tables, uploads, cached operand panels), of which out[5] building the
+ * plans' tables and descriptors on the host (with their small uploads and
+ * the operand scratch allocation), out[6] the upload of the offset tables
+ * and out[7] making the cached panels of frozen operands; each stage's
+ * device work is waited for. */
 int gccu_plan_stats(double* out);
 
 /* ---- statistics -----------------------------------------------------------
