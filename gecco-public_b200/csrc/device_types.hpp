@@ -76,7 +76,7 @@ struct GemmDesc {
   int64_t ma, mb;
   double *ma_ptr, *mb_ptr;
   int32_t i8;            // int8 slices per element of a tensor-core item (modes 2, 3), else 0
-  int32_t pad2;
+  int32_t ga;            // thin items: 1 + index of the row operand's gather description, or 0
   int32_t rowspace;      // kEx1 or kEx2 (swapped)
   int32_t cmapped;       // result components that need map lookups
   int32_t exclusive;     // no other tile writes these result elements: plain update

@@ -60,6 +60,7 @@ struct TilePolicy {
   int64_t tc_min_k = kTcMinK;     // shortest contraction sent to the tensor cores
   bool tc_thin = false;           // 9..medium_max columns go to the tensor cores too
   bool ksplit = true;             // split contractions over CTAs when a launch has few tiles
+  bool thin = true;               // <= 32 columns (results without map lookups): k_thin
 };
 
 // an autotuned alternative must take at most this fraction of the fixed
@@ -69,6 +70,9 @@ constexpr double kTuneMargin = 0.97;
 // candidates per precision mode; candidate 0 is the fixed rule
 inline std::vector<TilePolicy> tile_policies(int precision) {
   std::vector<TilePolicy> v(1);
+  TilePolicy nothin;
+  nothin.thin = false;
+  v.push_back(nothin);
   if (precision == 0) {
     TilePolicy a;
     a.medium_max = 64;
@@ -118,6 +122,9 @@ struct DevPlan {
   // precision mode 2 (int8 slices): the panels' row maxima, zeroed before
   // each slicing (workspace float range; the persistent panels' range)
   int i8 = 0;  // int8 slices per element (precision modes 2, 3), else 0
+  // the thin launch: column count it is compiled for, longest contraction range of a tile
+  int thin_nc = 1;
+  int64_t thin_kmax = 0;
   int64_t max_off = 0, max_floats = 0, max_off_c = 0, max_floats_c = 0;
   std::vector<int> const_lists;   // the frozen lists behind them
   bool const_stale = false;       // a list of const_lists was unfrozen since they were made
@@ -385,6 +392,8 @@ class Engine {
                 int64_t ntiles, double fact) {
     if (kind == kGemmTc && dp.i8)
       launch_gemm_i8(dp.i8, descs, tiles, ntiles, fact, d_err, wait_limit, stream);
+    else if (kind == kGemmThin)
+      launch_thin(dp.thin_nc, descs, tiles, ntiles, dp.d_gather, dp.thin_kmax, fact, stream);
     else
       launch_gemm(kind, descs, tiles, ntiles, fact, d_err, wait_limit, stream);
     ++launches;
@@ -827,6 +836,12 @@ class Engine {
         kind_of[i] = kGemmTc;
         swapped[i] = 0;
       }
+      // thin column side (after the swap), result without map lookups, long
+      // operand read in place: the streaming kernel
+      if (pol.thin && (kind_of[i] == kGemmMedium || kind_of[i] == kGemmSkinny) &&
+          (swapped[i] ? it.M : it.N) <= kThinMaxColumns && it.op[2].nmap == 0 &&
+          it.op[swapped[i] ? 1 : 0].nmap <= kTcGatherMaps)
+        kind_of[i] = kGemmThin;
     }
   }
 
@@ -1019,7 +1034,14 @@ class Engine {
     auto tcgather = [&](size_t i, int op) {
       return maps_of(i, op) && kind_of[i] == kGemmTc && P.items[i].op[op].nmap <= kTcGatherMaps;
     };
-    auto packed = [&](size_t i, int op) { return maps_of(i, op) && !tcgather(i, op); };
+    // the long operand of a thin item (the row side after the swap), read in
+    // place by k_thin through its gather description
+    auto thingather = [&](size_t i, int op) {
+      return maps_of(i, op) && kind_of[i] == kGemmThin && op == (swapped[i] ? 1 : 0);
+    };
+    auto packed = [&](size_t i, int op) {
+      return maps_of(i, op) && !tcgather(i, op) && !thingather(i, op);
+    };
     struct PackTab { int64_t roff, koff, rmi, kmi; };
     std::vector<PackTab> ptab1(P.items.size()), ptab2(P.items.size());
     auto pack_tabs = [&](const ItemDesc& it, int op, PackTab& pt) {
@@ -1036,7 +1058,7 @@ class Engine {
       Tab& t = toff[i];
       if (maps_of(i, 0)) pack_tabs(it, 0, ptab1[i]);
       if (maps_of(i, 1)) pack_tabs(it, 1, ptab2[i]);
-      if (tcgather(i, 0)) {  // read in place by the split pre-pass
+      if (tcgather(i, 0) || thingather(i, 0)) {  // read in place by the split pre-pass / k_thin
         t.aro = ptab1[i].roff;
         t.ako = ptab1[i].koff;
       } else if (packed(i, 0)) {  // panel[k*M + r]
@@ -1048,7 +1070,7 @@ class Engine {
         t.aro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kEx1, it.M, v); });
         t.ako = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kCnt, it.K, v); });
       }
-      if (tcgather(i, 1)) {
+      if (tcgather(i, 1) || thingather(i, 1)) {
         t.bco = ptab2[i].roff;
         t.bko = ptab2[i].koff;
       } else if (packed(i, 1)) {  // panel[k*N + c]
@@ -1149,6 +1171,11 @@ class Engine {
       }
       group_of[i] = kind;
       g[kind].push_back(d);
+      for (int op = 0; op < 2; ++op)
+        if (thingather(i, op)) {
+          g[kind].back().ga = (int32_t)gathers.size() + 1;
+          gathers.push_back(job_of(i, op, nullptr));
+        }
       for (int op = 0; op < 2; ++op) {
         if (!tcgather(i, op)) continue;
         GCCU_REQUIRE(!swapped[i], "tensor-core items keep their operand roles");
@@ -1196,6 +1223,12 @@ class Engine {
         }
       }
       auto width = [&](const GemmDesc& d) { return kind == kGemmTc ? d.tn : TN0; };
+      if (kind == kGemmThin) {  // one launch: the widest item's column count
+        dp.thin_nc = 1;
+        dp.thin_kmax = 0;
+        for (auto& d : g[kind]) dp.thin_nc = std::max(dp.thin_nc, thin_columns(d.N));
+        GCCU_REQUIRE(dp.thin_nc <= kThinMaxColumns, "thin tiles take at most 32 columns");
+      }
       std::vector<TileDesc> tiles;
       int64_t total = 0;
       for (auto& d : g[kind]) total += ((d.M + TM - 1) / TM) * ((d.N + width(d) - 1) / width(d));
@@ -1210,12 +1243,21 @@ class Engine {
         } else if (kind == kGemmTc) {  // FP32 (int32) accumulation over at most kTcChunk
           const int64_t ch = dp.i8 ? kI8Chunk : kTcChunk;  // (kI8Chunk) indices
           ks = std::max<int64_t>(1, (d.K + ch - 1) / ch);
+        } else if (kind == kGemmThin) {
+          // a tile's range of the thin operand fits the staged panel; with
+          // few tiles the contraction is split over CTAs as well
+          const int64_t lim = dp.thin_nc > 1 ? kThinMaxElems / dp.thin_nc : d.K;
+          ks = std::max<int64_t>(1, (d.K + lim - 1) / lim);
+          if (total < want && d.K > 64)
+            ks = std::max(ks, std::min<int64_t>((d.K + 63) / 64,
+                                                (want + total - 1) / std::max<int64_t>(total, 1)));
         } else if (pol.ksplit && total < want && d.K > 4 * kGemmK) {
           ks = std::min<int64_t>((d.K + 255) / 256, (want + total - 1) / std::max<int64_t>(total, 1));
           ks = std::max<int64_t>(ks, 1);
         }
         int64_t kchunk = ((d.K + ks - 1) / ks + kGemmK - 1) / kGemmK * kGemmK;
         d.exclusive = kind != kGemmSmall && !d.cmapped && writers[d.c] == 1 && kchunk >= d.K;
+        if (kind == kGemmThin) dp.thin_kmax = std::max(dp.thin_kmax, std::min(kchunk, d.K));
         auto add = [&](int64_t m, int64_t n, int64_t k0) {
           TileDesc tl{};
           tl.item = (int32_t)i;
@@ -1847,10 +1889,8 @@ int gccu_contract_noalloc(const gccu_bc_desc* bc, double fact, int64_t update, i
       }
       int64_t lo, hi;
       e.shard_range(dp.ntiles_g[kind], lo, hi);
-      if (hi > lo)
-        launch_gemm(kind, descs, dp.d_tiles_g[kind] + lo, hi - lo, fact, e.d_err, e.wait_limit,
-                    e.stream);
-      e.launches += 2;
+      if (hi > lo) e.run_gemm(dp, kind, descs, dp.d_tiles_g[kind] + lo, hi - lo, fact);
+      ++e.launches;
     }
     if (dp.plan.use_tr && dp.nflip) {
       launch_sym_ab(dp.d_flip, dp.nflip, r.d, 0.5, dp.flip_maxlen, e.stream);

@@ -19,8 +19,12 @@ void launch_strmap(const int32_t* tab1, int nel1, int64_t n1, const int32_t* tab
 // tile shapes of the grouped GEMM: regular items, medium (<= 32 columns) and
 // thin (<= 8 columns) items, items with at most 16 result elements
 constexpr int kGemmRegular = 0, kGemmSkinny = 1, kGemmSmall = 2, kGemmMedium = 3;
-constexpr int kGemmTc = 4;  // split-TF32 tensor-core tiles (precision mode 1)
-constexpr int kGemmKinds = 5;
+constexpr int kGemmTc = 4;  // tensor-core tiles (precision modes 1-3)
+constexpr int kGemmThin = 5;  // thin column side, streaming kernel (k_thin)
+constexpr int kGemmKinds = 6;
+constexpr int kGemmThinM = 256;       // rows of a thin tile (one thread each)
+constexpr int64_t kThinMaxElems = 12288;  // thin-operand elements staged per tile
+constexpr int kThinMaxColumns = 32;       // widest thin side (k_thin is compiled up to 32)
 constexpr int kGemmTcM = 128, kGemmTcN = 256;
 constexpr int64_t kTcChunk = 4096;  // contraction range of one FP32 accumulation
 constexpr int64_t kTcMinK = 256;    // shortest contraction sent to the tensor cores
@@ -35,6 +39,7 @@ inline void gemm_tile(int kind, int& TM, int& TN) {
        : kind == kGemmMedium ? kGemmMediumM
        : kind == kGemmSkinny ? kGemmSkinnyM
        : kind == kGemmTc     ? kGemmTcM
+       : kind == kGemmThin   ? kGemmThinM
                              : 1 << 30;
   TN = kind == kGemmRegular ? kGemmRegularN
        : kind == kGemmMedium ? kGemmMediumN
@@ -42,6 +47,14 @@ inline void gemm_tile(int kind, int& TM, int& TN) {
        : kind == kGemmTc     ? kGemmTcN
                              : 1 << 30;
 }
+
+// block contractions with at most 32 columns, one thread per row of the
+// long operand (read in place, through its gather description when it needs
+// map lookups: 1 + index in `gathers`, GemmDesc::ga); nc = thin_columns(the
+// launch's widest item), kmax = its longest contraction range per tile
+int thin_columns(int64_t N);
+void launch_thin(int nc, const GemmDesc* descs, const TileDesc* tiles, int64_t ntiles,
+                 const PackJob* gathers, int64_t kmax, double alpha, cudaStream_t s);
 
 // gather map-addressed operands into dense panels (one job per operand/item);
 // pack_geometry gives the grid extent one job needs, the launch uses the

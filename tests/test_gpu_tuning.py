@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 SPACE = (1, [[6], [24], [0], [0]])
 TOL = {0: 1e-12, 1: 2e-5}
-NCAND = {0: 3, 1: 5}
+NCAND = {0: 4, 1: 6}
 
 
 def _run(e, o, case, seed, mode):
