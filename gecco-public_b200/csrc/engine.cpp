@@ -60,7 +60,7 @@ struct TilePolicy {
   int64_t tc_min_k = kTcMinK;     // shortest contraction sent to the tensor cores
   bool tc_thin = false;           // 9..medium_max columns go to the tensor cores too
   bool ksplit = true;             // split contractions over CTAs when a launch has few tiles
-  bool thin = true;               // <= 32 columns (results without map lookups): k_thin
+  bool thin = false;              // <= 32 columns (results without map lookups): k_thin
 };
 
 // an autotuned alternative must take at most this fraction of the fixed
@@ -70,9 +70,9 @@ constexpr double kTuneMargin = 0.97;
 // candidates per precision mode; candidate 0 is the fixed rule
 inline std::vector<TilePolicy> tile_policies(int precision) {
   std::vector<TilePolicy> v(1);
-  TilePolicy nothin;
-  nothin.thin = false;
-  v.push_back(nothin);
+  TilePolicy thin;
+  thin.thin = true;
+  v.push_back(thin);
   if (precision == 0) {
     TilePolicy a;
     a.medium_max = 64;
@@ -955,20 +955,29 @@ class Engine {
   // space sp, for every composite index of that space
   static void part_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
                          std::vector<int64_t>& out) {
-    int32_t comp[kDevMaxComp];
+    // offset = sum over the space's components q of comp_q * coef_q; the
+    // composite index advances like an odometer (first component fastest),
+    // so each entry costs one addition instead of a mixed-radix division
+    const int nq = it.nsp[sp];
+    int64_t coef[kDevMaxComp] = {};
+    for (int j = 0; j < od.ncomp; ++j) {
+      if (od.map[j] || (od.sp1[j] != kNone && od.sp2[j] != kNone)) continue;
+      if (od.sp1[j] == sp) coef[od.ci1[j]] += od.ldim[j];
+      else if (od.sp2[j] == sp) coef[od.ci2[j]] += od.ldim[j];
+    }
+    out.reserve(out.size() + n);
+    int64_t comp[kDevMaxComp] = {};
+    int64_t off = 0;
     for (int64_t x = 0; x < n; ++x) {
-      int64_t y = x;
-      for (int q = 0; q < it.nsp[sp]; ++q) {
-        comp[q] = (int32_t)(y % it.rad[sp][q]);
-        y /= it.rad[sp][q];
-      }
-      int64_t off = 0;
-      for (int j = 0; j < od.ncomp; ++j) {
-        if (od.map[j] || (od.sp1[j] != kNone && od.sp2[j] != kNone)) continue;
-        if (od.sp1[j] == sp) off += (int64_t)comp[od.ci1[j]] * od.ldim[j];
-        else if (od.sp2[j] == sp) off += (int64_t)comp[od.ci2[j]] * od.ldim[j];
-      }
       out.push_back(off);
+      for (int q = 0; q < nq; ++q) {
+        if (++comp[q] < it.rad[sp][q]) {
+          off += coef[q];
+          break;
+        }
+        off -= (comp[q] - 1) * coef[q];  // the component wraps to 0, carry
+        comp[q] = 0;
+      }
     }
   }
 
@@ -977,16 +986,18 @@ class Engine {
   // the map lookup (layout [map component][index])
   static void map_index_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
                               std::vector<int64_t>& out) {
-    int32_t comp[kDevMaxComp];
+    const int nq = it.nsp[sp];
     for (int j = 0; j < od.ncomp; ++j) {
       if (!od.map[j]) continue;
+      const int c = od.sp1[j] == sp ? od.ci1[j] : od.ci2[j];
+      out.reserve(out.size() + n);
+      int64_t comp[kDevMaxComp] = {};
       for (int64_t x = 0; x < n; ++x) {
-        int64_t y = x;
-        for (int q = 0; q < it.nsp[sp]; ++q) {
-          comp[q] = (int32_t)(y % it.rad[sp][q]);
-          y /= it.rad[sp][q];
+        out.push_back(comp[c]);
+        for (int q = 0; q < nq; ++q) {
+          if (++comp[q] < it.rad[sp][q]) break;
+          comp[q] = 0;
         }
-        out.push_back(od.sp1[j] == sp ? comp[od.ci1[j]] : comp[od.ci2[j]]);
       }
     }
   }
