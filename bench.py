@@ -287,7 +287,7 @@ def run_gpu(args, cfg):
         print(json.dumps({"trace": args.trace_contraction, "workload": cfg["name"],
                           "ms_including_planning": ms}), flush=True)
         return
-    modes = [args.precision] + ([0] if args.precision == 1 and not args.no_fp64 else [])
+    modes = [args.precision] + ([0] if args.precision != 0 and not args.no_fp64 else [])
     results = {}
     for mode in modes:
         reset_amplitudes(eng, solver)
@@ -338,8 +338,8 @@ def run_gpu(args, cfg):
         line["precision"] = dict(
             evaluation_errors(eng, solver, modes[0]),
             amplitudes="after two FP64 Jacobi iterations from T=0",
-            note="mixed evaluation (split TF32, FP32 accumulation per 4096-index chunk, "
-                 "FP64 sums) minus FP64 evaluation; R*_max_rel relative to max|R|")
+            note=f"evaluation with {METRIC_MODE[modes[0]]} minus FP64 evaluation; "
+                 "R*_max_rel relative to max|R|")
 
     if args.tune:
         rows = eng.tuning_report()
@@ -364,9 +364,11 @@ def run_gpu(args, cfg):
     eng.close()
     del solver
     torch.cuda.empty_cache()
-    if args.precision == 1 and not args.no_i8:
-        line["i8"] = measure_i8(args, cfg, local, dist, peak, 2)
-        line["i8_fast"] = measure_i8(args, cfg, local, dist, peak, 3)
+    if args.precision != 0 and not args.no_i8:
+        # the other tensor-core modes, each on an engine of its own
+        for mode in (3, 2, 1):
+            if mode != args.precision:
+                line[MODE_LABEL[mode]] = measure_i8(args, cfg, local, dist, peak, mode)
     if args.tune and world == 1 and not args.no_fixed_rule:
         line["tuning"]["fixed_rule"] = measure_fixed_rule(args, cfg, local, modes[0])
     if not args.no_d2h and world == 1:
@@ -388,7 +390,11 @@ def run_gpu(args, cfg):
         print(json.dumps(line), flush=True)
 
 
-METRIC_MODE = {0: "plain FP64", 1: "split-TF32 tensor cores, FP64 accumulation"}
+METRIC_MODE = {0: "plain FP64", 1: "split TF32 on the tensor cores (FP32 accumulation per "
+                                   "4096-index chunk, FP64 sums)",
+               2: "FP64 emulated with five int8 slices on the tensor cores",
+               3: "FP64 emulated with four int8 slices on the tensor cores"}
+MODE_LABEL = {0: "fp64", 1: "tf32", 2: "i8", 3: "i8_fast"}
 DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums",
          2: "s8 slices x5 (15 products), s32 exact accumulate, f64 combine",
          3: "s8 slices x4 (10 products), s32 exact accumulate, f64 combine"}
@@ -511,9 +517,9 @@ def measure_e2e(args, eng, solver):
 
 
 def measure_i8(args, cfg, local, dist, peak, mode):
-    """seconds per iteration with FP64 emulated by int8 slices (precision
-    mode 2: five slices, 3: four) on an engine of its own (the plans and
-    cached operand panels of three precision modes do not fit one device
+    """seconds per iteration in a tensor-core precision mode (1: split TF32,
+    2: five int8 slices, 3: four) on an engine of its own (the plans and
+    cached operand panels of several precision modes do not fit one device
     together), its roofline launch, and the errors of one evaluation against
     FP64 from identical amplitudes"""
     import torch
@@ -531,8 +537,7 @@ def measure_i8(args, cfg, local, dist, peak, mode):
         s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
         eng.set_precision(mode)
         f = measure(args, cfg, eng, s, local, dist, mode, main=True)
-        out = {"metric": metric_of(cfg) + f" FP64 emulated with {SLICE_PRODUCTS[mode]} int8 "
-                                          "slice products",
+        out = {"metric": metric_of(cfg) + f" {METRIC_MODE[mode]}",
                "value": f["ms"] / 1e3, "unit": "s", "ms_per_step": f["ms"], "e2e": f["e2e"],
                "gpu_launches": f["launches"], "dtype": DTYPE[mode],
                "roofline": roofline(f, peak, mode, s, eng),
@@ -547,7 +552,7 @@ def measure_i8(args, cfg, local, dist, peak, mode):
             out["precision"] = dict(
                 evaluation_errors(eng, s, mode),
                 amplitudes="after two FP64 Jacobi iterations from T=0",
-                note="evaluation with FP64 emulated by int8 slices minus FP64 evaluation; "
+                note=f"evaluation with {METRIC_MODE[mode]} minus FP64 evaluation; "
                      "R*_max_rel relative to max|R|")
     finally:
         eng.close()
@@ -581,7 +586,7 @@ def measure_use_tr(args, cfg, local, dist, modes, plain_energies):
                         profile=False, e2e=False)
             ref = plain_energies[mode]
             k = min(3, len(ref), len(r["energies"]))
-            out[{0: "fp64", 1: "mixed", 2: "i8"}[mode]] = {
+            out[MODE_LABEL[mode]] = {
                 "value": r["ms"] / 1e3, "unit": "s", "gpu_launches": r["launches"],
                 "clocks": clock_summary(r["samples"]),
                 "dE_first_iterations_vs_plain": max(
@@ -741,11 +746,11 @@ def measured_bf16_tflops(key="bf16_tflops"):
 
 def convergence(local, cfg, weights=None, maxiter=80, variants=None):
     """time to |dE| < 1 uEh against the converged FP64 energy, per solve
-    variant: plain FP64 ("fp64"), FP64 emulated with five int8 slices
-    throughout ("i8"), four slices until the residual norm is below 1e-7 and
-    five after it ("mixed"), split TF32 until 1e-4 and five slices after it
-    ("mixed_tf32") and, given weights, "mixed" with the learned step
-    ("mixed_learned"); `variants` adds labels: options of
+    variant: plain FP64 ("fp64"), four int8 slices until the residual norm
+    is below 1e-7 and five after it ("mixed"), four slices throughout
+    ("i8_fast"), five throughout ("i8"), split TF32 until 1e-4 and five
+    slices after it ("mixed_tf32") and, given weights, "mixed" with the
+    learned step ("mixed_learned"); `variants` adds labels: options of
     CCSolver.solve_mixed, or {"plain": mode} for one precision throughout.
     Each variant is solved twice on one engine: from its first call, with
     every contraction planned and autotuned during the first iteration of
@@ -759,8 +764,8 @@ def convergence(local, cfg, weights=None, maxiter=80, variants=None):
     from devfill import TorchIntegrals
 
     mixed = {"schedule": [(3, 1e-7), (2, None)]}
-    runs = {"fp64": {"plain": 0}, "i8": {"plain": 2}, "mixed": dict(mixed),
-            "mixed_tf32": {"schedule": [(1, 1e-4), (2, None)]}}
+    runs = {"fp64": {"plain": 0}, "mixed": dict(mixed), "i8_fast": {"plain": 3},
+            "i8": {"plain": 2}, "mixed_tf32": {"schedule": [(1, 1e-4), (2, None)]}}
     if weights is not None:
         runs["mixed_learned"] = dict(mixed, learned=True)
     runs.update(variants or {})
@@ -1047,12 +1052,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", type=int, default=1,
-                    help="1 (default): split-TF32 tensor-core contractions, with the FP64 "
-                         "path measured beside them; 2: FP64 emulated with int8 slices on "
-                         "the tensor cores; 0: FP64 only")
+    ap.add_argument("--precision", type=int, default=3,
+                    help="precision mode of the headline line: 3 (default): FP64 emulated "
+                         "with four int8 slices on the tensor cores (the bulk mode of the "
+                         "mixed solve), 2: five slices, 1: split TF32, 0: FP64 only; the "
+                         "FP64 path and the other tensor-core modes are measured beside it")
     ap.add_argument("--no-i8", action="store_true",
-                    help="skip the s/iteration of FP64 emulated with int8 slices")
+                    help="skip the s/iteration of the other tensor-core precision modes")
     ap.add_argument("--no-fp64", action="store_true",
                     help="with --precision 1, skip the FP64 measurement")
     ap.add_argument("--no-use-tr", action="store_true",
