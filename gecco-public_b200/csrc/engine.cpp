@@ -5,6 +5,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
+#include <atomic>
+#include <thread>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -258,8 +261,10 @@ class Engine {
   // autotuner trials, plan build (tables, packs and splits of cached panels)
   struct PlanStats {
     double host_s = 0, maps_s = 0, tune_s = 0, build_s = 0;
-    // parts of build_s: host tables, their upload, cached operand panels
-    double tables_s = 0, upload_s = 0, const_s = 0;
+    // parts of build_s: host tables, their upload, descriptors / tiles /
+    // allocations, cached operand panels; alloc_s: cudaMalloc and cudaFree
+    // calls of plans (inside the stages above)
+    double tables_s = 0, upload_s = 0, desc_s = 0, const_s = 0, alloc_s = 0;
     int64_t plans = 0;
   } pstats;
   std::chrono::steady_clock::time_point bt;  // stage clock inside build_gemm
@@ -307,7 +312,9 @@ class Engine {
     if (memmax > 0 && mem_used + (int64_t)bytes > memmax)
       throw Error("device memory cap (memmax) exceeded");
     void* p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    pstats.alloc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     allocs.push_back(p);
     if (track) track->push_back({p, bytes});
     mem_used += (int64_t)bytes;
@@ -317,7 +324,10 @@ class Engine {
     for (size_t i = 0; i < allocs.size(); ++i)
       if (allocs[i] == p) {
         allocs.erase(allocs.begin() + (long)i);
+        const auto t0 = std::chrono::steady_clock::now();
         CUDA_OK(cudaFree(p));
+        pstats.alloc_s +=
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         mem_used -= (int64_t)bytes;
         return;
       }
@@ -954,7 +964,7 @@ class Engine {
   // offsets of the single-source components of operand od that belong to
   // space sp, for every composite index of that space
   static void part_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
-                         std::vector<int64_t>& out) {
+                         int64_t* out) {
     // offset = sum over the space's components q of comp_q * coef_q; the
     // composite index advances like an odometer (first component fastest),
     // so each entry costs one addition instead of a mixed-radix division
@@ -965,11 +975,10 @@ class Engine {
       if (od.sp1[j] == sp) coef[od.ci1[j]] += od.ldim[j];
       else if (od.sp2[j] == sp) coef[od.ci2[j]] += od.ldim[j];
     }
-    out.reserve(out.size() + n);
     int64_t comp[kDevMaxComp] = {};
     int64_t off = 0;
     for (int64_t x = 0; x < n; ++x) {
-      out.push_back(off);
+      out[x] = off;
       for (int q = 0; q < nq; ++q) {
         if (++comp[q] < it.rad[sp][q]) {
           off += coef[q];
@@ -983,17 +992,16 @@ class Engine {
 
   // for each map component of operand od (in component order) and every
   // composite index of space sp: the string index that space contributes to
-  // the map lookup (layout [map component][index])
+  // the map lookup (layout [map component][index]), nmap * n entries
   static void map_index_table(const ItemDesc& it, const OpndDesc& od, int sp, int64_t n,
-                              std::vector<int64_t>& out) {
+                              int64_t* out) {
     const int nq = it.nsp[sp];
     for (int j = 0; j < od.ncomp; ++j) {
       if (!od.map[j]) continue;
       const int c = od.sp1[j] == sp ? od.ci1[j] : od.ci2[j];
-      out.reserve(out.size() + n);
       int64_t comp[kDevMaxComp] = {};
       for (int64_t x = 0; x < n; ++x) {
-        out.push_back(comp[c]);
+        *out++ = comp[c];
         for (int q = 0; q < nq; ++q) {
           if (++comp[q] < it.rad[sp][q]) break;
           comp[q] = 0;
@@ -1013,6 +1021,27 @@ class Engine {
     return step;
   }
 
+  // run njobs table fills on up to 16 host threads, the largest first, each
+  // thread taking the next unclaimed job
+  template <typename Run, typename Size>
+  static void fill_tables(size_t njobs, Run run, Size size) {
+    std::vector<size_t> order(njobs);
+    for (size_t j = 0; j < njobs; ++j) order[j] = j;
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return size(a) > size(b); });
+    int64_t total = 0;
+    for (size_t j = 0; j < njobs; ++j) total += size(j);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = total < (1 << 20) ? 1u : std::min<unsigned>(16u, hw);
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+      for (size_t q; (q = next.fetch_add(1)) < njobs;) run(order[q]);
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+  }
+
   // GEMM descriptors, offset tables, pack jobs and tiles of one plan
   void build_gemm(DevPlan& dp, const TilePolicy& pol) {
     bt = std::chrono::steady_clock::now();
@@ -1030,9 +1059,18 @@ class Engine {
     bool const_used[2] = {false, false};
     int64_t scratch = 0;
     dp.pack_gx = dp.pack_gy = 0;
-    auto put = [&](auto&& fill) {
-      int64_t o = (int64_t)tabs.size();
-      fill(tabs);
+    // the tables are laid out first (offsets in `tabs`) and filled
+    // afterwards, several at a time on the host's cores
+    struct TabJob {
+      int64_t off, n;
+      std::function<void(int64_t*)> fill;
+    };
+    std::vector<TabJob> tjobs;
+    int64_t ntab = 0;
+    auto put = [&](int64_t n, std::function<void(int64_t*)> fill) {
+      const int64_t o = ntab;
+      tjobs.push_back({o, n, std::move(fill)});
+      ntab += n;
       return o;
     };
     std::vector<int> kind_of;
@@ -1056,13 +1094,27 @@ class Engine {
     struct PackTab { int64_t roff, koff, rmi, kmi; };
     std::vector<PackTab> ptab1(P.items.size()), ptab2(P.items.size());
     auto pack_tabs = [&](const ItemDesc& it, int op, PackTab& pt) {
-      const OpndDesc& od = it.op[op];
+      const OpndDesc* od = &it.op[op];
+      const ItemDesc* ip = &it;
       const int rsp = op == 0 ? kEx1 : kEx2;
-      const int64_t R = op == 0 ? it.M : it.N;
-      pt.roff = put([&](std::vector<int64_t>& v) { part_table(it, od, rsp, R, v); });
-      pt.koff = put([&](std::vector<int64_t>& v) { part_table(it, od, kCnt, it.K, v); });
-      pt.rmi = put([&](std::vector<int64_t>& v) { map_index_table(it, od, rsp, R, v); });
-      pt.kmi = put([&](std::vector<int64_t>& v) { map_index_table(it, od, kCnt, it.K, v); });
+      const int64_t R = op == 0 ? it.M : it.N, K = it.K;
+      int64_t nm = 0;  // the components map_index_table writes a block for
+      for (int j = 0; j < od->ncomp; ++j) nm += od->map[j] != nullptr;
+      pt.roff = put(R, [=](int64_t* v) { part_table(*ip, *od, rsp, R, v); });
+      pt.koff = put(K, [=](int64_t* v) { part_table(*ip, *od, kCnt, K, v); });
+      pt.rmi = put(nm * R, [=](int64_t* v) { map_index_table(*ip, *od, rsp, R, v); });
+      pt.kmi = put(nm * K, [=](int64_t* v) { map_index_table(*ip, *od, kCnt, K, v); });
+    };
+    // identity tables of a packed panel: rows r, indices k * rows
+    auto iota = [&](int64_t n, int64_t step) {
+      return put(n, [=](int64_t* v) {
+        for (int64_t x = 0; x < n; ++x) v[x] = x * step;
+      });
+    };
+    auto part = [&](const ItemDesc& it, int op, int sp, int64_t n) {
+      const ItemDesc* ip = &it;
+      const OpndDesc* od = &it.op[op];
+      return put(n, [=](int64_t* v) { part_table(*ip, *od, sp, n, v); });
     };
     for (size_t i = 0; i < P.items.size(); ++i) {
       const ItemDesc& it = P.items[i];
@@ -1075,11 +1127,11 @@ class Engine {
       } else if (packed(i, 0)) {  // panel[k*M + r]
         pack_off1[i] = scratch;
         scratch += it.M * it.K;
-        t.aro = put([&](std::vector<int64_t>& v) { for (int64_t r = 0; r < it.M; ++r) v.push_back(r); });
-        t.ako = put([&](std::vector<int64_t>& v) { for (int64_t k = 0; k < it.K; ++k) v.push_back(k * it.M); });
+        t.aro = iota(it.M, 1);
+        t.ako = iota(it.K, it.M);
       } else {
-        t.aro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kEx1, it.M, v); });
-        t.ako = put([&](std::vector<int64_t>& v) { part_table(it, it.op[0], kCnt, it.K, v); });
+        t.aro = part(it, 0, kEx1, it.M);
+        t.ako = part(it, 0, kCnt, it.K);
       }
       if (tcgather(i, 1) || thingather(i, 1)) {
         t.bco = ptab2[i].roff;
@@ -1087,16 +1139,18 @@ class Engine {
       } else if (packed(i, 1)) {  // panel[k*N + c]
         pack_off2[i] = scratch;
         scratch += it.N * it.K;
-        t.bco = put([&](std::vector<int64_t>& v) { for (int64_t c = 0; c < it.N; ++c) v.push_back(c); });
-        t.bko = put([&](std::vector<int64_t>& v) { for (int64_t k = 0; k < it.K; ++k) v.push_back(k * it.N); });
+        t.bco = iota(it.N, 1);
+        t.bko = iota(it.K, it.N);
       } else {
-        t.bco = put([&](std::vector<int64_t>& v) { part_table(it, it.op[1], kEx2, it.N, v); });
-        t.bko = put([&](std::vector<int64_t>& v) { part_table(it, it.op[1], kCnt, it.K, v); });
+        t.bco = part(it, 1, kEx2, it.N);
+        t.bko = part(it, 1, kCnt, it.K);
       }
-      t.cro = put([&](std::vector<int64_t>& v) { part_table(it, it.op[2], kEx1, it.M, v); });
-      t.cco = put([&](std::vector<int64_t>& v) { part_table(it, it.op[2], kEx2, it.N, v); });
+      t.cro = part(it, 2, kEx1, it.M);
+      t.cco = part(it, 2, kEx2, it.N);
     }
-    if (tabs.empty()) tabs.push_back(0);
+    tabs.resize(std::max<int64_t>(ntab, 1));
+    fill_tables(tjobs.size(), [&](size_t j) { tjobs[j].fill(tabs.data() + tjobs[j].off); },
+                [&](size_t j) { return tjobs[j].n; });
     blap(pstats.tables_s);
     dp.d_tabs = upload(tabs);
     blap(pstats.upload_s);
@@ -1374,7 +1428,7 @@ class Engine {
     for (int kind = 0; kind < kGemmKinds; ++kind) dp.ntiles += dp.ntiles_g[kind];
     if (const_used[0]) dp.const_lists.push_back(dp.list1);
     if (const_used[1] && dp.list2 != dp.list1) dp.const_lists.push_back(dp.list2);
-    blap(pstats.tables_s);
+    blap(pstats.desc_s);
     run_const(dp, true);  // the cached panels, made once here
     blap(pstats.const_s);
   }
@@ -2390,6 +2444,8 @@ int gccu_plan_stats(double* out) {
     out[5] = e.pstats.tables_s;
     out[6] = e.pstats.upload_s;
     out[7] = e.pstats.const_s;
+    out[8] = e.pstats.desc_s;
+    out[9] = e.pstats.alloc_s;
   });
 }
 

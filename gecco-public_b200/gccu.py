@@ -320,11 +320,11 @@ class Engine:
     def plan_stats(self):
         """{"plans", "host_s", "maps_s", "tune_s", "build_s"}: time spent
         making contraction plans, by stage"""
-        out = np.zeros(8)
+        out = np.zeros(10)
         _call("gccu_plan_stats", _pd(out))
-        return {"plans": int(out[0]), "host_s": float(out[1]), "maps_s": float(out[2]),
-                "tune_s": float(out[3]), "build_s": float(out[4]), "tables_s": float(out[5]),
-                "upload_s": float(out[6]), "const_s": float(out[7])}
+        keys = ("plans", "host_s", "maps_s", "tune_s", "build_s", "tables_s", "upload_s",
+                "const_s", "desc_s", "alloc_s")
+        return {k: (int(v) if k == "plans" else float(v)) for k, v in zip(keys, out)}
 
     def set_shard(self, rank=0, nranks=1):
         """run only this rank's share of every contraction's output tiles"""

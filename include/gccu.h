@@ -344,10 +344,11 @@ int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows);
  * counterpart in the reference): out[0] plans made, out[1..4] seconds in the
  * host planner, the string maps, the autotuner's trials and the plan builds
  * (tables, uploads, cached operand panels), of which out[5] building the
- * plans' tables and descriptors on the host (with their small uploads and
- * the operand scratch allocation), out[6] the upload of the offset tables
- * and out[7] making the cached panels of frozen operands; each stage's
- * device work is waited for. */
+ * offset tables on the host, out[6] their upload, out[8] the descriptors,
+ * tiles, job lists and allocations after it and out[7] making the cached
+ * panels of frozen operands; out[9] the time inside cudaMalloc / cudaFree
+ * (part of the stages above).  Each stage's device work is waited for; out
+ * holds 10 values. */
 int gccu_plan_stats(double* out);
 
 /* ---- statistics -----------------------------------------------------------
