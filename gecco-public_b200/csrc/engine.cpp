@@ -299,7 +299,25 @@ class Engine {
         for (auto ev : pr) cudaEventDestroy(ev);
     if (stream) cudaStreamSynchronize(stream);
     for (void* p : allocs) cudaFree(p);
+    if (tabs_host) cudaFreeHost(tabs_host);
     if (stream) cudaStreamDestroy(stream);
+  }
+
+  // page-locked host buffer the offset tables of a plan are built in (grown
+  // to the largest plan so far, reused): filled by the host threads, then
+  // copied at the link's rate instead of through a pageable staging copy
+  int64_t* tabs_host = nullptr;
+  int64_t tabs_cap = 0;
+  int64_t* host_tables(int64_t n) {
+    if (n > tabs_cap) {
+      CUDA_OK(cudaStreamSynchronize(stream));
+      if (tabs_host) CUDA_OK(cudaFreeHost(tabs_host));
+      tabs_host = nullptr;
+      const int64_t cap = std::max<int64_t>(n, tabs_cap + tabs_cap / 2);
+      CUDA_OK(cudaMallocHost(&tabs_host, (size_t)cap * sizeof(int64_t)));
+      tabs_cap = cap;
+    }
+    return tabs_host;
   }
 
   // allocations made while set are also recorded here (plans built on trial
@@ -1012,7 +1030,7 @@ class Engine {
 
   // step of an offset table that is affine in its index (tab[k] = tab[0] +
   // k * step, step != 0), else 0
-  static int64_t affine_step(const std::vector<int64_t>& tabs, int64_t at, int64_t n) {
+  static int64_t affine_step(const int64_t* tabs, int64_t at, int64_t n) {
     if (n < 2) return 0;
     const int64_t step = tabs[at + 1] - tabs[at];
     if (step == 0) return 0;
@@ -1049,7 +1067,6 @@ class Engine {
     const double* x1 = list(dp.list1).d;
     const double* x2 = list(dp.list2).d;
     double* x12 = list(dp.list12).d;
-    std::vector<int64_t> tabs;
     struct Tab { int64_t aro, ako, bco, bko, cro, cco; };
     std::vector<Tab> toff(P.items.size());
     std::vector<PackJob> jobs, jobs_c;
@@ -1148,11 +1165,15 @@ class Engine {
       t.cro = part(it, 2, kEx1, it.M);
       t.cco = part(it, 2, kEx2, it.N);
     }
-    tabs.resize(std::max<int64_t>(ntab, 1));
-    fill_tables(tjobs.size(), [&](size_t j) { tjobs[j].fill(tabs.data() + tjobs[j].off); },
+    int64_t* tabs = host_tables(std::max<int64_t>(ntab, 1));
+    if (!ntab) tabs[0] = 0;
+    fill_tables(tjobs.size(), [&](size_t j) { tjobs[j].fill(tabs + tjobs[j].off); },
                 [&](size_t j) { return tjobs[j].n; });
     blap(pstats.tables_s);
-    dp.d_tabs = upload(tabs);
+    dp.d_tabs = (int64_t*)alloc((size_t)std::max<int64_t>(ntab, 1) * sizeof(int64_t));
+    CUDA_OK(cudaMemcpyAsync(dp.d_tabs, tabs, (size_t)std::max<int64_t>(ntab, 1) * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, stream));
+    CUDA_OK(cudaStreamSynchronize(stream));
     blap(pstats.upload_s);
     dp.scratch = scratch ? (double*)alloc(scratch * sizeof(double)) : nullptr;
     dp.scratch_len = scratch;
