@@ -169,6 +169,10 @@ class Engine {
   int device = 0;
   int64_t memmax = 0, mem_used = 0;
   cudaStream_t stream = nullptr;
+  // host-to-device copies of plan tables and descriptors: a stream of their
+  // own, so that planning the next contraction does not wait for the
+  // kernels already queued on `stream` (the host waits for the copy only)
+  cudaStream_t ustream = nullptr;
   std::vector<DevList> lists;
   std::map<int, DevGraph> dgraphs;
   std::map<MapKey, int32_t*> maps;
@@ -269,7 +273,6 @@ class Engine {
   } pstats;
   std::chrono::steady_clock::time_point bt;  // stage clock inside build_gemm
   void blap(double& acc) {
-    CUDA_OK(cudaStreamSynchronize(stream));
     const auto now = std::chrono::steady_clock::now();
     acc += std::chrono::duration<double>(now - bt).count();
     bt = now;
@@ -285,6 +288,7 @@ class Engine {
     if (host_only) return;
     CUDA_OK(cudaSetDevice(dev));
     CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUDA_OK(cudaStreamCreateWithFlags(&ustream, cudaStreamNonBlocking));
     d_red = (double*)alloc(64 * sizeof(double));
     d_err = (int*)alloc(sizeof(int));
     CUDA_OK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
@@ -300,6 +304,7 @@ class Engine {
     if (stream) cudaStreamSynchronize(stream);
     for (void* p : allocs) cudaFree(p);
     if (tabs_host) cudaFreeHost(tabs_host);
+    if (ustream) cudaStreamDestroy(ustream);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -310,7 +315,7 @@ class Engine {
   int64_t tabs_cap = 0;
   int64_t* host_tables(int64_t n) {
     if (n > tabs_cap) {
-      CUDA_OK(cudaStreamSynchronize(stream));
+      CUDA_OK(cudaStreamSynchronize(ustream));
       if (tabs_host) CUDA_OK(cudaFreeHost(tabs_host));
       tabs_host = nullptr;
       const int64_t cap = std::max<int64_t>(n, tabs_cap + tabs_cap / 2);
@@ -372,8 +377,9 @@ class Engine {
   T* upload(const std::vector<T>& v) {
     T* p = (T*)alloc(v.size() * sizeof(T));
     if (!v.empty())
-      CUDA_OK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
-    CUDA_OK(cudaStreamSynchronize(stream));
+      CUDA_OK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice,
+                              ustream));
+    CUDA_OK(cudaStreamSynchronize(ustream));
     return p;
   }
 
@@ -780,9 +786,9 @@ class Engine {
     dp->res_len = B12.len;
     Plan& P = dp->plan;
     if (host_only) return *(plans[key] = std::move(dp));
-    // planning time by stage (device work of each stage waited for)
+    // host time of each planning stage (the device work a stage queues, for
+    // instance cached panels, is not waited for)
     auto lap = [&](double& acc, std::chrono::steady_clock::time_point& t) {
-      CUDA_OK(cudaStreamSynchronize(stream));
       const auto now = std::chrono::steady_clock::now();
       acc += std::chrono::duration<double>(now - t).count();
       t = now;
@@ -1172,8 +1178,8 @@ class Engine {
     blap(pstats.tables_s);
     dp.d_tabs = (int64_t*)alloc((size_t)std::max<int64_t>(ntab, 1) * sizeof(int64_t));
     CUDA_OK(cudaMemcpyAsync(dp.d_tabs, tabs, (size_t)std::max<int64_t>(ntab, 1) * sizeof(int64_t),
-                            cudaMemcpyHostToDevice, stream));
-    CUDA_OK(cudaStreamSynchronize(stream));
+                            cudaMemcpyHostToDevice, ustream));
+    CUDA_OK(cudaStreamSynchronize(ustream));
     blap(pstats.upload_s);
     dp.scratch = scratch ? (double*)alloc(scratch * sizeof(double)) : nullptr;
     dp.scratch_len = scratch;

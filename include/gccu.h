@@ -347,8 +347,8 @@ int gccu_tuning_report(double* rows, int64_t maxrows, int64_t* nrows);
  * offset tables on the host, out[6] their upload, out[8] the descriptors,
  * tiles, job lists and allocations after it and out[7] making the cached
  * panels of frozen operands; out[9] the time inside cudaMalloc / cudaFree
- * (part of the stages above).  Each stage's device work is waited for; out
- * holds 10 values. */
+ * (part of the stages above).  Host time: the device work a stage queues
+ * is not waited for.  out holds 10 values. */
 int gccu_plan_stats(double* out);
 
 /* ---- statistics -----------------------------------------------------------
