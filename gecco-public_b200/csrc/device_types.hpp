@@ -107,14 +107,20 @@ struct ReoItem {
 // tensor core's K-major core-matrix order, [k/4][row][k%4]:
 //   panel[((band * nslice + slice) * 2 + plane) * TR * 32 + (k/4) * TR * 4 + row * 4 + k%4]
 // with rows and contraction indices outside the item set to zero.  The job's
-// blocks are 128-row x 32-index chunks numbered from cstart.  An operand whose
+// blocks (128 rows x up to four 32-index slices) are numbered from cstart.
+// An operand whose
 // strings merge an external and a contracted component is read through its
 // gather description (PackJob index `gather`, -1: through the descriptor's
 // offset tables).
+// With int8 slices (two passes over the same chunks) a gathered operand's
+// chunks are also kept densely (`stage`: float offset of 128 x 32 FP64 per
+// chunk in the workspace, -1 for none), written by the row-maxima pass and
+// read by the slicing pass instead of gathering twice.
 struct SplitJob {
   int32_t desc, op;
   int64_t cstart;
   int32_t gather, pad;
+  int64_t stage;
 };
 
 // gather of one operand of one block contraction into a dense panel

@@ -1394,19 +1394,27 @@ class Engine {
             const int tr = op == 0 ? kGemmTcM : d.tn;
             const int64_t fl =
                 dp.i8 ? i8_panel_floats(rows, tr, d.K, dp.i8) : tc_panel_floats(rows, tr, d.K);
-            const int64_t ch = tc_split_chunks(rows, tr, d.K);
+            const int64_t ch = tc_split_chunks(rows, tr, d.K);   // 128 x 32 chunks
+            const int64_t nb = tc_split_blocks(rows, tr, d.K);   // pre-pass blocks
             int64_t& po = op == 0 ? d.pa : d.pb;
             if (frozen_op[op]) {
               po = off_c;  // made absolute below
               off_c += fl;
-              sj_c.push_back(SplitJob{(int32_t)i, op, cs_c, gat(op), 0});
-              cs_c += ch;
+              sj_c.push_back(SplitJob{(int32_t)i, op, cs_c, gat(op), 0, -1});
+              cs_c += nb;
               const_used[op] = true;
             } else {
               po = off;
               off += fl;
-              sj.push_back(SplitJob{(int32_t)i, op, cs, gat(op), 0});
-              cs += ch;
+              // int8 slices of a gathered operand: its chunks kept densely
+              // between the two passes
+              int64_t stage = -1;
+              if (dp.i8 && gat(op) >= 0) {
+                stage = off;
+                off += ch * kTcGemmChunkFloats;
+              }
+              sj.push_back(SplitJob{(int32_t)i, op, cs, gat(op), 0, stage});
+              cs += nb;
             }
           }
         }

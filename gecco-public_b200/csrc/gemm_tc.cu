@@ -192,7 +192,9 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 }
 
 // ---- split pre-pass -------------------------------------------------------
-// One block per 128-row x 32-index chunk of one operand.  The chunk is read
+// One block per 128 rows x kSplitGroup consecutive 32-index slices of one
+// operand (the rows' offsets and map indices loaded once), one slice after
+// the other.  A 128-row x 32-index chunk is read
 // coalesced along the operand's contiguous direction (contraction index when
 // kfast, else row), split, staged in shared memory in the panel order (each
 // k/4 plane padded by 4 floats so that neither read direction conflicts on
@@ -212,6 +214,7 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPitch = 128 * 4 + 4;  // floats per k/4 plane of a staged chunk
 constexpr int kValPitch = SK + 1;         // doubles per row of a staged chunk (OUT > 0)
+constexpr int kSplitGroup = (int)kTcSplitGroup;  // 32-index slices per block
 union SplitStage {
   float sh[2][8 * kSplitPitch];  // split-TF32 planes (OUT = 0)
   double v[128][kValPitch];      // values (OUT = 1, 2)
@@ -253,18 +256,23 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
   const int64_t* rtab = gat ? gp->roff : row_op ? d.aro : d.bco;
   const int64_t* ktab = gat ? gp->koff : row_op ? d.ako : d.bko;
   const int kfast = gat ? gp->kfast : row_op ? d.afast : d.bfast;
-  const int64_t nsl = (K + SK - 1) / SK;
-  const int64_t c = blk - J.cstart;  // chunk = row chunk * nsl + slice
-  const int64_t r0 = (c / nsl) * 128, k0 = (c % nsl) * SK;
+  const int64_t nsl = (K + SK - 1) / SK, ngrp = (nsl + kSplitGroup - 1) / kSplitGroup;
+  const int64_t c = blk - J.cstart;  // block = row chunk * ngrp + slice group
+  const int64_t rc = c / ngrp, r0 = rc * 128;
+  const int64_t sl0 = (c % ngrp) * kSplitGroup;
+  const int64_t sl1 = sl0 + kSplitGroup < nsl ? sl0 + kSplitGroup : nsl;
+  // the chunk's rows: offsets, map string indices and (OUT = 2) scales, once
+  // for the block's slices
   if (tid < 128) ro[tid] = r0 + tid < R ? __ldg(rtab + r0 + tid) : -1;
-  else if (tid < 128 + SK) ko[tid - 128] = k0 + (tid - 128) < K ? __ldg(ktab + k0 + tid - 128) : -1;
   if constexpr (OUT == 2) {
     if (tid < 128) {
       const double m = r0 + tid < R ? panel_max(d, row_op)[r0 + tid] : 0.0;
       inv_s[tid] = m > 0.0 ? 127.0 / m : 0.0;
     }
   }
-  if (gat) {
+  // int8 slicing of a gathered operand whose chunks the row-maxima pass kept
+  const bool staged = OUT == 2 && J.stage >= 0;
+  if (gat && !staged) {
     const int nw = (int)(sizeof(PackJob) / sizeof(int));
     for (int i = tid; i < nw; i += kSplitThreads)
       reinterpret_cast<int*>(&G)[i] = reinterpret_cast<const int*>(gp)[i];
@@ -273,210 +281,231 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
       const int m = i >> 7, r = i & 127;
       if (r0 + r < R) rmi_s[m][r] = (int32_t)__ldg(gp->rmi + (int64_t)m * R + r0 + r);
     }
-    for (int i = tid; i < nm * SK; i += kSplitThreads) {
-      const int m = i / SK, k = i % SK;
-      if (k0 + k < K) kmi_s[m][k] = (int32_t)__ldg(gp->kmi + (int64_t)m * K + k0 + k);
-    }
   }
-  __syncthreads();
-  // element (local row r, local index k) of a direct operand
-  auto direct = [&](int r, int k) -> double {
-    const int64_t rof = ro[r], kof = ko[k];
-    return (rof >= 0 && kof >= 0) ? __ldg(x + rof + kof) : 0.0;
-  };
-  // staging of one chunk of a direct operand: thread mappings per read
-  // direction, the element function a template argument so that the loads
-  // stay independent (no map branch between them)
-  auto stage = [&](auto&& elem) {
-    if (kfast) {  // warp: 16 rows, lane: contraction index
-      const int warp = tid >> 5, lane = tid & 31;
+  // a 128-row chunk may span two row bands when TR is not a multiple of 128
+  const int64_t padded = (R + TR - 1) / TR * TR;
+  double mrow = 0.0;  // OUT = 1: this thread's half row, over the block's slices
+  for (int64_t sl = sl0; sl < sl1; ++sl) {
+    const int64_t k0 = sl * SK;
+    double* const stg = J.stage >= 0 ? reinterpret_cast<double*>(g_tc_ws + J.stage) +
+                                           (rc * nsl + sl) * (128 * SK)
+                                     : nullptr;
+    if (tid >= 128 && tid < 128 + SK)
+      ko[tid - 128] = k0 + (tid - 128) < K ? __ldg(ktab + k0 + tid - 128) : -1;
+    if (gat && !staged) {
+      const int nm = gp->nm;
+      for (int i = tid; i < nm * SK; i += kSplitThreads) {
+        const int m = i / SK, k = i % SK;
+        if (k0 + k < K) kmi_s[m][k] = (int32_t)__ldg(gp->kmi + (int64_t)m * K + k0 + k);
+      }
+    }
+    __syncthreads();
+    // element (local row r, local index k) of a direct operand
+    auto direct = [&](int r, int k) -> double {
+      const int64_t rof = ro[r], kof = ko[k];
+      return (rof >= 0 && kof >= 0) ? __ldg(x + rof + kof) : 0.0;
+    };
+    // staging of one chunk of a direct operand: thread mappings per read
+    // direction, the element function a template argument so that the loads
+    // stay independent (no map branch between them)
+    auto stage = [&](auto&& elem) {
+      if (kfast) {  // warp: 16 rows, lane: contraction index
+        const int warp = tid >> 5, lane = tid & 31;
 #pragma unroll 8
-      for (int i = 0; i < 16; ++i) {
-        const int r = warp * 16 + i;
-        const double v = elem(r, lane);
-        if constexpr (OUT == 0) {
-          float h, l;
-          split_tf32(v, h, l);
-          sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
-          sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
-        } else {
-          U.v[r][lane] = v;
-        }
-      }
-    } else {  // thread: one row, 16 contraction indices
-      const int r = tid & 127, kh = tid >> 7;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if constexpr (OUT == 0) {
-          float4 h4, l4;
-          float* hp = &h4.x;
-          float* lp = &l4.x;
-#pragma unroll
-          for (int e = 0; e < 4; ++e) split_tf32(elem(r, 16 * kh + 4 * q + e), hp[e], lp[e]);
-          *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
-          *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) U.v[r][16 * kh + 4 * q + e] = elem(r, 16 * kh + 4 * q + e);
-        }
-      }
-    }
-  };
-  // map-addressed operand: eight elements at a time, their map lookups of
-  // each component issued together, then their value loads, so that the
-  // dependent loads of different elements overlap (rows or indices outside
-  // the block have ro / ko < 0 and load nothing)
-  auto gather8 = [&](const int (&rr)[8], const int (&kk)[8], double (&val)[8]) {
-    int64_t off[8];
-    bool ok[8], neg[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int64_t rof = ro[rr[e]], kof = ko[kk[e]];
-      ok[e] = rof >= 0 && kof >= 0;
-      off[e] = ok[e] ? rof + kof : 0;
-      neg[e] = false;
-    }
-    for (int m = 0; m < G.nm; ++m) {
-      const bool r1 = G.row_is_1[m] != 0;
-      const int32_t* __restrict__ mp = G.map[m];
-      const int64_t n1 = G.n1[m], ld = G.ldim[m];
-      int v[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const int32_t ir = rmi_s[m][rr[e]], ik = kmi_s[m][kk[e]];
-        v[e] = ok[e] ? __ldg(mp + (int64_t)(r1 ? ik : ir) * n1 + (r1 ? ir : ik)) : 1;
-      }
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        int w = v[e];
-        if (w == 0) ok[e] = false;
-        if (w < 0) {
-          neg[e] = !neg[e];
-          w = -w;
-        }
-        off[e] += (int64_t)(w - 1) * ld;
-      }
-    }
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const double x0 = ok[e] ? __ldg(x + off[e]) : 0.0;
-      val[e] = neg[e] ? -x0 : x0;
-    }
-  };
-  auto stage_mapped = [&]() {
-    if (kfast) {  // warp: 16 rows, lane: contraction index
-      const int warp = tid >> 5, lane = tid & 31;
-#pragma unroll 1
-      for (int i0 = 0; i0 < 16; i0 += 8) {
-        int rr[8], kk[8];
-        double v[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          rr[e] = warp * 16 + i0 + e;
-          kk[e] = lane;
-        }
-        gather8(rr, kk, v);
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
+        for (int i = 0; i < 16; ++i) {
+          const int r = warp * 16 + i;
+          const double v = elem(r, lane);
           if constexpr (OUT == 0) {
             float h, l;
-            split_tf32(v[e], h, l);
-            sh[0][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = h;
-            sh[1][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = l;
+            split_tf32(v, h, l);
+            sh[0][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = h;
+            sh[1][(lane >> 2) * kSplitPitch + 4 * r + (lane & 3)] = l;
           } else {
-            U.v[rr[e]][lane] = v[e];
+            U.v[r][lane] = v;
           }
         }
-      }
-    } else {  // thread: one row, 16 contraction indices
-      const int r = tid & 127, kh = tid >> 7;
-#pragma unroll 1
-      for (int q0 = 0; q0 < 4; q0 += 2) {
-        int rr[8], kk[8];
-        double v[8];
+      } else {  // thread: one row, 16 contraction indices
+        const int r = tid & 127, kh = tid >> 7;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          rr[e] = r;
-          kk[e] = 16 * kh + 4 * q0 + e;
-        }
-        gather8(rr, kk, v);
-        if constexpr (OUT == 0) {
-#pragma unroll
-          for (int qq = 0; qq < 2; ++qq) {
+        for (int q = 0; q < 4; ++q) {
+          if constexpr (OUT == 0) {
             float4 h4, l4;
             float* hp = &h4.x;
             float* lp = &l4.x;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) split_tf32(v[4 * qq + e], hp[e], lp[e]);
-            *reinterpret_cast<float4*>(&sh[0][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = h4;
-            *reinterpret_cast<float4*>(&sh[1][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = l4;
-          }
-        } else {
+            for (int e = 0; e < 4; ++e) split_tf32(elem(r, 16 * kh + 4 * q + e), hp[e], lp[e]);
+            *reinterpret_cast<float4*>(&sh[0][(4 * kh + q) * kSplitPitch + 4 * r]) = h4;
+            *reinterpret_cast<float4*>(&sh[1][(4 * kh + q) * kSplitPitch + 4 * r]) = l4;
+          } else {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) U.v[r][kk[e]] = v[e];
+            for (int e = 0; e < 4; ++e) U.v[r][16 * kh + 4 * q + e] = elem(r, 16 * kh + 4 * q + e);
+          }
         }
       }
+    };
+    // map-addressed operand: eight elements at a time, their map lookups of
+    // each component issued together, then their value loads, so that the
+    // dependent loads of different elements overlap (rows or indices outside
+    // the block have ro / ko < 0 and load nothing)
+    auto gather8 = [&](const int (&rr)[8], const int (&kk)[8], double (&val)[8]) {
+      int64_t off[8];
+      bool ok[8], neg[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int64_t rof = ro[rr[e]], kof = ko[kk[e]];
+        ok[e] = rof >= 0 && kof >= 0;
+        off[e] = ok[e] ? rof + kof : 0;
+        neg[e] = false;
+      }
+      for (int m = 0; m < G.nm; ++m) {
+        const bool r1 = G.row_is_1[m] != 0;
+        const int32_t* __restrict__ mp = G.map[m];
+        const int64_t n1 = G.n1[m], ld = G.ldim[m];
+        int v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int32_t ir = rmi_s[m][rr[e]], ik = kmi_s[m][kk[e]];
+          v[e] = ok[e] ? __ldg(mp + (int64_t)(r1 ? ik : ir) * n1 + (r1 ? ir : ik)) : 1;
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          int w = v[e];
+          if (w == 0) ok[e] = false;
+          if (w < 0) {
+            neg[e] = !neg[e];
+            w = -w;
+          }
+          off[e] += (int64_t)(w - 1) * ld;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const double x0 = ok[e] ? __ldg(x + off[e]) : 0.0;
+        val[e] = neg[e] ? -x0 : x0;
+      }
+    };
+    auto stage_mapped = [&]() {
+      if (kfast) {  // warp: 16 rows, lane: contraction index
+        const int warp = tid >> 5, lane = tid & 31;
+#pragma unroll 1
+        for (int i0 = 0; i0 < 16; i0 += 8) {
+          int rr[8], kk[8];
+          double v[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            rr[e] = warp * 16 + i0 + e;
+            kk[e] = lane;
+          }
+          gather8(rr, kk, v);
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            if constexpr (OUT == 0) {
+              float h, l;
+              split_tf32(v[e], h, l);
+              sh[0][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = h;
+              sh[1][(lane >> 2) * kSplitPitch + 4 * rr[e] + (lane & 3)] = l;
+            } else {
+              U.v[rr[e]][lane] = v[e];
+            }
+          }
+        }
+      } else {  // thread: one row, 16 contraction indices
+        const int r = tid & 127, kh = tid >> 7;
+#pragma unroll 1
+        for (int q0 = 0; q0 < 4; q0 += 2) {
+          int rr[8], kk[8];
+          double v[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            rr[e] = r;
+            kk[e] = 16 * kh + 4 * q0 + e;
+          }
+          gather8(rr, kk, v);
+          if constexpr (OUT == 0) {
+#pragma unroll
+            for (int qq = 0; qq < 2; ++qq) {
+              float4 h4, l4;
+              float* hp = &h4.x;
+              float* lp = &l4.x;
+#pragma unroll
+              for (int e = 0; e < 4; ++e) split_tf32(v[4 * qq + e], hp[e], lp[e]);
+              *reinterpret_cast<float4*>(&sh[0][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = h4;
+              *reinterpret_cast<float4*>(&sh[1][(4 * kh + q0 + qq) * kSplitPitch + 4 * r]) = l4;
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) U.v[r][kk[e]] = v[e];
+          }
+        }
+      }
+    };
+    if (staged) {
+      for (int i = tid; i < 128 * SK; i += kSplitThreads) U.v[i / SK][i % SK] = stg[i];
+    } else if (gat) {
+      stage_mapped();
+    } else {
+        stage(direct);
     }
-  };
-  if (gat)
-    stage_mapped();
-  else
-    stage(direct);
-  __syncthreads();
-  // a 128-row chunk may span two row bands when TR is not a multiple of 128
-  const int64_t padded = (R + TR - 1) / TR * TR;
-  if constexpr (OUT == 1) {  // rows' maxima: each thread half a row of the chunk
-    const int r = tid & 127, kh = tid >> 7;
-    double m = 0.0;
+    __syncthreads();
+    if constexpr (OUT == 1) {  // rows' maxima: each thread half a row of the chunk
+      if (stg)  // the gathered chunk, kept for the slicing pass
+        for (int i = tid; i < 128 * SK; i += kSplitThreads) stg[i] = U.v[i / SK][i % SK];
+      const int r = tid & 127, kh = tid >> 7;
 #pragma unroll
-    for (int j = 0; j < 16; ++j) m = fmax(m, fabs(U.v[r][16 * kh + j]));
-    if (m > 0.0 && r0 + r < R)
-      atomicMax(reinterpret_cast<unsigned long long*>(panel_max(d, row_op) + r0 + r),
-                (unsigned long long)__double_as_longlong(m));
-    return;
-  } else if constexpr (OUT == 2) {  // slices: thread = one row x 16 indices (one plane)
-    const int r = tid & 127, kh = tid >> 7;
-    const int64_t row = r0 + r;
-    if (row >= padded) return;
-    const double inv = inv_s[r];
-    uint32_t w[IS][4];
+      for (int j = 0; j < 16; ++j) mrow = fmax(mrow, fabs(U.v[r][16 * kh + j]));
+    } else if constexpr (OUT == 2) {  // slices: thread = one row x 16 indices (one plane)
+      const int r = tid & 127, kh = tid >> 7;
+      const int64_t row = r0 + r;
+      if (row < padded) {
+        const double inv = inv_s[r];
+        uint32_t w[IS][4];
 #pragma unroll
-    for (int s = 0; s < IS; ++s)
+        for (int s = 0; s < IS; ++s)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+          for (int q = 0; q < 4; ++q) w[s][q] = 0u;
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      double u = U.v[r][16 * kh + j] * inv;  // |u| <= 127
+        for (int j = 0; j < 16; ++j) {
+          double u = U.v[r][16 * kh + j] * inv;  // |u| <= 127
 #pragma unroll
-      for (int s = 0; s < IS; ++s) {
-        const int a = __double2int_rn(u);  // |a| <= 127, then <= 64
-        w[s][j >> 2] |= (uint32_t)(a & 0xff) << (8 * (j & 3));
-        u = (u - (double)a) * 128.0;  // exact
+          for (int s = 0; s < IS; ++s) {
+            const int a = __double2int_rn(u);  // |a| <= 127, then <= 64
+            w[s][j >> 2] |= (uint32_t)(a & 0xff) << (8 * (j & 3));
+            u = (u - (double)a) * 128.0;  // exact
+          }
+        }
+        uint8_t* const panel = reinterpret_cast<uint8_t*>(
+            row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa)
+                   : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb));
+        const int64_t band = row / TR, rr = row % TR;
+        uint8_t* base = panel + ((band * nsl + sl) * IS * 2 + kh) * TR * 16 + rr * 16;
+#pragma unroll
+        for (int s = 0; s < IS; ++s)
+          *reinterpret_cast<uint4*>(base + (int64_t)s * 2 * TR * 16) =
+              make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+      }
+    } else {  // split TF32: the staged planes as 16-byte vectors
+      float* const panel = row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa)
+                                  : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb);
+      float* __restrict__ base = panel + sl * 2 * TR * SK;
+#pragma unroll
+      for (int i = 0; i < 2 * 8 * 128 / kSplitThreads; ++i) {
+        const int u = tid + kSplitThreads * i;
+        const int plane = u >> 10, kq = (u >> 7) & 7, r = u & 127;
+        const int64_t row = r0 + r;
+        if (row >= padded) continue;
+        const int64_t band = row / TR, rr = row % TR;
+        const float4 v = *reinterpret_cast<const float4*>(&sh[plane][kq * kSplitPitch + 4 * r]);
+        *reinterpret_cast<float4*>(base + band * nsl * 2 * TR * SK + plane * TR * SK +
+                                   kq * TR * 4 + rr * 4) = v;
       }
     }
-    uint8_t* const panel = reinterpret_cast<uint8_t*>(
-        row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa) : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb));
-    const int64_t band = row / TR, rr = row % TR, slice = c % nsl;
-    uint8_t* base = panel + ((band * nsl + slice) * IS * 2 + kh) * TR * 16 + rr * 16;
-#pragma unroll
-    for (int s = 0; s < IS; ++s)
-      *reinterpret_cast<uint4*>(base + (int64_t)s * 2 * TR * 16) =
-          make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
-    return;
+    __syncthreads();  // the staging buffers are reused by the next slice
   }
-  float* const panel = row_op ? (d.pa_ptr ? d.pa_ptr : g_tc_ws + d.pa)
-                              : (d.pb_ptr ? d.pb_ptr : g_tc_ws + d.pb);
-  float* __restrict__ base = panel + (c % nsl) * 2 * TR * SK;
-#pragma unroll
-  for (int i = 0; i < 2 * 8 * 128 / kSplitThreads; ++i) {
-    const int u = tid + kSplitThreads * i;
-    const int plane = u >> 10, kq = (u >> 7) & 7, r = u & 127;
-    const int64_t row = r0 + r;
-    if (row >= padded) continue;
-    const int64_t band = row / TR, rr = row % TR;
-    const float4 v = *reinterpret_cast<const float4*>(&sh[plane][kq * kSplitPitch + 4 * r]);
-    *reinterpret_cast<float4*>(base + band * nsl * 2 * TR * SK + plane * TR * SK + kq * TR * 4 +
-                               rr * 4) = v;
+  if constexpr (OUT == 1) {
+    const int r = tid & 127;
+    if (mrow > 0.0 && r0 + r < R)
+      atomicMax(reinterpret_cast<unsigned long long*>(panel_max(d, row_op) + r0 + r),
+                (unsigned long long)__double_as_longlong(mrow));
   }
 }
 

@@ -75,10 +75,20 @@ inline int64_t tc_panel_floats(int64_t rows, int tile_rows, int64_t K) {
   return (rows + tile_rows - 1) / tile_rows * tile_rows * ((K + kTcSlice - 1) / kTcSlice) *
          kTcSlice * 2;
 }
+// floats of one 128-row x 32-index chunk kept in FP64 (int8 two-pass staging)
+constexpr int64_t kTcGemmChunkFloats = 128 * kTcSlice * 2;
 // number of 128-row x 32-index chunks of one operand's panel
 inline int64_t tc_split_chunks(int64_t rows, int tile_rows, int64_t K) {
   const int64_t padded = (rows + tile_rows - 1) / tile_rows * tile_rows;
   return (padded + 127) / 128 * ((K + kTcSlice - 1) / kTcSlice);
+}
+// the split pre-pass's blocks for one operand: 128 rows x kTcSplitGroup
+// consecutive 32-index slices each (the rows' tables loaded once)
+constexpr int64_t kTcSplitGroup = 4;
+inline int64_t tc_split_blocks(int64_t rows, int tile_rows, int64_t K) {
+  const int64_t padded = (rows + tile_rows - 1) / tile_rows * tile_rows;
+  const int64_t nsl = (K + kTcSlice - 1) / kTcSlice;
+  return (padded + 127) / 128 * ((nsl + kTcSplitGroup - 1) / kTcSplitGroup);
 }
 // tile width of a tensor-core item with N columns: as many tiles as
 // widest-wide ones would need, each narrowed to the multiple of 32 that
