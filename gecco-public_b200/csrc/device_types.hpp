@@ -124,7 +124,7 @@ struct SplitJob {
 };
 
 // gather of one operand of one block contraction into a dense panel
-// panel[k * R + r] = sign * x[address(r, k)],
+// panel[k * R + r] (or panel[r * K + k] when dkfast) = sign * x[address(r, k)],
 // address(r, k) = roff[r] + koff[k] + sum_m (|map_m[i2 * n1_m + i1]| - 1) * ldim_m
 // where the string indices of map component m come from the tables rmi
 // (row side, rmi[m * R + r]) and kmi (contraction side, kmi[m * K + k]);
@@ -141,6 +141,7 @@ struct PackJob {
   int32_t kfast;  // threads run fastest along k
   int32_t F;      // power of two <= 256
   int32_t nm;     // map components
+  int32_t dkfast; // panel layout: 0 panel[k * R + r], 1 panel[r * K + k] (written along k)
   int32_t row_is_1[kDevMaxComp];
   int32_t n1[kDevMaxComp];
   int64_t ldim[kDevMaxComp];

@@ -1147,11 +1147,11 @@ class Engine {
       if (tcgather(i, 0) || thingather(i, 0)) {  // read in place by the split pre-pass / k_thin
         t.aro = ptab1[i].roff;
         t.ako = ptab1[i].koff;
-      } else if (packed(i, 0)) {  // panel[k*M + r]
+      } else if (packed(i, 0)) {  // panel[k*M + r], or panel[r*K + k] when read along k
         pack_off1[i] = scratch;
         scratch += it.M * it.K;
-        t.aro = iota(it.M, 1);
-        t.ako = iota(it.K, it.M);
+        t.aro = it.kfast1 ? iota(it.M, it.K) : iota(it.M, 1);
+        t.ako = it.kfast1 ? iota(it.K, 1) : iota(it.K, it.M);
       } else {
         t.aro = part(it, 0, kEx1, it.M);
         t.ako = part(it, 0, kCnt, it.K);
@@ -1159,11 +1159,11 @@ class Engine {
       if (tcgather(i, 1) || thingather(i, 1)) {
         t.bco = ptab2[i].roff;
         t.bko = ptab2[i].koff;
-      } else if (packed(i, 1)) {  // panel[k*N + c]
+      } else if (packed(i, 1)) {  // panel[k*N + c], or panel[c*K + k] when read along k
         pack_off2[i] = scratch;
         scratch += it.N * it.K;
-        t.bco = iota(it.N, 1);
-        t.bko = iota(it.K, it.N);
+        t.bco = it.kfast2 ? iota(it.N, it.K) : iota(it.N, 1);
+        t.bko = it.kfast2 ? iota(it.K, 1) : iota(it.K, it.N);
       } else {
         t.bco = part(it, 1, kEx2, it.N);
         t.bko = part(it, 1, kCnt, it.K);
@@ -1215,6 +1215,7 @@ class Engine {
       }
       GCCU_REQUIRE(j.R < INT32_MAX && j.K < INT32_MAX, "block too large for the pack kernel");
       j.kfast = op == 0 ? it.kfast1 : it.kfast2;
+      j.dkfast = j.kfast;  // the panel is written along the direction it is read
       const int64_t nf = j.kfast ? j.K : j.R;
       j.F = 1;
       while (j.F < 256 && j.F < nf) j.F *= 2;
@@ -1234,12 +1235,12 @@ class Engine {
       d.aro = dp.d_tabs + t.aro;
       d.ako = dp.d_tabs + t.ako;
       d.akstep = affine_step(tabs, t.ako, it.K);
-      d.afast = pack_off1[i] >= 0 ? 0 : it.kfast1;
+      d.afast = it.kfast1;  // a packed panel keeps the operand's fast direction
       d.b = pack_off2[i] >= 0 ? dp.scratch + pack_off2[i] : x2 + it.base2;
       d.bco = dp.d_tabs + t.bco;
       d.bko = dp.d_tabs + t.bko;
       d.bkstep = affine_step(tabs, t.bko, it.K);
-      d.bfast = pack_off2[i] >= 0 ? 0 : it.kfast2;
+      d.bfast = it.kfast2;
       d.c = x12 + it.base12;
       d.cro = dp.d_tabs + t.cro;
       d.cco = dp.d_tabs + t.cco;

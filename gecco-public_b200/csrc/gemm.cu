@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack(const PackJob* __restrict
     }
     const int64_t r = kf ? s : f, k = kf ? f : s;
     double x = ok ? __ldg(src + off) : 0.0;
-    dst[k * J.R + r] = neg ? -x : x;
+    dst[J.dkfast ? r * J.K + k : k * J.R + r] = neg ? -x : x;
   }
 }
 
