@@ -53,7 +53,11 @@ ROOFLINE_CONTRACTION = "r2_ladder"
 # profiles/k_gemm_ladder_ccsd_o12v100.md: 1.2436 GB and 1.2470 GB against
 # 1.2423 GB of algorithmic bytes); the full-size traffic is this ratio times
 # the full-size algorithmic bytes
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"k_gemm_tc": 1.2436 / 1.2423, "k_gemm": 1.2470 / 1.2423}
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"k_gemm_tc": 1.2436 / 1.2423, "k_gemm": 1.2470 / 1.2423,
+                                # four int8 slices (4 bytes per operand element):
+                                # profiles/k_gemm_i8_4slices_ladder_ccsd_o12v100.md,
+                                # 0.6385 GB against 0.6379 GB
+                                "k_gemm_i8_4": 0.6385 / 0.6379}
 
 SIGMA_SPEC = 0.05
 CONFIGS = {
@@ -672,7 +676,7 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
     """dominant kernel: the GEMM launch(es) of the pp-ladder contraction (the
     leading term; no operand gathers), timed with events in the profiled
     iteration: k_gemm<128,64> (FP64 DMMA) in mode 0, k_gemm_tc (split TF32 on
-    tcgen05) in mode 1"""
+    tcgen05) in mode 1, k_gemm_i8 (int8 slices on tcgen05) in modes 2 and 3"""
     names, prof = r["names"], r["prof"]
     dom = prof[names.index(ROOFLINE_CONTRACTION)]
     dom_ms = (dom[2] - dom[5]) / dom[1]
@@ -680,13 +684,16 @@ def roofline(r, fp64_peak_tflops, mode, solver, eng):
     total_flops = float(np.sum(prof[:, 0] * prof[:, 1]))
     rows = plan_rows(eng, solver, ROOFLINE_CONTRACTION).astype(float)
     M, N, K = rows[:, 0], rows[:, 1], rows[:, 2]
-    alg_bytes = float(8 * np.sum(M * K + N * K) + 16 * np.sum(M * N))
+    # operands read once (8 bytes per element in FP64 and split TF32, one byte
+    # per slice with int8 slices), the result read and written
+    op_bytes = {2: 5, 3: 4}.get(mode, 8)
+    alg_bytes = float(op_bytes * np.sum(M * K + N * K) + 16 * np.sum(M * N))
     out = {"bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
            "flops_per_launch": dom[0], "ms_per_launch": dom_ms,
            "iteration_flops": total_flops,
            "iteration_tflops": total_flops / (r["ms"] * 1e-3) / 1e12,
            "algorithmic_bytes_per_launch": alg_bytes}
-    kern = {0: "k_gemm", 1: "k_gemm_tc", 2: "k_gemm_i8", 3: "k_gemm_i8"}[mode]
+    kern = {0: "k_gemm", 1: "k_gemm_tc", 2: "k_gemm_i8_5", 3: "k_gemm_i8_4"}[mode]
     if kern in TRAFFIC_PER_ALGORITHMIC_BYTE:
         out["traffic"] = TRAFFIC_PER_ALGORITHMIC_BYTE[kern] * alg_bytes
         out["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
