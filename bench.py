@@ -537,7 +537,8 @@ def measure_i8(args, cfg, local, dist, peak, mode):
     eng = gccu.Engine(local)
     try:
         eng.set_tuning(args.tune)
-        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd")
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsd",
+                        shard=cc.Shard(dist) if dist else None)
         s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
         eng.set_precision(mode)
         f = measure(args, cfg, eng, s, local, dist, mode, main=True)

@@ -797,7 +797,10 @@ class Engine {
     lap(pstats.host_s, t);
     for (auto& r : P.maps) P.items[r.item].op[r.opnd].map[r.comp] = strmap(r.key);
     lap(pstats.maps_s, t);
-    dp->policy = tune == 2 ? tune_forced : tune == 1 ? autotune(*dp) : 0;
+    // a sharded engine keeps the fixed rule: the ranks' shares partition the
+    // tile lists only if every rank builds the same ones, which independent
+    // timings do not guarantee
+    dp->policy = tune == 2 ? tune_forced : (tune == 1 && shard_n == 1) ? autotune(*dp) : 0;
     lap(pstats.tune_s, t);
     build_gemm(*dp, tile_policies(precision).at(dp->policy));
     if (P.use_tr) build_flip(*dp, list(bc->list_res), (int)bc->iblk_res);

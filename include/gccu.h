@@ -314,7 +314,10 @@ int gccu_set_precision(int64_t mode);
  * range [n*rank/nranks, n*(rank+1)/nranks) of each tile list n (operand
  * gathers and splits run in full); the host sums the partial results of the
  * ranks (an all-reduce of the residual lists) and keeps everything else
- * replicated.  (0, 1) restores whole contractions. */
+ * replicated.  (0, 1) restores whole contractions.  Contractions planned
+ * while nranks > 1 use the fixed tile rule even with gccu_set_tuning(1):
+ * the shares partition the work only if every rank builds the same tile
+ * lists. */
 int gccu_set_shard(int64_t rank, int64_t nranks);
 /* Polls of one pipeline wait of the tensor-core kernel before it gives up
  * (polls < 0: the default, 4194304); on time-out the kernel stops, waits for

@@ -1,4 +1,4 @@
-"""bench.py's multi-process timing on CPU: with two gloo ranks (the replicas
+"""bench.py's multi-process timing on CPU: with two gloo ranks (the process
 layout of `bench.py --gpus 2` under torchrun, one process per device), every
 rank ends up with the slowest rank's time, and without a process group the
 time is returned unchanged."""
