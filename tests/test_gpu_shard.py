@@ -1,8 +1,8 @@
 """The engine's share of a sharded evaluation (gccu_set_shard), on one GPU:
 the ranks' shares of one CCSD evaluation are run one after another in one
 process (no rank waits for another), and the sum of their residual and
-energy lists equals the unsharded evaluation, in FP64 and in split TF32, for
-two and three ranks."""
+energy lists equals the unsharded evaluation, in FP64, split TF32 and four
+int8 slices, for two and three ranks."""
 import numpy as np
 import pytest
 
@@ -19,7 +19,7 @@ class _Rank:
         self.rank, self.n = rank, n
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["fp64", "split_tf32"])
+@pytest.mark.parametrize("mode", [0, 1, 3], ids=["fp64", "split_tf32", "int8_slices"])
 def test_shares_sum_to_the_whole_evaluation(built, mode):
     sp, eps, B = hm.synthetic(6, 30, 60, seed=6030)
     e = gccu.Engine(0)
