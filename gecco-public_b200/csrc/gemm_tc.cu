@@ -965,6 +965,7 @@ __global__ void __launch_bounds__(TNT, 1)
         const int64_t nk = (td.k1 - td.k0 + SK - 1) / SK;
         const int bn = descs[td.item].tn;
         const uint32_t idesc = idesc_i8(TBM, bn), kB = (uint32_t)bn * 16;
+        const uint32_t bslice = 2 * kB / 16;  // next column-operand slice, descriptor units
         if (lt >= 1 &&  // the epilogue has read the previous tile's accumulators
             !mbar_wait(smem_u32(&S.acce), (uint32_t)((lt - 1) & 1), failed, wait_limit)) {
           *failed = 1;
@@ -978,15 +979,26 @@ __global__ void __launch_bounds__(TNT, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t a0 = smem_u32(S.a[s]), b0 = smem_u32(S.b[s]);
+          // the stage's descriptors once; a slice's descriptor is the base's
+          // plus its offset / 16 in the address field (offsets stay inside
+          // the 256 KB window the 14-bit field addresses, no carry)
+          const uint64_t da0 = smem_desc(smem_u32(S.a[s]), kA, 128);
+          const uint64_t db0 = smem_desc(smem_u32(S.b[s]), kB, 128);
+          if (t == 0) {
 #pragma unroll
-          for (int dd = 0; dd < IS; ++dd)
+            for (int dd = 0; dd < IS; ++dd)
 #pragma unroll
-            for (int sa = 0; sa <= dd; ++sa) {
-              const uint64_t da = smem_desc(a0 + (uint32_t)sa * 2 * kA, kA, 128);
-              const uint64_t db = smem_desc(b0 + (uint32_t)(dd - sa) * 2 * kB, kB, 128);
-              mma_i8(tmem + (uint32_t)(dd * bn), da, db, idesc, (t > 0 || sa > 0) ? 1u : 0u);
-            }
+              for (int sa = 0; sa <= dd; ++sa)
+                mma_i8(tmem + (uint32_t)(dd * bn), da0 + (uint64_t)(sa * 2 * kA / 16),
+                       db0 + (uint64_t)((dd - sa) * bslice), idesc, sa > 0 ? 1u : 0u);
+          } else {
+#pragma unroll
+            for (int dd = 0; dd < IS; ++dd)
+#pragma unroll
+              for (int sa = 0; sa <= dd; ++sa)
+                mma_i8(tmem + (uint32_t)(dd * bn), da0 + (uint64_t)(sa * 2 * kA / 16),
+                       db0 + (uint64_t)((dd - sa) * bslice), idesc, 1u);
+          }
           mma_commit(smem_u32(&S.empty[s]));
           S.consumed = it + 1;
         }
