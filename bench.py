@@ -1081,11 +1081,11 @@ def main():
                     help="skip the D2h CCSD workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned preconditioner's instance stream")
-    ap.add_argument("--c4-train", type=int, default=32,
-                    help="training instances of the learned preconditioner's stream (64: the "
-                         "full stream)")
-    ap.add_argument("--c4-test", type=int, default=16,
-                    help="held-out instances of the stream (192: the full stream)")
+    ap.add_argument("--c4-train", type=int, default=64,
+                    help="training instances of the learned preconditioner's stream (the first "
+                         "64 solves of the 256-instance stream)")
+    ap.add_argument("--c4-test", type=int, default=32,
+                    help="held-out instances of the stream (192: the rest of the full stream)")
     ap.add_argument("--trace-contraction", default=None,
                     help="set up, run one named [CONTR] of the formula once and exit "
                          "(the command the ncu captures in profiles/ run)")
