@@ -64,6 +64,8 @@ def lib():
         L.ora_sym_ab_blk.restype = ctypes.c_int
         L.ora_sym_ab_blk.argtypes = [ctypes.c_void_p, I64, I64, PD, ctypes.c_double,
                                      ctypes.c_double]
+        L.ora_spin_prj_list.restype = ctypes.c_int
+        L.ora_spin_prj_list.argtypes = [ctypes.c_void_p, I64, I64, PD, PD]
         L.ora_add_opblk.restype = ctypes.c_int
         L.ora_add_opblk.argtypes = [PD, I64, ctypes.c_double, PD, PD, I64, I64]
         L.ora_diavc.restype = None
@@ -211,6 +213,13 @@ class Oracle:
                                     _pd(np.ascontiguousarray(xin)), lout, bout, _pd(xout),
                                     int(tra_in), int(tra_out), int(reset)))
         return float(xn[0])
+
+    def spin_prj(self, lst, x, nblk, s2=0):
+        """spin_prj_list: x (the whole list) projected onto its singlet part in
+        place; returns the squared norm of every occupation class"""
+        xn = np.zeros(max(nblk, 1))
+        _chk(lib().ora_spin_prj_list(self.ctx, lst, s2, _pd(x), _pd(xn)))
+        return xn[:nblk]
 
     def sym_ab(self, lst, iblk, x, prefac=0.5, relfac=1.0):
         _chk(lib().ora_sym_ab_blk(self.ctx, lst, iblk, _pd(x), prefac, relfac))

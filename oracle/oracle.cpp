@@ -339,6 +339,7 @@ struct ora_ctx {
   // string map blocks, keyed by (g1,g2,idxms1,idxms2,gam1,gam2)
   std::map<std::array<int, 6>, std::vector<int>> strmaps;
   std::map<std::array<int, 3>, std::vector<int>> flipmaps;  // (g,idxms,gam)
+  std::map<std::array<int, 3>, std::vector<int>> spprjmaps;  // (g,idxms,gam)
 
   int graph(int type, int nel) {
     auto k = std::make_pair(type, nel);
@@ -1887,6 +1888,381 @@ void sym_ab_blk(ora_ctx* cx, List& L, int iblk, double* buf, double prefac, doub
   }
 }
 
+// ---- spin projection (contract/spin_prj_list.f, contract/spin_prj_blk.f) ----
+
+// spin patterns of n electrons (set_spprjmap_cases,
+// strings/set_spprjmap_cases.f:24-41): position i (0-based) carries bit
+// n-1-i, set for beta.  The reference pattern alternates and ends in alpha
+// (..., beta, alpha); it is number 0, the others are numbered 1.. in
+// increasing bit order.
+int spin_ref_bits(int n) {
+  int b = 0;
+  for (int i = 1; i < n; i += 2) b |= 1 << i;
+  return b;
+}
+int spin_case_number(int n, int bits) {
+  int ref = spin_ref_bits(n);
+  if (bits == ref) return 0;
+  return bits < ref ? bits + 1 : bits;
+}
+int spin_pattern_bits(const int* spn, int n) {
+  int b = 0;
+  for (int i = 0; i < n; ++i)
+    if (spn[i] == -1) b |= 1 << (n - 1 - i);
+  return b;
+}
+
+// set_spprjmap_kernel (strings/set_spprjmap_kernel.f:60-130): for every
+// string of the block whose spins alternate from the right end (alpha
+// last; paired orbitals pass), and every non-reference pattern k = 1..2^n-1,
+// sign * (address of the string with the same orbitals and the spins of
+// pattern k, + 1); 0 when the string is not of the reference pattern or a
+// paired orbital would get two equal spins
+const std::vector<int>& spprjmap(ora_ctx* cx, int g, int idxms, int gam) {
+  std::array<int, 3> k{g, idxms, gam};
+  auto it = cx->spprjmaps.find(k);
+  if (it != cx->spprjmaps.end()) return it->second;
+  const Graph& Gr = cx->G(g);
+  const int nel = Gr.nel;
+  CHECK(nel >= 2, "set_spprjmap_kernel: occ=1 uses the trivial map");
+  const int ms = nel - (idxms - 1) * 2;
+  CHECK(!(nel % 2 == 0 && ms != 0), "set_spprjmap_kernel: only ms=0 for even occ");
+  CHECK(!(nel % 2 == 1 && ms != 1), "set_spprjmap_kernel: only ms=1/2 for odd occ");
+  const int nmaps = (1 << nel) - 1;
+  const StrBlock& b = Gr.blk[idxms - 1][gam - 1];
+  std::vector<int> m;
+  m.reserve(b.n() * nmaps);
+  std::vector<int> pat(nel), sf(nel);
+  // patterns in case order
+  std::vector<std::vector<int>> cases(nmaps + 1, std::vector<int>(nel));
+  for (int bits = 0; bits < (1 << nel); ++bits) {
+    int c = spin_case_number(nel, bits);
+    for (int i = 0; i < nel; ++i) cases[c][i] = ((bits >> (nel - 1 - i)) & 1) ? -1 : +1;
+  }
+  for (int64_t s = 0; s < b.n(); ++s) {
+    const int* o = b.orb.data() + s * nel;
+    const int* sp = b.spn.data() + s * nel;
+    bool ref = true;
+    for (int i = nel - 1, sg = +1; i >= 0; --i, sg = -sg)
+      if (sp[i] != sg && sp[i] != 2) ref = false;
+    if (!ref) {
+      m.insert(m.end(), nmaps, 0);
+      continue;
+    }
+    for (int c = 1; c <= nmaps; ++c) {
+      sf = cases[c];
+      bool ok = true;
+      for (int i = 0; i < nel && ok; ++i) {
+        if (sp[i] == 2 && sf[i] != 2) {
+          CHECK(i + 1 < nel && sp[i + 1] == 2, "set_spprjmap_kernel: broken spin pair");
+          if (sf[i] * sf[i + 1] != -1) ok = false;
+          else sf[i] = sf[i + 1] = 2;
+        }
+      }
+      if (!ok) {
+        m.push_back(0);
+        continue;
+      }
+      int msf = 0;
+      for (int i = 0; i < nel; ++i) msf += sf[i] == 2 ? 0 : sf[i];
+      const StrBlock& bf = Gr.blk[(nel - msf) / 2][gam - 1];
+      auto f = bf.index.find(key_of(nel, o, sf.data()));
+      CHECK(f != bf.index.end(), "set_spprjmap_kernel: flipped string not addressable");
+      int sg = std_spsign(sp, nel) * std_spsign(sf.data(), nel);
+      m.push_back(sg * (int)(f->second + 1));
+    }
+  }
+  return cx->spprjmaps[k] = std::move(m);
+}
+
+// get_genealogical_coeff (baserout/get_genealogical_coeff.f:32-106) for
+// s2 = 0, ms2 = 0: the coefficients of every singlet coupling path (paths of
+// the branching diagram that never go below S = 0, in lexical order of the
+// up/down sequence) for creators with spins c[0..n-1] followed by the
+// annihilators in reverse order a[n-1..0]
+std::vector<double> genealogical(const std::vector<int>& c, const std::vector<int>& a) {
+  const int nc = (int)c.size(), na = (int)a.size(), nel = nc + na;
+  const int nup = nel / 2;
+  std::vector<int> br(nel, 1);
+  std::fill(br.begin(), br.begin() + nup, 0);
+  std::vector<double> out;
+  do {
+    bool valid = true;
+    int down = 0;
+    for (int i = 0; i < nel; ++i) {
+      down += br[i];
+      if (down > (i + 1) / 2) valid = false;
+    }
+    if (!valid) continue;
+    int is2 = 0, ims2 = 0, iel = 0;
+    double x = 1.0;
+    auto step = [&](int ms_step, double sigma) {
+      is2 += 1 - 2 * br[iel];
+      ims2 += ms_step;
+      if (br[iel] == 0)
+        x *= std::sqrt(std::max(0.0, (is2 / 2.0 + sigma * ims2) / is2));
+      else
+        x = -2.0 * sigma * x * std::sqrt(std::max(0.0, (is2 / 2.0 + 1.0 - sigma * ims2) / (is2 + 2.0)));
+      ++iel;
+    };
+    for (int i = 0; i < nc; ++i) step(c[i], 0.5 * c[i]);
+    for (int i = na - 1; i >= 0; --i) {
+      step(-a[i], -0.5 * a[i]);
+      if (a[i] == -1) x = -x;
+    }
+    out.push_back(x);
+  } while (std::next_permutation(br.begin(), br.end()));
+  return out;
+}
+
+// get_target_dis (contract/spin_prj_blk.f:440-524): Ms distribution of the
+// skeleton strings over the components -- 0 for even occupations; odd ones
+// +1 (occupations above 1 first), then +1 from the left and -1 from the
+// right in turn
+std::vector<int> target_dis(const std::vector<int>& occ) {
+  const int n = (int)occ.size();
+  std::vector<int> t(n, 0);
+  std::vector<bool> as(n, false);
+  int nodd = 0, nlarge = 0;
+  for (int i = 0; i < n; ++i) {
+    if (occ[i] % 2 == 1) {
+      ++nodd;
+      if (occ[i] > 1) ++nlarge;
+    } else {
+      as[i] = true;
+    }
+  }
+  const int k = std::min(nlarge, (nodd + 1) / 2);
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i < n; ++i)
+      if (!as[i] && occ[i] > 1) {
+        t[i] = +1;
+        as[i] = true;
+        break;
+      }
+  int icnt = k;
+  auto done = [&] { return std::all_of(as.begin(), as.end(), [](bool b) { return b; }); };
+  while (!done()) {
+    if (icnt <= 0) {
+      for (int i = 0; i < n; ++i)
+        if (!as[i]) {
+          t[i] = +1, as[i] = true, ++icnt;
+          break;
+        }
+    } else {
+      for (int i = n - 1; i >= 0; --i)
+        if (!as[i]) {
+          t[i] = -1, as[i] = true, --icnt;
+          break;
+        }
+    }
+  }
+  return t;
+}
+
+// one spin case of a class (set_spinprj_info.f set_case): spins of every
+// creator / annihilator, Ms per component, pattern number per component
+// relative to the skeleton's reference pattern (0 = the skeleton string
+// itself), coupling coefficients
+struct SpinCase {
+  std::vector<int> sc, sa, msc, msa, mapc, mapa;
+  std::vector<double> coeff;
+};
+
+// spin_prj_blk (contract/spin_prj_blk.f:97-425) with set_spinprj_info
+// (contract/set_spinprj_info.f:55-305), s2 = 0, in place on buf (the whole
+// list)
+void spin_prj_blk(ora_ctx* cx, List& L, int iblk, double* buf) {
+  CHECK(L.mst == 0, "spin_prj_blk: ms.ne.0 not yet considered");
+  ListBlock& B = L.blk[iblk - 1];
+  const int nsym = cx->oi.nsym;
+  const int msc_max = sum_occ(B.c), msa_max = sum_occ(B.a);
+  CHECK(msc_max == msa_max, "spin_prj_blk: only particle-conserving operators!");
+  if (msc_max == 0) return;  // scalar: the singlet part is the element
+  const int npart = msc_max;
+  CHECK(npart <= 8, "spin_prj_blk: more than eight creators");
+  const std::vector<int> oc = occs(B.c), oa = occs(B.a);
+  const std::vector<int> tc = target_dis(oc), ta = target_dis(oa);
+  // reference spins per particle: per component alternating, starting with
+  // alpha for a +1 target and beta otherwise
+  auto ref_spins = [](const std::vector<int>& occ, const std::vector<int>& tgt) {
+    std::vector<int> s;
+    for (size_t i = 0; i < occ.size(); ++i)
+      for (int e = 0, sg = tgt[i] == 1 ? 1 : -1; e < occ[i]; ++e, sg = -sg) s.push_back(sg);
+    return s;
+  };
+  const std::vector<int> setc = ref_spins(oc, tc), seta = ref_spins(oa, ta);
+  auto map_type = [](const int* tgt, const int* ref, int n) {
+    if (n == 1) return tgt[0] == ref[0] ? 0 : 1;
+    CHECK(spin_pattern_bits(ref, n) == spin_ref_bits(n), "set_spinprj_info: error in map_type");
+    return spin_case_number(n, spin_pattern_bits(tgt, n));
+  };
+  // spin cases: annihilator spins outer, creator spins inner, each running
+  // from all alpha with the first particle fastest (next_dist2, inc -2);
+  // equal Ms on both sides
+  std::vector<SpinCase> cases;
+  std::vector<int> omni;
+  int pm[64][2];
+  for (int i = 0; i < npart; ++i) pm[i][0] = -1, pm[i][1] = 1;
+  std::vector<int> da(npart, 1), dc(npart, 1);
+  for (bool more_a = true; more_a; more_a = next_dist(da.data(), npart, pm, -2)) {
+    std::fill(dc.begin(), dc.end(), 1);
+    for (bool more_c = true; more_c; more_c = next_dist(dc.data(), npart, pm, -2)) {
+      int sc = 0, sa = 0;
+      for (int i = 0; i < npart; ++i) sc += dc[i], sa += da[i];
+      if (sc != sa) continue;
+      SpinCase k;
+      k.sc = dc;
+      k.sa = da;
+      for (int i = 0, o = 0; i < (int)oc.size(); o += oc[i], ++i) {
+        int m = 0;
+        for (int e = 0; e < oc[i]; ++e) m += dc[o + e];
+        k.msc.push_back(m);
+        k.mapc.push_back(map_type(dc.data() + o, setc.data() + o, oc[i]));
+      }
+      for (int i = 0, o = 0; i < (int)oa.size(); o += oa[i], ++i) {
+        int m = 0;
+        for (int e = 0; e < oa[i]; ++e) m += da[o + e];
+        k.msa.push_back(m);
+        k.mapa.push_back(map_type(da.data() + o, seta.data() + o, oa[i]));
+      }
+      k.coeff = genealogical(dc, da);
+      // both strings alternate over all particles ("omnipresent" case)
+      bool alt = npart > 1;
+      for (int i = 0; i + 1 < npart; ++i)
+        if (dc[i] * dc[i + 1] != -1 || da[i] * da[i + 1] != -1) alt = false;
+      if (alt) omni.push_back((int)cases.size());
+      cases.push_back(std::move(k));
+    }
+  }
+  CHECK(omni.size() <= 4, "set_case: increase bound for nomni");
+  const int ncase = (int)cases.size(), ncoup = (int)cases[0].coeff.size();
+
+  const int msa = msa_max % 2, msc = msa;
+  const int idxmsa = msa2idxms4op(msa, 0, msa_max, msc_max);
+  const size_t ncc = B.c.size(), nca = B.a.size();
+  for (int gama = 1; gama <= nsym; ++gama) {
+    const int gamc = mult(gama, L.gamt);
+    auto itl = B.gm_len.find({idxmsa, gama});
+    if (itl == B.gm_len.end() || itl->second <= 0) continue;
+    MsGamDist d;
+    for (bool first = true; next_msgamdist2(first, d, oc, oa, msc, msa, gamc, gama, nsym);
+         first = false) {
+      if (d.msc != tc || d.msa != ta) continue;
+      auto ixc = ixms(B.c, d.msc), ixa = ixms(B.a, d.msa);
+      auto lc = lens(cx, B.c, ixc, d.gc), la = lens(cx, B.a, ixa, d.ga);
+      const int64_t lenc = prod(lc, 0, lc.size()), lena = prod(la, 0, la.size());
+      if (lenc == 0 || lena == 0) continue;
+      // per case: offset of its distribution and its leading dimensions
+      std::vector<int64_t> off(ncase, -1);
+      std::vector<std::vector<int64_t>> ldc(ncase), lda(ncase);
+      for (int k = 0; k < ncase; ++k) {
+        const SpinCase& K = cases[k];
+        auto kxc = ixms(B.c, K.msc), kxa = ixms(B.a, K.msa);
+        int msak = 0;
+        for (int m : K.msa) msak += m;
+        const int kidx = msa2idxms4op(msak, 0, msa_max, msc_max);
+        auto kl = cat(lens(cx, B.c, kxc, d.gc), lens(cx, B.a, kxa, d.ga));
+        ldims(B.c, B.a, kl, ldc[k], lda[k]);
+        auto dit = B.dis.find({kidx, gama});
+        if (dit == B.dis.end()) continue;
+        const int64_t did = msgmdid2(B.c, kxc, d.gc, B.a, kxa, d.ga, nsym);
+        for (const DistRow& r : dit->second)
+          if (r.did == did) off[k] = r.off;
+      }
+      // spin projection maps of the skeleton strings (get_spprjmap_blk,
+      // strings/get_spprjmap_blk.f:48-95; one electron: the identity)
+      std::vector<const int*> mc(ncc, nullptr), ma(nca, nullptr);
+      std::vector<int> nmc(ncc), nma(nca);
+      for (size_t i = 0; i < ncc; ++i) {
+        nmc[i] = (1 << B.c[i].occ) - 1;
+        if (B.c[i].occ > 1) mc[i] = spprjmap(cx, B.c[i].graph, ixc[i], d.gc[i]).data();
+      }
+      for (size_t i = 0; i < nca; ++i) {
+        nma[i] = (1 << B.a[i].occ) - 1;
+        if (B.a[i].occ > 1) ma[i] = spprjmap(cx, B.a[i].graph, ixa[i], d.ga[i]).data();
+      }
+      std::vector<int64_t> sc0(ncc), sa0(nca);
+      std::vector<int64_t> idxel(ncase);
+      std::vector<int> psign(ncase);
+      std::vector<double> value(ncase), overl(ncoup);
+      std::vector<char> okc(ncase), oka(ncase);
+      std::vector<int64_t> pa(ncase), pc(ncase);
+      for (int64_t ia = 0; ia < lena; ++ia) {
+        decompose(ia, la, sa0.data());
+        for (int k = 0; k < ncase; ++k) {
+          oka[k] = 1;
+          pa[k] = 0;
+          for (size_t i = 0; i < nca; ++i) {
+            int64_t s = sa0[i];
+            const int mi = cases[k].mapa[i];
+            if (mi != 0) {
+              const int v = ma[i] ? ma[i][s * nma[i] + mi - 1] : (int)s + 1;
+              if (v == 0) oka[k] = 0;
+              s = std::abs(v) - 1;
+            }
+            pa[k] += s * lda[k][i];
+          }
+        }
+        for (int64_t ic = 0; ic < lenc; ++ic) {
+          decompose(ic, lc, sc0.data());
+          for (int k = 0; k < ncase; ++k) {
+            okc[k] = 1;
+            pc[k] = 0;
+            for (size_t i = 0; i < ncc; ++i) {
+              int64_t s = sc0[i];
+              const int mi = cases[k].mapc[i];
+              if (mi != 0) {
+                const int v = mc[i] ? mc[i][s * nmc[i] + mi - 1] : (int)s + 1;
+                if (v == 0) okc[k] = 0;
+                s = std::abs(v) - 1;
+              }
+              pc[k] += s * ldc[k][i];
+            }
+          }
+          for (int k = 0; k < ncase; ++k) {
+            idxel[k] = -1;
+            value[k] = 0.0;
+            if (!okc[k] || !oka[k] || off[k] < 0) continue;
+            idxel[k] = off[k] + pc[k] + pa[k];
+            // the element appears more than once (paired orbitals): the
+            // parity of (count - 1) in bits (popcnt_par)
+            int cnt = 0;
+            for (int j = 0; j <= k; ++j) cnt += idxel[j] == idxel[k];
+            psign[k] = (__builtin_popcount(cnt - 1) & 1) ? -1 : 1;
+            value[k] = buf[idxel[k]] * psign[k];
+          }
+          bool skip = false;
+          for (int k : omni) skip = skip || idxel[k] < 0;
+          if (skip) continue;
+          for (int q = 0; q < ncoup; ++q) {
+            double s = 0.0;
+            for (int k = 0; k < ncase; ++k) s += cases[k].coeff[q] * value[k];
+            overl[q] = s;
+          }
+          for (int k = 0; k < ncase; ++k) {
+            double s = 0.0;
+            for (int q = 0; q < ncoup; ++q) s += cases[k].coeff[q] * overl[q];
+            value[k] = s;
+          }
+          for (int k = 0; k < ncase; ++k)
+            if (idxel[k] >= 0) buf[idxel[k]] = value[k] * psign[k];
+        }
+      }
+    }
+  }
+}
+
+void spin_prj_list(ora_ctx* cx, List& L, double* x, double* xnorm2) {
+  for (size_t ib = 0; ib < L.blk.size(); ++ib) {
+    const ListBlock& B = L.blk[ib];
+    if (xnorm2) xnorm2[ib] = 0.0;
+    if (B.len_occ == 0) continue;
+    spin_prj_blk(cx, L, (int)ib + 1, x);
+    if (xnorm2) xnorm2[ib] = ddot_blk(x + B.off_occ, B.len_occ);
+  }
+}
+
 // add_opblk_transp (contract/add_opblk_transp.f:195-321): OUT(IC,IA) +=
 // fac * IN(IA,IC) for a class of the output whose adjoint is the input class
 // (op_in^tra_in = op_out^tra_out).  Loops over the output's Ms(A), IRREP(A)
@@ -2173,6 +2549,14 @@ int ora_sym_ab_blk(ora_ctx* c, int64_t list, int64_t iblk, double* x, double pre
                    double relfac) {
   GUARD_BEGIN
   sym_ab_blk(c, c->lists.at(list - 1), (int)iblk, x, prefac, relfac);
+  return 0;
+  GUARD_END(-1)
+}
+
+int ora_spin_prj_list(ora_ctx* c, int64_t list, int64_t s2, double* x, double* xnorm2) {
+  GUARD_BEGIN
+  CHECK(s2 == 0, "spin_prj_list: not a singlet case");
+  spin_prj_list(c, c->lists.at(list - 1), x, xnorm2);
   return 0;
   GUARD_END(-1)
 }

@@ -96,6 +96,11 @@ int ora_trace(ora_ctx*, int64_t list_op, int64_t iblk_op, const double* xop,
 int ora_sym_ab_blk(ora_ctx*, int64_t list, int64_t iblk, double* x,
                    double prefac, double relfac);
 
+/* spin projection of a whole list onto its singlet part, in place --
+ * contract/spin_prj_list.f with contract/spin_prj_blk.f; s2 must be 0;
+ * xnorm2 (may be NULL) receives the squared norm of every projected class */
+int ora_spin_prj_list(ora_ctx*, int64_t list, int64_t s2, double* x, double* xnorm2);
+
 /* route-3 dgemm through an ILP64 BLAS (e.g. the OpenBLAS bundled with numpy)
  * instead of the plain loop; nthreads > 0 sets the BLAS thread count */
 int ora_set_blas(const char* path, int64_t nthreads);
