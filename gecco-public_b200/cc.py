@@ -229,8 +229,11 @@ class CCSolver:
     diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
 
     def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
-                 learned=None, shard=None):
+                 learned=None, shard=None, spin_project=False):
         self.e = engine
+        # project the residuals onto their singlet part after each evaluation
+        # (result lists with a spin, frm_sched2's end-of-target step)
+        self.spin_project = spin_project
         self.shard = shard  # Shard: residual contractions split over ranks
         self.ints = ints
         self.method = method
@@ -483,9 +486,17 @@ class CCSolver:
             self.evaluate()
         if self.shard is not None:
             self.shard.reduce(self)
+        if self.spin_project:
+            self.project_residuals()
         en = self.energy()
         rn = self.residual_norm()
         return en, rn
+
+    def project_residuals(self):
+        """singlet projection of the residual lists (spin_prj_list at the end
+        of each target, contract/frm_sched2.f:146-149)"""
+        for a in self.amps:
+            self.e.spin_prj(self.lid(self.res[a]))
 
     def capture(self):
         """record one formula evaluation as a CUDA graph (plans must exist)"""

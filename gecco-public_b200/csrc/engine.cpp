@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <functional>
 #include <atomic>
 #include <thread>
@@ -162,6 +163,127 @@ struct DevReo {
   int64_t reo_off = 0, reo_len = 0;
 };
 
+// singlet spin projection of one list (spin_prj_list), planned on first
+// use: per case-count bucket (2, 6, 20, 70 cases) the skeleton descriptors
+struct DevSpinPrj {
+  SpinPrjDesc* d[4] = {};
+  int64_t n[4] = {}, maxlen[4] = {};
+};
+constexpr int kSpinPrjBucket[4] = {2, 6, 20, kSpinPrjMaxCases};
+
+// spin patterns of n electrons (set_spprjmap_cases,
+// strings/set_spprjmap_cases.f:24-41): bit n-1-i set for a beta spin at
+// position i; the pattern that alternates and ends in alpha is number 0, the
+// others are numbered from 1 in increasing bit order
+int spin_ref_bits(int n) {
+  int b = 0;
+  for (int i = 1; i < n; i += 2) b |= 1 << i;
+  return b;
+}
+int spin_pattern_number(int n, int bits) {
+  const int ref = spin_ref_bits(n);
+  return bits == ref ? 0 : (bits < ref ? bits + 1 : bits);
+}
+int spin_bits(const int* s, int n) {
+  int b = 0;
+  for (int i = 0; i < n; ++i)
+    if (s[i] == -1) b |= 1 << (n - 1 - i);
+  return b;
+}
+// std_spsign (strings/std_spsign_msdis.f): parity of moving every alpha in
+// front of the betas
+int spin_sign(const int* s, int ne) {
+  int trp = 0, nb = 0;
+  for (int i = 0; i < ne;) {
+    const int sg = s[i];
+    if (sg == 1 || sg == 2) trp += nb, ++i;
+    if (sg == -1 || sg == 2) ++nb, ++i;
+  }
+  return (trp & 1) ? -1 : 1;
+}
+
+// singlet genealogical coupling coefficients (get_genealogical_coeff,
+// baserout/get_genealogical_coeff.f:32-106, S = Ms = 0) of the creator spins
+// c followed by the annihilator spins a in reverse order: one value per path
+// of the branching diagram that stays at S >= 0, paths in lexical order of
+// their up (0) / down (1) steps
+std::vector<double> singlet_coupling(const std::vector<int>& c, const std::vector<int>& a) {
+  const int nc = (int)c.size(), na = (int)a.size(), nel = nc + na;
+  std::vector<int> step(nel, 1);
+  std::fill(step.begin(), step.begin() + nel / 2, 0);
+  std::vector<double> out;
+  do {
+    int down = 0;
+    bool ok = true;
+    for (int i = 0; i < nel; ++i) {
+      down += step[i];
+      ok = ok && down <= (i + 1) / 2;
+    }
+    if (!ok) continue;
+    int s2 = 0, m2 = 0, k = 0;
+    double x = 1.0;
+    auto couple = [&](int dm, double sigma) {
+      s2 += 1 - 2 * step[k];
+      m2 += dm;
+      if (step[k] == 0)
+        x *= std::sqrt(std::max(0.0, (0.5 * s2 + sigma * m2) / s2));
+      else
+        x = -2.0 * sigma * x * std::sqrt(std::max(0.0, (0.5 * s2 + 1.0 - sigma * m2) / (s2 + 2.0)));
+      ++k;
+    };
+    for (int i = 0; i < nc; ++i) couple(c[i], 0.5 * c[i]);
+    for (int i = na - 1; i >= 0; --i) {
+      couple(-a[i], -0.5 * a[i]);
+      if (a[i] == -1) x = -x;
+    }
+    out.push_back(x);
+  } while (std::next_permutation(step.begin(), step.end()));
+  return out;
+}
+
+// Ms per component of the skeleton distribution (get_target_dis,
+// contract/spin_prj_blk.f:440-524): 0 for even occupations; odd ones +1
+// (occupations above 1 first), the rest +1 from the left and -1 from the
+// right in turn
+std::vector<int> skeleton_ms(const std::vector<int>& occ) {
+  const int n = (int)occ.size();
+  std::vector<int> t(n, 0);
+  std::vector<char> set(n, 0);
+  int nodd = 0, nlarge = 0;
+  for (int i = 0; i < n; ++i) {
+    if (occ[i] % 2) {
+      ++nodd;
+      nlarge += occ[i] > 1;
+    } else {
+      set[i] = 1;
+    }
+  }
+  const int k = std::min(nlarge, (nodd + 1) / 2);
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i < n; ++i)
+      if (!set[i] && occ[i] > 1) {
+        t[i] = 1, set[i] = 1;
+        break;
+      }
+  int bal = k;
+  for (int left = nodd - k; left > 0; --left) {
+    if (bal <= 0) {
+      for (int i = 0; i < n; ++i)
+        if (!set[i]) {
+          t[i] = 1, set[i] = 1, ++bal;
+          break;
+        }
+    } else {
+      for (int i = n - 1; i >= 0; --i)
+        if (!set[i]) {
+          t[i] = -1, set[i] = 1, --bal;
+          break;
+        }
+    }
+  }
+  return t;
+}
+
 class Engine {
  public:
   Model model;
@@ -177,6 +299,8 @@ class Engine {
   std::map<int, DevGraph> dgraphs;
   std::map<MapKey, int32_t*> maps;
   std::map<std::array<int, 3>, int32_t*> flips;
+  std::map<std::array<int, 3>, int32_t*> spprjs;  // spin-projection pattern maps
+  std::map<int64_t, std::unique_ptr<DevSpinPrj>> spinprjs;  // singlet projection per list
   std::map<std::string, std::unique_ptr<DevPlan>> plans;
   std::vector<void*> allocs;
   double* d_red = nullptr;  // reduction scalars
@@ -1472,6 +1596,236 @@ class Engine {
     blap(pstats.const_s);
   }
 
+  // pattern map of one string block for the spin projection
+  // (set_spprjmap_kernel, strings/set_spprjmap_kernel.f:60-130): for every
+  // string whose spins alternate from the right end (alpha last; the two
+  // members of a paired orbital pass) and every pattern k = 1..2^n-1,
+  // sign * (address of the string with the same orbitals and the spins of
+  // pattern k, + 1), sign = std_spsign(string) * std_spsign(result); 0 for
+  // the other strings and where a paired orbital would get two equal spins
+  int32_t* spprjmap(int gid, int idxms, int gam) {
+    std::array<int, 3> key{gid, idxms, gam};
+    auto it = spprjs.find(key);
+    if (it != spprjs.end()) return it->second;
+    Graph& g = model.G(gid);
+    const int nel = g.nel, nmaps = (1 << nel) - 1;
+    const int ms = nel - 2 * (idxms - 1);
+    GCCU_REQUIRE(nel % 2 == 0 ? ms == 0 : ms == 1,
+                 "spin projection: skeleton strings need Ms 0 (even occupation) or 1/2 (odd)");
+    const auto& t = g.table(idxms, gam);
+    const int64_t n = g.nstr(idxms, gam);
+    std::vector<std::vector<int>> pat(nmaps + 1, std::vector<int>(nel));
+    for (int bits = 0; bits <= nmaps; ++bits) {
+      const int c = spin_pattern_number(nel, bits);
+      for (int i = 0; i < nel; ++i) pat[c][i] = ((bits >> (nel - 1 - i)) & 1) ? -1 : 1;
+    }
+    std::vector<int32_t> m(std::max<int64_t>(n * nmaps, 1), 0);
+    std::vector<int> orb(nel), spn(nel), sf(nel);
+    for (int64_t s = 0; s < n; ++s) {
+      for (int p = 0; p < nel; ++p) {
+        const int v = t[s * nel + p], c = v & 3;
+        orb[p] = v >> 2;
+        spn[p] = c == 1 ? 1 : (c == 2 ? -1 : 2);
+      }
+      bool ref = true;
+      for (int i = nel - 1, sg = 1; i >= 0; --i, sg = -sg) ref = ref && (spn[i] == sg || spn[i] == 2);
+      if (!ref) continue;
+      for (int c = 1; c <= nmaps; ++c) {
+        sf = pat[c];
+        bool ok = true;
+        for (int i = 0; i < nel && ok; ++i) {
+          if (spn[i] != 2 || sf[i] == 2) continue;
+          GCCU_REQUIRE(i + 1 < nel && spn[i + 1] == 2, "spin projection: broken spin pair");
+          if (sf[i] * sf[i + 1] != -1) ok = false;
+          else sf[i] = sf[i + 1] = 2;
+        }
+        if (!ok) continue;
+        m[s * nmaps + c - 1] = spin_sign(spn.data(), nel) * spin_sign(sf.data(), nel) *
+                               (int32_t)(g.address(orb.data(), sf.data()) + 1);
+      }
+    }
+    return spprjs[key] = upload(m);
+  }
+
+  // singlet projection plan of a list (spin_prj_list, contract/spin_prj_list.f:
+  // 166-199, with spin_prj_blk, contract/spin_prj_blk.f:97-400, and
+  // set_spinprj_info, contract/set_spinprj_info.f:55-305, per class)
+  DevSpinPrj& spinprj_for(int64_t list_id) {
+    auto it = spinprjs.find(list_id);
+    if (it != spinprjs.end()) return *it->second;
+    GCCU_REQUIRE(!capturing, "spin projection must be run once before it is captured in a graph");
+    const ListLayout& L = list(list_id).L;
+    GCCU_REQUIRE(L.mst == 0, "spin projection: ms.ne.0 not yet considered (lists of Ms 0 only)");
+    const int nsym = model.os.nsym;
+    std::vector<SpinPrjDesc> descs[4];
+    std::vector<int64_t> case_base[4], coef_base[4];
+    std::vector<SpinPrjCase> cases;
+    std::vector<double> coef;
+    for (const LayoutBlock& B : L.blk) {
+      if (B.len <= 0) continue;
+      const std::vector<int> oc = comp_occs(B.c), oa = comp_occs(B.a);
+      int np = 0, na_el = 0;
+      for (int v : oc) np += v;
+      for (int v : oa) na_el += v;
+      GCCU_REQUIRE(np == na_el, "spin projection: only particle-conserving operators");
+      if (np == 0) continue;  // scalar: its own singlet part
+      GCCU_REQUIRE(np <= kSpinPrjMaxPart,
+                   "spin projection: at most four creators and annihilators per class");
+      const std::vector<int> tc = skeleton_ms(oc), ta = skeleton_ms(oa);
+      // reference spins of the skeleton strings per particle: alternating in
+      // each component, starting with alpha for Ms +1, beta otherwise
+      auto ref_spins = [](const std::vector<int>& occ, const std::vector<int>& ms) {
+        std::vector<int> s;
+        for (size_t i = 0; i < occ.size(); ++i)
+          for (int e = 0, sg = ms[i] == 1 ? 1 : -1; e < occ[i]; ++e, sg = -sg) s.push_back(sg);
+        return s;
+      };
+      const std::vector<int> rc = ref_spins(oc, tc), ra = ref_spins(oa, ta);
+      auto pattern = [](const int* spins, const int* ref, int n) {
+        if (n == 1) return spins[0] == ref[0] ? 0 : 1;
+        GCCU_REQUIRE(spin_bits(ref, n) == spin_ref_bits(n),
+                     "spin projection: odd component with skeleton Ms -1/2 (map_type)");
+        return spin_pattern_number(n, spin_bits(spins, n));
+      };
+      // the spin cases: annihilator spins outer, creator spins inner, each
+      // from all alpha with the first particle changing fastest; Ms equal on
+      // both sides
+      struct Case {
+        std::vector<int> msc, msa, mc, ma;
+      };
+      std::vector<Case> cs;
+      std::vector<int> omni;
+      const size_t coef0 = coef.size();
+      std::vector<int> sa(np, 1), sc(np, 1);
+      auto next = [np](std::vector<int>& s) {
+        for (int i = 0; i < np; ++i) {
+          if (s[i] == 1) {
+            s[i] = -1;
+            return true;
+          }
+          s[i] = 1;
+        }
+        return false;
+      };
+      for (bool ma = true; ma; ma = next(sa)) {
+        std::fill(sc.begin(), sc.end(), 1);
+        for (bool mc = true; mc; mc = next(sc)) {
+          int msc = 0, msa = 0;
+          for (int i = 0; i < np; ++i) msc += sc[i], msa += sa[i];
+          if (msc != msa) continue;
+          Case k;
+          for (size_t i = 0, o = 0; i < oc.size(); o += oc[i], ++i) {
+            int m = 0;
+            for (int e = 0; e < oc[i]; ++e) m += sc[o + e];
+            k.msc.push_back(m);
+            k.mc.push_back(pattern(sc.data() + o, rc.data() + o, oc[i]));
+          }
+          for (size_t i = 0, o = 0; i < oa.size(); o += oa[i], ++i) {
+            int m = 0;
+            for (int e = 0; e < oa[i]; ++e) m += sa[o + e];
+            k.msa.push_back(m);
+            k.ma.push_back(pattern(sa.data() + o, ra.data() + o, oa[i]));
+          }
+          bool alt = np > 1;
+          for (int i = 0; i + 1 < np; ++i)
+            alt = alt && sc[i] * sc[i + 1] == -1 && sa[i] * sa[i + 1] == -1;
+          if (alt) omni.push_back((int)cs.size());
+          const std::vector<double> cf = singlet_coupling(sc, sa);
+          coef.insert(coef.end(), cf.begin(), cf.end());
+          cs.push_back(std::move(k));
+        }
+      }
+      const int ncase = (int)cs.size();
+      const int ncoup = (int)((coef.size() - coef0) / ncase);
+      GCCU_REQUIRE(ncase <= kSpinPrjMaxCases && ncoup <= kSpinPrjMaxCoup &&
+                       omni.size() <= (size_t)kSpinPrjMaxOmni,
+                   "spin projection: case tables exceed their bounds");
+      int bucket = 0;
+      while (kSpinPrjBucket[bucket] < ncase) ++bucket;
+      // skeleton distributions: Ms(A) = Ms(C) = np mod 2 and the skeleton Ms
+      // per component, every IRREP distribution
+      const int msa = np % 2;
+      const int ix_skel = msa_to_idxms(msa, 0, np, np);
+      for (int gama = 1; gama <= nsym; ++gama) {
+        const int gamc = irrep_mult(gama, L.gamt);
+        if (B.gmlen(ix_skel, gama) <= 0) continue;
+        MsGam d;
+        for (bool first = true; next_msgam(first, d, oc, oa, msa, msa, gamc, gama, nsym);
+             first = false) {
+          if (d.msc != tc || d.msa != ta) continue;
+          SpinPrjDesc D{};
+          D.nc = (int32_t)B.c.size();
+          D.na = (int32_t)B.a.size();
+          D.lenc = D.lena = 1;
+          std::vector<int> ixc(B.c.size()), ixa(B.a.size());
+          for (size_t i = 0; i < B.c.size(); ++i) {
+            ixc[i] = ms_index(B.c[i].occ, d.msc[i]);
+            D.lc[i] = (int32_t)model.G(B.c[i].graph).nstr(ixc[i], d.gc[i]);
+            D.lenc *= D.lc[i];
+            D.nmc[i] = (1 << B.c[i].occ) - 1;
+          }
+          for (size_t i = 0; i < B.a.size(); ++i) {
+            ixa[i] = ms_index(B.a[i].occ, d.msa[i]);
+            D.la[i] = (int32_t)model.G(B.a[i].graph).nstr(ixa[i], d.ga[i]);
+            D.lena *= D.la[i];
+            D.nma[i] = (1 << B.a[i].occ) - 1;
+          }
+          if (D.lenc == 0 || D.lena == 0) continue;
+          for (size_t i = 0; i < B.c.size(); ++i)
+            if (B.c[i].occ > 1) D.mapc[i] = spprjmap(B.c[i].graph, ixc[i], d.gc[i]);
+          for (size_t i = 0; i < B.a.size(); ++i)
+            if (B.a[i].occ > 1) D.mapa[i] = spprjmap(B.a[i].graph, ixa[i], d.ga[i]);
+          D.ncase = ncase;
+          D.ncoup = ncoup;
+          D.nomni = (int32_t)omni.size();
+          for (size_t j = 0; j < omni.size(); ++j) D.omni[j] = omni[j];
+          case_base[bucket].push_back((int64_t)cases.size());
+          coef_base[bucket].push_back((int64_t)coef0);
+          for (const Case& k : cs) {
+            SpinPrjCase K{};
+            std::vector<int> kxc(B.c.size()), kxa(B.a.size());
+            std::vector<int64_t> klc(B.c.size()), kla(B.a.size());
+            int kmsa = 0;
+            for (size_t i = 0; i < B.c.size(); ++i) {
+              kxc[i] = ms_index(B.c[i].occ, k.msc[i]);
+              klc[i] = model.G(B.c[i].graph).nstr(kxc[i], d.gc[i]);
+              K.mc[i] = (int16_t)k.mc[i];
+            }
+            for (size_t i = 0; i < B.a.size(); ++i) {
+              kxa[i] = ms_index(B.a[i].occ, k.msa[i]);
+              kla[i] = model.G(B.a[i].graph).nstr(kxa[i], d.ga[i]);
+              K.ma[i] = (int16_t)k.ma[i];
+              kmsa += k.msa[i];
+            }
+            op_ldims(B.c, B.a, klc, kla, false, K.ldc, K.lda);
+            K.off = -1;
+            auto f = B.dis.find({msa_to_idxms(kmsa, 0, np, np), gama});
+            if (f != B.dis.end()) {
+              const int64_t did = dist_id(B.c, kxc, d.gc, B.a, kxa, d.ga, nsym);
+              for (const Dist& x : f->second)
+                if (x.did == did) K.off = x.off;
+            }
+            cases.push_back(K);
+          }
+          descs[bucket].push_back(D);
+        }
+      }
+    }
+    auto sp = std::make_unique<DevSpinPrj>();
+    SpinPrjCase* d_cases = cases.empty() ? nullptr : upload(cases);
+    double* d_coef = coef.empty() ? nullptr : upload(coef);
+    for (int b = 0; b < 4; ++b) {
+      for (size_t j = 0; j < descs[b].size(); ++j) {
+        descs[b][j].cases = d_cases + case_base[b][j];
+        descs[b][j].coeff = d_coef + coef_base[b][j];
+        sp->maxlen[b] = std::max(sp->maxlen[b], descs[b][j].lenc * descs[b][j].lena);
+      }
+      sp->n[b] = (int64_t)descs[b].size();
+      if (sp->n[b]) sp->d[b] = upload(descs[b]);
+    }
+    return *(spinprjs[list_id] = std::move(sp));
+  }
+
   // sym_ab descriptors of one result class (contract/sym_ab_blk.f:170-330)
   void build_flip(DevPlan& dp, DevList& dl, int iblk) {
     ListLayout& L = dl.L;
@@ -2203,6 +2557,39 @@ int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac) {
     launch_sym_ab(d, (int64_t)v.size(), l.d, prefac, maxlen, e.stream);
     ++e.launches;
     CUDA_OK(cudaGetLastError());
+  });
+}
+
+int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_spin_prj_list needs a device");
+    GCCU_REQUIRE(s2 == 0, "spin projection: not a singlet case (s2 = 0 only)");
+    DevList& l = e.wlist(list_id);
+    DevSpinPrj& sp = e.spinprj_for(list_id);
+    for (int b = 0; b < 4; ++b) {
+      if (sp.n[b] == 0) continue;
+      launch_spin_prj(sp.d[b], sp.n[b], kSpinPrjBucket[b], l.d, sp.maxlen[b], e.stream);
+      e.launches += (sp.n[b] + 65534) / 65535;
+    }
+    CUDA_OK(cudaGetLastError());
+    if (!xnorm2_blk) return;
+    GCCU_REQUIRE(!e.capturing, "xnorm2_blk must be NULL inside a graph capture");
+    const int64_t nb = (int64_t)l.L.blk.size();
+    for (int64_t b0 = 0; b0 < nb; b0 += 64) {
+      const int64_t m = std::min<int64_t>(64, nb - b0);
+      CUDA_OK(cudaMemsetAsync(e.d_red, 0, m * sizeof(double), e.stream));
+      for (int64_t i = 0; i < m; ++i) {
+        const LayoutBlock& B = l.L.blk[b0 + i];
+        if (B.len <= 0) continue;
+        launch_sumsq(l.d + B.off, B.len, e.d_red + i, e.stream);
+        ++e.launches;
+      }
+      CUDA_OK(cudaMemcpyAsync(xnorm2_blk + b0, e.d_red, m * sizeof(double),
+                              cudaMemcpyDeviceToHost, e.stream));
+      CUDA_OK(cudaStreamSynchronize(e.stream));
+    }
+    e.check_err();
   });
 }
 

@@ -209,6 +209,41 @@ struct TranspDesc {
 void launch_add_transp(const TranspDesc* d, int64_t n, const double* in, double* out, double fac,
                        int64_t maxlen, cudaStream_t s);
 
+// Singlet spin projection of one occupation class (spin_prj_blk,
+// spinprj.cu).  A class with n creators and n annihilators has
+// C(2n, n) spin cases (spins of every particle with equal Ms on both sides);
+// the elements of one spatial configuration, one per case, are gathered
+// from the skeleton element (the strings whose spins alternate, alpha last)
+// through the per-component pattern maps, projected with C C^T (C: the
+// genealogical singlet coupling coefficients, [case][path]) and written
+// back.  One descriptor per skeleton distribution.
+constexpr int kSpinPrjMaxPart = 4;     // creators (= annihilators) per class
+constexpr int kSpinPrjMaxCases = 70;   // C(8, 4)
+constexpr int kSpinPrjMaxOmni = 4;     // cases with both strings alternating
+constexpr int kSpinPrjMaxCoup = 14;    // singlet coupling paths of eight spins
+struct SpinPrjCase {
+  int64_t off;  // offset of the case's distribution in the list, -1: absent
+  int64_t ldc[kDevMaxComp], lda[kDevMaxComp];
+  int16_t mc[kDevMaxComp], ma[kDevMaxComp];  // pattern number per component, 0 = skeleton's
+};
+struct SpinPrjDesc {
+  int64_t lenc, lena;  // skeleton strings (creator / annihilator side)
+  int32_t nc, na, ncase, ncoup, nomni;
+  int32_t omni[kSpinPrjMaxOmni];
+  int32_t lc[kDevMaxComp], la[kDevMaxComp];
+  int32_t nmc[kDevMaxComp], nma[kDevMaxComp];  // map entries per string (2^occ - 1)
+  // pattern maps of the skeleton strings, [string][pattern-1] = sign *
+  // (address of the string with those spins + 1), 0 = not a skeleton
+  // string or Pauli-forbidden; null for one electron (same address)
+  const int32_t* mapc[kDevMaxComp];
+  const int32_t* mapa[kDevMaxComp];
+  const SpinPrjCase* cases;  // ncase
+  const double* coeff;       // [ncase][ncoup]
+};
+// descriptors d[0..n) whose case count is at most maxcase (2, 6, 20 or 70)
+void launch_spin_prj(const SpinPrjDesc* d, int64_t n, int maxcase, double* x, int64_t maxlen,
+                     cudaStream_t s);
+
 // Learned correction of the diagonal step (learned.cu): a perceptron with
 // kLpInputs inputs, two tanh layers of kLpHidden and one output; weights
 // W1[hidden][inputs], b1, W2[hidden][hidden], b2, W3[hidden], b3 (FP64)

@@ -89,6 +89,7 @@ _SIGS = {
     "gccu_add_block_transp": [ctypes.c_double, I64, I64, I64, I64, I64, I64, I64, I64, PD],
     "gccu_dot_lists": [I64, I64, PD],
     "gccu_sym_ab": [I64, I64, ctypes.c_double, ctypes.c_double],
+    "gccu_spin_prj_list": [I64, I64, PD],
     "gccu_precondition": [I64, I64, I64, ctypes.c_double, ctypes.c_double],
     "gccu_graph_begin": [],
     "gccu_graph_end": [P64],
@@ -476,6 +477,16 @@ class Engine:
 
     def sym_ab(self, lst, iblk, prefac=0.5, relfac=1.0):
         _call("gccu_sym_ab", lst, iblk, prefac, relfac)
+
+    def spin_prj(self, lst, nblk=0, s2=0):
+        """project the list onto its singlet part in place (spin_prj_list);
+        with nblk > 0 return the squared norm of each of its nblk classes"""
+        if nblk:
+            r = np.zeros(nblk)
+            _call("gccu_spin_prj_list", lst, s2, _pd(r))
+            return r
+        _call("gccu_spin_prj_list", lst, s2, PD())
+        return None
 
     def precondition(self, out, inp, diag, fac=1.0, shift=0.0):
         _call("gccu_precondition", out, inp, diag, fac, shift)

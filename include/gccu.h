@@ -243,6 +243,19 @@ int gccu_dot_lists(int64_t list_a, int64_t list_b, double* dot);
  * x <- prefac*(x + relfac*flip(x)) */
 int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac);
 
+/* ---- spin projection -----------------------------------------------------
+ * replaces: spin_prj_list (contract/spin_prj_list.f:2-215) with
+ * spin_prj_blk (contract/spin_prj_blk.f:2-527), the end-of-target step of
+ * frm_sched2 for result lists with a spin (contract/frm_sched2.f:146-149):
+ * every occupation class of the list is projected onto its singlet part in
+ * place.  s2 (= 2S) must be 0 and the list's total Ms 0, as in the
+ * reference; each class needs as many creators as annihilators (at most
+ * four; a scalar class is left as it is).  xnorm2_blk (may be NULL): one
+ * value per occupation class, the squared norm of the projected class
+ * (spin_prj_list's update_norm); must be NULL inside a graph capture.  The
+ * plan is made on the first call for a list (not inside a capture). */
+int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk);
+
 /* ---- preconditioner ------------------------------------------------------
  * replaces: diavc (baserout/diavc.f:31-35) on whole lists:
  * out = fac*in/(diag+shift), |diag+shift| <= 1e-10 -> 1e-10 */

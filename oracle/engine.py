@@ -19,6 +19,7 @@ class OracleEngine:
         self.data = {}
         self.occs = {}
         self.absym = {}
+        self.nblk = {}
         self.stats = np.zeros(8)
 
     def close(self):
@@ -39,6 +40,7 @@ class OracleEngine:
         lid, n = self.o.define_list(op, gamt, mst, absym)
         self.data[lid] = np.zeros(max(n, 1))[:n] if n else np.zeros(0)
         self.absym[lid] = absym
+        self.nblk[lid] = len(self.occs[op])
         return lid, n
 
     def dists(self, lid):
@@ -98,6 +100,10 @@ class OracleEngine:
 
     def sym_ab(self, lid, iblk, prefac=0.5, relfac=1.0):
         self.o.sym_ab(lid, iblk, self.data[lid], prefac, relfac)
+
+    def spin_prj(self, lid, nblk=0, s2=0):
+        xn = self.o.spin_prj(lid, self.data[lid], self.nblk[lid], s2)
+        return xn[:nblk] if nblk else None
 
     def graph_begin(self):
         raise NotImplementedError("no graphs on the CPU oracle")

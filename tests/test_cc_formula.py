@@ -104,3 +104,30 @@ def test_ccsd_synthetic_d2h(built):
     s.load_hamiltonian()
     eo = s.solve(maxiter=40, conv=1e-9)
     assert abs(ed - eo) < 1e-10
+
+
+def test_ccsd_residuals_of_a_closed_shell_are_singlets(hf_ints):
+    # the residual lists of a spin-free Hamiltonian and singlet amplitudes are
+    # singlet operators: projecting them (spin_prj_list, which frm_sched2
+    # applies to result lists with a spin at the end of each target) leaves
+    # the iterates of the reference's HF/cc-pVDZ case unchanged; residuals of
+    # amplitudes with a triplet part do change
+    hist = []
+    for proj in (False, True):
+        s = cc.CCSolver(OracleEngine(route=3), hf_ints, method="ccsd", spin_project=proj)
+        s.load_hamiltonian()
+        s.solve(maxiter=6, conv=1e-14)
+        hist.append(s.history)
+    for (i, ea, ra), (_, eb, rb) in zip(*hist):
+        assert abs(ea - eb) < 1e-12 and abs(ra - rb) < 1e-11 * max(1.0, ra), (i, ea, eb)
+    for a in ("R1", "R2"):
+        r = s.e.data[s.lid(a)].copy()
+        s.e.spin_prj(s.lid(a))
+        assert np.abs(s.e.data[s.lid(a)] - r).max() <= 1e-13 * np.abs(r).max(), a
+    t2 = s.lid("T2")
+    s.e.data[t2] += 1e-3 * np.random.default_rng(5).standard_normal(s.e.data[t2].shape)
+    s.evaluate()
+    r2 = s.e.data[s.lid("R2")].copy()
+    s.project_residuals()
+    moved = np.abs(s.e.data[s.lid("R2")] - r2).max()
+    assert moved > 1e-6 * np.abs(r2).max()

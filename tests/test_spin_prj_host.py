@@ -161,6 +161,21 @@ def test_projection_rank_is_the_singlet_dimension(built, name):
     assert np.abs(Pm.T @ G @ Pm).max() <= 1e-10 * max(1.0, np.abs(G).max())
 
 
+@pytest.mark.parametrize("name", ["p4_h4", "pphh_pphh"])
+def test_four_body_projection_commutes_with_spin_ladders(built, name):
+    # four creators and four annihilators: 70 spin cases, 14 coupling paths
+    space = (1, [[3], [2], [0], [0]])
+    occ = {"p4_h4": occ8({P: 4}, {H: 4}), "pphh_pphh": occ8({P: 2, H: 2}, {P: 2, H: 2})}[name]
+    o, lid, n = _setup(space, occ)
+    fock, ops = _operators(space, occ, o, lid)
+    x = np.random.default_rng(9).standard_normal(n)
+    c0, x0 = _commutator_norm(fock, ops, x)
+    assert c0 > 1e-3 * x0
+    o.spin_prj(lid, x, 1)
+    c1, x1 = _commutator_norm(fock, ops, x)
+    assert x1 > 1e-3 * x0 and c1 <= 1e-12 * x1, (c1, x1)
+
+
 def test_one_body_class_averages_alpha_and_beta(built):
     occ = CLASSES["t1"]
     o, lid, n = _setup(SPACE, occ)
