@@ -1802,8 +1802,14 @@ class Engine {
             auto f = B.dis.find({msa_to_idxms(kmsa, 0, np, np), gama});
             if (f != B.dis.end()) {
               const int64_t did = dist_id(B.c, kxc, d.gc, B.a, kxa, d.ga, nsym);
+              int64_t klen = 1;
+              for (int64_t v : klc) klen *= v;
+              for (int64_t v : kla) klen *= v;
               for (const Dist& x : f->second)
-                if (x.did == did) K.off = x.off;
+                if (x.did == did) {
+                  GCCU_REQUIRE(x.len == klen, "spin projection: distribution length mismatch");
+                  K.off = x.off;
+                }
             }
             cases.push_back(K);
           }
