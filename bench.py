@@ -7,12 +7,15 @@ norm read back, DIIS update of the amplitudes.  Default workload: closed-shell
 CCSD, C1, n_occ=24, n_virt=200, n_aux=900 (the metric's headline size);
 --config 0 selects n_occ=8, n_virt=32, n_aux=160.
 
-The line's `value` is the split-TF32 (mixed) iteration, with `precision`
-giving its errors against FP64 from identical amplitudes and `fp64` the
-plain FP64 iteration measured in the same run; `use_tr` times both with the
-spin-flip symmetry the reference uses by default; `convergence` gives the
-time to |dE| < 1 uEh of FP64 and mixed at o24/v200 on a variant of the
-Hamiltonian whose CC iteration converges.
+The line's `value` is the iteration with FP64 emulated by four int8 slices
+on the tensor cores (precision mode 3, the bulk mode of the mixed solve),
+with `precision` giving its errors against FP64 from identical amplitudes,
+`fp64` the plain FP64 iteration and `i8` / `tf32` the other tensor-core
+modes measured in the same run; `use_tr` times the iteration with the
+spin-flip symmetry the reference uses by default; `spin_prj` times the
+singlet projection of the doubles residual against the HBM roofline;
+`convergence` gives the time to |dE| < 1 uEh of FP64 and the mixed solves at
+o24/v200 on a variant of the Hamiltonian whose CC iteration converges.
 
 --impl reference times the CPU restatement of the reference path (oracle/,
 route 3: gather, ILP64 OpenBLAS dgemm on all host cores, scatter) on the same
@@ -248,7 +251,7 @@ def run_gpu(args, cfg):
         print(json.dumps({"convergence": convergence(local, cfgc, maxiter=args.conv_maxiter,
                                                      variants=variants)}), flush=True)
         return
-    tracing = args.trace_contraction or args.trace_learned
+    tracing = args.trace_contraction or args.trace_learned or args.trace_spin_prj
     peak = fp64_peak() if rank == 0 and not tracing else None
     sp, eps, B = setup_hamiltonian(cfg)
     eng = gccu.Engine(local)
@@ -277,6 +280,15 @@ def run_gpu(args, cfg):
         eng.close()
         print(json.dumps({"trace": "learned step", "workload": cfg["name"], "elements": n,
                           "ms": ms, "GB_per_s": 32.0 * n / (ms * 1e-3) / 1e9}), flush=True)
+        return
+    if args.trace_spin_prj:
+        # the singlet projection of the doubles residual (the command the
+        # profilers capture)
+        singlet_residuals(eng, solver)
+        out = measure_spin_prj(eng, solver, reps=3)
+        eng.close()
+        print(json.dumps({"trace": "spin projection", "workload": cfg["name"], **out}),
+              flush=True)
         return
     if args.trace_contraction:
         # one formula item, run once eagerly (the command profilers capture)
@@ -345,6 +357,10 @@ def run_gpu(args, cfg):
             note=f"evaluation with {METRIC_MODE[modes[0]]} minus FP64 evaluation; "
                  "R*_max_rel relative to max|R|")
 
+    if world == 1 and not args.no_spin_prj:
+        singlet_residuals(eng, solver)
+        line["spin_prj"] = measure_spin_prj(eng, solver)
+
     if args.tune:
         rows = eng.tuning_report()
         line["tuning"] = {
@@ -403,6 +419,58 @@ DTYPE = {0: "f64", 1: "tf32x3 products, f32 accumulate per 4096-chunk, f64 sums"
          2: "s8 slices x5 (15 products), s32 exact accumulate, f64 combine",
          3: "s8 slices x4 (10 products), s32 exact accumulate, f64 combine"}
 SLICE_PRODUCTS = {2: 15, 3: 10}
+
+
+def measure_spin_prj(eng, solver, reps=10):
+    """singlet projection (gccu_spin_prj_list, one k_spin_prj launch) of the
+    doubles residual list of the benchmark: ms per projection (median of
+    reps, L2 flushed before each), achieved HBM bandwidth for its algorithmic
+    bytes (16 per element: one read, one write), and two size-independent
+    checks -- the closed-shell residual is a singlet (the projection leaves it
+    unchanged) and the projection of a random list is idempotent"""
+    import torch
+    lid, n, _ = solver.lists["R2"]
+    r0 = eng.download(lid, n)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    eng.spin_prj(lid)  # plans the list
+    moved = float(np.abs(eng.download(lid, n) - r0).max() / max(np.abs(r0).max(), 1e-300))
+    times = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        eng.sync()
+        eng.event_record(0)
+        eng.spin_prj(lid)
+        eng.event_record(1)
+        times.append(eng.event_elapsed(0, 1))
+    x = np.random.default_rng(12).standard_normal(n)
+    eng.upload(lid, x)
+    eng.spin_prj(lid)
+    y = eng.download(lid, n)
+    eng.spin_prj(lid)
+    z = eng.download(lid, n)
+    eng.upload(lid, r0)
+    del flush
+    ms = float(np.median(times))
+    peak, src = measured_bf16_tflops("hbm_gbs")
+    gbs = 16.0 * n / (ms * 1e-3) / 1e9
+    return {"list": "R2 (PP;HH), FP64", "elements": n, "ms": ms,
+            "algorithmic_bytes": 16 * n, "achieved_GBps": gbs, "peak_GBps": peak,
+            "peak_source": src + " HBM copy", "frac": gbs / peak,
+            "singlet_residual_change_rel": moved,
+            "random_list_change_rel": float(np.abs(y - x).max() / np.abs(x).max()),
+            "idempotence_rel": float(np.abs(z - y).max() / np.abs(y).max())}
+
+
+def singlet_residuals(eng, solver):
+    """residuals of singlet amplitudes: two FP64 Jacobi steps from T = 0 and
+    one more evaluation"""
+    reset_amplitudes(eng, solver)
+    eng.set_precision(0)
+    for _ in range(2):
+        solver.iterate()
+        solver.step()
+    solver.iterate()
 
 
 def reset_amplitudes(eng, solver):
@@ -1092,6 +1160,11 @@ def main():
     ap.add_argument("--trace-learned", action="store_true",
                     help="set up, run the learned preconditioner step once on the doubles "
                          "lists and exit (the command the ncu captures in profiles/ run)")
+    ap.add_argument("--trace-spin-prj", action="store_true",
+                    help="set up, project the singlet residual of the doubles onto its "
+                         "singlet part and exit (the command the ncu captures in profiles/ run)")
+    ap.add_argument("--no-spin-prj", action="store_true",
+                    help="skip the timing of the singlet spin projection")
     ap.add_argument("--profile-out", default=None,
                     help="write per-contraction kernel times (JSON)")
     ap.add_argument("--validate-sampling", action="store_true",
