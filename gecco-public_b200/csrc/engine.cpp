@@ -167,9 +167,15 @@ struct DevReo {
 // use: per case-count bucket (2, 6, 20, 70 cases) the skeleton descriptors
 struct DevSpinPrj {
   SpinPrjDesc* d[4] = {};
-  int64_t n[4] = {}, maxlen[4] = {};
+  int64_t n[4] = {}, maxblocks[4] = {};
 };
 constexpr int kSpinPrjBucket[4] = {2, 6, 20, kSpinPrjMaxCases};
+// pattern map of one string block (set_spprjmap_kernel): per string
+// [pattern-1] entries, and whether the string is a skeleton string
+struct PatternMap {
+  std::vector<int32_t> m;
+  std::vector<char> skel;
+};
 
 // spin patterns of n electrons (set_spprjmap_cases,
 // strings/set_spprjmap_cases.f:24-41): bit n-1-i set for a beta spin at
@@ -299,7 +305,7 @@ class Engine {
   std::map<int, DevGraph> dgraphs;
   std::map<MapKey, int32_t*> maps;
   std::map<std::array<int, 3>, int32_t*> flips;
-  std::map<std::array<int, 3>, int32_t*> spprjs;  // spin-projection pattern maps
+  std::map<std::array<int, 3>, PatternMap> spprjs;  // spin-projection pattern maps (host)
   std::map<int64_t, std::unique_ptr<DevSpinPrj>> spinprjs;  // singlet projection per list
   std::map<std::string, std::unique_ptr<DevPlan>> plans;
   std::vector<void*> allocs;
@@ -1597,13 +1603,13 @@ class Engine {
   }
 
   // pattern map of one string block for the spin projection
-  // (set_spprjmap_kernel, strings/set_spprjmap_kernel.f:60-130): for every
-  // string whose spins alternate from the right end (alpha last; the two
-  // members of a paired orbital pass) and every pattern k = 1..2^n-1,
-  // sign * (address of the string with the same orbitals and the spins of
-  // pattern k, + 1), sign = std_spsign(string) * std_spsign(result); 0 for
-  // the other strings and where a paired orbital would get two equal spins
-  int32_t* spprjmap(int gid, int idxms, int gam) {
+  // (set_spprjmap_kernel, strings/set_spprjmap_kernel.f:60-130): a string is
+  // a skeleton string if its spins alternate from the right end (alpha
+  // last; the two members of a paired orbital pass); for those and every
+  // pattern k = 1..2^n-1, sign * (address of the string with the same
+  // orbitals and the spins of pattern k, + 1), sign = std_spsign(string) *
+  // std_spsign(result); 0 where a paired orbital would get two equal spins
+  const PatternMap& spprjmap(int gid, int idxms, int gam) {
     std::array<int, 3> key{gid, idxms, gam};
     auto it = spprjs.find(key);
     if (it != spprjs.end()) return it->second;
@@ -1619,7 +1625,9 @@ class Engine {
       const int c = spin_pattern_number(nel, bits);
       for (int i = 0; i < nel; ++i) pat[c][i] = ((bits >> (nel - 1 - i)) & 1) ? -1 : 1;
     }
-    std::vector<int32_t> m(std::max<int64_t>(n * nmaps, 1), 0);
+    PatternMap pm;
+    pm.m.assign(n * nmaps, 0);
+    pm.skel.assign(n, 0);
     std::vector<int> orb(nel), spn(nel), sf(nel);
     for (int64_t s = 0; s < n; ++s) {
       for (int p = 0; p < nel; ++p) {
@@ -1630,6 +1638,7 @@ class Engine {
       bool ref = true;
       for (int i = nel - 1, sg = 1; i >= 0; --i, sg = -sg) ref = ref && (spn[i] == sg || spn[i] == 2);
       if (!ref) continue;
+      pm.skel[s] = 1;
       for (int c = 1; c <= nmaps; ++c) {
         sf = pat[c];
         bool ok = true;
@@ -1640,11 +1649,57 @@ class Engine {
           else sf[i] = sf[i + 1] = 2;
         }
         if (!ok) continue;
-        m[s * nmaps + c - 1] = spin_sign(spn.data(), nel) * spin_sign(sf.data(), nel) *
-                               (int32_t)(g.address(orb.data(), sf.data()) + 1);
+        pm.m[s * nmaps + c - 1] = spin_sign(spn.data(), nel) * spin_sign(sf.data(), nel) *
+                                  (int32_t)(g.address(orb.data(), sf.data()) + 1);
       }
     }
-    return spprjs[key] = upload(m);
+    return spprjs[key] = std::move(pm);
+  }
+
+  // partial element offsets of one side of a skeleton distribution: the
+  // tuples of component strings (first component fastest) whose strings of
+  // two or more electrons are skeleton strings, and per spin case k the sum
+  // over the components of (the string of pattern pat[k][i]) * ld[k][i],
+  // -1 where a pattern map entry is 0; out is [case][tuple]
+  int64_t side_offsets(const std::vector<Comp>& comps, const std::vector<int>& ix,
+                       const std::vector<int>& gm, const std::vector<std::vector<int>>& pat,
+                       const std::vector<std::vector<int64_t>>& ld, std::vector<int64_t>& out) {
+    const size_t nc = comps.size(), ncase = pat.size();
+    std::vector<int64_t> len(nc);
+    std::vector<const PatternMap*> pm(nc, nullptr);
+    int64_t total = 1;
+    for (size_t i = 0; i < nc; ++i) {
+      len[i] = model.G(comps[i].graph).nstr(ix[i], gm[i]);
+      total *= len[i];
+      if (comps[i].occ > 1) pm[i] = &spprjmap(comps[i].graph, ix[i], gm[i]);
+    }
+    std::vector<std::vector<int64_t>> cols(ncase);
+    std::vector<int64_t> s(nc, 0);
+    for (int64_t t = 0; t < total; ++t) {
+      bool skel = true;
+      for (size_t i = 0; i < nc; ++i) skel = skel && (!pm[i] || pm[i]->skel[s[i]]);
+      if (skel) {
+        for (size_t k = 0; k < ncase; ++k) {
+          int64_t p = 0;
+          for (size_t i = 0; i < nc && p >= 0; ++i) {
+            int64_t si = s[i];
+            const int m = pat[k][i];
+            if (m != 0 && pm[i]) {
+              const int nm = (1 << comps[i].occ) - 1;
+              const int v = pm[i]->m[si * nm + m - 1];
+              if (v == 0) p = -1;
+              si = std::abs(v) - 1;
+            }
+            if (p >= 0) p += si * ld[k][i];
+          }
+          cols[k].push_back(p);
+        }
+      }
+      for (size_t i = 0; i < nc && ++s[i] == len[i]; ++i) s[i] = 0;
+    }
+    const int64_t nt = ncase ? (int64_t)cols[0].size() : 0;
+    for (auto& c : cols) out.insert(out.end(), c.begin(), c.end());
+    return nt;
   }
 
   // singlet projection plan of a list (spin_prj_list, contract/spin_prj_list.f:
@@ -1658,8 +1713,8 @@ class Engine {
     GCCU_REQUIRE(L.mst == 0, "spin projection: ms.ne.0 not yet considered (lists of Ms 0 only)");
     const int nsym = model.os.nsym;
     std::vector<SpinPrjDesc> descs[4];
-    std::vector<int64_t> case_base[4], coef_base[4];
-    std::vector<SpinPrjCase> cases;
+    std::vector<int64_t> tab_t[4], tab_l[4], coef_at[4];
+    std::vector<int64_t> tables;
     std::vector<double> coef;
     for (const LayoutBlock& B : L.blk) {
       if (B.len <= 0) continue;
@@ -1689,12 +1744,8 @@ class Engine {
       };
       // the spin cases: annihilator spins outer, creator spins inner, each
       // from all alpha with the first particle changing fastest; Ms equal on
-      // both sides
-      struct Case {
-        std::vector<int> msc, msa, mc, ma;
-      };
-      std::vector<Case> cs;
-      std::vector<int> omni;
+      // both sides (set_spinprj_info.f set_case)
+      std::vector<std::vector<int>> msc, msa, patc, pata;
       const size_t coef0 = coef.size();
       std::vector<int> sa(np, 1), sc(np, 1);
       auto next = [np](std::vector<int>& s) {
@@ -1710,121 +1761,136 @@ class Engine {
       for (bool ma = true; ma; ma = next(sa)) {
         std::fill(sc.begin(), sc.end(), 1);
         for (bool mc = true; mc; mc = next(sc)) {
-          int msc = 0, msa = 0;
-          for (int i = 0; i < np; ++i) msc += sc[i], msa += sa[i];
-          if (msc != msa) continue;
-          Case k;
+          int tsc = 0, tsa = 0;
+          for (int i = 0; i < np; ++i) tsc += sc[i], tsa += sa[i];
+          if (tsc != tsa) continue;
+          std::vector<int> m1, m2, p1, p2;
           for (size_t i = 0, o = 0; i < oc.size(); o += oc[i], ++i) {
             int m = 0;
             for (int e = 0; e < oc[i]; ++e) m += sc[o + e];
-            k.msc.push_back(m);
-            k.mc.push_back(pattern(sc.data() + o, rc.data() + o, oc[i]));
+            m1.push_back(m);
+            p1.push_back(pattern(sc.data() + o, rc.data() + o, oc[i]));
           }
           for (size_t i = 0, o = 0; i < oa.size(); o += oa[i], ++i) {
             int m = 0;
             for (int e = 0; e < oa[i]; ++e) m += sa[o + e];
-            k.msa.push_back(m);
-            k.ma.push_back(pattern(sa.data() + o, ra.data() + o, oa[i]));
+            m2.push_back(m);
+            p2.push_back(pattern(sa.data() + o, ra.data() + o, oa[i]));
           }
-          bool alt = np > 1;
-          for (int i = 0; i + 1 < np; ++i)
-            alt = alt && sc[i] * sc[i + 1] == -1 && sa[i] * sa[i + 1] == -1;
-          if (alt) omni.push_back((int)cs.size());
+          msc.push_back(m1);
+          msa.push_back(m2);
+          patc.push_back(p1);
+          pata.push_back(p2);
           const std::vector<double> cf = singlet_coupling(sc, sa);
           coef.insert(coef.end(), cf.begin(), cf.end());
-          cs.push_back(std::move(k));
         }
       }
-      const int ncase = (int)cs.size();
+      const int ncase = (int)msc.size();
       const int ncoup = (int)((coef.size() - coef0) / ncase);
-      GCCU_REQUIRE(ncase <= kSpinPrjMaxCases && ncoup <= kSpinPrjMaxCoup &&
-                       omni.size() <= (size_t)kSpinPrjMaxOmni,
-                   "spin projection: case tables exceed their bounds");
       int bucket = 0;
       while (kSpinPrjBucket[bucket] < ncase) ++bucket;
+      GCCU_REQUIRE(kSpinPrjBucket[bucket] == ncase && ncoup == spin_prj_paths(ncase),
+                   "spin projection: unexpected number of spin cases");
+      // the side whose first component has leading dimension 1 (the first
+      // hpvx type of X,P,V,H with a component; creators before annihilators)
+      bool thread_c = false;
+      for (int ih = 0; ih < 4; ++ih) {
+        const int t = kHpvxSeq[ih];
+        bool hc = false, ha = false;
+        for (auto& c : B.c) hc = hc || c.hpvx == t;
+        for (auto& a : B.a) ha = ha || a.hpvx == t;
+        if (hc || ha) {
+          thread_c = hc;
+          break;
+        }
+      }
       // skeleton distributions: Ms(A) = Ms(C) = np mod 2 and the skeleton Ms
       // per component, every IRREP distribution
-      const int msa = np % 2;
-      const int ix_skel = msa_to_idxms(msa, 0, np, np);
+      const int msk = np % 2;
+      const int ix_skel = msa_to_idxms(msk, 0, np, np);
       for (int gama = 1; gama <= nsym; ++gama) {
         const int gamc = irrep_mult(gama, L.gamt);
         if (B.gmlen(ix_skel, gama) <= 0) continue;
         MsGam d;
-        for (bool first = true; next_msgam(first, d, oc, oa, msa, msa, gamc, gama, nsym);
+        for (bool first = true; next_msgam(first, d, oc, oa, msk, msk, gamc, gama, nsym);
              first = false) {
           if (d.msc != tc || d.msa != ta) continue;
-          SpinPrjDesc D{};
-          D.nc = (int32_t)B.c.size();
-          D.na = (int32_t)B.a.size();
-          D.lenc = D.lena = 1;
           std::vector<int> ixc(B.c.size()), ixa(B.a.size());
+          int64_t lenc = 1, lena = 1;
           for (size_t i = 0; i < B.c.size(); ++i) {
             ixc[i] = ms_index(B.c[i].occ, d.msc[i]);
-            D.lc[i] = (int32_t)model.G(B.c[i].graph).nstr(ixc[i], d.gc[i]);
-            D.lenc *= D.lc[i];
-            D.nmc[i] = (1 << B.c[i].occ) - 1;
+            lenc *= model.G(B.c[i].graph).nstr(ixc[i], d.gc[i]);
           }
           for (size_t i = 0; i < B.a.size(); ++i) {
             ixa[i] = ms_index(B.a[i].occ, d.msa[i]);
-            D.la[i] = (int32_t)model.G(B.a[i].graph).nstr(ixa[i], d.ga[i]);
-            D.lena *= D.la[i];
-            D.nma[i] = (1 << B.a[i].occ) - 1;
+            lena *= model.G(B.a[i].graph).nstr(ixa[i], d.ga[i]);
           }
-          if (D.lenc == 0 || D.lena == 0) continue;
-          for (size_t i = 0; i < B.c.size(); ++i)
-            if (B.c[i].occ > 1) D.mapc[i] = spprjmap(B.c[i].graph, ixc[i], d.gc[i]);
-          for (size_t i = 0; i < B.a.size(); ++i)
-            if (B.a[i].occ > 1) D.mapa[i] = spprjmap(B.a[i].graph, ixa[i], d.ga[i]);
-          D.ncase = ncase;
-          D.ncoup = ncoup;
-          D.nomni = (int32_t)omni.size();
-          for (size_t j = 0; j < omni.size(); ++j) D.omni[j] = omni[j];
-          case_base[bucket].push_back((int64_t)cases.size());
-          coef_base[bucket].push_back((int64_t)coef0);
-          for (const Case& k : cs) {
-            SpinPrjCase K{};
+          if (lenc == 0 || lena == 0) continue;
+          // per case: distribution offset and leading dimensions
+          std::vector<int64_t> off(ncase, -1);
+          std::vector<std::vector<int64_t>> ldc(ncase), lda(ncase);
+          for (int k = 0; k < ncase; ++k) {
             std::vector<int> kxc(B.c.size()), kxa(B.a.size());
             std::vector<int64_t> klc(B.c.size()), kla(B.a.size());
             int kmsa = 0;
+            int64_t klen = 1;
             for (size_t i = 0; i < B.c.size(); ++i) {
-              kxc[i] = ms_index(B.c[i].occ, k.msc[i]);
+              kxc[i] = ms_index(B.c[i].occ, msc[k][i]);
               klc[i] = model.G(B.c[i].graph).nstr(kxc[i], d.gc[i]);
-              K.mc[i] = (int16_t)k.mc[i];
+              klen *= klc[i];
             }
             for (size_t i = 0; i < B.a.size(); ++i) {
-              kxa[i] = ms_index(B.a[i].occ, k.msa[i]);
+              kxa[i] = ms_index(B.a[i].occ, msa[k][i]);
               kla[i] = model.G(B.a[i].graph).nstr(kxa[i], d.ga[i]);
-              K.ma[i] = (int16_t)k.ma[i];
-              kmsa += k.msa[i];
+              klen *= kla[i];
+              kmsa += msa[k][i];
             }
-            op_ldims(B.c, B.a, klc, kla, false, K.ldc, K.lda);
-            K.off = -1;
+            ldc[k].assign(B.c.size(), 0);
+            lda[k].assign(B.a.size(), 0);
+            op_ldims(B.c, B.a, klc, kla, false, ldc[k].data(), lda[k].data());
             auto f = B.dis.find({msa_to_idxms(kmsa, 0, np, np), gama});
-            if (f != B.dis.end()) {
-              const int64_t did = dist_id(B.c, kxc, d.gc, B.a, kxa, d.ga, nsym);
-              int64_t klen = 1;
-              for (int64_t v : klc) klen *= v;
-              for (int64_t v : kla) klen *= v;
-              for (const Dist& x : f->second)
-                if (x.did == did) {
-                  GCCU_REQUIRE(x.len == klen, "spin projection: distribution length mismatch");
-                  K.off = x.off;
-                }
-            }
-            cases.push_back(K);
+            if (f == B.dis.end()) continue;
+            const int64_t did = dist_id(B.c, kxc, d.gc, B.a, kxa, d.ga, nsym);
+            for (const Dist& x : f->second)
+              if (x.did == did) {
+                GCCU_REQUIRE(x.len == klen, "spin projection: distribution length mismatch");
+                off[k] = x.off;
+              }
           }
+          std::vector<int64_t> tcv, tav;
+          const int64_t nrc = side_offsets(B.c, ixc, d.gc, patc, ldc, tcv);
+          const int64_t nra = side_offsets(B.a, ixa, d.ga, pata, lda, tav);
+          if (nrc == 0 || nra == 0) continue;
+          // the case's distribution offset goes into the loop side
+          std::vector<int64_t>& lv = thread_c ? tav : tcv;
+          const int64_t nl = thread_c ? nra : nrc;
+          for (int k = 0; k < ncase; ++k)
+            for (int64_t j = 0; j < nl; ++j) {
+              int64_t& v = lv[k * nl + j];
+              v = (v < 0 || off[k] < 0) ? -1 : v + off[k];
+            }
+          SpinPrjDesc D{};
+          D.nt = thread_c ? nrc : nra;
+          D.nl = nl;
+          tab_t[bucket].push_back((int64_t)tables.size());
+          tables.insert(tables.end(), (thread_c ? tcv : tav).begin(), (thread_c ? tcv : tav).end());
+          tab_l[bucket].push_back((int64_t)tables.size());
+          tables.insert(tables.end(), lv.begin(), lv.end());
+          coef_at[bucket].push_back((int64_t)coef0);
           descs[bucket].push_back(D);
         }
       }
     }
     auto sp = std::make_unique<DevSpinPrj>();
-    SpinPrjCase* d_cases = cases.empty() ? nullptr : upload(cases);
+    int64_t* d_tab = tables.empty() ? nullptr : upload(tables);
     double* d_coef = coef.empty() ? nullptr : upload(coef);
     for (int b = 0; b < 4; ++b) {
       for (size_t j = 0; j < descs[b].size(); ++j) {
-        descs[b][j].cases = d_cases + case_base[b][j];
-        descs[b][j].coeff = d_coef + coef_base[b][j];
-        sp->maxlen[b] = std::max(sp->maxlen[b], descs[b][j].lenc * descs[b][j].lena);
+        SpinPrjDesc& D = descs[b][j];
+        D.pt = d_tab + tab_t[b][j];
+        D.pl = d_tab + tab_l[b][j];
+        D.coeff = d_coef + coef_at[b][j];
+        sp->maxblocks[b] = std::max(sp->maxblocks[b], spin_prj_blocks(D.nt, D.nl));
       }
       sp->n[b] = (int64_t)descs[b].size();
       if (sp->n[b]) sp->d[b] = upload(descs[b]);
@@ -2575,7 +2641,7 @@ int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk) {
     DevSpinPrj& sp = e.spinprj_for(list_id);
     for (int b = 0; b < 4; ++b) {
       if (sp.n[b] == 0) continue;
-      launch_spin_prj(sp.d[b], sp.n[b], kSpinPrjBucket[b], l.d, sp.maxlen[b], e.stream);
+      launch_spin_prj(sp.d[b], sp.n[b], kSpinPrjBucket[b], l.d, sp.maxblocks[b], e.stream);
       e.launches += (sp.n[b] + 65534) / 65535;
     }
     CUDA_OK(cudaGetLastError());

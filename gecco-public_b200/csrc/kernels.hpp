@@ -210,38 +210,38 @@ void launch_add_transp(const TranspDesc* d, int64_t n, const double* in, double*
                        int64_t maxlen, cudaStream_t s);
 
 // Singlet spin projection of one occupation class (spin_prj_blk,
-// spinprj.cu).  A class with n creators and n annihilators has
-// C(2n, n) spin cases (spins of every particle with equal Ms on both sides);
-// the elements of one spatial configuration, one per case, are gathered
-// from the skeleton element (the strings whose spins alternate, alpha last)
-// through the per-component pattern maps, projected with C C^T (C: the
-// genealogical singlet coupling coefficients, [case][path]) and written
-// back.  One descriptor per skeleton distribution.
+// spinprj.cu).  A class with n creators and n annihilators has C(2n, n)
+// spin cases (spins of every particle, equal Ms on both sides); the
+// elements of one spatial configuration, one per case, are projected with
+// C C^T (C: the genealogical singlet coupling coefficients, [case][path])
+// and written back.  One descriptor per skeleton distribution: the
+// skeleton's string tuples of each side whose strings are all of the
+// reference spin pattern (alternating, alpha last), and for every case the
+// partial element offset of each tuple on that side (-1: the case does not
+// exist for it; the case's distribution offset is in the loop side's
+// values), so that an element's address is the sum of the two sides'.
+// Threads run over the side whose strings are contiguous in the list.
 constexpr int kSpinPrjMaxPart = 4;     // creators (= annihilators) per class
 constexpr int kSpinPrjMaxCases = 70;   // C(8, 4)
-constexpr int kSpinPrjMaxOmni = 4;     // cases with both strings alternating
 constexpr int kSpinPrjMaxCoup = 14;    // singlet coupling paths of eight spins
-struct SpinPrjCase {
-  int64_t off;  // offset of the case's distribution in the list, -1: absent
-  int64_t ldc[kDevMaxComp], lda[kDevMaxComp];
-  int16_t mc[kDevMaxComp], ma[kDevMaxComp];  // pattern number per component, 0 = skeleton's
-};
+// coupling paths of the singlet of 2n spins for C(2n, n) cases
+constexpr int spin_prj_paths(int ncase) {
+  return ncase == 2 ? 1 : ncase == 6 ? 2 : ncase == 20 ? 5 : 14;
+}
 struct SpinPrjDesc {
-  int64_t lenc, lena;  // skeleton strings (creator / annihilator side)
-  int32_t nc, na, ncase, ncoup, nomni;
-  int32_t omni[kSpinPrjMaxOmni];
-  int32_t lc[kDevMaxComp], la[kDevMaxComp];
-  int32_t nmc[kDevMaxComp], nma[kDevMaxComp];  // map entries per string (2^occ - 1)
-  // pattern maps of the skeleton strings, [string][pattern-1] = sign *
-  // (address of the string with those spins + 1), 0 = not a skeleton
-  // string or Pauli-forbidden; null for one electron (same address)
-  const int32_t* mapc[kDevMaxComp];
-  const int32_t* mapa[kDevMaxComp];
-  const SpinPrjCase* cases;  // ncase
-  const double* coeff;       // [ncase][ncoup]
+  int64_t nt, nl;           // tuples of the thread side and of the loop side
+  const int64_t* pt;        // [case][nt] partial offsets of the thread side
+  const int64_t* pl;        // [case][nl] of the loop side (distribution offset included)
+  const double* coeff;      // [case][path]
 };
-// descriptors d[0..n) whose case count is at most maxcase (2, 6, 20 or 70)
-void launch_spin_prj(const SpinPrjDesc* d, int64_t n, int maxcase, double* x, int64_t maxlen,
+// thread-side tuples per block and loop-side tuples per thread
+constexpr int kSpinPrjThreads = 128, kSpinPrjLoop = 16;
+constexpr int64_t spin_prj_blocks(int64_t nt, int64_t nl) {
+  return (nt + kSpinPrjThreads - 1) / kSpinPrjThreads * ((nl + kSpinPrjLoop - 1) / kSpinPrjLoop);
+}
+// descriptors d[0..n), every one with ncase cases (2, 6, 20 or 70);
+// maxblocks: the largest spin_prj_blocks among them
+void launch_spin_prj(const SpinPrjDesc* d, int64_t n, int ncase, double* x, int64_t maxblocks,
                      cudaStream_t s);
 
 // Learned correction of the diagonal step (learned.cu): a perceptron with

@@ -1,22 +1,22 @@
 // Singlet spin projection of ME lists (spin_prj_blk,
 // contract/spin_prj_blk.f:254-400).
 //
-// k_spin_prj  one thread per skeleton element of one skeleton distribution
-//             (grid.y): the element of every spin case of the element's
-//             spatial configuration is found through the pattern maps of
-//             the skeleton's component strings (spprjmap,
-//             strings/set_spprjmap_kernel.f:60-130) and the case's
-//             distribution offset and leading dimensions; the values (with
-//             the sign -1 for every second appearance of an element whose
-//             paired orbitals make two cases coincide) are projected with
-//             C C^T and written back in case order.  A skeleton element whose
-//             alternating cases do not all exist (a skeleton string that is
-//             not of the reference spin pattern) is skipped: its
-//             configuration is handled by the element that is.  Every element
-//             of the class belongs to exactly one configuration, so the
-//             threads write disjoint elements and the projection runs in
-//             place.  HBM-bound: each element is read and written once, the
-//             maps and case tables stay in L1/L2.
+// k_spin_prj<MC>  one thread per (thread-side tuple, loop-side tuple) pair
+//                 of one skeleton distribution (grid.y), kSpinPrjLoop
+//                 loop-side tuples per thread: the elements of the MC spin
+//                 cases of the pair's spatial configuration are at the sums
+//                 of the two sides' partial offsets (planned on the host with
+//                 the reference's pattern maps, strings/set_spprjmap_kernel.f
+//                 :60-130); their values, with the sign -1 for every second
+//                 appearance of an element that two cases share (paired
+//                 orbitals), are projected with C C^T (C: the singlet
+//                 coupling coefficients, staged in shared memory) and written
+//                 back in case order.  Only skeleton strings of the reference
+//                 spin pattern are listed, so every spatial configuration of
+//                 the class is handled by exactly one thread: the threads
+//                 write disjoint elements and the projection runs in place.
+//                 HBM-bound: each element read and written once; the offset
+//                 tables are O(square root) of the class and stay in L2.
 #include <algorithm>
 
 #include "kernels.hpp"
@@ -24,93 +24,69 @@
 namespace gccu {
 namespace {
 
-constexpr int kSpinPrjThreads = 128;
-
-// address of case k's element for the skeleton strings sc / sa, -1 if the
-// case does not exist for them
-__device__ __forceinline__ int64_t case_element(const SpinPrjDesc& d, const SpinPrjCase& K,
-                                                const int32_t* sc, const int32_t* sa) {
-  if (K.off < 0) return -1;
-  int64_t p = K.off;
-  for (int i = 0; i < d.nc; ++i) {
-    int64_t s = sc[i];
-    const int m = K.mc[i];
-    if (m != 0) {
-      const int v = d.mapc[i] ? __ldg(d.mapc[i] + s * d.nmc[i] + m - 1) : (int)s + 1;
-      if (v == 0) return -1;
-      s = (v < 0 ? -v : v) - 1;
-    }
-    p += s * K.ldc[i];
-  }
-  for (int i = 0; i < d.na; ++i) {
-    int64_t s = sa[i];
-    const int m = K.ma[i];
-    if (m != 0) {
-      const int v = d.mapa[i] ? __ldg(d.mapa[i] + s * d.nma[i] + m - 1) : (int)s + 1;
-      if (v == 0) return -1;
-      s = (v < 0 ? -v : v) - 1;
-    }
-    p += s * K.lda[i];
-  }
-  return p;
-}
-
 template <int MC>
 __global__ void __launch_bounds__(kSpinPrjThreads)
     k_spin_prj(const SpinPrjDesc* __restrict__ ds, double* __restrict__ x) {
-  const SpinPrjDesc& d = ds[blockIdx.y];
-  const int64_t n = d.lenc * d.lena;
-  const int ncase = d.ncase, ncoup = d.ncoup;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    int32_t sc[kDevMaxComp], sa[kDevMaxComp];
-    int64_t ia = e / d.lenc, ic = e - ia * d.lenc;
-    for (int i = 0; i < d.nc; ++i) {
-      sc[i] = (int32_t)(ic % d.lc[i]);
-      ic /= d.lc[i];
-    }
-    for (int i = 0; i < d.na; ++i) {
-      sa[i] = (int32_t)(ia % d.la[i]);
-      ia /= d.la[i];
-    }
-    // skeleton strings of a non-reference pattern: nothing to do here
-    bool skip = false;
-    for (int j = 0; j < d.nomni && !skip; ++j)
-      skip = case_element(d, d.cases[d.omni[j]], sc, sa) < 0;
-    if (skip) continue;
-    int64_t idx[MC];
-    double val[MC];
-    for (int k = 0; k < ncase; ++k) {
-      idx[k] = case_element(d, d.cases[k], sc, sa);
-      val[k] = 0.0;
-      if (idx[k] < 0) continue;
-      int cnt = 0;
-      for (int j = 0; j <= k; ++j) cnt += idx[j] == idx[k];
-      const double ps = (__popc(cnt - 1) & 1) ? -1.0 : 1.0;
-      val[k] = x[idx[k]] * ps;
-    }
-    // C^T v, then C (C^T v): summed in case order, then in path order
-    double ov[MC == 2 ? 1 : MC == 6 ? 2 : MC == 20 ? 5 : kSpinPrjMaxCoup];
-    for (int q = 0; q < ncoup; ++q) {
-      double s = 0.0;
-      for (int k = 0; k < ncase; ++k) s += __ldg(d.coeff + k * ncoup + q) * val[k];
-      ov[q] = s;
-    }
-    for (int k = 0; k < ncase; ++k) {
-      if (idx[k] < 0) continue;
-      double s = 0.0;
-      for (int q = 0; q < ncoup; ++q) s += __ldg(d.coeff + k * ncoup + q) * ov[q];
-      int cnt = 0;
-      for (int j = 0; j <= k; ++j) cnt += idx[j] == idx[k];
-      x[idx[k]] = (__popc(cnt - 1) & 1) ? -s : s;
+  constexpr int NP = spin_prj_paths(MC);
+  constexpr int UNR = MC <= 20 ? MC : 1;
+  __shared__ double cs[MC * NP];
+  const SpinPrjDesc d = ds[blockIdx.y];
+  for (int i = threadIdx.x; i < MC * NP; i += blockDim.x) cs[i] = d.coeff[i];
+  __syncthreads();
+  const int64_t tchunks = (d.nt + kSpinPrjThreads - 1) / kSpinPrjThreads;
+  const int64_t nb = spin_prj_blocks(d.nt, d.nl);
+  for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    const int64_t lb = b / tchunks;
+    const int64_t it = (b - lb * tchunks) * kSpinPrjThreads + threadIdx.x;
+    if (it >= d.nt) continue;
+    int64_t pt[MC];
+#pragma unroll UNR
+    for (int k = 0; k < MC; ++k) pt[k] = __ldg(d.pt + k * d.nt + it);
+    const int64_t l1 = min(d.nl, (lb + 1) * kSpinPrjLoop);
+    for (int64_t il = lb * kSpinPrjLoop; il < l1; ++il) {
+      int64_t idx[MC];
+      double val[MC];
+#pragma unroll UNR
+      for (int k = 0; k < MC; ++k) {
+        const int64_t l = __ldg(d.pl + k * d.nl + il);
+        idx[k] = (pt[k] < 0 || l < 0) ? -1 : pt[k] + l;
+      }
+#pragma unroll UNR
+      for (int k = 0; k < MC; ++k) {
+        int cnt = 0;
+#pragma unroll UNR
+        for (int j = 0; j < k; ++j) cnt += idx[j] == idx[k];
+        const double v = idx[k] < 0 ? 0.0 : x[idx[k]];
+        val[k] = (__popc(cnt) & 1) ? -v : v;
+      }
+      // C^T v, then C (C^T v): summed in case order, then in path order
+      double ov[NP];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        double s = 0.0;
+#pragma unroll UNR
+        for (int k = 0; k < MC; ++k) s += cs[k * NP + q] * val[k];
+        ov[q] = s;
+      }
+#pragma unroll UNR
+      for (int k = 0; k < MC; ++k) {
+        if (idx[k] < 0) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) s += cs[k * NP + q] * ov[q];
+        int cnt = 0;
+#pragma unroll UNR
+        for (int j = 0; j < k; ++j) cnt += idx[j] == idx[k];
+        x[idx[k]] = (__popc(cnt) & 1) ? -s : s;
+      }
     }
   }
 }
 
 template <int MC>
-void launch_t(const SpinPrjDesc* d, int64_t n, double* x, int64_t maxlen, cudaStream_t s) {
+void launch_t(const SpinPrjDesc* d, int64_t n, double* x, int64_t maxblocks, cudaStream_t s) {
   for (int64_t b = 0; b < n; b += 65535) {
-    dim3 grid((unsigned)std::min<int64_t>((maxlen + kSpinPrjThreads - 1) / kSpinPrjThreads, 2048),
+    dim3 grid((unsigned)std::min<int64_t>(maxblocks, 4096),
               (unsigned)std::min<int64_t>(n - b, 65535));
     k_spin_prj<MC><<<grid, kSpinPrjThreads, 0, s>>>(d + b, x);
   }
@@ -118,13 +94,15 @@ void launch_t(const SpinPrjDesc* d, int64_t n, double* x, int64_t maxlen, cudaSt
 
 }  // namespace
 
-void launch_spin_prj(const SpinPrjDesc* d, int64_t n, int maxcase, double* x, int64_t maxlen,
+void launch_spin_prj(const SpinPrjDesc* d, int64_t n, int ncase, double* x, int64_t maxblocks,
                      cudaStream_t s) {
-  if (n == 0 || maxlen == 0) return;
-  if (maxcase <= 2) launch_t<2>(d, n, x, maxlen, s);
-  else if (maxcase <= 6) launch_t<6>(d, n, x, maxlen, s);
-  else if (maxcase <= 20) launch_t<20>(d, n, x, maxlen, s);
-  else launch_t<kSpinPrjMaxCases>(d, n, x, maxlen, s);
+  if (n == 0 || maxblocks == 0) return;
+  switch (ncase) {
+    case 2: launch_t<2>(d, n, x, maxblocks, s); break;
+    case 6: launch_t<6>(d, n, x, maxblocks, s); break;
+    case 20: launch_t<20>(d, n, x, maxblocks, s); break;
+    default: launch_t<kSpinPrjMaxCases>(d, n, x, maxblocks, s); break;
+  }
 }
 
 }  // namespace gccu
