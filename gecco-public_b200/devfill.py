@@ -1,13 +1,16 @@
-"""Filling ME lists on the device (set-up of large Hamiltonians).
+"""Filling ME lists on the device (set-up of the Hamiltonian).
 
 The reference sorts integrals into its ME lists on the host during import
-(input/import_h2_molpro_dump.f, "no batch algorithm").  Here the two-electron
-list is generated on the GPU from the factorised integrals (pq|rs) = sum_P
-B_pq^P B_rs^P and written in place into the engine's device memory: per
-(class, Ms, IRREP, distribution) block the component strings are turned into
-spin orbitals, the antisymmetrised <c1c2||a1a2> are gathered from spatial
-integral matrices and scattered to the block's element positions.  torch is
-used as device-memory plumbing for this set-up step only.
+(input/import_h2_molpro_dump.f, "no batch algorithm").  Here the lists are
+generated on the GPU and written in place into the engine's device memory:
+per (class, Ms, IRREP, distribution) block the component strings are turned
+into spin orbitals, the Fock elements and the antisymmetrised <c1c2||a1a2>
+are gathered from spatial integrals on the device and scattered to the
+block's element positions.  The spatial integrals are either factorised,
+(pq|rs) = sum_P B_pq^P B_rs^P (TorchIntegrals), or dense (pq|rs) with the
+Fock matrix (TorchDenseIntegrals; from_fcidump scatters an FCIDUMP's records
+into them on the device).  torch is used as device-memory plumbing for this
+set-up step only.
 """
 import numpy as np
 import torch
@@ -74,6 +77,70 @@ class DeviceListView:
                     pos = pos + base.reshape(shape) * ld[j]
                 pos = pos.expand(grid)
                 x[off + pos.reshape(-1)] = vals.reshape(-1)
+
+
+class TorchDenseIntegrals:
+    """device form of DenseIntegrals: the spatial Fock matrix f and (pq|rs);
+    the denominators use the Fock matrix's diagonal"""
+
+    def __init__(self, space, f, eri, device="cuda"):
+        self.space = space
+        self.device = device
+        self.f = torch.as_tensor(f, device=device, dtype=torch.float64)
+        self.eri_pqrs = torch.as_tensor(eri, device=device, dtype=torch.float64)
+        self.eps = torch.diagonal(self.f).clone()
+        self.orbs = [torch.as_tensor(space.type_orbitals(t), device=device) for t in (0, 1)]
+        self.ecore = 0.0
+
+    @classmethod
+    def from_fcidump(cls, path, nocc, nfrozen=None, ndeleted=None, device="cuda"):
+        """the FCIDUMP's records (parsed on the host) scattered into h and
+        (pq|rs) with its eight-fold symmetry on the device, the closed-shell
+        Fock matrix f = h + 2J - K of the nocc (per irrep) lowest orbitals
+        formed there"""
+        import hamiltonian as hm
+        r = hm.fcidump_records(path)
+        n = int(r["norb"])
+        space = hm.OrbitalSpace(r["orbsym"], nocc, nfrozen, ndeleted)
+        vals = torch.as_tensor(np.asarray(r["vals"], dtype=np.float64), device=device)
+        idx = torch.as_tensor(np.asarray(r["idx"], dtype=np.int64), device=device)
+        core = (idx == 0).all(dim=1)
+        one = (idx[:, 2] == 0) & (idx[:, 3] == 0) & ~core
+        two = ~(core | one)
+        h = torch.zeros((n, n), dtype=torch.float64, device=device)
+        p, q = idx[one, 0] - 1, idx[one, 1] - 1
+        h[p, q] = vals[one]
+        h[q, p] = vals[one]
+        eri = torch.zeros((n,) * 4, dtype=torch.float64, device=device)
+        ix = (idx[two] - 1).t()
+        for perm in hm.ERI_PERMS:
+            eri[ix[perm[0]], ix[perm[1]], ix[perm[2]], ix[perm[3]]] = vals[two]
+        occ = torch.as_tensor(space.occ_all, device=device)
+        J = torch.einsum("pqkk->pq", eri[:, :, occ][:, :, :, occ])
+        K = torch.einsum("pkkq->pq", eri[:, occ][:, :, occ])
+        out = cls(space, h + 2 * J - K, eri, device)
+        out.ecore = float(vals[core][-1]) if bool(core.any()) else 0.0
+        return out
+
+    def glob(self, t, so):
+        return self.orbs[t][so // 2], so % 2
+
+    def fock(self, t1, so1, t2, so2):
+        (p, s1), (q, s2) = self.glob(t1, so1), self.glob(t2, so2)
+        return torch.where(s1 == s2, self.f[p, q],
+                           torch.zeros((), device=self.device, dtype=torch.float64))
+
+    def eri(self, t, so):
+        """<c1 c2 || a1 a2> = (c1 a1|c2 a2) - (c1 a2|c2 a1) with spin deltas"""
+        (c1, s1), (c2, s2) = self.glob(t[0], so[0]), self.glob(t[1], so[1])
+        (a1, r1), (a2, r2) = self.glob(t[2], so[2]), self.glob(t[3], so[3])
+        direct = self.eri_pqrs[c1, a1, c2, a2] * ((s1 == r1) & (s2 == r2))
+        exch = self.eri_pqrs[c1, a2, c2, a1] * ((s1 == r2) & (s2 == r1))
+        return direct - exch
+
+    def release(self):
+        if self.device != "cpu":
+            torch.cuda.empty_cache()
 
 
 class TorchIntegrals:

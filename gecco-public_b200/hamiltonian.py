@@ -54,37 +54,49 @@ class OrbitalSpace:
         return len(self.part)
 
 
-def read_fcidump(path):
-    """FCIDUMP text (&FCI NORB,NELEC,MS2,ORBSYM,ISYM namelist, then value p q r s
-    records, input/read_env_molpro_dump.f:39-57) or the fixture .npz form"""
+def fcidump_records(path):
+    """header and records of an FCIDUMP: text (&FCI NORB,NELEC,MS2,ORBSYM,ISYM
+    namelist, then value p q r s records, input/read_env_molpro_dump.f:39-57)
+    or the fixture .npz form; returns norb, orbsym, vals, idx (1-based
+    orbital indices, 0 for the absent ones)"""
     if path.endswith(".npz"):
         d = np.load(path)
-        norb = int(d["norb"])
-        vals, idx, orbsym = d["vals"], d["idx"], d["orbsym"]
-    else:
-        import re
-        text = open(path).read()
-        head, body = text.split("/", 1)
-        norb = int(re.search(r"NORB\s*=\s*(\d+)", head).group(1))
-        orbsym = np.array([int(x) for x in re.search(r"ORBSYM\s*=\s*([\d,\s]+?),\s*ISYM", head)
-                           .group(1).replace(",", " ").split()])
-        rec = np.array([l.split() for l in body.splitlines() if len(l.split()) == 5])
-        vals = rec[:, 0].astype(float)
-        idx = rec[:, 1:].astype(int)
+        return dict(norb=int(d["norb"]), orbsym=d["orbsym"], vals=d["vals"], idx=d["idx"])
+    import re
+    text = open(path).read()
+    head, body = text.split("/", 1)
+    norb = int(re.search(r"NORB\s*=\s*(\d+)", head).group(1))
+    orbsym = np.array([int(x) for x in re.search(r"ORBSYM\s*=\s*([\d,\s]+?),\s*ISYM", head)
+                       .group(1).replace(",", " ").split()])
+    rec = np.array([l.split() for l in body.splitlines() if len(l.split()) == 5])
+    return dict(norb=norb, orbsym=orbsym, vals=rec[:, 0].astype(float),
+                idx=rec[:, 1:].astype(int))
+
+
+# the eight index orders of a real (pq|rs)
+ERI_PERMS = ((0, 1, 2, 3), (1, 0, 2, 3), (0, 1, 3, 2), (1, 0, 3, 2),
+             (2, 3, 0, 1), (3, 2, 0, 1), (2, 3, 1, 0), (3, 2, 1, 0))
+
+
+def read_fcidump(path):
+    """one-electron matrix h, (pq|rs) with its eight-fold symmetry and the
+    core energy from an FCIDUMP (records with r = s = 0 are h_pq, all-zero
+    indices the core energy)"""
+    r = fcidump_records(path)
+    norb, vals, idx = r["norb"], np.asarray(r["vals"], float), np.asarray(r["idx"], int)
+    core = (idx == 0).all(axis=1)
+    one = (idx[:, 2] == 0) & (idx[:, 3] == 0) & ~core
+    two = ~(core | one)
     h = np.zeros((norb, norb))
+    p, q = idx[one, 0] - 1, idx[one, 1] - 1
+    h[p, q] = vals[one]
+    h[q, p] = vals[one]
     eri = np.zeros((norb,) * 4)
-    ecore = 0.0
-    for v, (p, q, r, s) in zip(vals, idx):
-        if p == q == r == s == 0:
-            ecore = v
-        elif r == 0 and s == 0:
-            h[p - 1, q - 1] = h[q - 1, p - 1] = v
-        else:
-            p, q, r, s = p - 1, q - 1, r - 1, s - 1
-            for a, b, c, d in ((p, q, r, s), (q, p, r, s), (p, q, s, r), (q, p, s, r),
-                               (r, s, p, q), (s, r, p, q), (r, s, q, p), (s, r, q, p)):
-                eri[a, b, c, d] = v
-    return dict(norb=norb, orbsym=orbsym, h=h, eri=eri, ecore=ecore)
+    ix = (idx[two] - 1).T
+    for perm in ERI_PERMS:
+        eri[ix[perm[0]], ix[perm[1]], ix[perm[2]], ix[perm[3]]] = vals[two]
+    ecore = float(vals[core][-1]) if core.any() else 0.0
+    return dict(norb=norb, orbsym=r["orbsym"], h=h, eri=eri, ecore=ecore)
 
 
 def fock(h, eri, occ):

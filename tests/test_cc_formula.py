@@ -131,3 +131,22 @@ def test_ccsd_residuals_of_a_closed_shell_are_singlets(hf_ints):
     s.project_residuals()
     moved = np.abs(s.e.data[s.lid("R2")] - r2).max()
     assert moved > 1e-6 * np.abs(r2).max()
+
+
+def test_fcidump_filled_through_the_device_path_equals_host_fill(hf_ints, gold):
+    # the FCIDUMP's records scattered into h and (pq|rs) by torch, the Fock
+    # matrix and the lists formed from them (the device path, here with torch
+    # on the CPU): the same lists as the host fill and the reference's MP2
+    # energy
+    from devfill import TorchDenseIntegrals
+    path = os.path.join(GOLD, "hf_ccpvdz_fcidump.npz")
+    tints = TorchDenseIntegrals.from_fcidump(path, [3, 1, 1, 0], [1, 0, 0, 0], device="cpu")
+    host = cc.CCSolver(OracleEngine(route=3), hf_ints, method="mp2")
+    host.load_hamiltonian()
+    dev = cc.CCSolver(OracleEngine(route=3), tints, method="mp2")
+    dev.load_hamiltonian_device(tints)
+    for name in ("F", "V", "DT2"):
+        a, b = host.e.data[host.lid(name)], dev.e.data[dev.lid(name)]
+        assert np.max(np.abs(a - b)) <= 1e-13 * max(1.0, np.abs(a).max()), name
+    e = dev.solve(maxiter=5, conv=1e-10)
+    assert abs(e + gold["lmp2_norm"]) < 1e-13

@@ -119,3 +119,25 @@ def test_ccsd_spin_flip_symmetry_same_iterates(built, mode):
     for (i, ea, ra), (_, eb, rb) in zip(*hist):
         assert abs(ea - eb) < tol * max(1.0, abs(ea)), (i, ea, eb)
         assert abs(ra - rb) < tol * max(1.0, ra), (i, ra, rb)
+
+
+def test_fcidump_filled_on_the_device_gives_the_reference_mp2(engine):
+    # the FCIDUMP's records scattered into h and (pq|rs) in device memory,
+    # the Fock matrix and the lists formed there: the lists of the host fill
+    # and the reference's MP2 energy
+    from devfill import TorchDenseIntegrals, list_tensor
+    path = os.path.join(GOLD, "hf_ccpvdz_fcidump.npz")
+    gold = json.load(open(os.path.join(GOLD, "hf_ccpvdz_ref.json")))
+    tints = TorchDenseIntegrals.from_fcidump(path, [3, 1, 1, 0], [1, 0, 0, 0])
+    s = cc.CCSolver(engine, tints, method="mp2")
+    s.load_hamiltonian_device(tints)
+    host = cc.CCSolver(OracleEngine(route=3), hm.DenseIntegrals(
+        tints.space, tints.f.cpu().numpy(), tints.eri_pqrs.cpu().numpy()), method="mp2")
+    host.load_hamiltonian()
+    for name in ("F", "V", "DT2"):
+        lid, n, _ = s.lists[name]
+        got = list_tensor(engine, lid, n).cpu().numpy()
+        ref = host.e.data[host.lid(name)]
+        assert np.max(np.abs(got - ref)) <= 1e-13 * max(1.0, np.abs(ref).max()), name
+    e = s.solve(maxiter=5, conv=1e-10)
+    assert abs(e + gold["lmp2_norm"]) < 1e-13
