@@ -228,9 +228,18 @@ class CCSolver:
     lists (solve_nleq with method=diis, solve/solve_nleq.f; diagonal step
     diavc, baserout/diavc.f; DIIS subspace, solve/optc_diis_extr.f)."""
 
+    # lists that hold the Hamiltonian, amplitudes, residuals and the energy;
+    # the others of a formula are its intermediates
+    PERSISTENT = ("F", "V", "T1", "T2", "R1", "R2", "E")
+
     def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
-                 learned=None, shard=None, spin_project=False):
+                 learned=None, shard=None, spin_project=False, native_formula=False):
         self.e = engine
+        # native_formula: the formula runs as one item list in the engine
+        # (gccu_formula_run), its intermediates created and deleted by
+        # [NEW] / [DEL] items in one arena (not with a sharded solve)
+        self.native = native_formula and shard is None
+        self.fid = None
         # project the residuals onto their singlet part after each evaluation
         # (result lists with a spin, frm_sched2's end-of-target step)
         self.spin_project = spin_project
@@ -257,7 +266,10 @@ class CCSolver:
             absym = 1 if use_tr and name not in ("F", "V", "E") else 0
             if use_tr and name in ("F", "V"):
                 absym = 1
-            lid, n = engine.register_list(opid, absym=absym)
+            if self.native and name not in self.PERSISTENT:
+                lid, n = engine.register_intermediate(opid, absym=absym)
+            else:
+                lid, n = engine.register_list(opid, absym=absym)
             self.lists[name] = (lid, n, blocks)
         self.amps = ["T2"] if method == "mp2" else ["T1", "T2"]
         self.res = {"T1": "R1", "T2": "R2"}
@@ -273,6 +285,62 @@ class CCSolver:
         self.history = []
         if self.learned:
             engine.lp_set_weights(learned)
+        if self.native:
+            self.fid = engine.formula_define(self.formula_items())
+
+    def formula_items(self):
+        """the formula as engine items (frm_sched2's commands): [INIT
+        TARGET] wherever the result list changes (the residuals' last ones
+        project onto the singlet with spin_project), [NEW] before an
+        intermediate's first item and [DEL] after its last"""
+        import gccu
+        inter = {n for n in self.lists if n not in self.PERSISTENT and n in
+                 {x for it in self.formula for x in self._names(it)}}
+        first, last = {}, {}
+        for i, it in enumerate(self.formula):
+            for n in self._names(it):
+                if n in inter:
+                    first.setdefault(n, i)
+                    last[n] = i
+        last_seg = {}
+        for i, it in enumerate(self.formula):
+            if i == 0 or self.formula[i - 1]["res"][0] != it["res"][0]:
+                last_seg[it["res"][0]] = i
+        items = []
+        for i, it in enumerate(self.formula):
+            for n in sorted(n for n, f in first.items() if f == i):
+                items.append(gccu.FormulaItem(command=gccu.CMD_NEW, list=self.lid(n)))
+            res = it["res"][0]
+            if i == 0 or self.formula[i - 1]["res"][0] != res:
+                proj = self.spin_project and res in self.res.values() and last_seg[res] == i
+                items.append(gccu.FormulaItem(command=gccu.CMD_TARGET, list=self.lid(res),
+                                              s2=0 if proj else -1))
+            if it["kind"] == "ADD":
+                (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
+                items.append(gccu.FormulaItem(command=gccu.CMD_ADD, list=lo, iblk_out=bo,
+                                              list_in=li, iblk_in=bi, fac=it["fac"],
+                                              reset=int(it["reset"])))
+            else:
+                bc, use_tr = self._bc(it)
+                items.append(gccu.FormulaItem(command=gccu.CMD_CONTR, bc=bc, fac=it["fac"],
+                                              update=int(it["update"]), use_tr=int(use_tr)))
+            for n in sorted(n for n, l in last.items() if l == i):
+                items.append(gccu.FormulaItem(command=gccu.CMD_DEL, list=self.lid(n)))
+        return items
+
+    @staticmethod
+    def _names(it):
+        ops = [it["src"]] if it["kind"] == "ADD" else [it["op1"], it["op2"]]
+        return [it["res"][0]] + [o[0] for o in ops]
+
+    def _bc(self, it):
+        """engine descriptor of a [CONTR] item and whether it runs under use_tr"""
+        o1, o2, r = self.blk(it["op1"]), self.blk(it["op2"]), self.blk(it["res"])
+        c = np.asarray(it["cnt"])
+        ex1 = np.asarray(it["op1"][1]) - c
+        ex2 = np.asarray(it["op2"][1]) - np.concatenate([c[4:], c[:4]])
+        use_tr = self.use_tr and it["res"][0] not in ("E",)
+        return self.e.desc(o1, o2, r, ex1, ex2, c), use_tr
 
     def lid(self, name):
         return self.lists[name][0]
@@ -354,6 +422,9 @@ class CCSolver:
 
     def evaluate(self):
         """one formula evaluation (frm_sched2 over the item list)"""
+        if self.fid is not None:
+            self.e.formula_run(self.fid)
+            return
         for it in self.formula:
             self.run_item(it)
 
@@ -486,7 +557,7 @@ class CCSolver:
             self.evaluate()
         if self.shard is not None:
             self.shard.reduce(self)
-        if self.spin_project:
+        if self.spin_project and self.fid is None:
             self.project_residuals()
         en = self.energy()
         rn = self.residual_norm()

@@ -11,6 +11,7 @@
 #include <thread>
 #include <cstring>
 #include <map>
+#include <set>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -49,6 +50,18 @@ struct DevList {
   // plans may cache panels derived from it; epoch counts unfreezes
   bool frozen = false;
   int64_t epoch = 0;
+  // an intermediate of a formula (gccu_register_intermediate): memory is a
+  // range of its formula's arena, set when the formula is defined
+  bool intermediate = false;
+  int64_t formula = 0, arena_off = -1;
+};
+
+// a defined formula (gccu_formula_define): its items and the arena holding
+// its intermediates
+struct FormulaPlan {
+  std::vector<gccu_formula_item> items;
+  double* arena = nullptr;
+  int64_t arena_bytes = 0, sum_bytes = 0, ntargets = 0;
 };
 
 struct DevGraph {
@@ -307,6 +320,7 @@ class Engine {
   std::map<std::array<int, 3>, int32_t*> flips;
   std::map<std::array<int, 3>, PatternMap> spprjs;  // spin-projection pattern maps (host)
   std::map<int64_t, std::unique_ptr<DevSpinPrj>> spinprjs;  // singlet projection per list
+  std::vector<FormulaPlan> formulas;  // gccu_formula_define
   std::map<std::string, std::unique_ptr<DevPlan>> plans;
   std::vector<void*> allocs;
   double* d_red = nullptr;  // reduction scalars
@@ -514,6 +528,13 @@ class Engine {
   }
 
   DevList& list(int64_t id) {
+    DevList& l = layout_list(id);
+    GCCU_REQUIRE(host_only || l.d,
+                 "intermediate list without memory: define the formula that creates it first");
+    return l;
+  }
+  // a list whose layout (not its memory) is needed
+  DevList& layout_list(int64_t id) {
     GCCU_REQUIRE(id >= 1 && id <= (int64_t)lists.size(), "invalid ME-list handle");
     return lists[id - 1];
   }
@@ -2044,6 +2065,29 @@ int guarded(F&& f) {
   }
 }
 
+// lists a formula item names
+std::vector<int64_t> item_lists(const gccu_formula_item& it) {
+  switch (it.command) {
+    case GCCU_CMD_TARGET:
+    case GCCU_CMD_NEW:
+    case GCCU_CMD_DEL:
+      return {it.list};
+    case GCCU_CMD_ADD:
+      return {it.list, it.list_in};
+    case GCCU_CMD_CONTR:
+      return {it.bc.list_op1, it.bc.list_op2, it.bc.list_res};
+    case GCCU_CMD_REORDER:
+      return {it.reo.list_ori, it.reo.list_reo};
+    default:
+      throw Error("formula: unknown command");
+  }
+}
+
+// a nested entry point's status as an exception (its message kept)
+void check_rc(int rc) {
+  if (rc != 0) throw Error(g_error);
+}
+
 }  // namespace
 }  // namespace gccu
 
@@ -2197,9 +2241,29 @@ int gccu_register_list(int64_t op_id, int64_t gamt, int64_t mst, int64_t absym, 
   });
 }
 
+int gccu_register_intermediate(int64_t op_id, int64_t gamt, int64_t mst, int64_t absym,
+                               int64_t* list_id, int64_t* len_op) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(e.have_orbs, "orbital space not registered");
+    GCCU_REQUIRE(op_id >= 1 && op_id <= (int64_t)e.model.ops.size(), "invalid operator id");
+    GCCU_REQUIRE(gamt >= 1 && gamt <= e.model.os.nsym, "invalid total irrep");
+    DevList dl;
+    dl.L.op = (int)op_id;
+    dl.L.gamt = (int)gamt;
+    dl.L.mst = (int)mst;
+    dl.L.absym = (int)absym;
+    e.model.layout(dl.L);
+    dl.intermediate = true;
+    e.lists.push_back(std::move(dl));
+    *list_id = (int64_t)e.lists.size();
+    *len_op = e.lists.back().L.len;
+  });
+}
+
 int gccu_list_block(int64_t list_id, int64_t iblk, int64_t* off, int64_t* len) {
   return guarded([&] {
-    DevList& dl = eng().list(list_id);
+    DevList& dl = eng().layout_list(list_id);
     GCCU_REQUIRE(iblk >= 1 && iblk <= (int64_t)dl.L.blk.size(), "invalid occupation class");
     *off = dl.L.blk[iblk - 1].off;
     *len = dl.L.blk[iblk - 1].len;
@@ -2208,7 +2272,7 @@ int gccu_list_block(int64_t list_id, int64_t iblk, int64_t* off, int64_t* len) {
 
 int gccu_list_dists(int64_t list_id, int64_t* rows, int64_t maxrows, int64_t* nrows) {
   return guarded([&] {
-    DevList& dl = eng().list(list_id);
+    DevList& dl = eng().layout_list(list_id);
     int64_t n = 0;
     for (size_t ib = 0; ib < dl.L.blk.size(); ++ib)
       for (auto& kv : dl.L.blk[ib].dis)
@@ -2662,6 +2726,171 @@ int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk) {
       CUDA_OK(cudaStreamSynchronize(e.stream));
     }
     e.check_err();
+  });
+}
+
+int gccu_formula_define(const gccu_formula_item* items, int64_t n, int64_t* formula_id) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(n >= 0 && (items || n == 0), "formula: no items");
+    GCCU_REQUIRE(!e.capturing, "formula: define it outside a graph capture");
+    FormulaPlan F;
+    F.items.assign(items, items + n);
+    const int64_t fid = (int64_t)e.formulas.size() + 1;
+    std::map<int64_t, int64_t> open;           // intermediate -> item of its [NEW]
+    std::vector<std::array<int64_t, 3>> life;  // ([NEW] item, [DEL] item, list)
+    std::set<int64_t> made;
+    for (int64_t i = 0; i < n; ++i) {
+      const gccu_formula_item& it = F.items[i];
+      for (int64_t l : item_lists(it)) {
+        DevList& dl = e.layout_list(l);
+        if (!dl.intermediate) continue;
+        GCCU_REQUIRE(dl.formula == 0, "formula: an intermediate belongs to one formula");
+        GCCU_REQUIRE(it.command == GCCU_CMD_NEW || open.count(l),
+                     "formula: intermediate named outside its [NEW] .. [DEL]");
+      }
+      switch (it.command) {
+        case GCCU_CMD_TARGET:
+          GCCU_REQUIRE(it.s2 >= -1, "formula: s2 of a target is -1 or 2S");
+          ++F.ntargets;
+          break;
+        case GCCU_CMD_NEW:
+          GCCU_REQUIRE(e.layout_list(it.list).intermediate,
+                       "formula: [NEW] of a list that is not an intermediate");
+          GCCU_REQUIRE(!made.count(it.list), "formula: an intermediate is created once");
+          made.insert(it.list);
+          open[it.list] = i;
+          break;
+        case GCCU_CMD_DEL:
+          GCCU_REQUIRE(e.layout_list(it.list).intermediate,
+                       "formula: [DEL] of a list that is not an intermediate");
+          life.push_back({open[it.list], i, it.list});
+          open.erase(it.list);
+          break;
+        case GCCU_CMD_ADD:
+        case GCCU_CMD_CONTR:
+        case GCCU_CMD_REORDER:
+          break;
+        default:
+          GCCU_REQUIRE(false, "formula: unknown command");
+      }
+    }
+    for (auto& kv : open) life.push_back({kv.second, n, kv.first});
+    std::sort(life.begin(), life.end());
+    // first fit in the order of the [NEW]s among the ranges still alive
+    struct Range {
+      int64_t off, bytes, until;
+    };
+    std::vector<Range> live;
+    std::map<int64_t, int64_t> offset_of;
+    for (const auto& lf : life) {
+      live.erase(std::remove_if(live.begin(), live.end(),
+                                [&](const Range& r) { return r.until < lf[0]; }),
+                 live.end());
+      std::sort(live.begin(), live.end(),
+                [](const Range& a, const Range& b) { return a.off < b.off; });
+      const int64_t len = std::max<int64_t>(e.layout_list(lf[2]).L.len, 1);
+      const int64_t bytes = (len * (int64_t)sizeof(double) + 255) / 256 * 256;
+      int64_t off = 0;
+      for (const Range& r : live) {
+        if (off + bytes <= r.off) break;
+        off = std::max(off, r.off + r.bytes);
+      }
+      live.push_back({off, bytes, lf[1]});
+      offset_of[lf[2]] = off;
+      F.arena_bytes = std::max(F.arena_bytes, off + bytes);
+      F.sum_bytes += bytes;
+    }
+    if (!e.host_only && F.arena_bytes > 0) {
+      F.arena = (double*)e.alloc(F.arena_bytes);
+      CUDA_OK(cudaMemsetAsync(F.arena, 0, F.arena_bytes, e.stream));
+    }
+    for (const auto& kv : offset_of) {
+      DevList& dl = e.layout_list(kv.first);
+      dl.formula = fid;
+      dl.arena_off = kv.second;
+      if (F.arena) dl.d = F.arena + kv.second / (int64_t)sizeof(double);
+    }
+    e.formulas.push_back(std::move(F));
+    *formula_id = fid;
+  });
+}
+
+int gccu_formula_run(int64_t formula_id, double* xret, int64_t nxret) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(!e.host_only, "gccu_formula_run needs a device");
+    GCCU_REQUIRE(formula_id >= 1 && formula_id <= (int64_t)e.formulas.size(),
+                 "invalid formula id");
+    const FormulaPlan& F = e.formulas[formula_id - 1];
+    GCCU_REQUIRE(!xret || nxret >= F.ntargets,
+                 "formula: xret is shorter than the number of targets");
+    GCCU_REQUIRE(!xret || !e.capturing, "formula: xret must be NULL inside a graph capture");
+    int64_t target = 0, s2 = -1, ti = -1;
+    auto end_target = [&] {
+      if (!target) return;
+      if (s2 >= 0) check_rc(gccu_spin_prj_list(target, s2, nullptr));
+      if (!xret) return;
+      DevList& l = e.list(target);
+      if (l.L.len == 1) {
+        CUDA_OK(cudaMemcpyAsync(&xret[ti], l.d, sizeof(double), cudaMemcpyDeviceToHost,
+                                e.stream));
+        CUDA_OK(cudaStreamSynchronize(e.stream));
+      } else {
+        double d2 = 0;
+        check_rc(gccu_dot_lists(target, target, &d2));
+        xret[ti] = std::sqrt(d2);
+      }
+    };
+    for (const gccu_formula_item& it : F.items) {
+      switch (it.command) {
+        case GCCU_CMD_TARGET:
+          end_target();
+          target = it.list;
+          s2 = it.s2;
+          ++ti;
+          if (it.init) check_rc(gccu_zero_list(it.list));
+          break;
+        case GCCU_CMD_ADD:
+          if (it.tra_in || it.tra_out)
+            check_rc(gccu_add_block_transp(it.fac, it.list_in, it.iblk_in, it.list, it.iblk_out,
+                                           it.tra_in, it.tra_out, it.reset, 0, nullptr));
+          else
+            check_rc(gccu_add_block(it.fac, it.list_in, it.iblk_in, it.list, it.iblk_out,
+                                    it.reset, 0, nullptr));
+          break;
+        case GCCU_CMD_CONTR:
+          check_rc(gccu_contract(&it.bc, it.fac, it.update, it.use_tr, 0, nullptr));
+          break;
+        case GCCU_CMD_REORDER:
+          check_rc(gccu_reorder(&it.reo, it.fac, it.sign_reo, it.update, 0, nullptr));
+          break;
+        default:  // [NEW] / [DEL]: the arena was laid out when the formula was defined
+          break;
+      }
+    }
+    end_target();
+  });
+}
+
+int gccu_formula_info(int64_t formula_id, int64_t* info4) {
+  return guarded([&] {
+    Engine& e = eng();
+    GCCU_REQUIRE(formula_id >= 1 && formula_id <= (int64_t)e.formulas.size(),
+                 "invalid formula id");
+    const FormulaPlan& F = e.formulas[formula_id - 1];
+    info4[0] = F.arena_bytes;
+    info4[1] = F.sum_bytes;
+    info4[2] = F.ntargets;
+    info4[3] = (int64_t)F.items.size();
+  });
+}
+
+int gccu_intermediate_offset(int64_t list_id, int64_t* offset) {
+  return guarded([&] {
+    DevList& dl = eng().layout_list(list_id);
+    GCCU_REQUIRE(dl.intermediate, "not an intermediate list");
+    *offset = dl.arena_off;
   });
 }
 

@@ -36,6 +36,17 @@ class ReoDesc(ctypes.Structure):
                 ("to_vtx", I64 * 4)]
 
 
+# commands of a formula item (include/gccu.h)
+CMD_TARGET, CMD_NEW, CMD_DEL, CMD_ADD, CMD_CONTR, CMD_REORDER = 1, 2, 3, 4, 5, 6
+
+
+class FormulaItem(ctypes.Structure):
+    _fields_ = [("command", I64), ("list", I64), ("init", I64), ("s2", I64), ("list_in", I64),
+                ("iblk_in", I64), ("iblk_out", I64), ("reset", I64), ("tra_in", I64),
+                ("tra_out", I64), ("update", I64), ("use_tr", I64), ("sign_reo", I64),
+                ("fac", ctypes.c_double), ("bc", BcDesc), ("reo", ReoDesc)]
+
+
 class GccuError(RuntimeError):
     pass
 
@@ -90,6 +101,11 @@ _SIGS = {
     "gccu_dot_lists": [I64, I64, PD],
     "gccu_sym_ab": [I64, I64, ctypes.c_double, ctypes.c_double],
     "gccu_spin_prj_list": [I64, I64, PD],
+    "gccu_register_intermediate": [I64, I64, I64, I64, P64, P64],
+    "gccu_formula_define": [ctypes.c_void_p, I64, P64],
+    "gccu_formula_run": [I64, PD, I64],
+    "gccu_formula_info": [I64, P64],
+    "gccu_intermediate_offset": [I64, P64],
     "gccu_precondition": [I64, I64, I64, ctypes.c_double, ctypes.c_double],
     "gccu_graph_begin": [],
     "gccu_graph_end": [P64],
@@ -370,6 +386,41 @@ class Engine:
         ln = np.zeros(1, np.int64)
         _call("gccu_register_list", op, gamt, mst, absym, _p64(lid), _p64(ln))
         return int(lid[0]), int(ln[0])
+
+    def register_intermediate(self, op, gamt=1, mst=0, absym=0):
+        """a list without memory of its own, placed in the arena of the
+        formula whose [NEW] names it"""
+        lid = np.zeros(1, np.int64)
+        ln = np.zeros(1, np.int64)
+        _call("gccu_register_intermediate", op, gamt, mst, absym, _p64(lid), _p64(ln))
+        return int(lid[0]), int(ln[0])
+
+    def formula_define(self, items):
+        """items: FormulaItem sequence; returns the formula id"""
+        arr = (FormulaItem * max(len(items), 1))(*items)
+        fid = np.zeros(1, np.int64)
+        _call("gccu_formula_define", ctypes.cast(arr, ctypes.c_void_p), len(items), _p64(fid))
+        return int(fid[0])
+
+    def formula_run(self, fid, ntargets=0):
+        """run a formula; with ntargets > 0 return the targets' values"""
+        if ntargets:
+            r = np.zeros(ntargets)
+            _call("gccu_formula_run", fid, _pd(r), ntargets)
+            return r
+        _call("gccu_formula_run", fid, PD(), 0)
+        return None
+
+    def formula_info(self, fid):
+        r = np.zeros(4, np.int64)
+        _call("gccu_formula_info", fid, _p64(r))
+        return dict(arena_bytes=int(r[0]), sum_bytes=int(r[1]), targets=int(r[2]),
+                    items=int(r[3]))
+
+    def intermediate_offset(self, lst):
+        r = np.zeros(1, np.int64)
+        _call("gccu_intermediate_offset", lst, _p64(r))
+        return int(r[0])
 
     def block(self, lst, iblk):
         off = np.zeros(1, np.int64)

@@ -256,6 +256,56 @@ int gccu_sym_ab(int64_t list_id, int64_t iblk, double prefac, double relfac);
  * plan is made on the first call for a list (not inside a capture). */
 int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk);
 
+/* ---- formula evaluation --------------------------------------------------
+ * replaces: the command loop of frm_sched2 (contract/frm_sched2.f:117-365)
+ * for one formula, with fs_newintm_drv / fs_delintm_drv (the [NEW] / [DEL]
+ * intermediate commands, :239-252).  A formula is defined once
+ * (gccu_formula_define) as an array of items and run any number of times
+ * (gccu_formula_run), also inside a graph capture.  Intermediates are lists
+ * registered with gccu_register_intermediate: they have no memory of their
+ * own; when the formula is defined each gets a fixed byte range of one arena
+ * owned by the formula, shared with the intermediates whose [NEW] .. [DEL]
+ * windows do not overlap its own (first fit in the order of the [NEW]s), so
+ * the arena holds the largest set of intermediates alive at one time instead
+ * of all of them.  The addresses never change, so plans and captured graphs
+ * stay valid.  An intermediate belongs to one formula and is named only
+ * between its [NEW] and its [DEL] (or the end of the formula); outside a run
+ * of that formula its contents are undefined. */
+#define GCCU_CMD_TARGET 1  /* [INIT TARGET]: item.list becomes the target; init != 0 zeroes
+                              it; s2 >= 0: at the target's end the list is projected onto
+                              spin s2 (spin_prj_list, frm_sched2.f:146-149), s2 = -1: not */
+#define GCCU_CMD_NEW 2     /* [NEW] intermediate item.list */
+#define GCCU_CMD_DEL 3     /* [DEL] intermediate item.list */
+#define GCCU_CMD_ADD 4     /* [ADD] (fs_add_drv): class iblk_out of item.list =
+                              (reset ? 0 : itself) + fac * class iblk_in of list_in; with
+                              tra_in or tra_out the transposed add (gccu_add_block_transp) */
+#define GCCU_CMD_CONTR 5   /* [CONTR] (fs_contr_drv): gccu_contract(&bc, fac, update, use_tr) */
+#define GCCU_CMD_REORDER 6 /* [REORDER] (fs_reo_drv): gccu_reorder(&reo, fac, sign_reo, update) */
+typedef struct gccu_formula_item {
+  int64_t command;
+  int64_t list;
+  int64_t init, s2;
+  int64_t list_in, iblk_in, iblk_out, reset, tra_in, tra_out;
+  int64_t update, use_tr, sign_reo;
+  double fac;
+  gccu_bc_desc bc;
+  gccu_reo_desc reo;
+} gccu_formula_item;
+/* an ME list without memory of its own (an intermediate of a formula) */
+int gccu_register_intermediate(int64_t op_id, int64_t gamt, int64_t mst, int64_t absym,
+                               int64_t* list_id, int64_t* len_op);
+int gccu_formula_define(const gccu_formula_item* items, int64_t n, int64_t* formula_id);
+/* runs the items in order on the engine's stream.  xret (may be NULL: then
+ * nothing is read back and the run may be captured in a graph): per
+ * [INIT TARGET] item, in order, the target's value after its last item --
+ * the element of a one-element list, else the list's 2-norm (frm_sched2's
+ * xret); nxret must be at least the number of targets */
+int gccu_formula_run(int64_t formula_id, double* xret, int64_t nxret);
+/* info4: arena bytes, bytes of the intermediates one by one, targets, items */
+int gccu_formula_info(int64_t formula_id, int64_t* info4);
+/* byte offset of an intermediate in its formula's arena, -1 before its formula is defined */
+int gccu_intermediate_offset(int64_t list_id, int64_t* offset);
+
 /* ---- preconditioner ------------------------------------------------------
  * replaces: diavc (baserout/diavc.f:31-35) on whole lists:
  * out = fac*in/(diag+shift), |diag+shift| <= 1e-10 -> 1e-10 */
