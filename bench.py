@@ -52,14 +52,14 @@ ROOFLINE_CONTRACTION = "r2_ladder"
 # DRAM traffic of the roofline launch per algorithmic byte (operands read
 # once at 8 bytes per element, FP64 or split TF32 hi + lo, plus the result's
 # read-modify-write), measured by ncu on the same launch at the reduced size
-# o12/v100 (profiles/k_gemm_tc_ladder_ccsd_o12v100.md,
-# profiles/k_gemm_ladder_ccsd_o12v100.md: 1.2436 GB and 1.2470 GB against
-# 1.2423 GB of algorithmic bytes); the full-size traffic is this ratio times
-# the full-size algorithmic bytes
+# o12/v100 (dram__bytes_read.sum + dram__bytes_write.sum of k_gemm_tc and of
+# k_gemm<128,64>: 1.2436 GB and 1.2470 GB against 1.2423 GB of algorithmic
+# bytes); the full-size traffic is this ratio times the full-size
+# algorithmic bytes
 TRAFFIC_PER_ALGORITHMIC_BYTE = {"k_gemm_tc": 1.2436 / 1.2423, "k_gemm": 1.2470 / 1.2423,
                                 # four int8 slices (4 bytes per operand element):
-                                # profiles/k_gemm_i8_4slices_ladder_ccsd_o12v100.md,
-                                # 0.6385 GB against 0.6379 GB
+                                # k_gemm_i8<4,128> at o12/v100, 0.6385 GB
+                                # against 0.6379 GB
                                 "k_gemm_i8_4": 0.6385 / 0.6379}
 
 SIGMA_SPEC = 0.05
