@@ -314,7 +314,7 @@ class CCSolver:
             if i == 0 or self.formula[i - 1]["res"][0] != res:
                 proj = self.spin_project and res in self.res.values() and last_seg[res] == i
                 items.append(gccu.FormulaItem(command=gccu.CMD_TARGET, list=self.lid(res),
-                                              s2=0 if proj else -1))
+                                              mult=1 if proj else 0))
             if it["kind"] == "ADD":
                 (lo, bo), (li, bi) = self.blk(it["res"]), self.blk(it["src"])
                 items.append(gccu.FormulaItem(command=gccu.CMD_ADD, list=lo, iblk_out=bo,

@@ -2751,7 +2751,8 @@ int gccu_formula_define(const gccu_formula_item* items, int64_t n, int64_t* form
       }
       switch (it.command) {
         case GCCU_CMD_TARGET:
-          GCCU_REQUIRE(it.s2 >= -1, "formula: s2 of a target is -1 or 2S");
+          GCCU_REQUIRE(it.mult == 0 || it.mult == 1,
+                       "formula: a target is projected onto the singlet (mult 1) or not (0)");
           ++F.ntargets;
           break;
         case GCCU_CMD_NEW:
@@ -2826,10 +2827,10 @@ int gccu_formula_run(int64_t formula_id, double* xret, int64_t nxret) {
     GCCU_REQUIRE(!xret || nxret >= F.ntargets,
                  "formula: xret is shorter than the number of targets");
     GCCU_REQUIRE(!xret || !e.capturing, "formula: xret must be NULL inside a graph capture");
-    int64_t target = 0, s2 = -1, ti = -1;
+    int64_t target = 0, mult = 0, ti = -1;
     auto end_target = [&] {
       if (!target) return;
-      if (s2 >= 0) check_rc(gccu_spin_prj_list(target, s2, nullptr));
+      if (mult > 0) check_rc(gccu_spin_prj_list(target, mult - 1, nullptr));
       if (!xret) return;
       DevList& l = e.list(target);
       if (l.L.len == 1) {
@@ -2847,7 +2848,7 @@ int gccu_formula_run(int64_t formula_id, double* xret, int64_t nxret) {
         case GCCU_CMD_TARGET:
           end_target();
           target = it.list;
-          s2 = it.s2;
+          mult = it.mult;
           ++ti;
           if (it.init) check_rc(gccu_zero_list(it.list));
           break;

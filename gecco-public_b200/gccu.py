@@ -41,7 +41,7 @@ CMD_TARGET, CMD_NEW, CMD_DEL, CMD_ADD, CMD_CONTR, CMD_REORDER = 1, 2, 3, 4, 5, 6
 
 
 class FormulaItem(ctypes.Structure):
-    _fields_ = [("command", I64), ("list", I64), ("init", I64), ("s2", I64), ("list_in", I64),
+    _fields_ = [("command", I64), ("list", I64), ("init", I64), ("mult", I64), ("list_in", I64),
                 ("iblk_in", I64), ("iblk_out", I64), ("reset", I64), ("tra_in", I64),
                 ("tra_out", I64), ("update", I64), ("use_tr", I64), ("sign_reo", I64),
                 ("fac", ctypes.c_double), ("bc", BcDesc), ("reo", ReoDesc)]

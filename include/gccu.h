@@ -272,8 +272,9 @@ int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk);
  * between its [NEW] and its [DEL] (or the end of the formula); outside a run
  * of that formula its contents are undefined. */
 #define GCCU_CMD_TARGET 1  /* [INIT TARGET]: item.list becomes the target; init != 0 zeroes
-                              it; s2 >= 0: at the target's end the list is projected onto
-                              spin s2 (spin_prj_list, frm_sched2.f:146-149), s2 = -1: not */
+                              it; mult = 2S+1 of the spin the list is projected onto at the
+                              target's end (spin_prj_list for me_res%s2 = mult-1 >= 0,
+                              frm_sched2.f:146-149): 1 = singlet, the only one; 0 = none */
 #define GCCU_CMD_NEW 2     /* [NEW] intermediate item.list */
 #define GCCU_CMD_DEL 3     /* [DEL] intermediate item.list */
 #define GCCU_CMD_ADD 4     /* [ADD] (fs_add_drv): class iblk_out of item.list =
@@ -284,7 +285,7 @@ int gccu_spin_prj_list(int64_t list_id, int64_t s2, double* xnorm2_blk);
 typedef struct gccu_formula_item {
   int64_t command;
   int64_t list;
-  int64_t init, s2;
+  int64_t init, mult;
   int64_t list_in, iblk_in, iblk_out, reset, tra_in, tra_out;
   int64_t update, use_tr, sign_reo;
   double fac;

@@ -22,12 +22,12 @@ def host_engine(built):
 
 
 def _item(cmd, lst, **kw):
-    return gccu.FormulaItem(command=cmd, list=lst, s2=kw.pop("s2", -1), **kw)
+    return gccu.FormulaItem(command=cmd, list=lst, **kw)
 
 
 def _add(out, src, fac=1.0, reset=1):
     return gccu.FormulaItem(command=gccu.CMD_ADD, list=out, iblk_out=1, list_in=src, iblk_in=1,
-                            fac=fac, reset=reset, s2=-1)
+                            fac=fac, reset=reset)
 
 
 def test_arena_reuses_the_ranges_of_deleted_intermediates(host_engine):
