@@ -473,21 +473,45 @@ class Engine {
   // by the autotuner, released afterwards)
   std::vector<std::pair<void*, size_t>>* track = nullptr;
 
+  // Device memory.  Requests up to kSlabSmall bytes (plan tables and
+  // descriptors, hundreds per formula) are cut from kSlabBytes slabs, 256-byte
+  // aligned, and never handed out again; larger ones get their own
+  // cudaMalloc.  One cudaMalloc per plan table would cost 0.2-0.7 ms each.
+  static constexpr size_t kSlabBytes = size_t(16) << 20, kSlabSmall = size_t(1) << 20;
+  char* slab = nullptr;
+  size_t slab_used = kSlabBytes;
   void* alloc(size_t bytes) {
     GCCU_REQUIRE(!host_only, "engine was initialised without a device (host-only mode)");
     GCCU_REQUIRE(!capturing, "device allocation requested while capturing a CUDA graph");
     if (memmax > 0 && mem_used + (int64_t)bytes > memmax)
       throw Error("device memory cap (memmax) exceeded");
+    const size_t rounded = (std::max<size_t>(bytes, 16) + 255) / 256 * 256;
     void* p = nullptr;
-    const auto t0 = std::chrono::steady_clock::now();
-    CUDA_OK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
-    pstats.alloc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    allocs.push_back(p);
+    if (rounded <= kSlabSmall) {
+      if (slab_used + rounded > kSlabBytes) {
+        slab = (char*)device_malloc(kSlabBytes);
+        slab_used = 0;
+      }
+      p = slab + slab_used;
+      slab_used += rounded;
+    } else {
+      p = device_malloc(rounded);
+    }
     if (track) track->push_back({p, bytes});
     mem_used += (int64_t)bytes;
     return p;
   }
+  void* device_malloc(size_t bytes) {
+    void* p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    CUDA_OK(cudaMalloc(&p, bytes));
+    pstats.alloc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    allocs.push_back(p);
+    return p;
+  }
+  // frees an allocation of its own; a slab piece is only taken off the count
   void release(void* p, size_t bytes) {
+    mem_used -= (int64_t)bytes;
     for (size_t i = 0; i < allocs.size(); ++i)
       if (allocs[i] == p) {
         allocs.erase(allocs.begin() + (long)i);
@@ -495,7 +519,6 @@ class Engine {
         CUDA_OK(cudaFree(p));
         pstats.alloc_s +=
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        mem_used -= (int64_t)bytes;
         return;
       }
   }
