@@ -322,7 +322,8 @@ class Engine {
   std::map<int64_t, std::unique_ptr<DevSpinPrj>> spinprjs;  // singlet projection per list
   std::vector<FormulaPlan> formulas;  // gccu_formula_define
   std::map<std::string, std::unique_ptr<DevPlan>> plans;
-  std::vector<void*> allocs;
+  std::vector<void*> allocs;  // cudaMalloc'd one per request, freed by release()
+  std::vector<void*> slabs;   // bases of the slabs small requests are cut from
   double* d_red = nullptr;  // reduction scalars
   double stats[8] = {};
   int64_t launches = 0;
@@ -447,6 +448,7 @@ class Engine {
         for (auto ev : pr) cudaEventDestroy(ev);
     if (stream) cudaStreamSynchronize(stream);
     for (void* p : allocs) cudaFree(p);
+    for (void* p : slabs) cudaFree(p);
     if (tabs_host) cudaFreeHost(tabs_host);
     if (ustream) cudaStreamDestroy(ustream);
     if (stream) cudaStreamDestroy(stream);
@@ -489,27 +491,30 @@ class Engine {
     void* p = nullptr;
     if (rounded <= kSlabSmall) {
       if (slab_used + rounded > kSlabBytes) {
-        slab = (char*)device_malloc(kSlabBytes);
+        // slab bases are kept apart from allocs: the first piece of a slab has
+        // the slab's address, and release() must not free the slab with it
+        slab = (char*)device_malloc(kSlabBytes, slabs);
         slab_used = 0;
       }
       p = slab + slab_used;
       slab_used += rounded;
     } else {
-      p = device_malloc(rounded);
+      p = device_malloc(rounded, allocs);
     }
     if (track) track->push_back({p, bytes});
     mem_used += (int64_t)bytes;
     return p;
   }
-  void* device_malloc(size_t bytes) {
+  void* device_malloc(size_t bytes, std::vector<void*>& owner) {
     void* p = nullptr;
     const auto t0 = std::chrono::steady_clock::now();
     CUDA_OK(cudaMalloc(&p, bytes));
     pstats.alloc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    allocs.push_back(p);
+    owner.push_back(p);
     return p;
   }
-  // frees an allocation of its own; a slab piece is only taken off the count
+  // frees an allocation of its own (found in allocs); a slab piece is never
+  // in allocs and is only taken off the count
   void release(void* p, size_t bytes) {
     mem_used -= (int64_t)bytes;
     for (size_t i = 0; i < allocs.size(); ++i)
