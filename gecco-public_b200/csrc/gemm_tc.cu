@@ -127,7 +127,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
                : "memory");
 }
 
-// bulk asynchronous copy global -> shared (no multicast), counted on bar
+// bulk asynchronous copy global -> this CTA's shared memory, counted on bar
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
                                          uint32_t bar) {
   asm volatile(
