@@ -47,7 +47,7 @@ def test_layout_matches_oracle(host_engine, space):
             assert np.array_equal(o.dists(lo), host_engine.dists(le))
 
 
-@pytest.mark.parametrize("space", ["c1_small", "c2v", "d2h"])
+@pytest.mark.parametrize("space", list(SPACES))
 def test_plan_matches_oracle_enumeration(host_engine, space):
     # the planner's block contractions, counted in the reference's dgemm
     # accounting, equal the blocks the oracle enumerates (random, unscreened data)
@@ -63,7 +63,7 @@ def test_plan_matches_oracle_enumeration(host_engine, space):
         assert np.array_equal(st, sto), (name, st, sto)
 
 
-@pytest.mark.parametrize("space", ["c1_small", "c2v", "d2h"])
+@pytest.mark.parametrize("space", list(SPACES))
 def test_plan_items_agree_with_plan_info(host_engine, space):
     # gccu_plan_items lists the same block contractions gccu_plan_info counts;
     # their 2*M*N*K sums to the reference's dgemm flop accounting, and the
