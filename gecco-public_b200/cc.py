@@ -5,8 +5,9 @@ The reference generates its CC equations as formula files (lists of [ADD] /
 them with frm_sched2 (contract/frm_sched2.f:117-365) inside solve_nleq
 (solve/solve_nleq.f:377-787).  Formula generation is outside the engine's
 scope; the formulas below are closed-shell spin-orbital CCSD (the
-Stanton-Gauss intermediates, J. Chem. Phys. 94, 4334 (1991)) and MP2 written
-directly as binary contractions in the reference's occupation language.
+Stanton-Gauss intermediates, J. Chem. Phys. 94, 4334 (1991)), MP2, and CCSDT
+(the connected expansion of e^-T H e^T term by term) written directly as
+binary contractions in the reference's occupation language.
 Each [CONTR] factor is the product of the topological sign and the
 combinatorial factor of that contraction (what the reference stores as
 binary_contr%fact); tests/test_cc_formula.py checks every item against its
@@ -126,6 +127,222 @@ CCSD_FORMULA = [
 ]
 
 
+# ---- CCSDT (maxexc = 3) ----------------------------------------------------------
+# The residuals R_mu = <mu| (H e^T)_c |0> for mu up to triples and the energy
+# E = <0| (H e^T)_c |0>, T = T1 + T2 + T3, written term by term as chains of
+# binary contractions: a class of F or V, then T_n1, T_n2, ... attached one
+# [CONTR] at a time, attachment (n, h, p) contracting h hole creators and p
+# particle annihilators of the Hamiltonian class with T_n (T's lines can only
+# meet the Hamiltonian's).  The T's commute, so each term is listed once, with
+# its attachments in non-decreasing (n, h, p) order.  A term's factor is its
+# topological sign (CCSDT_SIGNS) over the product of m! for every group of m
+# identical attachments; the intermediates of a chain are formed with factor 1
+# and its last contraction carries the factor.  The signs are those of the
+# engine's string-contraction convention; they were read off by matching
+# each term's contribution to the Fock-space expansion on two small spaces
+# (every factor came out as +-1 over the m! product).  Unfactorised (no shared
+# dressed intermediates beyond common chain prefixes): the terms are those of
+# the reference's CC maxexc=3 equations; tests/test_ccsdt_formula.py checks
+# each residual and the energy against <mu| e^-T H e^T |0> evaluated in the
+# full Fock space of a few spin orbitals, with a non-canonical Fock matrix.
+
+FOCK_CLASSES = {"HH": HH, "HP": HP, "PH": PH, "PP": PP}
+V_CLASSES = {"HHHH": HHHH, "HHPH": HHPH, "HHPP": HHPP, "PHHH": PHHH, "PHPH": PHPH,
+             "PHPP": PHPP, "PPHH": PPHH, "PPPH": PPPH, "PPPP": PPPP}
+PPPHHH = occ8({P: 3}, {H: 3})
+T_CLASSES = {1: PH, 2: PPHH, 3: PPPHHH}
+
+
+def attach(x, n, h, p):
+    """(ex1, ex2, cnt, result) of contracting h hole creators and p particle
+    annihilators of class x with T_n"""
+    c = np.asarray(cnt({H: h} if h else None, {P: p} if p else None))
+    ex1 = np.asarray(x) - c
+    ex2 = np.asarray(T_CLASSES[n]) - np.concatenate([c[4:], c[:4]])
+    return ex1, ex2, c, ex1 + ex2
+
+
+def excitation_terms(maxexc):
+    """every connected term of <mu| (H e^T)_c |0>, rank(mu) <= maxexc (0 =
+    the energy), T up to T_maxexc: [(list, class, attachments, rank)]"""
+    terms = []
+
+    def rec(name, key, x, steps):
+        if x[0] == 0 and x[5] == 0:  # no hole creator, no particle annihilator left
+            if x[1] == x[4] <= maxexc:
+                terms.append((name, key, tuple(steps), int(x[1])))
+            return
+        last = steps[-1] if steps else (0, 0, 0)
+        for n in range(1, maxexc + 1):
+            for h in range(min(x[0], n) + 1):
+                for p in range(min(x[5], n) + 1):
+                    if h + p == 0 or (n, h, p) < last:
+                        continue
+                    y = attach(x, n, h, p)[3]
+                    if y[1] <= maxexc and y[4] <= maxexc:
+                        rec(name, key, y, steps + [(n, h, p)])
+
+    for key, occ in FOCK_CLASSES.items():
+        rec("F", key, np.asarray(occ), [])
+    for key, occ in V_CLASSES.items():
+        rec("V", key, np.asarray(occ), [])
+    return terms
+
+
+def term_factor(steps, sign):
+    """topological sign over the product of m! of identical attachments"""
+    from math import factorial
+    den = 1
+    for st in set(steps):
+        den *= factorial(steps.count(st))
+    return sign / den
+
+
+def excitation_formula(maxexc, signs):
+    """operators and [ADD]/[CONTR] items of the residuals and the energy;
+    the first item writing a result list overwrites it"""
+    ops = {"F": FOCK_BLOCKS, "V": V_BLOCKS, "E": [SCAL]}
+    for n in range(1, maxexc + 1):
+        ops[f"T{n}"] = [T_CLASSES[n]]
+        ops[f"R{n}"] = [T_CLASSES[n]]
+    items, inter, written = [], {}, set()
+    for name, key, steps, rank in excitation_terms(maxexc):
+        fac = term_factor(steps, signs[(name, key, steps)])
+        x = np.asarray((FOCK_CLASSES if name == "F" else V_CLASSES)[key])
+        res = "E" if rank == 0 else f"R{rank}"
+        rocc = SCAL if rank == 0 else T_CLASSES[rank]
+        label = name + key + "".join(f"_{n}{h}{p}" for n, h, p in steps)
+        if not steps:
+            items.append(_A((res, rocc), (name, x), fac, res not in written, label))
+            written.add(res)
+            continue
+        src = (name, x)
+        for k, (n, h, p) in enumerate(steps):
+            c, y = attach(x, n, h, p)[2:]
+            if k == len(steps) - 1:
+                items.append(_C((res, rocc), src, (f"T{n}", T_CLASSES[n]), c, fac,
+                                res in written, label))
+                written.add(res)
+            else:
+                prefix = (name, key, steps[:k + 1])
+                if prefix not in inter:
+                    inter[prefix] = f"X{len(inter) + 1}"
+                    ops[inter[prefix]] = [y]
+                    items.append(_C((inter[prefix], y), src, (f"T{n}", T_CLASSES[n]), c, 1.0,
+                                    False, label[:len(name + key)] + "".join(
+                                        f"_{a}{b}{d}" for a, b, d in steps[:k + 1])))
+                src = (inter[prefix], y)
+            x = y
+    return ops, items
+
+
+# topological signs of the CCSDT terms, keyed by (list, class, attachments)
+CCSDT_SIGNS = {
+    ("F", "HH", ((1, 1, 0),)): -1,
+    ("F", "HH", ((2, 1, 0),)): +1,
+    ("F", "HH", ((3, 1, 0),)): -1,
+    ("F", "HP", ((1, 0, 1), (1, 1, 0))): -1,
+    ("F", "HP", ((1, 0, 1), (2, 1, 0))): +1,
+    ("F", "HP", ((1, 0, 1), (3, 1, 0))): -1,
+    ("F", "HP", ((1, 1, 0), (2, 0, 1))): -1,
+    ("F", "HP", ((1, 1, 0), (3, 0, 1))): -1,
+    ("F", "HP", ((1, 1, 1),)): +1,
+    ("F", "HP", ((2, 0, 1), (2, 1, 0))): +1,
+    ("F", "HP", ((2, 1, 1),)): +1,
+    ("F", "HP", ((3, 1, 1),)): +1,
+    ("F", "PH", ()): +1,
+    ("F", "PP", ((1, 0, 1),)): +1,
+    ("F", "PP", ((2, 0, 1),)): +1,
+    ("F", "PP", ((3, 0, 1),)): +1,
+    ("V", "HHHH", ((1, 1, 0), (1, 1, 0))): +1,
+    ("V", "HHHH", ((1, 1, 0), (2, 1, 0))): +1,
+    ("V", "HHHH", ((2, 2, 0),)): +1,
+    ("V", "HHHH", ((3, 2, 0),)): +1,
+    ("V", "HHPH", ((1, 0, 1), (1, 1, 0), (1, 1, 0))): +1,
+    ("V", "HHPH", ((1, 0, 1), (1, 1, 0), (2, 1, 0))): +1,
+    ("V", "HHPH", ((1, 0, 1), (2, 2, 0))): +1,
+    ("V", "HHPH", ((1, 0, 1), (3, 2, 0))): +1,
+    ("V", "HHPH", ((1, 1, 0), (1, 1, 0), (2, 0, 1))): -1,
+    ("V", "HHPH", ((1, 1, 0), (1, 1, 1))): +1,
+    ("V", "HHPH", ((1, 1, 0), (2, 1, 1))): -1,
+    ("V", "HHPH", ((1, 1, 0), (3, 1, 1))): +1,
+    ("V", "HHPH", ((1, 1, 1), (2, 1, 0))): +1,
+    ("V", "HHPH", ((1, 1, 1), (3, 1, 0))): -1,
+    ("V", "HHPH", ((2, 0, 1), (2, 2, 0))): -1,
+    ("V", "HHPH", ((2, 1, 0), (2, 1, 1))): -1,
+    ("V", "HHPH", ((2, 2, 1),)): -1,
+    ("V", "HHPH", ((3, 2, 1),)): +1,
+    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0), (1, 1, 0))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0), (2, 1, 0))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (2, 2, 0))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (3, 2, 0))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (1, 1, 0), (2, 0, 1))): +1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (1, 1, 1))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (2, 1, 1))): +1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (3, 1, 1))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 1), (2, 1, 0))): -1,
+    ("V", "HHPP", ((1, 0, 1), (1, 1, 1), (3, 1, 0))): +1,
+    ("V", "HHPP", ((1, 0, 1), (2, 0, 1), (2, 2, 0))): +1,
+    ("V", "HHPP", ((1, 0, 1), (2, 1, 0), (2, 1, 1))): +1,
+    ("V", "HHPP", ((1, 0, 1), (2, 2, 1))): +1,
+    ("V", "HHPP", ((1, 0, 1), (3, 2, 1))): -1,
+    ("V", "HHPP", ((1, 1, 0), (1, 1, 0), (2, 0, 2))): +1,
+    ("V", "HHPP", ((1, 1, 0), (1, 1, 0), (3, 0, 2))): +1,
+    ("V", "HHPP", ((1, 1, 0), (1, 1, 1), (2, 0, 1))): +1,
+    ("V", "HHPP", ((1, 1, 0), (1, 1, 1), (3, 0, 1))): +1,
+    ("V", "HHPP", ((1, 1, 0), (2, 0, 1), (2, 1, 1))): -1,
+    ("V", "HHPP", ((1, 1, 0), (2, 0, 2), (2, 1, 0))): +1,
+    ("V", "HHPP", ((1, 1, 0), (2, 1, 2))): +1,
+    ("V", "HHPP", ((1, 1, 0), (3, 1, 2))): +1,
+    ("V", "HHPP", ((1, 1, 1), (1, 1, 1))): +1,
+    ("V", "HHPP", ((1, 1, 1), (2, 0, 1), (2, 1, 0))): +1,
+    ("V", "HHPP", ((1, 1, 1), (2, 1, 1))): +1,
+    ("V", "HHPP", ((1, 1, 1), (3, 1, 1))): +1,
+    ("V", "HHPP", ((2, 0, 1), (2, 2, 1))): -1,
+    ("V", "HHPP", ((2, 0, 1), (3, 2, 1))): -1,
+    ("V", "HHPP", ((2, 0, 2), (2, 2, 0))): +1,
+    ("V", "HHPP", ((2, 0, 2), (3, 2, 0))): +1,
+    ("V", "HHPP", ((2, 1, 0), (2, 1, 2))): +1,
+    ("V", "HHPP", ((2, 1, 0), (3, 1, 2))): -1,
+    ("V", "HHPP", ((2, 1, 1), (2, 1, 1))): -1,
+    ("V", "HHPP", ((2, 1, 1), (3, 1, 1))): +1,
+    ("V", "HHPP", ((2, 1, 2), (3, 1, 0))): -1,
+    ("V", "HHPP", ((2, 2, 0), (3, 0, 2))): +1,
+    ("V", "HHPP", ((2, 2, 1), (3, 0, 1))): -1,
+    ("V", "HHPP", ((2, 2, 2),)): +1,
+    ("V", "HHPP", ((3, 2, 2),)): +1,
+    ("V", "PHHH", ((1, 1, 0),)): -1,
+    ("V", "PHHH", ((2, 1, 0),)): -1,
+    ("V", "PHPH", ((1, 0, 1), (1, 1, 0))): -1,
+    ("V", "PHPH", ((1, 0, 1), (2, 1, 0))): -1,
+    ("V", "PHPH", ((1, 1, 0), (2, 0, 1))): +1,
+    ("V", "PHPH", ((1, 1, 1),)): -1,
+    ("V", "PHPH", ((2, 1, 1),)): +1,
+    ("V", "PHPH", ((3, 1, 1),)): -1,
+    ("V", "PHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0))): +1,
+    ("V", "PHPP", ((1, 0, 1), (1, 0, 1), (2, 1, 0))): +1,
+    ("V", "PHPP", ((1, 0, 1), (1, 1, 0), (2, 0, 1))): -1,
+    ("V", "PHPP", ((1, 0, 1), (1, 1, 1))): +1,
+    ("V", "PHPP", ((1, 0, 1), (2, 1, 1))): -1,
+    ("V", "PHPP", ((1, 0, 1), (3, 1, 1))): +1,
+    ("V", "PHPP", ((1, 1, 0), (2, 0, 2))): -1,
+    ("V", "PHPP", ((1, 1, 0), (3, 0, 2))): -1,
+    ("V", "PHPP", ((1, 1, 1), (2, 0, 1))): -1,
+    ("V", "PHPP", ((1, 1, 1), (3, 0, 1))): -1,
+    ("V", "PHPP", ((2, 0, 1), (2, 1, 1))): +1,
+    ("V", "PHPP", ((2, 0, 2), (2, 1, 0))): -1,
+    ("V", "PHPP", ((2, 1, 2),)): -1,
+    ("V", "PHPP", ((3, 1, 2),)): -1,
+    ("V", "PPHH", ()): +1,
+    ("V", "PPPH", ((1, 0, 1),)): +1,
+    ("V", "PPPH", ((2, 0, 1),)): -1,
+    ("V", "PPPP", ((1, 0, 1), (1, 0, 1))): -1,
+    ("V", "PPPP", ((1, 0, 1), (2, 0, 1))): +1,
+    ("V", "PPPP", ((2, 0, 2),)): +1,
+    ("V", "PPPP", ((3, 0, 2),)): +1,
+}
+
+
 # ---- filling the Hamiltonian lists -------------------------------------------
 
 def _axis_types(occ):
@@ -230,7 +447,7 @@ class CCSolver:
 
     # lists that hold the Hamiltonian, amplitudes, residuals and the energy;
     # the others of a formula are its intermediates
-    PERSISTENT = ("F", "V", "T1", "T2", "R1", "R2", "E")
+    PERSISTENT = ("F", "V", "T1", "T2", "T3", "R1", "R2", "R3", "E")
 
     def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
                  learned=None, shard=None, spin_project=False, native_formula=False):
@@ -258,8 +475,11 @@ class CCSolver:
         sp = ints.space
         self.nsym = sp.nsym
         engine.register_orbinfo(sp.nsym, sp.norb)
-        ops = MP2_OPERATORS if method == "mp2" else CCSD_OPERATORS
-        self.formula = MP2_FORMULA if method == "mp2" else CCSD_FORMULA
+        if method == "ccsdt":
+            ops, self.formula = excitation_formula(3, CCSDT_SIGNS)
+        else:
+            ops = MP2_OPERATORS if method == "mp2" else CCSD_OPERATORS
+            self.formula = MP2_FORMULA if method == "mp2" else CCSD_FORMULA
         self.lists = {}
         for name, blocks in ops.items():
             opid = engine.define_operator(blocks)
@@ -271,8 +491,8 @@ class CCSolver:
             else:
                 lid, n = engine.register_list(opid, absym=absym)
             self.lists[name] = (lid, n, blocks)
-        self.amps = ["T2"] if method == "mp2" else ["T1", "T2"]
-        self.res = {"T1": "R1", "T2": "R2"}
+        self.amps = {"mp2": ["T2"], "ccsdt": ["T1", "T2", "T3"]}.get(method, ["T1", "T2"])
+        self.res = {"T1": "R1", "T2": "R2", "T3": "R3"}
         # denominators, steps (the last one kept for the learned step's
         # inputs) and DIIS subspace
         for a in self.amps:

@@ -1,0 +1,87 @@
+"""CCSDT (the reference's CC maxexc=3, test/CC-energy-I.inp) as chains of
+binary contractions (cc.excitation_formula with cc.CCSDT_SIGNS) on the CPU
+oracle, against <mu| e^-T H e^T |0> evaluated in the full Fock space of ten
+spin orbitals with a non-canonical Fock matrix, so that every term of the
+formula contributes; and a CCSDT solve, whose converged amplitudes make the
+Fock-space residuals vanish and whose energy lies closer to the full CI
+energy than the CCSD one."""
+import numpy as np
+import pytest
+
+import cc
+import dense_cc
+import hamiltonian as hm
+from engine import OracleEngine
+from fock_cc import FockSpace, non_canonical_fock, random_amplitudes
+
+
+def _system(no, nv, seed, method="ccsdt"):
+    sp, eps, B = hm.synthetic(no, nv, 12, seed=seed)
+    ints = hm.FactorizedIntegrals(sp, eps, B)
+    dense = hm.DenseIntegrals(sp, np.diag(eps), ints.dense_eri())
+    F, W, nso = dense_cc.spin_orbital(sp, dense.f, dense.eri_elems)
+    s = cc.CCSolver(OracleEngine(route=3), ints, method=method)
+    s.load_hamiltonian()
+    return s, F, W, nso
+
+
+def _set_fock(s, F, nso):
+    o, v = slice(0, nso), slice(nso, F.shape[0])
+    s.freeze_hamiltonian(False)
+    s.e.upload(s.lid("F"), s.view("F").from_dense(
+        {1: F[o, o], 2: F[o, v], 3: F[v, o], 4: F[v, v]}, s.lists["F"][1]))
+    s.freeze_hamiltonian(True)
+
+
+def _dense(s, name, shape):
+    x = s.e.download(s.lid(name), s.lists[name][1])
+    return s.view(name).to_dense(x, 1, shape)
+
+
+def test_terms_and_signs_agree():
+    terms = cc.excitation_terms(3)
+    assert len(terms) == len(cc.CCSDT_SIGNS) == 102
+    assert {t[:3] for t in terms} == set(cc.CCSDT_SIGNS)
+    # the CCSD subset: T up to T2 and residuals up to doubles
+    assert len(cc.excitation_terms(2)) == 48
+
+
+@pytest.mark.parametrize("no,nv,seed", [(3, 2, 21), (2, 3, 22)])
+def test_ccsdt_residuals_match_fock_space(built, no, nv, seed):
+    s, F, W, nso = _system(no, nv, seed)
+    rng = np.random.default_rng(seed)
+    F = non_canonical_fock(F, nso, rng)
+    _set_fock(s, F, nso)
+    nvo = F.shape[0] - nso
+    amps = {r: random_amplitudes(r, nvo, nso, rng) for r in (1, 2, 3)}
+    for r, t in amps.items():
+        s.e.upload(s.lid(f"T{r}"), s.view(f"T{r}").from_dense({1: t}, s.lists[f"T{r}"][1]))
+    s.evaluate()
+    ref = FockSpace(F, W, nso).residuals(amps, 3)
+    assert abs(s.energy() - ref[0]) < 1e-13
+    for r in (1, 2, 3):
+        got = _dense(s, f"R{r}", ref[r].shape)
+        assert np.abs(ref[r]).max() > 1e-3
+        assert np.abs(got - ref[r]).max() < 1e-12 * np.abs(ref[r]).max(), r
+
+
+def test_ccsdt_solve_zeroes_the_fock_space_residuals():
+    s, F, W, nso = _system(2, 2, 23)
+    e = s.solve(maxiter=80, conv=1e-11)
+    assert s.history[-1][2] < 1e-11
+    nvo = F.shape[0] - nso
+    amps = {r: _dense(s, f"T{r}", (nvo,) * r + (nso,) * r) for r in (1, 2, 3)}
+    assert np.abs(amps[3]).max() > 1e-6
+    fs = FockSpace(F, W, nso)
+    ref = fs.residuals(amps, 3)
+    assert abs(e - ref[0]) < 1e-12
+    for r in (1, 2, 3):
+        assert np.abs(ref[r]).max() < 1e-9, r
+    # full CI in the sector of the reference's electron count
+    dim = 1 << fs.n
+    sector = [d for d in range(dim) if bin(d).count("1") == nso]
+    Hs = fs.H[sector][:, sector].toarray()
+    e_fci = np.linalg.eigvalsh(Hs)[0] - fs.H[fs.ref, fs.ref]
+    s2, _, _, _ = _system(2, 2, 23, method="ccsd")
+    e_ccsd = s2.solve(maxiter=80, conv=1e-11)
+    assert abs(e - e_fci) < abs(e_ccsd - e_fci)
