@@ -85,3 +85,26 @@ def test_ccsdt_solve_zeroes_the_fock_space_residuals():
     s2, _, _, _ = _system(2, 2, 23, method="ccsd")
     e_ccsd = s2.solve(maxiter=80, conv=1e-11)
     assert abs(e - e_fci) < abs(e_ccsd - e_fci)
+
+
+def test_ccsdt_formula_plans_on_the_product_engine(built):
+    # every [CONTR] of the formula passes the product planner's checks
+    # (host-only engine, no device) on a C2v space
+    import gccu
+    sp, eps, B = hm.synthetic(3, 6, 12, seed=24, nsym=4)
+    e = gccu.Engine(-1)
+    try:
+        s = cc.CCSolver(e, hm.FactorizedIntegrals(sp, eps, B), method="ccsdt")
+        nitems = 0
+        for it in s.formula:
+            if it["kind"] != "CONTR":
+                continue
+            c = np.asarray(it["cnt"])
+            ex1 = np.asarray(it["op1"][1]) - c
+            ex2 = np.asarray(it["op2"][1]) - np.concatenate([c[4:], c[:4]])
+            n, st = e.plan_info(s.blk(it["op1"]), s.blk(it["op2"]), s.blk(it["res"]), ex1, ex2,
+                                c)
+            nitems += n
+        assert nitems > 0
+    finally:
+        e.close()
