@@ -15,14 +15,22 @@ from engine import OracleEngine
 from fock_cc import FockSpace, non_canonical_fock, random_amplitudes
 
 
-def _system(no, nv, seed, method="ccsdt"):
-    sp, eps, B = hm.synthetic(no, nv, 12, seed=seed)
+def _system(no, nv, seed, method="ccsdt", nsym=1):
+    sp, eps, B = hm.synthetic(no, nv, 12, seed=seed, nsym=nsym)
     ints = hm.FactorizedIntegrals(sp, eps, B)
     dense = hm.DenseIntegrals(sp, np.diag(eps), ints.dense_eri())
     F, W, nso = dense_cc.spin_orbital(sp, dense.f, dense.eri_elems)
     s = cc.CCSolver(OracleEngine(route=3), ints, method=method)
     s.load_hamiltonian()
     return s, F, W, nso
+
+
+def _spin_orbital_irreps(s):
+    """0-based irrep of every spin orbital (holes, then particles), for the
+    direct product as XOR"""
+    sp = s.ints.space
+    orbs = np.concatenate([sp.hole, sp.part])
+    return np.asarray(sp.orbsym)[orbs[np.arange(2 * len(orbs)) // 2]] - 1
 
 
 def _set_fock(s, F, nso):
@@ -108,3 +116,33 @@ def test_ccsdt_formula_plans_on_the_product_engine(built):
         assert nitems > 0
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("no,nv,nsym,seed", [(2, 3, 4, 25), (3, 2, 2, 26)])
+def test_ccsdt_residuals_with_point_group_symmetry(built, no, nv, nsym, seed):
+    # symmetry-blocked lists (irreps round-robin over the orbitals): the
+    # formula's residuals equal the Fock-space ones for totally symmetric
+    # amplitudes and a totally symmetric non-canonical Fock matrix
+    s, F, W, nso = _system(no, nv, seed, nsym=nsym)
+    assert s.nsym == nsym
+    irr = _spin_orbital_irreps(s)
+    rng = np.random.default_rng(seed)
+    F = non_canonical_fock(F, nso, rng) * (irr[:, None] == irr[None, :])
+    _set_fock(s, F, nso)
+    nvo = F.shape[0] - nso
+    amps = {}
+    for r in (1, 2, 3):
+        t = random_amplitudes(r, nvo, nso, rng)
+        grids = np.meshgrid(*([irr[nso:]] * r + [irr[:nso]] * r), indexing="ij")
+        prod = np.zeros(t.shape, dtype=np.int64)
+        for g in grids:
+            prod ^= g
+        amps[r] = t * (prod == 0)
+        s.e.upload(s.lid(f"T{r}"), s.view(f"T{r}").from_dense({1: amps[r]}, s.lists[f"T{r}"][1]))
+    s.evaluate()
+    ref = FockSpace(F, W, nso).residuals(amps, 3)
+    assert abs(s.energy() - ref[0]) < 1e-13
+    for r in (1, 2, 3):
+        got = _dense(s, f"R{r}", ref[r].shape)
+        assert np.abs(ref[r]).max() > 1e-4, r
+        assert np.abs(got - ref[r]).max() < 1e-12 * np.abs(ref[r]).max(), r
