@@ -146,3 +146,27 @@ def test_ccsdt_residuals_with_point_group_symmetry(built, no, nv, nsym, seed):
         got = _dense(s, f"R{r}", ref[r].shape)
         assert np.abs(ref[r]).max() > 1e-4, r
         assert np.abs(got - ref[r]).max() < 1e-12 * np.abs(ref[r]).max(), r
+
+
+def test_ccsdt_lists_filled_through_the_device_path(built):
+    # the Hamiltonian and the T1..T3 denominators generated by torch (the
+    # device fill, here on the CPU) equal the host fill on a space of four
+    # irreps, and one evaluation from the same amplitudes agrees
+    from devfill import TorchIntegrals
+    sp, eps, B = hm.synthetic(3, 6, 12, seed=27, nsym=4)
+    ints = hm.FactorizedIntegrals(sp, eps, B)
+    host = cc.CCSolver(OracleEngine(route=3), ints, method="ccsdt")
+    host.load_hamiltonian()
+    dev = cc.CCSolver(OracleEngine(route=3), ints, method="ccsdt")
+    dev.load_hamiltonian_device(TorchIntegrals(sp, eps, B, device="cpu"))
+    for name in ("F", "V", "DT1", "DT2", "DT3"):
+        a, b = host.e.data[host.lid(name)], dev.e.data[dev.lid(name)]
+        assert a.size > 0 and np.max(np.abs(a - b)) <= 1e-13 * max(1.0, np.abs(a).max()), name
+    for s in (host, dev):
+        for r in (1, 2, 3):
+            n = s.lists[f"T{r}"][1]
+            s.e.upload(s.lid(f"T{r}"), 0.05 * np.random.default_rng(r).standard_normal(n))
+        s.evaluate()
+    for name in ("R1", "R2", "R3"):
+        a, b = host.e.data[host.lid(name)], dev.e.data[dev.lid(name)]
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.abs(a).max(), name
