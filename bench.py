@@ -15,7 +15,9 @@ modes measured in the same run; `use_tr` times the iteration with the
 spin-flip symmetry the reference uses by default; `spin_prj` times the
 singlet projection of the doubles residual against the HBM roofline;
 `convergence` gives the time to |dE| < 1 uEh of FP64 and the mixed solves at
-o24/v200 on a variant of the Hamiltonian whose CC iteration converges.
+o24/v200 on a variant of the Hamiltonian whose CC iteration converges;
+`d2h` times the CCSD iteration and `ccsdt` the CCSDT iteration (FP64, fixed
+tile rule) on the CCSDT configuration's workload (D2h, o6/v48, naux 300).
 
 --impl reference times the CPU restatement of the reference path (oracle/,
 route 3: gather, ILP64 OpenBLAS dgemm on all host cores, scatter) on the same
@@ -419,6 +421,8 @@ def run_gpu(args, cfg):
         side("convergence", lambda: convergence(local, CONFIGS[args.conv_config], weights,
                                                 maxiter=args.conv_maxiter))
         side("convergence_small", lambda: convergence(local, CONFIGS[0], weights))
+    if not args.no_ccsdt and world == 1:
+        side("ccsdt", lambda: measure_ccsdt(args, local))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -709,6 +713,44 @@ def measure_fixed_rule(args, cfg, local, mode):
     finally:
         eng.close()
         torch.cuda.empty_cache()
+
+
+def measure_ccsdt(args, local):
+    """the CCSDT iteration (cc.excitation_formula: the connected terms as 102
+    chains of binary contractions, 143 [CONTR] per evaluation) on the CCSDT
+    configuration's workload (D2h, o6/v48, naux 300) in FP64 with the fixed
+    tile rule: seconds per iteration, block contractions, flops and kernel
+    launches per iteration"""
+    import cc
+    import gccu
+    from devfill import TorchIntegrals
+    import hamiltonian as hm
+
+    cfg = CONFIGS[1]
+    sp, eps, B = setup_hamiltonian(cfg)
+    eng = gccu.Engine(local)
+    try:
+        eng.set_precision(0)
+        eng.set_tuning(0)
+        t0 = time.perf_counter()
+        s = cc.CCSolver(eng, hm.FactorizedIntegrals(sp, eps, B), method="ccsdt")
+        s.load_hamiltonian_device(TorchIntegrals(sp, eps, B))
+        steps = min(args.steps, 5)
+        r = measure(args, cfg, eng, s, local, None, 0, steps=steps, profile=True, e2e=False)
+        prof = r["prof"]
+        en = r["energies"][-1]
+        return {"workload": cfg["name"].replace("CCSD", "CCSDT", 1),
+                "method": "CCSDT, unfactorised connected terms",
+                "precision": "FP64", "tile_rule": "fixed", "value": r["ms"] / 1e3, "unit": "s",
+                "steps": steps, "contractions": len(r["names"]),
+                "block_contractions": int(np.sum(prof[:, 3])),
+                "gflop_per_iteration": float(np.sum(prof[:, 0])) / 1e9,
+                "launches_per_iteration": r["launches"] / max(steps, 1),
+                "energy_last": en if math.isfinite(en) else None,
+                "wall_s_with_planning": round(time.perf_counter() - t0, 2),
+                "clocks": clock_summary(r["samples"])}
+    finally:
+        eng.close()
 
 
 def measure_d2h(args, local):
@@ -1163,6 +1205,8 @@ def main():
                     help="skip the fixed-rule comparison of the autotuned iteration")
     ap.add_argument("--no-d2h", action="store_true",
                     help="skip the D2h CCSD workload")
+    ap.add_argument("--no-ccsdt", action="store_true",
+                    help="skip the CCSDT iteration on the CCSDT configuration's workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned preconditioner's instance stream")
     ap.add_argument("--c4-train", type=int, default=64,
