@@ -170,3 +170,29 @@ def test_ccsdt_lists_filled_through_the_device_path(built):
     for name in ("R1", "R2", "R3"):
         a, b = host.e.data[host.lid(name)], dev.e.data[dev.lid(name)]
         assert np.max(np.abs(a - b)) <= 1e-12 * np.abs(a).max(), name
+
+
+def test_ccsdt_plans_at_the_ccsdt_configuration(built):
+    # the CCSDT configuration's orbital space (D2h, irreps round-robin,
+    # o6/v48): every [CONTR] plans on the product engine (host-only), with
+    # hundreds of thousands of uneven block contractions per evaluation
+    import gccu
+    sp, eps, B = hm.synthetic(6, 48, 8, seed=1001, nsym=8)
+    e = gccu.Engine(-1)
+    try:
+        s = cc.CCSolver(e, hm.FactorizedIntegrals(sp, eps, B), method="ccsdt")
+        nitems, flops = 0, 0.0
+        for it in s.formula:
+            if it["kind"] != "CONTR":
+                continue
+            c = np.asarray(it["cnt"])
+            ex1 = np.asarray(it["op1"][1]) - c
+            ex2 = np.asarray(it["op2"][1]) - np.concatenate([c[4:], c[:4]])
+            n, st = e.plan_info(s.blk(it["op1"]), s.blk(it["op2"]), s.blk(it["res"]), ex1, ex2,
+                                c)
+            nitems += n
+            flops += st[7]
+        assert nitems == 659388
+        assert 0.05e12 < flops < 0.2e12
+    finally:
+        e.close()
