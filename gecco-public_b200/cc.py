@@ -127,30 +127,27 @@ CCSD_FORMULA = [
 ]
 
 
-# ---- CCSDT (maxexc = 3) ----------------------------------------------------------
-# The residuals R_mu = <mu| (H e^T)_c |0> for mu up to triples and the energy
-# E = <0| (H e^T)_c |0>, T = T1 + T2 + T3, written term by term as chains of
-# binary contractions: a class of F or V, then T_n1, T_n2, ... attached one
-# [CONTR] at a time, attachment (n, h, p) contracting h hole creators and p
-# particle annihilators of the Hamiltonian class with T_n (T's lines can only
-# meet the Hamiltonian's).  The T's commute, so each term is listed once, with
-# its attachments in non-decreasing (n, h, p) order.  A term's factor is its
-# topological sign (CCSDT_SIGNS) over the product of m! for every group of m
-# identical attachments; the intermediates of a chain are formed with factor 1
-# and its last contraction carries the factor.  The signs are those of the
-# engine's string-contraction convention; they were read off by matching
-# each term's contribution to the Fock-space expansion on two small spaces
-# (every factor came out as +-1 over the m! product).  Unfactorised (no shared
-# dressed intermediates beyond common chain prefixes): the terms are those of
-# the reference's CC maxexc=3 equations; tests/test_ccsdt_formula.py checks
-# each residual and the energy against <mu| e^-T H e^T |0> evaluated in the
-# full Fock space of a few spin orbitals, with a non-canonical Fock matrix.
+# ---- CC of any excitation level (CCSDT = maxexc 3) -------------------------------
+# The residuals R_mu = <mu| (H e^T)_c |0> for mu up to maxexc-fold excitations
+# and the energy E = <0| (H e^T)_c |0>, T = T1 + ... + T_maxexc, written term
+# by term as chains of binary contractions: a class of F or V, then T_n1,
+# T_n2, ... attached one [CONTR] at a time, attachment (n, h, p) contracting h
+# hole creators and p particle annihilators of the Hamiltonian class with T_n
+# (T's lines can only meet the Hamiltonian's).  The T's commute, so each term
+# is listed once, with its attachments in non-decreasing (n, h, p) order.  A
+# term's factor is the product of the Wick signs of its attachments
+# (contraction_sign) over the product of m! for every group of m identical
+# attachments; the intermediates of a chain are formed with factor 1 and its
+# last contraction carries the factor.  Unfactorised: no dressed
+# intermediates are shared between terms beyond common chain prefixes.
+# tests/test_ccsdt_formula.py checks the residuals and the energy of CCSDT
+# and CCSDTQ against <mu| e^-T H e^T |0> evaluated in the full Fock space of
+# a few spin orbitals, with a non-canonical Fock matrix.
 
 FOCK_CLASSES = {"HH": HH, "HP": HP, "PH": PH, "PP": PP}
 V_CLASSES = {"HHHH": HHHH, "HHPH": HHPH, "HHPP": HHPP, "PHHH": PHHH, "PHPH": PHPH,
              "PHPP": PHPP, "PPHH": PPHH, "PPPH": PPPH, "PPPP": PPPP}
-PPPHHH = occ8({P: 3}, {H: 3})
-T_CLASSES = {1: PH, 2: PPHH, 3: PPPHHH}
+T_CLASSES = {n: occ8({P: n}, {H: n}) for n in range(1, 5)}
 
 
 def attach(x, n, h, p):
@@ -189,16 +186,58 @@ def excitation_terms(maxexc):
     return terms
 
 
-def term_factor(steps, sign):
-    """topological sign over the product of m! of identical attachments"""
+def contraction_sign(x, n, h, p):
+    """Wick sign of attaching T_n to class x over h hole and p particle lines.
+    An element's operator is a+(C string) a(A string reversed); each string
+    is the concatenation over the types, in the condensed order (particles
+    before holes), of that type's piece, and a merged piece lists its
+    sources in the order the string maps merge them: op1 (cnt, ex1), op2
+    (cnt+, ex2), result creators (ex1, ex2), result annihilators (ex2, ex1).
+    The sign is the parity of the permutation that brings every contracted
+    pair together (op1's operator on the left) and the rest into the
+    result's order."""
+    ex1, ex2, c, _ = attach(x, n, h, p)
+    order = (P, H)
+    lab = iter(range(1 << 20))
+    pieces = {}
+    for t in order:
+        for key, k in (("cC", c[t]), ("cA", c[4 + t]), ("1C", ex1[t]), ("1A", ex1[4 + t]),
+                       ("2C", ex2[t]), ("2A", ex2[4 + t])):
+            pieces[key, t] = [next(lab) for _ in range(int(k))]
+
+    def operator(tag, cre, ann):
+        cs = sum((pieces[k, t] for t in order for k in cre), [])
+        an = sum((pieces[k, t] for t in order for k in ann), [])
+        return [(tag, "c", i) for i in cs] + [(tag, "a", i) for i in reversed(an)]
+
+    seq = operator(1, ("cC", "1C"), ("cA", "1A")) + operator(2, ("cA", "2C"), ("cC", "2A"))
+    target = []
+    for t in order:
+        target += sum(([(1, "c", i), (2, "a", i)] for i in pieces["cC", t]), [])
+        target += sum(([(1, "a", i), (2, "c", i)] for i in pieces["cA", t]), [])
+    owner = {(k, i): tag for tag, k, i in seq}
+    target += [(owner[k, i], k, i) for _, k, i in operator(0, ("1C", "2C"), ("2A", "1A"))]
+    pos = {o: i for i, o in enumerate(seq)}
+    perm = [pos[o] for o in target]
+    inv = sum(1 for a in range(len(perm)) for b in range(a + 1, len(perm)) if perm[a] > perm[b])
+    return -1.0 if inv % 2 else 1.0
+
+
+def term_factor(name, key, steps):
+    """product of the attachments' Wick signs over the product of m! of
+    identical attachments"""
     from math import factorial
-    den = 1
+    x = np.asarray((FOCK_CLASSES if name == "F" else V_CLASSES)[key])
+    f = 1.0
+    for n, h, p in steps:
+        f *= contraction_sign(x, n, h, p)
+        x = attach(x, n, h, p)[3]
     for st in set(steps):
-        den *= factorial(steps.count(st))
-    return sign / den
+        f /= factorial(steps.count(st))
+    return f
 
 
-def excitation_formula(maxexc, signs):
+def excitation_formula(maxexc):
     """operators and [ADD]/[CONTR] items of the residuals and the energy;
     the first item writing a result list overwrites it"""
     ops = {"F": FOCK_BLOCKS, "V": V_BLOCKS, "E": [SCAL]}
@@ -207,7 +246,7 @@ def excitation_formula(maxexc, signs):
         ops[f"R{n}"] = [T_CLASSES[n]]
     items, inter, written = [], {}, set()
     for name, key, steps, rank in excitation_terms(maxexc):
-        fac = term_factor(steps, signs[(name, key, steps)])
+        fac = term_factor(name, key, steps)
         x = np.asarray((FOCK_CLASSES if name == "F" else V_CLASSES)[key])
         res = "E" if rank == 0 else f"R{rank}"
         rocc = SCAL if rank == 0 else T_CLASSES[rank]
@@ -236,111 +275,6 @@ def excitation_formula(maxexc, signs):
     return ops, items
 
 
-# topological signs of the CCSDT terms, keyed by (list, class, attachments)
-CCSDT_SIGNS = {
-    ("F", "HH", ((1, 1, 0),)): -1,
-    ("F", "HH", ((2, 1, 0),)): +1,
-    ("F", "HH", ((3, 1, 0),)): -1,
-    ("F", "HP", ((1, 0, 1), (1, 1, 0))): -1,
-    ("F", "HP", ((1, 0, 1), (2, 1, 0))): +1,
-    ("F", "HP", ((1, 0, 1), (3, 1, 0))): -1,
-    ("F", "HP", ((1, 1, 0), (2, 0, 1))): -1,
-    ("F", "HP", ((1, 1, 0), (3, 0, 1))): -1,
-    ("F", "HP", ((1, 1, 1),)): +1,
-    ("F", "HP", ((2, 0, 1), (2, 1, 0))): +1,
-    ("F", "HP", ((2, 1, 1),)): +1,
-    ("F", "HP", ((3, 1, 1),)): +1,
-    ("F", "PH", ()): +1,
-    ("F", "PP", ((1, 0, 1),)): +1,
-    ("F", "PP", ((2, 0, 1),)): +1,
-    ("F", "PP", ((3, 0, 1),)): +1,
-    ("V", "HHHH", ((1, 1, 0), (1, 1, 0))): +1,
-    ("V", "HHHH", ((1, 1, 0), (2, 1, 0))): +1,
-    ("V", "HHHH", ((2, 2, 0),)): +1,
-    ("V", "HHHH", ((3, 2, 0),)): +1,
-    ("V", "HHPH", ((1, 0, 1), (1, 1, 0), (1, 1, 0))): +1,
-    ("V", "HHPH", ((1, 0, 1), (1, 1, 0), (2, 1, 0))): +1,
-    ("V", "HHPH", ((1, 0, 1), (2, 2, 0))): +1,
-    ("V", "HHPH", ((1, 0, 1), (3, 2, 0))): +1,
-    ("V", "HHPH", ((1, 1, 0), (1, 1, 0), (2, 0, 1))): -1,
-    ("V", "HHPH", ((1, 1, 0), (1, 1, 1))): +1,
-    ("V", "HHPH", ((1, 1, 0), (2, 1, 1))): -1,
-    ("V", "HHPH", ((1, 1, 0), (3, 1, 1))): +1,
-    ("V", "HHPH", ((1, 1, 1), (2, 1, 0))): +1,
-    ("V", "HHPH", ((1, 1, 1), (3, 1, 0))): -1,
-    ("V", "HHPH", ((2, 0, 1), (2, 2, 0))): -1,
-    ("V", "HHPH", ((2, 1, 0), (2, 1, 1))): -1,
-    ("V", "HHPH", ((2, 2, 1),)): -1,
-    ("V", "HHPH", ((3, 2, 1),)): +1,
-    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0), (1, 1, 0))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0), (2, 1, 0))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (2, 2, 0))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 0, 1), (3, 2, 0))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (1, 1, 0), (2, 0, 1))): +1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (1, 1, 1))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (2, 1, 1))): +1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 0), (3, 1, 1))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 1), (2, 1, 0))): -1,
-    ("V", "HHPP", ((1, 0, 1), (1, 1, 1), (3, 1, 0))): +1,
-    ("V", "HHPP", ((1, 0, 1), (2, 0, 1), (2, 2, 0))): +1,
-    ("V", "HHPP", ((1, 0, 1), (2, 1, 0), (2, 1, 1))): +1,
-    ("V", "HHPP", ((1, 0, 1), (2, 2, 1))): +1,
-    ("V", "HHPP", ((1, 0, 1), (3, 2, 1))): -1,
-    ("V", "HHPP", ((1, 1, 0), (1, 1, 0), (2, 0, 2))): +1,
-    ("V", "HHPP", ((1, 1, 0), (1, 1, 0), (3, 0, 2))): +1,
-    ("V", "HHPP", ((1, 1, 0), (1, 1, 1), (2, 0, 1))): +1,
-    ("V", "HHPP", ((1, 1, 0), (1, 1, 1), (3, 0, 1))): +1,
-    ("V", "HHPP", ((1, 1, 0), (2, 0, 1), (2, 1, 1))): -1,
-    ("V", "HHPP", ((1, 1, 0), (2, 0, 2), (2, 1, 0))): +1,
-    ("V", "HHPP", ((1, 1, 0), (2, 1, 2))): +1,
-    ("V", "HHPP", ((1, 1, 0), (3, 1, 2))): +1,
-    ("V", "HHPP", ((1, 1, 1), (1, 1, 1))): +1,
-    ("V", "HHPP", ((1, 1, 1), (2, 0, 1), (2, 1, 0))): +1,
-    ("V", "HHPP", ((1, 1, 1), (2, 1, 1))): +1,
-    ("V", "HHPP", ((1, 1, 1), (3, 1, 1))): +1,
-    ("V", "HHPP", ((2, 0, 1), (2, 2, 1))): -1,
-    ("V", "HHPP", ((2, 0, 1), (3, 2, 1))): -1,
-    ("V", "HHPP", ((2, 0, 2), (2, 2, 0))): +1,
-    ("V", "HHPP", ((2, 0, 2), (3, 2, 0))): +1,
-    ("V", "HHPP", ((2, 1, 0), (2, 1, 2))): +1,
-    ("V", "HHPP", ((2, 1, 0), (3, 1, 2))): -1,
-    ("V", "HHPP", ((2, 1, 1), (2, 1, 1))): -1,
-    ("V", "HHPP", ((2, 1, 1), (3, 1, 1))): +1,
-    ("V", "HHPP", ((2, 1, 2), (3, 1, 0))): -1,
-    ("V", "HHPP", ((2, 2, 0), (3, 0, 2))): +1,
-    ("V", "HHPP", ((2, 2, 1), (3, 0, 1))): -1,
-    ("V", "HHPP", ((2, 2, 2),)): +1,
-    ("V", "HHPP", ((3, 2, 2),)): +1,
-    ("V", "PHHH", ((1, 1, 0),)): -1,
-    ("V", "PHHH", ((2, 1, 0),)): -1,
-    ("V", "PHPH", ((1, 0, 1), (1, 1, 0))): -1,
-    ("V", "PHPH", ((1, 0, 1), (2, 1, 0))): -1,
-    ("V", "PHPH", ((1, 1, 0), (2, 0, 1))): +1,
-    ("V", "PHPH", ((1, 1, 1),)): -1,
-    ("V", "PHPH", ((2, 1, 1),)): +1,
-    ("V", "PHPH", ((3, 1, 1),)): -1,
-    ("V", "PHPP", ((1, 0, 1), (1, 0, 1), (1, 1, 0))): +1,
-    ("V", "PHPP", ((1, 0, 1), (1, 0, 1), (2, 1, 0))): +1,
-    ("V", "PHPP", ((1, 0, 1), (1, 1, 0), (2, 0, 1))): -1,
-    ("V", "PHPP", ((1, 0, 1), (1, 1, 1))): +1,
-    ("V", "PHPP", ((1, 0, 1), (2, 1, 1))): -1,
-    ("V", "PHPP", ((1, 0, 1), (3, 1, 1))): +1,
-    ("V", "PHPP", ((1, 1, 0), (2, 0, 2))): -1,
-    ("V", "PHPP", ((1, 1, 0), (3, 0, 2))): -1,
-    ("V", "PHPP", ((1, 1, 1), (2, 0, 1))): -1,
-    ("V", "PHPP", ((1, 1, 1), (3, 0, 1))): -1,
-    ("V", "PHPP", ((2, 0, 1), (2, 1, 1))): +1,
-    ("V", "PHPP", ((2, 0, 2), (2, 1, 0))): -1,
-    ("V", "PHPP", ((2, 1, 2),)): -1,
-    ("V", "PHPP", ((3, 1, 2),)): -1,
-    ("V", "PPHH", ()): +1,
-    ("V", "PPPH", ((1, 0, 1),)): +1,
-    ("V", "PPPH", ((2, 0, 1),)): -1,
-    ("V", "PPPP", ((1, 0, 1), (1, 0, 1))): -1,
-    ("V", "PPPP", ((1, 0, 1), (2, 0, 1))): +1,
-    ("V", "PPPP", ((2, 0, 2),)): +1,
-    ("V", "PPPP", ((3, 0, 2),)): +1,
-}
 
 
 # ---- filling the Hamiltonian lists -------------------------------------------
@@ -447,7 +381,7 @@ class CCSolver:
 
     # lists that hold the Hamiltonian, amplitudes, residuals and the energy;
     # the others of a formula are its intermediates
-    PERSISTENT = ("F", "V", "T1", "T2", "T3", "R1", "R2", "R3", "E")
+    PERSISTENT = ("F", "V", "T1", "T2", "T3", "T4", "R1", "R2", "R3", "R4", "E")
 
     def __init__(self, engine, ints, method="ccsd", use_tr=False, maxsub=8, shift=0.0,
                  learned=None, shard=None, spin_project=False, native_formula=False):
@@ -475,8 +409,8 @@ class CCSolver:
         sp = ints.space
         self.nsym = sp.nsym
         engine.register_orbinfo(sp.nsym, sp.norb)
-        if method == "ccsdt":
-            ops, self.formula = excitation_formula(3, CCSDT_SIGNS)
+        if method in ("ccsdt", "ccsdtq"):
+            ops, self.formula = excitation_formula(3 if method == "ccsdt" else 4)
         else:
             ops = MP2_OPERATORS if method == "mp2" else CCSD_OPERATORS
             self.formula = MP2_FORMULA if method == "mp2" else CCSD_FORMULA
@@ -491,8 +425,9 @@ class CCSolver:
             else:
                 lid, n = engine.register_list(opid, absym=absym)
             self.lists[name] = (lid, n, blocks)
-        self.amps = {"mp2": ["T2"], "ccsdt": ["T1", "T2", "T3"]}.get(method, ["T1", "T2"])
-        self.res = {"T1": "R1", "T2": "R2", "T3": "R3"}
+        self.amps = {"mp2": ["T2"], "ccsdt": ["T1", "T2", "T3"],
+                     "ccsdtq": ["T1", "T2", "T3", "T4"]}.get(method, ["T1", "T2"])
+        self.res = {f"T{n}": f"R{n}" for n in range(1, 5)}
         # denominators, steps (the last one kept for the learned step's
         # inputs) and DIIS subspace
         for a in self.amps:

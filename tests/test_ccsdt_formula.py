@@ -1,10 +1,11 @@
-"""CCSDT (the reference's CC maxexc=3, test/CC-energy-I.inp) as chains of
-binary contractions (cc.excitation_formula with cc.CCSDT_SIGNS) on the CPU
-oracle, against <mu| e^-T H e^T |0> evaluated in the full Fock space of ten
-spin orbitals with a non-canonical Fock matrix, so that every term of the
-formula contributes; and a CCSDT solve, whose converged amplitudes make the
-Fock-space residuals vanish and whose energy lies closer to the full CI
-energy than the CCSD one."""
+"""CCSDT (the reference's CC maxexc=3, test/CC-energy-I.inp) and CCSDTQ as
+chains of binary contractions (cc.excitation_formula, factors from the Wick
+signs of cc.contraction_sign) on the CPU oracle, against <mu| e^-T H e^T |0>
+evaluated in the full Fock space of ten spin orbitals with a non-canonical
+Fock matrix, so that every term of the formula contributes; a CCSDT solve,
+whose converged amplitudes make the Fock-space residuals vanish and whose
+energy lies closer to the full CI energy than the CCSD one; the formula on
+the product planner, at the CCSDT configuration's size too."""
 import numpy as np
 import pytest
 
@@ -46,12 +47,15 @@ def _dense(s, name, shape):
     return s.view(name).to_dense(x, 1, shape)
 
 
-def test_terms_and_signs_agree():
-    terms = cc.excitation_terms(3)
-    assert len(terms) == len(cc.CCSDT_SIGNS) == 102
-    assert {t[:3] for t in terms} == set(cc.CCSDT_SIGNS)
-    # the CCSD subset: T up to T2 and residuals up to doubles
+def test_terms_and_factors():
+    # 48 terms up to doubles (CCSD, the energy included), 102 up to triples;
+    # every factor is +-1 over the m! of identical attachments
+    from math import factorial
     assert len(cc.excitation_terms(2)) == 48
+    assert len(cc.excitation_terms(3)) == 102
+    for name, key, steps, _ in cc.excitation_terms(3):
+        den = np.prod([factorial(steps.count(st)) for st in set(steps)])
+        assert abs(abs(cc.term_factor(name, key, steps)) * den - 1.0) < 1e-15
 
 
 @pytest.mark.parametrize("no,nv,seed", [(3, 2, 21), (2, 3, 22)])
@@ -196,3 +200,23 @@ def test_ccsdt_plans_at_the_ccsdt_configuration(built):
         assert 0.05e12 < flops < 0.2e12
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("no,nv,seed", [(3, 2, 28), (2, 3, 29)])
+def test_ccsdtq_residuals_match_fock_space(built, no, nv, seed):
+    # the same generator one excitation level higher: T1..T4, R1..R4
+    s, F, W, nso = _system(no, nv, seed, method="ccsdtq")
+    rng = np.random.default_rng(seed)
+    F = non_canonical_fock(F, nso, rng)
+    _set_fock(s, F, nso)
+    nvo = F.shape[0] - nso
+    amps = {r: random_amplitudes(r, nvo, nso, rng) for r in (1, 2, 3, 4)}
+    for r, t in amps.items():
+        s.e.upload(s.lid(f"T{r}"), s.view(f"T{r}").from_dense({1: t}, s.lists[f"T{r}"][1]))
+    s.evaluate()
+    ref = FockSpace(F, W, nso).residuals(amps, 4)
+    assert abs(s.energy() - ref[0]) < 1e-13
+    for r in (1, 2, 3, 4):
+        got = _dense(s, f"R{r}", ref[r].shape)
+        assert np.abs(ref[r]).max() > 1e-4, r
+        assert np.abs(got - ref[r]).max() < 1e-12 * np.abs(ref[r]).max(), r
