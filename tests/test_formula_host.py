@@ -90,3 +90,25 @@ def test_ccsd_formula_arena(built):
         assert info["arena_bytes"] < info["sum_bytes"], info
     finally:
         e.close()
+
+
+def test_ccsdt_formula_arena(built):
+    # the CCSDT formula (one intermediate per shared chain prefix, each alive
+    # only while the chains of its Hamiltonian class run) through the
+    # engine's item checks; the arena is a fraction of all intermediates
+    sp, eps, B = hm.synthetic(3, 8, 20, seed=2)
+    e = gccu.Engine(-1)
+    try:
+        s = cc.CCSolver(e, hm.FactorizedIntegrals(sp, eps, B), method="ccsdt",
+                        native_formula=True)
+        info = e.formula_info(s.fid)
+        inter = [n for n in s.lists if n not in cc.CCSolver.PERSISTENT and
+                 not n[:1] in "DSP"]
+        assert len(inter) == sum(1 for it in s.formula if it["res"][0] in inter)
+        ntarget = sum(1 for i, it in enumerate(s.formula)
+                      if i == 0 or s.formula[i - 1]["res"][0] != it["res"][0])
+        assert info["targets"] == ntarget
+        assert info["items"] == len(s.formula) + ntarget + 2 * len(inter)
+        assert info["arena_bytes"] < 0.5 * info["sum_bytes"], info
+    finally:
+        e.close()
