@@ -16,6 +16,9 @@ runs in the build container only; its outputs are committed):
     the energies the reference printed for CCSDT (CC maxexc=3) with the
     orbital space of test/CC-energy-I.inp: frozen (1,0,0,0), deleted
     (2,1,0,0), occupied (3,1,0,0) as the output lists its shells.
+  * test/CC-excite-I.e.ref -> ch2_dz_ccsd_ref.json
+    the CCSD ground-state iterations of that run (the block before its first
+    'final energy'): frozen (1,0,0,0), nothing deleted.
 
 usage: python tests/golden/make_ch2_dalton.py [/path/to/reference]
 """
@@ -83,12 +86,15 @@ def read_motwoint(path):
     return np.concatenate(vals), np.concatenate(idx)
 
 
-def read_ccsdt_ref(path):
-    lines = open(path).read().splitlines()
-    hist = [(int(l.split()[1]), float(l.split()[2]), float(l.split()[3]))
-            for l in lines if re.match(r">>>\s+\d+\s", l)]
-    final = float([l for l in lines if "final energy" in l][-1].split()[3])
-    return {"history": hist, "final_energy": final}
+def read_history(path):
+    """the '>>> iteration energy residual' lines up to the first final energy"""
+    hist = []
+    for line in open(path).read().splitlines():
+        if re.match(r">>>\s+\d+\s", line):
+            hist.append((int(line.split()[1]), float(line.split()[2]), float(line.split()[3])))
+        elif "final energy" in line:
+            return {"history": hist, "final_energy": float(line.split()[3])}
+    raise ValueError(path)
 
 
 def main():
@@ -97,12 +103,18 @@ def main():
     sir = read_sirifc(os.path.join(mol, "SIRIFC"))
     vals, idx = read_motwoint(os.path.join(mol, "MOTWOINT"))
     np.savez_compressed(os.path.join(HERE, "ch2_dz_dalton.npz"), vals=vals, idx=idx, **sir)
-    info = read_ccsdt_ref(os.path.join(ref, "test/CC-energy-I.e.ref"))
+    info = read_history(os.path.join(ref, "test/CC-energy-I.e.ref"))
     info["orbitals"] = {"occ": [3, 1, 0, 0], "frozen": [1, 0, 0, 0], "deleted": [2, 1, 0, 0]}
     info["method"] = "CC maxexc=3 (CCSDT), DIIS maxsub 8, conv 1e-10"
     with open(os.path.join(HERE, "ch2_dz_ccsdt_ref.json"), "w") as f:
         json.dump(info, f, indent=1)
-    print("wrote", len(vals), "integral records; E_ref", sir["eref"], "final", info["final_energy"])
+    ccsd = read_history(os.path.join(ref, "test/CC-excite-I.e.ref"))
+    ccsd["orbitals"] = {"occ": [3, 1, 0, 0], "frozen": [1, 0, 0, 0], "deleted": [0, 0, 0, 0]}
+    ccsd["method"] = "CC maxexc=2 (CCSD) ground state, DIIS maxsub 8"
+    with open(os.path.join(HERE, "ch2_dz_ccsd_ref.json"), "w") as f:
+        json.dump(ccsd, f, indent=1)
+    print("wrote", len(vals), "integral records; E_ref", sir["eref"], "final", info["final_energy"],
+          "CCSD final", ccsd["final_energy"], len(ccsd["history"]))
 
 
 if __name__ == "__main__":

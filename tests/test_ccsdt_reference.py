@@ -3,8 +3,9 @@ DALTON's interface files, C2v, CC maxexc=3, frozen (1,0,0,0), deleted
 (2,1,0,0), DIIS maxsub 8, conv 1e-10) reproduced through the CCSDT formula
 (cc.excitation_formula) and the DIIS solver on the CPU oracle: every
 iteration's energy and residual norm as the reference printed them
-(test/CC-energy-I.e.ref), the iteration count and the final energy.
-Fixtures from tests/golden/make_ch2_dalton.py."""
+(test/CC-energy-I.e.ref), the iteration count and the final energy; and the
+CCSD ground state of test/CC-excite-I.e.ref on the same integrals through
+the CCSD formula.  Fixtures from tests/golden/make_ch2_dalton.py."""
 import json
 import os
 
@@ -64,3 +65,24 @@ def test_ccsdt_iterations_match_the_reference():
         assert abs(eref + en - er) < 1e-11, (i, eref + en, er)   # 12 decimals printed
         assert rn == pytest.approx(rr, rel=6e-4), (i, rn, rr)    # 4 digits printed
     assert abs(eref + e - ref["final_energy"]) < 1e-11
+
+
+def test_ccsd_iterations_match_the_reference():
+    # the CCSD ground state of test/CC-excite-I.e.ref on the same integrals
+    # (frozen core, nothing deleted), through the CCSD formula: the 16
+    # iterations the reference printed, energies to 12 decimals
+    ints, eref, _ = ch2_dz_integrals()
+    ref = json.load(open(os.path.join(GOLD, "ch2_dz_ccsd_ref.json")))
+    o = ref["orbitals"]
+    sp = hm.OrbitalSpace(ints.space.orbsym, o["occ"], o["frozen"], o["deleted"])
+    s = cc.CCSolver(OracleEngine(route=3), hm.DenseIntegrals(sp, ints.f, ints.eri),
+                    method="ccsd")
+    s.load_hamiltonian()
+    n = len(ref["history"])
+    s.solve(maxiter=n, conv=0.0)
+    assert n == 16 and len(s.history) == n
+    for (i, en, rn), (j, er, rr) in zip(s.history, ref["history"]):
+        assert i == j
+        assert abs(eref + en - er) < 1e-11, (i, eref + en, er)
+        assert rn == pytest.approx(rr, rel=6e-4), (i, rn, rr)
+    assert abs(eref + s.history[-1][1] - ref["final_energy"]) < 1e-11
